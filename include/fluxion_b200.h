@@ -1,0 +1,216 @@
+/*
+ * fluxion_b200.h -- C ABI of the B200-native HAPR placement hot path.
+ *
+ * This header is the drop-in boundary. Each entry point names the reference
+ * interface it replaces (paths are relative to the reference project:
+ * H/ = HAPR_fluxion_v4/, O/ = neon_old_codebase/).
+ *
+ * Conventions
+ *   - Every call returns an int status: FX_OK (0) or a negative FX_E* code.
+ *     No exception or abort crosses this boundary. fx_last_error() returns a
+ *     thread-local message describing the most recent failure.
+ *   - Host arrays are caller-owned. They are read-only unless the parameter
+ *     name starts with out_ or the comment says "in/out".
+ *   - Device state lives behind opaque handles (fx_ctx, fx_design). One
+ *     context is driven by one host thread at a time; distinct contexts may
+ *     run on distinct host threads.
+ *   - Netlists are flat index arrays: net e connects the gates
+ *     net_gate[net_ptr[e] .. net_ptr[e+1]-1]. This is the reference's
+ *     Circuit::net_gate_indices (H/src/data/circuit.rs:62) flattened to CSR.
+ *   - Positions are SoA float32 x[N], y[N] (H/src/data/placement.rs:9-13).
+ */
+#ifndef FLUXION_B200_H_
+#define FLUXION_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define FX_OK        0
+#define FX_EINVAL   -1 /* bad argument, malformed CSR, out-of-range index     */
+#define FX_ENOMEM   -2 /* device or host allocation failed                    */
+#define FX_ECUDA    -3 /* a CUDA runtime/driver call failed                   */
+#define FX_ETIMEOUT -4 /* a bounded device-side wait gave up                  */
+#define FX_EADMIT   -5 /* serving admission refused (HBM budget exceeded)     */
+#define FX_ENODEV   -6 /* no usable sm_100 device                             */
+
+typedef struct fx_ctx fx_ctx;
+typedef struct fx_design fx_design;
+
+/* Thread-local description of the last failure on this thread. */
+const char *fx_last_error(void);
+/* Library version string ("fluxion_b200 <major>.<minor>"). */
+const char *fx_version(void);
+
+/* ---- context ----------------------------------------------------------- */
+/* Creates a context on CUDA device `device` (an sm_100 B200). Replaces
+ * GpuContext::new (H/src/gpu/context.rs:17-70); unlike the reference there is
+ * no CPU fallback: a missing device is FX_ENODEV. */
+int fx_ctx_create(fx_ctx **out_ctx, int device);
+int fx_ctx_destroy(fx_ctx *ctx);
+/* Turns per-stage CUDA-event timing on (1) or off (0). */
+int fx_ctx_set_profiling(fx_ctx *ctx, int enable);
+/* Per-stage timing accumulated since the last reset, in milliseconds:
+ * out_ms[s] total device time and out_calls[s] launches of stage s
+ * (FX_STAGE_*). n = capacity of both arrays. */
+int fx_ctx_stage_times(fx_ctx *ctx, double *out_ms, int64_t *out_calls, int n);
+int fx_ctx_reset_stage_times(fx_ctx *ctx);
+/* Number of kernels this library has launched on the context. */
+int64_t fx_ctx_kernel_launches(fx_ctx *ctx);
+
+/* Stage identifiers for fx_ctx_stage_times. */
+#define FX_STAGE_ATTRACT_INTEGRATE 0 /* rows A+E fused                        */
+#define FX_STAGE_BH_KEYS           1 /* row B: Morton keys                    */
+#define FX_STAGE_BH_SORT           2 /* row B: radix sort                     */
+#define FX_STAGE_BH_TREE           3 /* row B: radix tree + mass sums         */
+#define FX_STAGE_BH_WALK           4 /* row B: warp-cooperative walk          */
+#define FX_STAGE_DENSITY           5 /* row C: scatter + DCT GEMMs + field    */
+#define FX_STAGE_CONGESTION        6 /* rows D+F: bbox, counting, HPWL        */
+#define FX_STAGE_LEAF              7 /* row H: batched leaf placer            */
+#define FX_STAGE_FIEDLER           8 /* row G: power iteration                */
+#define FX_STAGE_COUNT             9
+
+/* ---- designs (device-resident netlists) -------------------------------- */
+/* Uploads a netlist and builds every device structure the hot path needs
+ * (net CSR, gate->net incidence CSR, the deduplicated clique-expansion
+ * adjacency of H/src/data/circuit.rs:154-171). Replaces the upload half of
+ * dispatch_forces / dispatch_congestion (H/src/gpu/dispatch.rs:31-45,
+ * 115-139). gate_w/gate_h may be NULL (reference defaults 2 x 10,
+ * H/src/parser/blif.rs:49). Positions start at (0,0) as in Placement::new
+ * (H/src/data/placement.rs:28-37). */
+int fx_design_load(fx_ctx *ctx, int32_t n_gates, int32_t n_nets,
+                   const int32_t *net_ptr, const int32_t *net_gate,
+                   const float *gate_w, const float *gate_h,
+                   float chip_w, float chip_h, fx_design **out_design);
+int fx_design_free(fx_design *design);
+/* Sizes: gates, nets, pins, directed adjacency entries. */
+int fx_design_sizes(const fx_design *design, int64_t *out_n, int64_t *out_m,
+                    int64_t *out_p, int64_t *out_a);
+/* Host copy of the device adjacency CSR (out_adj_ptr[N+1], out_adj_idx[A]).
+ * Each list holds the same neighbour set as circuit.rs:154-171. */
+int fx_design_adjacency(const fx_design *design, int32_t *out_adj_ptr,
+                        int32_t *out_adj_idx);
+/* Host <-> device copies of the resident positions (and velocities, which
+ * are zeroed by set_positions). */
+int fx_design_set_positions(fx_design *design, const float *x, const float *y);
+int fx_design_get_positions(fx_design *design, float *out_x, float *out_y);
+/* Device bytes held by the design (netlist + positions + workspaces). */
+int64_t fx_design_device_bytes(const fx_design *design);
+
+/* ---- rows D + F: congestion counting and HPWL --------------------------- */
+/* Mirrors compute_congestion_cpu (H/src/algorithm/congestion.rs:11-62) with
+ * the grid geometry of RoutingGrid::new / cell_at (H/src/data/grid.rs:25-62):
+ * every net with >= 2 gate entries adds +1 to each cell of its bounding box
+ * in both the h and v grids. The two grids are identical, so one uint32
+ * count grid (rows x cols, row-major) is returned; h[i] == v[i] ==
+ * (float)out_counts[i] exactly. Also returns the HPWL of
+ * Placement::compute_hpwl (H/src/data/placement.rs:48-74) summed in FP64,
+ * and the FP64 sum / f32 max of max(0, h+v-capacity) (grid.rs:71-91).
+ * x/y: host positions, or NULL to use the design's resident positions.
+ * Any out pointer may be NULL. */
+int fx_congestion(fx_ctx *ctx, fx_design *design, const float *x,
+                  const float *y, int32_t cols, int32_t rows,
+                  uint32_t *out_counts, double *out_hpwl,
+                  double *out_total_overflow, float *out_max_overflow);
+
+/* ---- rows A..F: the plain composite force iteration -------------------- */
+typedef struct fx_iter_cfg {
+  float attract_weight;  /* spring k (placer.rs:250, default 1.0)            */
+  float repel_weight;    /* Barnes-Hut k (placer.rs:264, default 0.5)        */
+  float min_dist;        /* distance floor (placer.rs:263, default 0.1)      */
+  float theta;           /* opening angle (BarnesHutTree.cpp:16, 0.5)        */
+  float density_weight;  /* weight of the DCT Poisson force (0 disables)     */
+  float target_density;  /* rho_target (force_electrostatic.py:37)           */
+  int32_t density_bins;  /* G: G x G density grid, G % 128 == 0 (0 = off)    */
+  int32_t dct_precision; /* FX_DCT_*                                         */
+  int32_t cong_cols;     /* congestion grid (0 = off)                        */
+  int32_t cong_rows;
+  float damping;         /* placer.rs:276 (0.9)                              */
+  float dt;              /* placer.rs:276-279 (0.1)                          */
+} fx_iter_cfg;
+
+#define FX_DCT_FP32  0 /* 3xTF32 split on the tensor cores (FP32 accuracy)   */
+#define FX_DCT_TF32  1 /* single-pass TF32 inputs, FP32 accumulate           */
+#define FX_DCT_BF16  2 /* BF16 inputs, FP32 accumulate                       */
+#define FX_DCT_SIMT  3 /* FP32 CUDA-core GEMM (no tensor cores)              */
+
+typedef struct fx_iter_stats {
+  double hpwl;            /* FP64 HPWL after the last iteration              */
+  double total_overflow;  /* FP64 sum of congestion overflow                 */
+  float max_overflow;     /* max cell overflow                               */
+  float pad0;
+  double density_energy;  /* 0.5 * sum q*phi at the gates (FP64)             */
+  int64_t iterations;     /* iterations run                                  */
+  int64_t bh_nodes;       /* internal nodes of the last Barnes-Hut tree      */
+} fx_iter_stats;
+
+/* Fills cfg with the defaults (H/config/default.yaml placement section plus
+ * the Barnes-Hut and density defaults above). */
+int fx_iter_cfg_default(fx_iter_cfg *cfg);
+
+/* Runs `iters` plain composite iterations: F = attraction (placer.rs:243-255
+ * over the full adjacency) + Barnes-Hut repulsion (law of placer.rs:258-272,
+ * tree rules of O/src/cpp/BarnesHutTree.cpp) + DCT Poisson density force
+ * (O/src/python/fluxion/force_electrostatic.py:47-150); then the damped
+ * Euler step clamped to the die (placer.rs:275-280); then congestion + HPWL
+ * on the new positions. Replaces dispatch_forces (H/src/gpu/dispatch.rs:
+ * 18-106). x/y are in/out host arrays (NULL = run on resident positions and
+ * leave them on the device). stats may be NULL. */
+int fx_force_iterate(fx_ctx *ctx, fx_design *design, const fx_iter_cfg *cfg,
+                     int32_t iters, float *x, float *y, fx_iter_stats *stats);
+
+/* Single-stage entry points on the resident positions (used by the parity
+ * tests; each writes float32 forces to host arrays). */
+/* Row A: out_f = k * sum_{j in adj(i)} (p_j - p_i)  (placer.rs:243-255). */
+int fx_stage_attraction(fx_ctx *ctx, fx_design *design, float k,
+                        float *out_fx, float *out_fy);
+/* Row B: Barnes-Hut repulsion. Also returns the Morton keys and the sorted
+ * order (out_keys[N], out_perm[N], either may be NULL) and the root square
+ * (out_root[3] = {x_min, y_min, size}, may be NULL). */
+int fx_stage_barnes_hut(fx_ctx *ctx, fx_design *design, float k, float theta,
+                        float min_dist, float *out_fx, float *out_fy,
+                        uint32_t *out_keys, int32_t *out_perm,
+                        float *out_root);
+/* Row C: DCT Poisson density force. Optional grids (G*G, row-major, may be
+ * NULL): out_rho (charge density rho - rho_target), out_phi, out_ex,
+ * out_ey. */
+int fx_stage_density(fx_ctx *ctx, fx_design *design, int32_t bins,
+                     float target_density, float weight, int32_t precision,
+                     float *out_fx, float *out_fy, float *out_rho,
+                     float *out_phi, float *out_ex, float *out_ey,
+                     double *out_energy);
+
+/* ---- synthetic netlists (host-only; no GPU needed) ---------------------- */
+typedef struct fx_netlist fx_netlist;
+/* Plain generator: n gates in leaf_size-gate leaves of a binary cluster
+ * tree, widths U{1..4} x 1, n_nets nets whose degree is 2 (p=0.6), 3
+ * (p=0.2) or power-law alpha=2.5 on [2,64]; pins from the driver's leaf
+ * (0.7), its sibling leaf (0.2) or anywhere (0.1); positions uniform on the
+ * die. Deterministic in seed (SplitMix64). */
+int fx_synth_plain(uint64_t seed, int32_t n_gates, int32_t n_nets,
+                   float die_w, float die_h, int32_t leaf_size,
+                   fx_netlist **out);
+/* Batched-leaf generator: n_clusters clusters of log-uniform size in
+ * [min_size, max_size]; per cluster round(nets_per_gate * n) intra-cluster
+ * nets of degree 2 + Geometric(0.5) capped at 8. Every cluster gets the unit
+ * box region. */
+int fx_synth_leaves(uint64_t seed, int32_t n_clusters, int32_t min_size,
+                    int32_t max_size, float nets_per_gate, fx_netlist **out);
+int fx_netlist_sizes(const fx_netlist *nl, int64_t *out_n, int64_t *out_m,
+                     int64_t *out_p, int64_t *out_leaves);
+/* Copies the arrays out; any pointer may be NULL. Leaves are contiguous
+ * gate ranges: out_leaf_ptr[L+1]; out_region[4L] = (cx, cy, w, h). */
+int fx_netlist_copy(const fx_netlist *nl, int32_t *out_net_ptr,
+                    int32_t *out_net_gate, float *out_w, float *out_h,
+                    float *out_x, float *out_y, float *out_die,
+                    int32_t *out_leaf_ptr, float *out_region);
+int fx_netlist_free(fx_netlist *nl);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLUXION_B200_H_ */

@@ -1,0 +1,438 @@
+// fx_core.cu -- context, error reporting, stage timing and design upload.
+#include <cstdarg>
+#include <cstring>
+#include <new>
+
+#include "fx_internal.h"
+
+namespace fx {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+cudaEvent_t StageTimer::get_event() {
+  if (!pool.empty()) {
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+
+void StageTimer::resolve() {
+  for (auto &p : pending) {
+    float t = 0.f;
+    if (cudaEventSynchronize(p.b) == cudaSuccess &&
+        cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) {
+      ms[p.stage] += t;
+      calls[p.stage] += 1;
+    }
+    pool.push_back(p.a);
+    pool.push_back(p.b);
+  }
+  pending.clear();
+}
+
+void StageTimer::destroy() {
+  resolve();
+  for (auto e : pool) cudaEventDestroy(e);
+  pool.clear();
+}
+
+void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a) {
+  *a = nullptr;
+  if (!ctx->timer.enabled) return;
+  (void)stage;
+  *a = ctx->timer.get_event();
+  if (*a) cudaEventRecord(*a, s);
+}
+
+void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a) {
+  if (!ctx->timer.enabled || !a) return;
+  cudaEvent_t b = ctx->timer.get_event();
+  if (!b) return;
+  cudaEventRecord(b, s);
+  ctx->timer.pending.push_back({stage, a, b});
+  if (ctx->timer.pending.size() > 4096) ctx->timer.resolve();
+}
+
+// Deduplicated clique-expansion adjacency (H/src/data/circuit.rs:154-171):
+// gate a's list holds every other gate sharing a net with it, once, and a
+// itself when a net names a twice. Built from the gate->net incidence in
+// O(sum over nets of degree^2) with a marker array.
+static int build_adjacency(int32_t N, int32_t M, const int32_t *net_ptr,
+                           const int32_t *net_gate, std::vector<int32_t> &ptr,
+                           std::vector<int32_t> &idx) {
+  const int64_t P = net_ptr[M];
+  std::vector<int32_t> inc_ptr((size_t)N + 1, 0);
+  for (int64_t q = 0; q < P; ++q) inc_ptr[(size_t)net_gate[q] + 1]++;
+  for (int32_t g = 0; g < N; ++g) inc_ptr[g + 1] += inc_ptr[g];
+  std::vector<int32_t> inc((size_t)P);
+  {
+    std::vector<int32_t> fill(inc_ptr.begin(), inc_ptr.end() - 1);
+    for (int32_t e = 0; e < M; ++e)
+      for (int32_t q = net_ptr[e]; q < net_ptr[e + 1]; ++q)
+        inc[fill[net_gate[q]]++] = e;
+  }
+  std::vector<int32_t> mark((size_t)N, -1);
+  ptr.assign((size_t)N + 1, 0);
+  idx.clear();
+  idx.reserve((size_t)P * 4);
+  for (int32_t a = 0; a < N; ++a) {
+    bool self = false;
+    int32_t prev_net = -1;
+    for (int32_t t = inc_ptr[a]; t < inc_ptr[a + 1]; ++t) {
+      int32_t e = inc[t];
+      if (e == prev_net) {  // a appears more than once in net e
+        self = true;
+        continue;
+      }
+      prev_net = e;
+      for (int32_t q = net_ptr[e]; q < net_ptr[e + 1]; ++q) {
+        int32_t b = net_gate[q];
+        if (b == a) continue;
+        if (mark[b] != a) {
+          mark[b] = a;
+          idx.push_back(b);
+        }
+      }
+    }
+    if (self) idx.push_back(a);
+    if (idx.size() > (size_t)INT32_MAX) {
+      set_error("adjacency exceeds 2^31 entries");
+      return FX_EINVAL;
+    }
+    ptr[(size_t)a + 1] = (int32_t)idx.size();
+  }
+  return FX_OK;
+}
+
+}  // namespace fx
+
+using namespace fx;
+
+extern "C" const char *fx_last_error(void) { return fx::g_err; }
+extern "C" const char *fx_version(void) { return "fluxion_b200 0.1"; }
+
+extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
+  if (!out_ctx) return FX_EINVAL;
+  *out_ctx = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    set_error("no CUDA device visible");
+    return FX_ENODEV;
+  }
+  if (device < 0 || device >= count) {
+    set_error("device %d out of range (%d devices)", device, count);
+    return FX_EINVAL;
+  }
+  cudaDeviceProp prop;
+  FX_CHECK_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) {
+    set_error("device %d is sm_%d%d; this build targets sm_100a", device,
+              prop.major, prop.minor);
+    return FX_ENODEV;
+  }
+  FX_CHECK_CUDA(cudaSetDevice(device));
+  fx_ctx *c = new (std::nothrow) fx_ctx();
+  if (!c) return FX_ENOMEM;
+  c->device = device;
+  c->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("stream/event creation failed");
+    delete c;
+    return FX_ECUDA;
+  }
+  *out_ctx = c;
+  return FX_OK;
+}
+
+extern "C" int fx_ctx_destroy(fx_ctx *ctx) {
+  if (!ctx) return FX_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->stream2);
+  ctx->timer.destroy();
+  cudaEventDestroy(ctx->fork);
+  cudaEventDestroy(ctx->join);
+  cudaStreamDestroy(ctx->stream);
+  cudaStreamDestroy(ctx->stream2);
+  delete ctx;
+  return FX_OK;
+}
+
+extern "C" int fx_ctx_set_profiling(fx_ctx *ctx, int enable) {
+  if (!ctx) return FX_EINVAL;
+  ctx->timer.enabled = enable != 0;
+  return FX_OK;
+}
+
+extern "C" int fx_ctx_stage_times(fx_ctx *ctx, double *out_ms,
+                                  int64_t *out_calls, int n) {
+  if (!ctx) return FX_EINVAL;
+  cudaSetDevice(ctx->device);
+  ctx->timer.resolve();
+  for (int s = 0; s < n && s < FX_STAGE_COUNT; ++s) {
+    if (out_ms) out_ms[s] = ctx->timer.ms[s];
+    if (out_calls) out_calls[s] = ctx->timer.calls[s];
+  }
+  return FX_OK;
+}
+
+extern "C" int fx_ctx_reset_stage_times(fx_ctx *ctx) {
+  if (!ctx) return FX_EINVAL;
+  cudaSetDevice(ctx->device);
+  ctx->timer.resolve();
+  for (int s = 0; s < FX_STAGE_COUNT; ++s) {
+    ctx->timer.ms[s] = 0.0;
+    ctx->timer.calls[s] = 0;
+  }
+  return FX_OK;
+}
+
+extern "C" int64_t fx_ctx_kernel_launches(fx_ctx *ctx) {
+  return ctx ? ctx->launches : -1;
+}
+
+extern "C" int fx_design_load(fx_ctx *ctx, int32_t n_gates, int32_t n_nets,
+                              const int32_t *net_ptr, const int32_t *net_gate,
+                              const float *gate_w, const float *gate_h,
+                              float chip_w, float chip_h,
+                              fx_design **out_design) {
+  if (!ctx || !out_design || n_gates <= 0 || n_nets < 0 || !net_ptr ||
+      (n_nets > 0 && !net_gate)) {
+    set_error("fx_design_load: invalid arguments");
+    return FX_EINVAL;
+  }
+  *out_design = nullptr;
+  if (!(chip_w > 0.f) || !(chip_h > 0.f)) {
+    set_error("fx_design_load: chip size must be positive");
+    return FX_EINVAL;
+  }
+  // Validate the CSR: monotone pointers starting at 0, gate ids in range.
+  if (net_ptr[0] != 0) {
+    set_error("fx_design_load: net_ptr[0] must be 0");
+    return FX_EINVAL;
+  }
+  for (int32_t e = 0; e < n_nets; ++e) {
+    if (net_ptr[e + 1] < net_ptr[e]) {
+      set_error("fx_design_load: net_ptr decreases at net %d", e);
+      return FX_EINVAL;
+    }
+  }
+  const int64_t P = net_ptr[n_nets];
+  for (int64_t q = 0; q < P; ++q) {
+    if (net_gate[q] < 0 || net_gate[q] >= n_gates) {
+      set_error("fx_design_load: pin %lld names gate %d (n_gates=%d)",
+                (long long)q, net_gate[q], n_gates);
+      return FX_EINVAL;
+    }
+  }
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  fx_design *d = new (std::nothrow) fx_design();
+  if (!d) return FX_ENOMEM;
+  d->ctx = ctx;
+  d->n = n_gates;
+  d->m = n_nets;
+  d->p = P;
+  d->chip_w = chip_w;
+  d->chip_h = chip_h;
+  int rc = build_adjacency(n_gates, n_nets, net_ptr, net_gate, d->h_adj_ptr,
+                           d->h_adj_idx);
+  if (rc != FX_OK) {
+    delete d;
+    return rc;
+  }
+  d->a = (int64_t)d->h_adj_idx.size();
+  d->h_w.resize(n_gates);
+  d->h_h.resize(n_gates);
+  std::vector<float> area(n_gates);
+  for (int32_t g = 0; g < n_gates; ++g) {
+    d->h_w[g] = gate_w ? gate_w[g] : 2.0f;
+    d->h_h[g] = gate_h ? gate_h[g] : 10.0f;
+    area[g] = d->h_w[g] * d->h_h[g];
+  }
+  const size_t N = (size_t)n_gates;
+  auto fail = [&](int code) {
+    fx_design_free(d);
+    return code;
+  };
+  if ((rc = d->net_ptr.alloc((size_t)n_nets + 1)) ||
+      (rc = d->net_gate.alloc(P > 0 ? (size_t)P : 1)) ||
+      (rc = d->adj_ptr.alloc(N + 1)) ||
+      (rc = d->adj_idx.alloc(d->a > 0 ? (size_t)d->a : 1)) ||
+      (rc = d->area.alloc(N)) || (rc = d->x[0].alloc(N)) ||
+      (rc = d->y[0].alloc(N)) || (rc = d->x[1].alloc(N)) ||
+      (rc = d->y[1].alloc(N)) || (rc = d->vx.alloc(N)) ||
+      (rc = d->vy.alloc(N)) || (rc = d->fattr.alloc(N)))
+    return fail(rc);
+  cudaStream_t s = ctx->stream;
+  if (cudaMemcpyAsync(d->net_ptr.p, net_ptr, ((size_t)n_nets + 1) * 4,
+                      cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      (P > 0 && cudaMemcpyAsync(d->net_gate.p, net_gate, (size_t)P * 4,
+                                cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+      cudaMemcpyAsync(d->adj_ptr.p, d->h_adj_ptr.data(), (N + 1) * 4,
+                      cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      (d->a > 0 && cudaMemcpyAsync(d->adj_idx.p, d->h_adj_idx.data(),
+                                   (size_t)d->a * 4, cudaMemcpyHostToDevice,
+                                   s) != cudaSuccess) ||
+      cudaMemcpyAsync(d->area.p, area.data(), N * 4, cudaMemcpyHostToDevice,
+                      s) != cudaSuccess ||
+      cudaMemsetAsync(d->x[0].p, 0, N * 4, s) != cudaSuccess ||
+      cudaMemsetAsync(d->y[0].p, 0, N * 4, s) != cudaSuccess ||
+      cudaMemsetAsync(d->vx.p, 0, N * 4, s) != cudaSuccess ||
+      cudaMemsetAsync(d->vy.p, 0, N * 4, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    set_error("fx_design_load: upload failed: %s",
+              cudaGetErrorString(cudaGetLastError()));
+    return fail(FX_ECUDA);
+  }
+  *out_design = d;
+  return FX_OK;
+}
+
+extern "C" int fx_design_free(fx_design *d) {
+  if (!d) return FX_OK;
+  cudaSetDevice(d->ctx->device);
+  cudaStreamSynchronize(d->ctx->stream);
+  cudaStreamSynchronize(d->ctx->stream2);
+  d->net_ptr.release();
+  d->net_gate.release();
+  d->adj_ptr.release();
+  d->adj_idx.release();
+  d->area.release();
+  for (int i = 0; i < 2; ++i) {
+    d->x[i].release();
+    d->y[i].release();
+  }
+  d->vx.release();
+  d->vy.release();
+  d->fattr.release();
+  BHWork &b = d->bh;
+  for (int i = 0; i < 2; ++i) {
+    b.keys[i].release();
+    b.idx[i].release();
+  }
+  b.tile_hist.release();
+  b.tile_scan.release();
+  b.spos.release();
+  b.prefix.release();
+  b.child.release();
+  b.range.release();
+  b.com.release();
+  b.meta.release();
+  b.root.release();
+  b.bbox.release();
+  b.force.release();
+  DensityWork &w = d->dens;
+  w.area_fx.release();
+  w.cmat.release();
+  w.cmat_t.release();
+  w.cmat_lo.release();
+  w.cmat_t_lo.release();
+  w.cmat_bf.release();
+  w.cmat_t_bf.release();
+  w.inv_eig.release();
+  for (int i = 0; i < 4; ++i) w.buf[i].release();
+  for (int i = 0; i < 3; ++i) w.lo[i].release();
+  for (int i = 0; i < 2; ++i) w.bf[i].release();
+  w.ex.release();
+  w.ey.release();
+  w.energy.release();
+  w.force.release();
+  CongWork &c = d->cong;
+  c.diff.release();
+  c.counts.release();
+  c.partial.release();
+  c.partial_max.release();
+  c.done.release();
+  c.result.release();
+  c.result_max.release();
+  delete d;
+  return FX_OK;
+}
+
+extern "C" int fx_design_sizes(const fx_design *d, int64_t *out_n,
+                               int64_t *out_m, int64_t *out_p,
+                               int64_t *out_a) {
+  if (!d) return FX_EINVAL;
+  if (out_n) *out_n = d->n;
+  if (out_m) *out_m = d->m;
+  if (out_p) *out_p = d->p;
+  if (out_a) *out_a = d->a;
+  return FX_OK;
+}
+
+extern "C" int fx_design_adjacency(const fx_design *d, int32_t *out_adj_ptr,
+                                   int32_t *out_adj_idx) {
+  if (!d) return FX_EINVAL;
+  if (out_adj_ptr)
+    memcpy(out_adj_ptr, d->h_adj_ptr.data(), d->h_adj_ptr.size() * 4);
+  if (out_adj_idx && !d->h_adj_idx.empty())
+    memcpy(out_adj_idx, d->h_adj_idx.data(), d->h_adj_idx.size() * 4);
+  return FX_OK;
+}
+
+extern "C" int fx_design_set_positions(fx_design *d, const float *x,
+                                       const float *y) {
+  if (!d || !x || !y) return FX_EINVAL;
+  FX_CHECK_CUDA(cudaSetDevice(d->ctx->device));
+  cudaStream_t s = d->ctx->stream;
+  const size_t b = (size_t)d->n * 4;
+  d->cur = 0;
+  FX_CHECK_CUDA(cudaMemcpyAsync(d->x[0].p, x, b, cudaMemcpyHostToDevice, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(d->y[0].p, y, b, cudaMemcpyHostToDevice, s));
+  FX_CHECK_CUDA(cudaMemsetAsync(d->vx.p, 0, b, s));
+  FX_CHECK_CUDA(cudaMemsetAsync(d->vy.p, 0, b, s));
+  FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  return FX_OK;
+}
+
+extern "C" int fx_design_get_positions(fx_design *d, float *out_x,
+                                       float *out_y) {
+  if (!d || !out_x || !out_y) return FX_EINVAL;
+  FX_CHECK_CUDA(cudaSetDevice(d->ctx->device));
+  cudaStream_t s = d->ctx->stream;
+  const size_t b = (size_t)d->n * 4;
+  FX_CHECK_CUDA(cudaMemcpyAsync(out_x, d->x[d->cur].p, b, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(out_y, d->y[d->cur].p, b, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  return FX_OK;
+}
+
+extern "C" int64_t fx_design_device_bytes(const fx_design *d) {
+  if (!d) return -1;
+  int64_t t = 0;
+  t += d->net_ptr.bytes() + d->net_gate.bytes() + d->adj_ptr.bytes() +
+       d->adj_idx.bytes() + d->area.bytes();
+  for (int i = 0; i < 2; ++i) t += d->x[i].bytes() + d->y[i].bytes();
+  t += d->vx.bytes() + d->vy.bytes() + d->fattr.bytes();
+  const BHWork &b = d->bh;
+  for (int i = 0; i < 2; ++i) t += b.keys[i].bytes() + b.idx[i].bytes();
+  t += b.tile_hist.bytes() + b.tile_scan.bytes() + b.spos.bytes() +
+       b.prefix.bytes() + b.child.bytes() + b.range.bytes() + b.com.bytes() +
+       b.meta.bytes() + b.force.bytes();
+  const DensityWork &w = d->dens;
+  t += w.area_fx.bytes() + w.cmat.bytes() + w.cmat_t.bytes() +
+       w.cmat_lo.bytes() + w.cmat_t_lo.bytes() + w.cmat_bf.bytes() +
+       w.cmat_t_bf.bytes() + w.inv_eig.bytes() + w.ex.bytes() + w.ey.bytes() +
+       w.force.bytes();
+  for (int i = 0; i < 4; ++i) t += w.buf[i].bytes();
+  for (int i = 0; i < 3; ++i) t += w.lo[i].bytes();
+  for (int i = 0; i < 2; ++i) t += w.bf[i].bytes();
+  const CongWork &c = d->cong;
+  t += c.diff.bytes() + c.counts.bytes();
+  return t;
+}

@@ -1,0 +1,104 @@
+// fx_device.cuh -- small device helpers shared by the kernels.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+
+namespace fx {
+
+__device__ __forceinline__ int lin_tid() {
+  return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+__device__ __forceinline__ int block_threads() {
+  return blockDim.x * blockDim.y * blockDim.z;
+}
+
+// Rust's `(v / cell) as usize` followed by `.min(n - 1)` (grid.rs:58-62):
+// IEEE f32 division, truncation toward zero, NaN and negatives saturate to 0,
+// large values (and +inf) clamp to n - 1. `cell` is the f32 cell size.
+__device__ __forceinline__ int cell_at(float v, float cell, int n) {
+  const float q = __fdiv_rn(v, cell);
+  if (!(q >= 1.0f)) return 0;
+  if (q >= (float)n) return n - 1;
+  const int c = (int)q;
+  return c < n - 1 ? c : n - 1;
+}
+
+// Deterministic block reductions (fixed shuffle tree, fixed warp order).
+// Every thread of the block must call them; the result is valid everywhere.
+__device__ __forceinline__ double block_sum_double(double v) {
+  __shared__ double ws[32];
+  __shared__ double total;
+  const int t = lin_tid(), lane = t & 31, w = t >> 5;
+  const int nw = (block_threads() + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double u = lane < nw ? ws[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) u += __shfl_down_sync(0xffffffffu, u, o);
+    if (lane == 0) total = u;
+  }
+  __syncthreads();
+  return total;
+}
+
+__device__ __forceinline__ float block_max_float(float v) {
+  __shared__ float ws[32];
+  __shared__ float total;
+  const int t = lin_tid(), lane = t & 31, w = t >> 5;
+  const int nw = (block_threads() + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    float u = lane < nw ? ws[lane] : -FLT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) u = fmaxf(u, __shfl_down_sync(0xffffffffu, u, o));
+    if (lane == 0) total = u;
+  }
+  __syncthreads();
+  return total;
+}
+
+// Cross-block FP64 sum in a fixed order: each block stores its partial, the
+// last block to finish adds all partials (same order every run) into
+// *result and re-arms the counter.
+__device__ __forceinline__ void last_block_sum(double block_value,
+                                               double *partial,
+                                               unsigned int *done,
+                                               double *result) {
+  __shared__ bool last;
+  const int t = lin_tid();
+  if (t == 0) {
+    partial[blockIdx.x] = block_value;
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double a = 0.0;
+  for (int i = t; i < (int)gridDim.x; i += block_threads())
+    a += ((volatile double *)partial)[i];
+  a = block_sum_double(a);
+  if (t == 0) {
+    *result = a;
+    *done = 0;
+  }
+}
+
+// Order-preserving float <-> uint mapping for atomicMin/atomicMax.
+__device__ __forceinline__ unsigned int f2ord(float f) {
+  const unsigned int u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(unsigned int u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+}  // namespace fx

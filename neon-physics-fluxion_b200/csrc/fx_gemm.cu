@@ -1,0 +1,100 @@
+// fx_gemm.cu -- NT GEMM dispatch for the DCT stage and the FP32 CUDA-core
+// (SIMT) variant. The tensor-core variants live in fx_gemm_tc.cu.
+#include "fx_internal.h"
+#include "fx_gemm.cuh"
+
+namespace fx {
+
+int gemm_nt_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
+               const GemmOperands &B, const float *S, const GemmOperands &D,
+               cudaStream_t s);
+
+constexpr int kBM = 128, kBN = 128, kBK = 16;
+
+// 128 x 128 tile per CTA, 8 x 8 outputs per thread in two 4-wide strips per
+// axis (conflict-free shared reads), K staged 16 at a time and stored
+// k-major in shared memory.
+__global__ void __launch_bounds__(256)
+sgemm_nt_kernel(const float *__restrict__ A, const float *__restrict__ B,
+                int G, const float *__restrict__ S, float *__restrict__ D,
+                float *__restrict__ Dlo, uint16_t *__restrict__ Dbf) {
+  __shared__ __align__(16) float As[kBK][kBM + 4];
+  __shared__ __align__(16) float Bs[kBK][kBN + 4];
+  const int t = threadIdx.x;
+  const int bm = blockIdx.y * kBM, bn = blockIdx.x * kBN;
+  const int lr = t >> 2, lk = (t & 3) * 4;
+  const int tx = t & 15, ty = t >> 4;
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+  const float *a0 = A + (size_t)(bm + lr) * G + lk;
+  const float *a1 = a0 + (size_t)64 * G;
+  const float *b0 = B + (size_t)(bn + lr) * G + lk;
+  const float *b1 = b0 + (size_t)64 * G;
+  float4 ra0 = *(const float4 *)a0, ra1 = *(const float4 *)a1;
+  float4 rb0 = *(const float4 *)b0, rb1 = *(const float4 *)b1;
+  for (int k0 = 0; k0 < G; k0 += kBK) {
+    As[lk + 0][lr] = ra0.x; As[lk + 1][lr] = ra0.y;
+    As[lk + 2][lr] = ra0.z; As[lk + 3][lr] = ra0.w;
+    As[lk + 0][lr + 64] = ra1.x; As[lk + 1][lr + 64] = ra1.y;
+    As[lk + 2][lr + 64] = ra1.z; As[lk + 3][lr + 64] = ra1.w;
+    Bs[lk + 0][lr] = rb0.x; Bs[lk + 1][lr] = rb0.y;
+    Bs[lk + 2][lr] = rb0.z; Bs[lk + 3][lr] = rb0.w;
+    Bs[lk + 0][lr + 64] = rb1.x; Bs[lk + 1][lr + 64] = rb1.y;
+    Bs[lk + 2][lr + 64] = rb1.z; Bs[lk + 3][lr + 64] = rb1.w;
+    __syncthreads();
+    if (k0 + kBK < G) {
+      ra0 = *(const float4 *)(a0 + k0 + kBK);
+      ra1 = *(const float4 *)(a1 + k0 + kBK);
+      rb0 = *(const float4 *)(b0 + k0 + kBK);
+      rb1 = *(const float4 *)(b1 + k0 + kBK);
+    }
+#pragma unroll
+    for (int kk = 0; kk < kBK; ++kk) {
+      const float4 x0 = *(const float4 *)&As[kk][ty * 4];
+      const float4 x1 = *(const float4 *)&As[kk][64 + ty * 4];
+      const float4 y0 = *(const float4 *)&Bs[kk][tx * 4];
+      const float4 y1 = *(const float4 *)&Bs[kk][64 + tx * 4];
+      const float a[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+      const float b[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = bm + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = bn + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+      const size_t o = (size_t)r * G + c;
+      float v = acc[i][j];
+      if (S) v *= S[o];
+      store_operand(v, o, D, Dlo, Dbf);
+    }
+  }
+}
+
+int gemm_nt(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
+            const GemmOperands &B, const float *S, const GemmOperands &D,
+            cudaStream_t s) {
+  if (G % 128 != 0) {
+    set_error("gemm_nt: G=%d is not a multiple of 128", G);
+    return FX_EINVAL;
+  }
+  if (precision == FX_DCT_SIMT) {
+    dim3 grid(G / kBN, G / kBM);
+    sgemm_nt_kernel<<<grid, 256, 0, s>>>(A.f32, B.f32, G, S, D.f32, D.lo, D.bf);
+    FX_CHECK_LAUNCH();
+    ctx->launches += 1;
+    return FX_OK;
+  }
+  return gemm_nt_tc(ctx, precision, G, A, B, S, D, s);
+}
+
+}  // namespace fx

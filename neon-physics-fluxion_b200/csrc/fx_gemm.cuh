@@ -1,0 +1,68 @@
+// fx_gemm.cuh -- NT GEMM interface used by the DCT Poisson stage.
+#pragma once
+#include <cstdint>
+#include <cstring>
+
+#include <cuda_bf16.h>
+
+namespace fx {
+
+// One GEMM operand in every format a precision path may read or write:
+//   f32 -- full values (SIMT, TF32) or the TF32 head (3xTF32 split),
+//   lo  -- residual f32 - head (3xTF32 only),
+//   bf  -- bfloat16 copy (BF16 only).
+struct GemmOperands {
+  float *f32;
+  float *lo;
+  uint16_t *bf;
+};
+
+// Round-to-nearest-even to TF32 (10 explicit mantissa bits). A value whose
+// low 13 bits are zero is read exactly by the tensor cores whatever their
+// rounding of f32 inputs.
+__host__ __device__ inline float tf32_round(float v) {
+  uint32_t u;
+  memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) {
+    u += 0xfffu + ((u >> 13) & 1u);
+    u &= 0xffffe000u;
+  }
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+inline float tf32_hi_host(float v) { return tf32_round(v); }
+
+inline uint16_t bf16_host(float v) {
+  uint32_t u;
+  memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+// Writes v in the formats requested by the non-null pointers: with `lo` the
+// head goes to f32 and the exact residual to lo.
+__device__ __forceinline__ void store_operand(float v, size_t i, float *f32,
+                                              float *lo, uint16_t *bf) {
+  if (lo) {
+    const float h = tf32_round(v);
+    f32[i] = h;
+    lo[i] = v - h;
+  } else if (f32) {
+    f32[i] = v;
+  }
+  if (bf) {
+    __nv_bfloat16 b = __float2bfloat16_rn(v);
+    bf[i] = *reinterpret_cast<uint16_t *>(&b);
+  }
+}
+
+// D[i][j] = sum_k A[i][k] * B[j][k] (* S[i][j] when S != nullptr) for G x G
+// row-major matrices, written to D in the formats of `precision`.
+int gemm_nt(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
+            const GemmOperands &B, const float *S, const GemmOperands &D,
+            cudaStream_t s);
+
+}  // namespace fx

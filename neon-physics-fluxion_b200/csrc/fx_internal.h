@@ -1,0 +1,181 @@
+// fx_internal.h -- shared declarations of libfluxion_b200 (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/fluxion_b200.h"
+
+namespace fx {
+
+// ---- error handling --------------------------------------------------------
+void set_error(const char *fmt, ...);
+
+struct Status {
+  int code = FX_OK;
+};
+
+#define FX_CHECK_CUDA(expr)                                                   \
+  do {                                                                        \
+    cudaError_t _e = (expr);                                                  \
+    if (_e != cudaSuccess) {                                                  \
+      ::fx::set_error("%s:%d %s: %s", __FILE__, __LINE__, #expr,              \
+                      cudaGetErrorString(_e));                                \
+      return FX_ECUDA;                                                        \
+    }                                                                         \
+  } while (0)
+
+#define FX_TRY(expr)                                                          \
+  do {                                                                        \
+    int _rc = (expr);                                                         \
+    if (_rc != FX_OK) return _rc;                                             \
+  } while (0)
+
+// Checks the launch that was just issued.
+#define FX_CHECK_LAUNCH() FX_CHECK_CUDA(cudaGetLastError())
+
+// ---- device buffers --------------------------------------------------------
+// A typed device allocation owned by a design or context.
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    if (count <= n && p) return FX_OK;
+    release();
+    if (count == 0) return FX_OK;
+    cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error("cudaMalloc(%zu bytes): %s", count * sizeof(T),
+                cudaGetErrorString(e));
+      return FX_ENOMEM;
+    }
+    n = count;
+    return FX_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---- per-stage timing ------------------------------------------------------
+struct StageTimer {
+  bool enabled = false;
+  double ms[FX_STAGE_COUNT] = {};
+  int64_t calls[FX_STAGE_COUNT] = {};
+  // Pending (start, stop) pairs, resolved lazily on query.
+  struct Pending {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t get_event();
+  void resolve();
+  void destroy();
+};
+
+// ---- Barnes-Hut workspace ----------------------------------------------------
+struct BHWork {
+  int n = 0;
+  DevBuf<uint32_t> keys[2];
+  DevBuf<int32_t> idx[2];
+  DevBuf<uint32_t> tile_hist;   // radix sort: digit x tile counts
+  DevBuf<uint32_t> tile_scan;
+  DevBuf<float2> spos;          // positions in sorted order
+  DevBuf<double2> prefix;       // inclusive prefix sums of spos (FP64)
+  DevBuf<int32_t> child;        // internal nodes: 2 per node (tagged)
+  DevBuf<int32_t> range;        // internal nodes: first,last
+  DevBuf<float4> com;           // internal nodes: {cx_hi, cy_hi, cx_lo, cy_lo}
+  DevBuf<float2> meta;          // internal nodes: {count, size^2 (or <0)}
+  DevBuf<float> root;           // {x_min, y_min, size, inv_size}
+  DevBuf<unsigned int> bbox;    // ordered-int min/max of x, y
+  DevBuf<float2> force;         // per gate (original order)
+};
+
+// ---- density (DCT Poisson) workspace -----------------------------------------
+struct DensityWork {
+  int G = 0;
+  int precision = -1;
+  DevBuf<unsigned long long> area_fx;  // fixed-point area per bin (G*G)
+  DevBuf<float> cmat;                  // DCT-II ortho matrix C (G*G)
+  DevBuf<float> cmat_t;                // C^T
+  DevBuf<float> cmat_lo;               // C - tf32(C) for the 3xTF32 split
+  DevBuf<float> cmat_t_lo;
+  DevBuf<uint16_t> cmat_bf, cmat_t_bf; // bf16 copies
+  DevBuf<float> inv_eig;               // -1/lambda with DC = 0 (G*G)
+  DevBuf<float> buf[4];                // rho, t1, t2, phi
+  DevBuf<float> lo[3];                 // low parts for 3xTF32 operands
+  DevBuf<uint16_t> bf[2];              // bf16 operand staging
+  DevBuf<float> ex, ey;                // field
+  DevBuf<double> energy;               // FP64 partials
+  DevBuf<float2> force;                // per gate
+};
+
+// ---- congestion workspace ----------------------------------------------------
+struct CongWork {
+  int cols = 0, rows = 0;
+  DevBuf<int32_t> diff;        // (rows+1) x (cols+1) difference array
+  DevBuf<uint32_t> counts;     // rows x cols
+  DevBuf<double> partial;      // per-block FP64 partial sums
+  DevBuf<float> partial_max;
+  DevBuf<unsigned int> done;   // last-block counters
+  DevBuf<double> result;       // {hpwl, total_overflow}
+  DevBuf<float> result_max;
+};
+
+}  // namespace fx
+
+struct fx_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;   // main stream
+  cudaStream_t stream2 = nullptr;  // side stream (density || Barnes-Hut)
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int num_sms = 0;
+  fx::StageTimer timer;
+  int64_t launches = 0;
+};
+
+struct fx_design {
+  fx_ctx *ctx = nullptr;
+  int32_t n = 0, m = 0;
+  int64_t p = 0, a = 0;
+  float chip_w = 0.f, chip_h = 0.f;
+  // netlist
+  fx::DevBuf<int32_t> net_ptr, net_gate;
+  fx::DevBuf<int32_t> adj_ptr, adj_idx;
+  fx::DevBuf<float> area;        // w*h per gate
+  std::vector<int32_t> h_adj_ptr, h_adj_idx;
+  std::vector<float> h_w, h_h;
+  // state: ping-pong positions, velocities
+  fx::DevBuf<float> x[2], y[2];
+  int cur = 0;
+  fx::DevBuf<float> vx, vy;
+  fx::DevBuf<float2> fattr;      // attraction-only force output (stage API)
+  // workspaces
+  fx::BHWork bh;
+  fx::DensityWork dens;
+  fx::CongWork cong;
+};
+
+namespace fx {
+// stage launchers (return FX_* codes), all on ctx->stream unless noted.
+int congestion_run(fx_ctx *ctx, fx_design *d, const float *dx, const float *dy,
+                   int cols, int rows, cudaStream_t s);
+int attraction_run(fx_ctx *ctx, fx_design *d, float k, float2 *out, cudaStream_t s);
+int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
+           cudaStream_t s);
+int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
+                int precision, cudaStream_t s);
+int fused_step(fx_ctx *ctx, fx_design *d, const fx_iter_cfg &cfg,
+               cudaStream_t s);
+void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a);
+void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a);
+}  // namespace fx

@@ -1,0 +1,145 @@
+"""ctypes binding of libfluxion_b200.so (the C ABI in include/fluxion_b200.h).
+
+The shared library is built in-tree next to this file. Importing this module
+never falls back to anything else: a missing library raises at load time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libfluxion_b200.so"
+
+FX_OK = 0
+FX_EINVAL = -1
+FX_ENOMEM = -2
+FX_ECUDA = -3
+FX_ETIMEOUT = -4
+FX_EADMIT = -5
+FX_ENODEV = -6
+
+FX_DCT_FP32 = 0
+FX_DCT_TF32 = 1
+FX_DCT_BF16 = 2
+FX_DCT_SIMT = 3
+
+STAGES = ["attract_integrate", "bh_keys", "bh_sort", "bh_tree", "bh_walk",
+          "density", "congestion", "leaf", "fiedler"]
+
+_CODES = {FX_EINVAL: "FX_EINVAL", FX_ENOMEM: "FX_ENOMEM", FX_ECUDA: "FX_ECUDA",
+          FX_ETIMEOUT: "FX_ETIMEOUT", FX_EADMIT: "FX_EADMIT",
+          FX_ENODEV: "FX_ENODEV"}
+
+
+class FluxionError(RuntimeError):
+    """A C-ABI call returned a negative status."""
+
+    def __init__(self, code: int, where: str, message: str):
+        super().__init__(f"{where}: {_CODES.get(code, code)}: {message}")
+        self.code = code
+
+
+class IterCfg(C.Structure):
+    _fields_ = [("attract_weight", C.c_float), ("repel_weight", C.c_float),
+                ("min_dist", C.c_float), ("theta", C.c_float),
+                ("density_weight", C.c_float), ("target_density", C.c_float),
+                ("density_bins", C.c_int32), ("dct_precision", C.c_int32),
+                ("cong_cols", C.c_int32), ("cong_rows", C.c_int32),
+                ("damping", C.c_float), ("dt", C.c_float)]
+
+
+class IterStats(C.Structure):
+    _fields_ = [("hpwl", C.c_double), ("total_overflow", C.c_double),
+                ("max_overflow", C.c_float), ("pad0", C.c_float),
+                ("density_energy", C.c_double), ("iterations", C.c_int64),
+                ("bh_nodes", C.c_int64)]
+
+
+class LeafCfg(C.Structure):
+    _fields_ = [("force_iterations", C.c_int32), ("attract_weight", C.c_float),
+                ("repel_weight", C.c_float), ("damping", C.c_float),
+                ("dt", C.c_float), ("schedule", C.c_int32),
+                ("threads_per_cluster", C.c_int32), ("use_graph", C.c_int32)]
+
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+F32 = C.c_float
+PI32 = C.POINTER(C.c_int32)
+PI64 = C.POINTER(C.c_int64)
+PU32 = C.POINTER(C.c_uint32)
+PF32 = C.POINTER(C.c_float)
+PF64 = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes). Every symbol declared in include/fluxion_b200.h.
+SIGNATURES = {
+    "fx_last_error": (C.c_char_p, []),
+    "fx_version": (C.c_char_p, []),
+    "fx_ctx_create": (C.c_int, [C.POINTER(P), C.c_int]),
+    "fx_ctx_destroy": (C.c_int, [P]),
+    "fx_ctx_set_profiling": (C.c_int, [P, C.c_int]),
+    "fx_ctx_stage_times": (C.c_int, [P, PF64, PI64, C.c_int]),
+    "fx_ctx_reset_stage_times": (C.c_int, [P]),
+    "fx_ctx_kernel_launches": (C.c_int64, [P]),
+    "fx_design_load": (C.c_int, [P, I32, I32, PI32, PI32, PF32, PF32, F32, F32,
+                                 C.POINTER(P)]),
+    "fx_design_free": (C.c_int, [P]),
+    "fx_design_sizes": (C.c_int, [P, PI64, PI64, PI64, PI64]),
+    "fx_design_adjacency": (C.c_int, [P, PI32, PI32]),
+    "fx_design_set_positions": (C.c_int, [P, PF32, PF32]),
+    "fx_design_get_positions": (C.c_int, [P, PF32, PF32]),
+    "fx_design_device_bytes": (C.c_int64, [P]),
+    "fx_congestion": (C.c_int, [P, P, PF32, PF32, I32, I32, PU32, PF64, PF64, PF32]),
+    "fx_iter_cfg_default": (C.c_int, [C.POINTER(IterCfg)]),
+    "fx_force_iterate": (C.c_int, [P, P, C.POINTER(IterCfg), I32, PF32, PF32,
+                                   C.POINTER(IterStats)]),
+    "fx_stage_attraction": (C.c_int, [P, P, F32, PF32, PF32]),
+    "fx_stage_barnes_hut": (C.c_int, [P, P, F32, F32, F32, PF32, PF32, PU32,
+                                      PI32, PF32]),
+    "fx_stage_density": (C.c_int, [P, P, I32, F32, F32, I32, PF32, PF32, PF32,
+                                   PF32, PF32, PF32, PF64]),
+    "fx_synth_plain": (C.c_int, [C.c_uint64, I32, I32, F32, F32, I32, C.POINTER(P)]),
+    "fx_synth_leaves": (C.c_int, [C.c_uint64, I32, I32, I32, F32, C.POINTER(P)]),
+    "fx_netlist_sizes": (C.c_int, [P, PI64, PI64, PI64, PI64]),
+    "fx_netlist_copy": (C.c_int, [P, PI32, PI32, PF32, PF32, PF32, PF32, PF32,
+                                  PI32, PF32]),
+    "fx_netlist_free": (C.c_int, [P]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the in-tree library once; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FluxionError(FX_ENODEV, "load",
+                           f"{LIB_PATH} is missing; build it with "
+                           "`python -c 'import __graft_entry__ as g; g.build()'`")
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_GLOBAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, where: str) -> int:
+    if rc < 0:
+        msg = load().fx_last_error()
+        raise FluxionError(rc, where, msg.decode() if msg else "")
+    return rc
+
+
+def ptr(a, ctype):
+    """Pointer to a contiguous numpy array (or NULL for None)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))

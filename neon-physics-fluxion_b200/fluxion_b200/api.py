@@ -1,0 +1,421 @@
+"""Host-side mirror of the reference's data types and entry points.
+
+The reference (HAPR_fluxion_v4, Rust) keeps a Circuit of flat per-gate arrays
+(src/data/circuit.rs:43-78), a Placement of per-gate f32 positions
+(src/data/placement.rs:9-24) and a RoutingGrid (src/data/grid.rs:10-21).
+The same shapes are kept here as numpy arrays, and every compute entry point
+runs on the B200 through the C ABI in include/fluxion_b200.h. There is no CPU
+compute path in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import FluxionError, IterCfg, IterStats, check, load, ptr
+
+
+# ---------------------------------------------------------------------------
+# data types
+@dataclass
+class Circuit:
+    """Flat netlist: net e joins net_gate[net_ptr[e]:net_ptr[e+1]].
+
+    Mirrors Circuit (circuit.rs:43-78): gate_widths/gate_heights per gate,
+    net_gate_indices per net (here as CSR), chip_width/chip_height.
+    """
+    num_gates: int
+    net_ptr: np.ndarray
+    net_gate: np.ndarray
+    gate_widths: np.ndarray
+    gate_heights: np.ndarray
+    chip_width: float
+    chip_height: float
+    name: str = "design"
+    gate_names: Optional[list] = None
+
+    @property
+    def num_nets(self) -> int:
+        return int(self.net_ptr.shape[0] - 1)
+
+    @property
+    def num_pins(self) -> int:
+        return int(self.net_ptr[-1])
+
+    @property
+    def net_gate_indices(self) -> list:
+        p, g = self.net_ptr, self.net_gate
+        return [g[p[e]:p[e + 1]].tolist() for e in range(self.num_nets)]
+
+    @staticmethod
+    def from_nets(nets: Sequence[Sequence[int]], num_gates: int,
+                  chip_width: float = 1000.0, chip_height: float = 1000.0,
+                  gate_widths=None, gate_heights=None, name: str = "design",
+                  gate_names=None) -> "Circuit":
+        ptr_ = np.zeros(len(nets) + 1, np.int32)
+        for e, n in enumerate(nets):
+            ptr_[e + 1] = ptr_[e] + len(n)
+        flat = np.fromiter((g for n in nets for g in n), np.int32, int(ptr_[-1]))
+        w = np.full(num_gates, 2.0, np.float32) if gate_widths is None else \
+            np.asarray(gate_widths, np.float32)
+        h = np.full(num_gates, 10.0, np.float32) if gate_heights is None else \
+            np.asarray(gate_heights, np.float32)
+        return Circuit(num_gates, ptr_, flat, w, h, float(chip_width),
+                       float(chip_height), name, gate_names)
+
+
+@dataclass
+class Placement:
+    """Per-gate f32 positions and quality metrics (placement.rs:9-24)."""
+    gate_x: np.ndarray
+    gate_y: np.ndarray
+    total_wirelength: float = 0.0
+    max_congestion: float = 0.0
+    wns: float = 0.0
+    runtime_ms: float = 0.0
+
+    @staticmethod
+    def new(num_gates: int) -> "Placement":
+        return Placement(np.zeros(num_gates, np.float32), np.zeros(num_gates, np.float32))
+
+    def set_position(self, g: int, x: float, y: float) -> None:
+        self.gate_x[g] = x
+        self.gate_y[g] = y
+
+
+@dataclass
+class RoutingGrid:
+    """Routing grid geometry and congestion (grid.rs:10-32).
+
+    h_congestion and v_congestion are f32 arrays of rows*cols (row-major),
+    equal to each other as in the reference; counts holds the exact uint32
+    crossing counts they were converted from.
+    """
+    cols: int
+    rows: int
+    cell_width: float
+    cell_height: float
+    h_congestion: np.ndarray
+    v_congestion: np.ndarray
+    capacity: np.ndarray
+    counts: Optional[np.ndarray] = None
+
+    @staticmethod
+    def new(chip_width: float, chip_height: float, cols: int, rows: int) -> "RoutingGrid":
+        cw = np.float32(chip_width) / np.float32(cols)
+        ch = np.float32(chip_height) / np.float32(rows)
+        cap = (cw + ch) * np.float32(0.5)
+        cells = cols * rows
+        return RoutingGrid(cols, rows, float(cw), float(ch),
+                           np.zeros(cells, np.float32), np.zeros(cells, np.float32),
+                           np.full(cells, cap, np.float32))
+
+    def cell_index(self, col: int, row: int) -> int:
+        return row * self.cols + col
+
+    def cell_at(self, x: float, y: float):
+        """grid.rs:58-62: f32 division, saturating cast, clamp to the grid."""
+        def one(v, cell, n):
+            q = np.float32(v) / np.float32(cell)
+            if not (q >= 1.0):
+                return 0
+            return int(min(int(q) if q < 2.0 ** 63 else n - 1, n - 1))
+        return one(x, self.cell_width, self.cols), one(y, self.cell_height, self.rows)
+
+    def cell_center(self, col: int, row: int):
+        return ((np.float32(col) + np.float32(0.5)) * np.float32(self.cell_width),
+                (np.float32(row) + np.float32(0.5)) * np.float32(self.cell_height))
+
+    def overflow(self) -> np.ndarray:
+        return np.maximum((self.h_congestion + self.v_congestion) - self.capacity,
+                          np.float32(0.0))
+
+    def max_overflow(self) -> float:
+        return float(self.overflow().max(initial=0.0))
+
+    def total_overflow(self) -> float:
+        return float(self.overflow().astype(np.float64).sum())
+
+
+# ---------------------------------------------------------------------------
+# device context and resident designs
+class Context:
+    """A CUDA context on one B200 (fx_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.fx_ctx_create(C.byref(h), device), "fx_ctx_create")
+        self.handle = h
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.fx_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_profiling(self, on: bool = True) -> None:
+        check(self.lib.fx_ctx_set_profiling(self.handle, int(on)), "set_profiling")
+
+    def stage_times(self) -> dict:
+        n = len(_lib.STAGES)
+        ms = (C.c_double * n)()
+        calls = (C.c_int64 * n)()
+        check(self.lib.fx_ctx_stage_times(self.handle, ms, calls, n), "stage_times")
+        return {s: (ms[i], calls[i]) for i, s in enumerate(_lib.STAGES)}
+
+    def reset_stage_times(self) -> None:
+        check(self.lib.fx_ctx_reset_stage_times(self.handle), "reset_stage_times")
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.fx_ctx_kernel_launches(self.handle))
+
+
+class Design:
+    """A device-resident netlist (fx_design) with positions and workspaces."""
+
+    def __init__(self, ctx: Context, circuit: Circuit):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.circuit = circuit
+        net_ptr = np.ascontiguousarray(circuit.net_ptr, np.int32)
+        net_gate = np.ascontiguousarray(circuit.net_gate, np.int32)
+        w = np.ascontiguousarray(circuit.gate_widths, np.float32)
+        h = np.ascontiguousarray(circuit.gate_heights, np.float32)
+        d = C.c_void_p()
+        check(self.lib.fx_design_load(ctx.handle, circuit.num_gates, circuit.num_nets,
+                                      ptr(net_ptr, C.c_int32), ptr(net_gate, C.c_int32),
+                                      ptr(w, C.c_float), ptr(h, C.c_float),
+                                      circuit.chip_width, circuit.chip_height,
+                                      C.byref(d)), "fx_design_load")
+        self.handle = d
+        n, m, p, a = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64())
+        check(self.lib.fx_design_sizes(d, C.byref(n), C.byref(m), C.byref(p),
+                                       C.byref(a)), "fx_design_sizes")
+        self.n, self.m, self.p, self.a = n.value, m.value, p.value, a.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.fx_design_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def adjacency(self):
+        ap = np.zeros(self.n + 1, np.int32)
+        ai = np.zeros(max(self.a, 1), np.int32)
+        check(self.lib.fx_design_adjacency(self.handle, ptr(ap, C.c_int32),
+                                           ptr(ai, C.c_int32)), "fx_design_adjacency")
+        return ap, ai[:self.a]
+
+    def set_positions(self, x, y) -> None:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        check(self.lib.fx_design_set_positions(self.handle, ptr(x, C.c_float),
+                                               ptr(y, C.c_float)), "set_positions")
+
+    def get_positions(self):
+        x = np.empty(self.n, np.float32)
+        y = np.empty(self.n, np.float32)
+        check(self.lib.fx_design_get_positions(self.handle, ptr(x, C.c_float),
+                                               ptr(y, C.c_float)), "get_positions")
+        return x, y
+
+    def device_bytes(self) -> int:
+        return int(self.lib.fx_design_device_bytes(self.handle))
+
+    # -- rows D+F -----------------------------------------------------------
+    def congestion(self, cols: int, rows: int, x=None, y=None):
+        """Returns (counts[rows*cols] uint32, hpwl f64, total_overflow, max_overflow)."""
+        counts = np.empty(cols * rows, np.uint32)
+        hp, tot, mx = C.c_double(), C.c_double(), C.c_float()
+        xa = None if x is None else np.ascontiguousarray(x, np.float32)
+        ya = None if y is None else np.ascontiguousarray(y, np.float32)
+        check(self.lib.fx_congestion(self.ctx.handle, self.handle, ptr(xa, C.c_float),
+                                     ptr(ya, C.c_float), cols, rows,
+                                     ptr(counts, C.c_uint32), C.byref(hp),
+                                     C.byref(tot), C.byref(mx)), "fx_congestion")
+        return counts, hp.value, tot.value, mx.value
+
+    # -- single stages --------------------------------------------------------
+    def attraction(self, k: float = 1.0):
+        fx = np.empty(self.n, np.float32)
+        fy = np.empty(self.n, np.float32)
+        check(self.lib.fx_stage_attraction(self.ctx.handle, self.handle, k,
+                                           ptr(fx, C.c_float), ptr(fy, C.c_float)),
+              "fx_stage_attraction")
+        return fx, fy
+
+    def barnes_hut(self, k: float = 0.5, theta: float = 0.5, min_dist: float = 0.1):
+        fx = np.empty(self.n, np.float32)
+        fy = np.empty(self.n, np.float32)
+        keys = np.empty(self.n, np.uint32)
+        perm = np.empty(self.n, np.int32)
+        root = np.empty(3, np.float32)
+        check(self.lib.fx_stage_barnes_hut(self.ctx.handle, self.handle, k, theta,
+                                           min_dist, ptr(fx, C.c_float),
+                                           ptr(fy, C.c_float), ptr(keys, C.c_uint32),
+                                           ptr(perm, C.c_int32), ptr(root, C.c_float)),
+              "fx_stage_barnes_hut")
+        return fx, fy, keys, perm, root
+
+    def density(self, bins: int, target: float = 0.7, weight: float = 1.0,
+                precision: int = _lib.FX_DCT_SIMT, grids: bool = False):
+        fx = np.empty(self.n, np.float32)
+        fy = np.empty(self.n, np.float32)
+        g = [np.empty(bins * bins, np.float32) for _ in range(4)] if grids else [None] * 4
+        e = C.c_double()
+        check(self.lib.fx_stage_density(self.ctx.handle, self.handle, bins, target, weight,
+                                        precision, ptr(fx, C.c_float), ptr(fy, C.c_float),
+                                        *(ptr(a, C.c_float) for a in g), C.byref(e)),
+              "fx_stage_density")
+        out = {"fx": fx, "fy": fy, "energy": e.value}
+        if grids:
+            out.update(rho=g[0].reshape(bins, bins), phi=g[1].reshape(bins, bins),
+                       ex=g[2].reshape(bins, bins), ey=g[3].reshape(bins, bins))
+        return out
+
+    # -- the plain composite iteration -------------------------------------
+    def force_iterate(self, cfg: "IterCfg", iters: int, x=None, y=None) -> IterStats:
+        st = IterStats()
+        xa = None if x is None else np.ascontiguousarray(x, np.float32)
+        ya = None if y is None else np.ascontiguousarray(y, np.float32)
+        check(self.lib.fx_force_iterate(self.ctx.handle, self.handle, C.byref(cfg), iters,
+                                        ptr(xa, C.c_float), ptr(ya, C.c_float),
+                                        C.byref(st)), "fx_force_iterate")
+        if x is not None:
+            x[...] = xa
+            y[...] = ya
+        return st
+
+
+def iter_cfg(**overrides) -> IterCfg:
+    cfg = IterCfg()
+    check(load().fx_iter_cfg_default(C.byref(cfg)), "fx_iter_cfg_default")
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# reference entry points
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def compute_congestion(grid: RoutingGrid, placement: Placement, circuit: Circuit,
+                       design: Optional[Design] = None) -> RoutingGrid:
+    """congestion.rs:11-62 compute_congestion_cpu, on the GPU.
+
+    Fills grid.h_congestion / grid.v_congestion (identical f32 grids) and
+    grid.counts from the exact device counts.
+    """
+    own = design is None
+    if own:
+        design = Design(default_context(), circuit)
+    try:
+        counts, hpwl, _, _ = design.congestion(grid.cols, grid.rows,
+                                               placement.gate_x, placement.gate_y)
+    finally:
+        if own:
+            design.close()
+    grid.counts = counts
+    grid.h_congestion = counts.astype(np.float32)
+    grid.v_congestion = grid.h_congestion.copy()
+    return grid
+
+
+def build_and_compute(placement: Placement, circuit: Circuit, cols: int, rows: int,
+                      design: Optional[Design] = None) -> RoutingGrid:
+    """congestion.rs:65-74 build_and_compute."""
+    grid = RoutingGrid.new(circuit.chip_width, circuit.chip_height, cols, rows)
+    return compute_congestion(grid, placement, circuit, design)
+
+
+def compute_hpwl(placement: Placement, circuit: Circuit,
+                 design: Optional[Design] = None) -> float:
+    """placement.rs:48-74 compute_hpwl, summed in FP64 on the GPU."""
+    own = design is None
+    if own:
+        design = Design(default_context(), circuit)
+    try:
+        _, hpwl, _, _ = design.congestion(1, 1, placement.gate_x, placement.gate_y)
+    finally:
+        if own:
+            design.close()
+    return hpwl
+
+
+# ---------------------------------------------------------------------------
+# synthetic netlists (host-only, no GPU needed)
+@dataclass
+class Synth:
+    circuit: Circuit
+    placement: Placement
+    leaf_ptr: np.ndarray
+    region: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+
+
+def _netlist_out(h) -> Synth:
+    lib = load()
+    n, m, p, nl = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+    check(lib.fx_netlist_sizes(h, C.byref(n), C.byref(m), C.byref(p), C.byref(nl)),
+          "fx_netlist_sizes")
+    N, M, Pn, L = n.value, m.value, p.value, nl.value
+    net_ptr = np.empty(M + 1, np.int32)
+    net_gate = np.empty(max(Pn, 1), np.int32)
+    w = np.empty(N, np.float32)
+    hh = np.empty(N, np.float32)
+    x = np.empty(N, np.float32)
+    y = np.empty(N, np.float32)
+    die = np.empty(2, np.float32)
+    leaf_ptr = np.empty(L + 1, np.int32)
+    region = np.empty(4 * max(L, 1), np.float32)
+    check(lib.fx_netlist_copy(h, ptr(net_ptr, C.c_int32), ptr(net_gate, C.c_int32),
+                              ptr(w, C.c_float), ptr(hh, C.c_float), ptr(x, C.c_float),
+                              ptr(y, C.c_float), ptr(die, C.c_float),
+                              ptr(leaf_ptr, C.c_int32), ptr(region, C.c_float)),
+          "fx_netlist_copy")
+    lib.fx_netlist_free(h)
+    circ = Circuit(N, net_ptr, net_gate[:Pn], w, hh, float(die[0]), float(die[1]),
+                   name="synthetic")
+    return Synth(circ, Placement(x, y), leaf_ptr, region[:4 * L])
+
+
+def synth_plain(seed: int, n_gates: int, n_nets: int, die: float,
+                leaf_size: int = 64) -> Synth:
+    """Seeded plain netlist (see fx_synth_plain in include/fluxion_b200.h)."""
+    h = C.c_void_p()
+    check(load().fx_synth_plain(seed, n_gates, n_nets, die, die, leaf_size, C.byref(h)),
+          "fx_synth_plain")
+    return _netlist_out(h)
+
+
+def synth_leaves(seed: int, n_clusters: int, min_size: int = 16, max_size: int = 128,
+                 nets_per_gate: float = 1.5) -> Synth:
+    """Seeded batch of independent leaf clusters (fx_synth_leaves)."""
+    h = C.c_void_p()
+    check(load().fx_synth_leaves(seed, n_clusters, min_size, max_size, nets_per_gate,
+                                 C.byref(h)), "fx_synth_leaves")
+    return _netlist_out(h)

@@ -1,0 +1,365 @@
+"""CPU oracle for the HAPR placement hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
+this module; the product never does.
+
+* liboracle.so  -- C++ restatement of the reference's Rust CPU path
+  (HAPR_fluxion_v4/src/...; see fx_oracle.cpp for the per-function citations)
+  plus the Barnes-Hut tree rules of neon_old_codebase/src/cpp/BarnesHutTree.cpp
+  restated on the Morton radix tree with FP64 accumulation.
+* _ref/libbh_ref.so -- the reference's own BarnesHutTree.cpp compiled from the
+  reference sources (Makefile target `ref`), when it was built.
+* DCT Poisson density in FP64: a restatement of ElectrostaticSmoothingForce
+  (neon_old_codebase/src/python/fluxion/force_electrostatic.py:47-150) on the
+  reference's own third-party dependency, scipy.fft (dctn/idctn, type 2,
+  norm='ortho'; scipy 1.18.1 in this image, unpinned by the reference).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libbh_ref.so"
+
+_lib = None
+_ref = None
+
+I32P = C.POINTER(C.c_int32)
+I64P = C.POINTER(C.c_int64)
+U32P = C.POINTER(C.c_uint32)
+F32P = C.POINTER(C.c_float)
+F64P = C.POINTER(C.c_double)
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        L.or_cell_at.restype = C.c_int64
+        L.or_cell_at.argtypes = [C.c_float, C.c_float, C.c_int64]
+        L.or_grid_geometry.argtypes = [C.c_float, C.c_float, C.c_int64, C.c_int64,
+                                       F32P, F32P, F32P]
+        L.or_congestion.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
+                                    C.c_float, C.c_int64, C.c_int64, F32P, F32P]
+        L.or_overflow.argtypes = [F32P, F32P, C.c_int64, C.c_int64, C.c_float, F32P, F32P]
+        L.or_hpwl_f32.restype = C.c_float
+        L.or_hpwl_f32.argtypes = [C.c_int32, I32P, I32P, F32P, F32P]
+        L.or_hpwl_f64.restype = C.c_double
+        L.or_hpwl_f64.argtypes = [C.c_int32, I32P, I32P, F32P, F32P]
+        L.or_build_adjacency.restype = C.c_int64
+        L.or_build_adjacency.argtypes = [C.c_int32, C.c_int32, I32P, I32P, I32P, I32P,
+                                         C.c_int64]
+        L.or_attraction_f32.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
+                                        F32P, F32P]
+        L.or_attraction_f64.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_double,
+                                        F64P, F64P]
+        L.or_integrate.argtypes = [C.c_int32, F32P, F32P, F32P, F32P, F32P, F32P,
+                                   C.c_float, C.c_float, C.c_float, C.c_float,
+                                   C.c_float, C.c_float]
+        L.or_place_leaf.argtypes = [C.c_int32, I32P, I32P, I32P, C.c_float, C.c_float,
+                                    C.c_float, C.c_float, C.c_int32, C.c_float,
+                                    C.c_float, C.c_float, C.c_float, F32P, F32P]
+        L.or_leaf_forces_f64.argtypes = [C.c_int32, I32P, I32P, I32P, F32P, F32P,
+                                         C.c_double, C.c_double, F64P, F64P]
+        L.or_build_hierarchy.restype = C.c_int32
+        L.or_build_hierarchy.argtypes = [C.c_int32, I32P, I32P, C.c_int32, C.c_int32,
+                                         C.c_float, C.c_int32, C.c_float, C.c_float,
+                                         I32P, I32P, F32P, I32P, I32P, I32P]
+        L.or_fiedler_vector.argtypes = [I32P, I32P, C.c_int32, I32P, C.c_int32, F32P]
+        L.or_bh_root.argtypes = [C.c_int32, F32P, F32P, F32P]
+        L.or_bh_keys.argtypes = [C.c_int32, F32P, F32P, F32P, U32P]
+        L.or_bh_forces.argtypes = [C.c_int32, F32P, F32P, C.c_double, C.c_float,
+                                   C.c_double, F64P, F64P, U32P, I32P, F32P, I64P,
+                                   C.c_int32]
+        L.or_repulsion_exact.argtypes = [C.c_int32, F32P, F32P, C.c_double, C.c_double,
+                                         F64P, F64P]
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's own BarnesHutTree.cpp, or None when it was not built."""
+    global _ref
+    if _ref is None and REF_LIB.exists():
+        R = C.CDLL(str(REF_LIB))
+        R.bh_ref_forces.argtypes = [C.c_int, F64P, F64P, F64P, C.c_double, C.c_double,
+                                    C.c_double, F64P, F64P, C.c_int]
+        _ref = R
+    return _ref
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, np.int32)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+# ---- grid / congestion / HPWL (grid.rs, congestion.rs, placement.rs) -------
+def cell_at(v: float, cell: float, n: int) -> int:
+    return int(lib().or_cell_at(v, cell, n))
+
+
+def grid_geometry(chip_w, chip_h, cols, rows):
+    cw, ch, cap = C.c_float(), C.c_float(), C.c_float()
+    lib().or_grid_geometry(chip_w, chip_h, cols, rows, C.byref(cw), C.byref(ch),
+                           C.byref(cap))
+    return cw.value, ch.value, cap.value
+
+
+def congestion(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows):
+    net_ptr, net_gate, x, y = _i32(net_ptr), _i32(net_gate), _f32(x), _f32(y)
+    h = np.empty(cols * rows, np.float32)
+    v = np.empty(cols * rows, np.float32)
+    lib().or_congestion(len(net_ptr) - 1, _p(net_ptr, C.c_int32), _p(net_gate, C.c_int32),
+                        _p(x, C.c_float), _p(y, C.c_float), chip_w, chip_h, cols, rows,
+                        _p(h, C.c_float), _p(v, C.c_float))
+    return h, v
+
+
+def overflow(h, v, cols, rows, capacity):
+    t, m = C.c_float(), C.c_float()
+    lib().or_overflow(_p(_f32(h), C.c_float), _p(_f32(v), C.c_float), cols, rows,
+                      capacity, C.byref(t), C.byref(m))
+    return t.value, m.value
+
+
+def hpwl_f32(net_ptr, net_gate, x, y) -> float:
+    net_ptr, net_gate, x, y = _i32(net_ptr), _i32(net_gate), _f32(x), _f32(y)
+    return float(lib().or_hpwl_f32(len(net_ptr) - 1, _p(net_ptr, C.c_int32),
+                                   _p(net_gate, C.c_int32), _p(x, C.c_float),
+                                   _p(y, C.c_float)))
+
+
+def hpwl_f64(net_ptr, net_gate, x, y) -> float:
+    net_ptr, net_gate, x, y = _i32(net_ptr), _i32(net_gate), _f32(x), _f32(y)
+    return float(lib().or_hpwl_f64(len(net_ptr) - 1, _p(net_ptr, C.c_int32),
+                                   _p(net_gate, C.c_int32), _p(x, C.c_float),
+                                   _p(y, C.c_float)))
+
+
+# ---- adjacency / attraction / integrate (circuit.rs, placer.rs) ------------
+def build_adjacency(n, net_ptr, net_gate):
+    net_ptr, net_gate = _i32(net_ptr), _i32(net_gate)
+    ap = np.zeros(n + 1, np.int32)
+    cap = 0
+    total = lib().or_build_adjacency(n, len(net_ptr) - 1, _p(net_ptr, C.c_int32),
+                                     _p(net_gate, C.c_int32), _p(ap, C.c_int32),
+                                     None, cap)
+    ai = np.zeros(max(total, 1), np.int32)
+    lib().or_build_adjacency(n, len(net_ptr) - 1, _p(net_ptr, C.c_int32),
+                             _p(net_gate, C.c_int32), _p(ap, C.c_int32),
+                             _p(ai, C.c_int32), total)
+    return ap, ai[:total]
+
+
+def attraction_f32(adj_ptr, adj_idx, x, y, k=1.0):
+    n = len(adj_ptr) - 1
+    fx, fy = np.empty(n, np.float32), np.empty(n, np.float32)
+    lib().or_attraction_f32(n, _p(_i32(adj_ptr), C.c_int32), _p(_i32(adj_idx), C.c_int32),
+                            _p(_f32(x), C.c_float), _p(_f32(y), C.c_float), k,
+                            _p(fx, C.c_float), _p(fy, C.c_float))
+    return fx, fy
+
+
+def attraction_f64(adj_ptr, adj_idx, x, y, k=1.0):
+    n = len(adj_ptr) - 1
+    fx, fy = np.empty(n), np.empty(n)
+    adj_ptr, adj_idx, x, y = _i32(adj_ptr), _i32(adj_idx), _f32(x), _f32(y)
+    lib().or_attraction_f64(n, _p(adj_ptr, C.c_int32), _p(adj_idx, C.c_int32),
+                            _p(x, C.c_float), _p(y, C.c_float), k,
+                            _p(fx, C.c_double), _p(fy, C.c_double))
+    return fx, fy
+
+
+def integrate(x, y, vx, vy, fx, fy, dt, damping, box):
+    """In place on float32 arrays (placer.rs:275-280)."""
+    n = len(x)
+    lib().or_integrate(n, _p(x, C.c_float), _p(y, C.c_float), _p(vx, C.c_float),
+                       _p(vy, C.c_float), _p(_f32(fx), C.c_float),
+                       _p(_f32(fy), C.c_float), dt, damping, *box)
+
+
+def place_leaf(gates, adj_ptr, adj_idx, region, iters, attract=1.0, repel=0.5,
+               damping=0.9, dt=0.1, out_x=None, out_y=None, n_total=None):
+    gates = _i32(gates)
+    n_total = n_total if n_total is not None else int(gates.max()) + 1
+    if out_x is None:
+        out_x = np.zeros(n_total, np.float32)
+        out_y = np.zeros(n_total, np.float32)
+    adj_ptr, adj_idx = _i32(adj_ptr), _i32(adj_idx)
+    lib().or_place_leaf(len(gates), _p(gates, C.c_int32), _p(adj_ptr, C.c_int32),
+                        _p(adj_idx, C.c_int32), *[float(r) for r in region], iters,
+                        attract, repel, damping, dt, _p(out_x, C.c_float),
+                        _p(out_y, C.c_float))
+    return out_x, out_y
+
+
+def leaf_forces_f64(gates, adj_ptr, adj_idx, px, py, attract=1.0, repel=0.5):
+    gates = _i32(gates)
+    n = len(gates)
+    fx, fy = np.empty(n), np.empty(n)
+    adj_ptr, adj_idx, px, py = _i32(adj_ptr), _i32(adj_idx), _f32(px), _f32(py)
+    lib().or_leaf_forces_f64(n, _p(gates, C.c_int32), _p(adj_ptr, C.c_int32),
+                             _p(adj_idx, C.c_int32), _p(px, C.c_float), _p(py, C.c_float),
+                             attract, repel, _p(fx, C.c_double), _p(fy, C.c_double))
+    return fx, fy
+
+
+# ---- hierarchy (partitioner.rs, placer.rs region pass) ---------------------
+def build_hierarchy(n, adj_ptr, adj_idx, chip_w, chip_h, max_leaf=64, min_cluster=8,
+                    balance=0.4, iters=30):
+    adj_ptr, adj_idx = _i32(adj_ptr), _i32(adj_idx)
+    cap_l = max(2 * n // max(1, min(max_leaf, min_cluster) // 2) + 2, 4)
+    lp = np.zeros(cap_l + 1, np.int32)
+    lg = np.zeros(n, np.int32)
+    rg = np.zeros(4 * cap_l, np.float32)
+    ld = np.zeros(cap_l, np.int32)
+    nodes, md = C.c_int32(), C.c_int32()
+    L = lib().or_build_hierarchy(n, _p(adj_ptr, C.c_int32), _p(adj_idx, C.c_int32),
+                                 max_leaf, min_cluster, balance, iters, chip_w, chip_h,
+                                 _p(lp, C.c_int32), _p(lg, C.c_int32), _p(rg, C.c_float),
+                                 _p(ld, C.c_int32), C.byref(nodes), C.byref(md))
+    return dict(leaf_ptr=lp[:L + 1], leaf_gate=lg, region=rg[:4 * L].reshape(L, 4),
+                leaf_depth=ld[:L], num_nodes=nodes.value, max_depth=md.value)
+
+
+def fiedler_vector(adj_ptr, adj_idx, gates, iters=30):
+    gates = _i32(gates)
+    out = np.empty(len(gates), np.float32)
+    lib().or_fiedler_vector(_p(_i32(adj_ptr), C.c_int32), _p(_i32(adj_idx), C.c_int32),
+                            len(gates), _p(gates, C.c_int32), iters, _p(out, C.c_float))
+    return out
+
+
+# ---- Barnes-Hut ------------------------------------------------------------
+def bh_root(x, y):
+    x, y = _f32(x), _f32(y)
+    r = np.empty(3, np.float32)
+    lib().or_bh_root(len(x), _p(x, C.c_float), _p(y, C.c_float), _p(r, C.c_float))
+    return r
+
+
+def bh_keys(x, y, root):
+    x, y, root = _f32(x), _f32(y), _f32(root)
+    k = np.empty(len(x), np.uint32)
+    lib().or_bh_keys(len(x), _p(x, C.c_float), _p(y, C.c_float), _p(root, C.c_float),
+                     _p(k, C.c_uint32))
+    return k
+
+
+def bh_forces(x, y, k=0.5, theta=0.5, min_dist=0.1, threads=1):
+    """FP64 forces with the device's tree and opening decisions.
+
+    min_dist enters the FP64 law as given; the opening decisions use its f32
+    rounding. Pass float(np.float32(v)) to reproduce a device run exactly.
+    """
+    x, y = _f32(x), _f32(y)
+    n = len(x)
+    fx, fy = np.empty(n), np.empty(n)
+    keys = np.empty(n, np.uint32)
+    perm = np.empty(n, np.int32)
+    root = np.empty(3, np.float32)
+    inter = np.empty(n, np.int64)
+    lib().or_bh_forces(n, _p(x, C.c_float), _p(y, C.c_float), k, theta, min_dist,
+                       _p(fx, C.c_double), _p(fy, C.c_double), _p(keys, C.c_uint32),
+                       _p(perm, C.c_int32), _p(root, C.c_float), _p(inter, C.c_int64),
+                       threads)
+    return dict(fx=fx, fy=fy, keys=keys, perm=perm, root=root, interactions=inter)
+
+
+def repulsion_exact(x, y, k=0.5, min_dist=0.1):
+    x, y = _f32(x), _f32(y)
+    n = len(x)
+    fx, fy = np.empty(n), np.empty(n)
+    lib().or_repulsion_exact(n, _p(x, C.c_float), _p(y, C.c_float), k, min_dist,
+                             _p(fx, C.c_double), _p(fy, C.c_double))
+    return fx, fy
+
+
+def bh_reference(x, y, k=0.5, theta=0.5, min_dist=0.1, threads=1):
+    """Forces from the reference's own BarnesHutTree.cpp (unit charges)."""
+    R = ref_lib()
+    if R is None:
+        return None
+    px = np.ascontiguousarray(x, np.float64)
+    py = np.ascontiguousarray(y, np.float64)
+    q = np.ones(len(px))
+    fx, fy = np.empty(len(px)), np.empty(len(px))
+    R.bh_ref_forces(len(px), _p(px, C.c_double), _p(py, C.c_double), _p(q, C.c_double),
+                    theta, k, min_dist, _p(fx, C.c_double), _p(fy, C.c_double), threads)
+    return fx, fy
+
+
+# ---- DCT Poisson density, FP64 (force_electrostatic.py) --------------------
+def density_bins(x, y, die_w, die_h, G):
+    """Point-in-bin (force_electrostatic.py:55-56) with the division in f32."""
+    bw = np.float32(die_w) / np.float32(G)
+    bh = np.float32(die_h) / np.float32(G)
+
+    def one(v, b):
+        q = _f32(v) / b
+        out = np.zeros(len(q), np.int64)
+        ok = q >= 1.0
+        out[ok] = np.minimum(np.floor(q[ok]).astype(np.int64), G - 1)
+        out[q >= np.float32(G - 1)] = G - 1
+        return out
+    return one(x, bw), one(y, bh), float(bw), float(bh)
+
+
+def density_map(x, y, area, die_w, die_h, G):
+    """rho[r, c] += area / (bw * bh) (force_electrostatic.py:47-60), FP64."""
+    col, row, bw, bh = density_bins(x, y, die_w, die_h, G)
+    rho = np.zeros((G, G))
+    np.add.at(rho, (row, col), np.asarray(area, np.float64) / (bw * bh))
+    return rho, col, row, bw, bh
+
+
+def solve_poisson(rho, wx, wy):
+    """_solve_poisson_fft (force_electrostatic.py:62-105) in FP64."""
+    from scipy.fft import dctn, idctn
+    rho_hat = dctn(rho, type=2, norm="ortho")
+    ny, nx = rho.shape
+    kx, ky = np.meshgrid(np.arange(nx), np.arange(ny))
+    eig = (wx * np.cos(np.pi * kx / nx) - wx) ** 2 + (wy * np.cos(np.pi * ky / ny) - wy) ** 2
+    eig[0, 0] = 1.0
+    phi_hat = -rho_hat / eig
+    phi_hat[0, 0] = 0.0
+    phi = idctn(phi_hat, type=2, norm="ortho")
+    ex = np.zeros_like(phi)
+    ey = np.zeros_like(phi)
+    ex[:, 1:-1] = -(phi[:, 2:] - phi[:, :-2]) * wx * 0.5
+    ey[1:-1, :] = -(phi[2:, :] - phi[:-2, :]) * wy * 0.5
+    ex[:, 0] = -(phi[:, 1] - phi[:, 0]) * wx
+    ex[:, -1] = -(phi[:, -1] - phi[:, -2]) * wx
+    ey[0, :] = -(phi[1, :] - phi[0, :]) * wy
+    ey[-1, :] = -(phi[-1, :] - phi[-2, :]) * wy
+    return phi, ex, ey
+
+
+def density_forces(x, y, area, die_w, die_h, G, target=0.7, weight=1.0):
+    """ElectrostaticSmoothingForce.calculate (force_electrostatic.py:107-157)."""
+    rho, col, row, bw, bh = density_map(x, y, area, die_w, die_h, G)
+    charge = rho - target
+    phi, ex, ey = solve_poisson(charge, 1.0 / bw, 1.0 / bh)
+    q = np.asarray(area, np.float64)
+    fx = q * ex[row, col] * weight
+    fy = q * ey[row, col] * weight
+    energy = float(np.sum(0.5 * q * phi[row, col]) * weight)
+    return dict(fx=fx, fy=fy, rho=charge, phi=phi, ex=ex, ey=ey, energy=energy)

@@ -1,0 +1,217 @@
+"""Parity of the CUDA hot path with the CPU oracle (runs on a B200).
+
+Bars: integer/index work bit-exact; forces within 1e-5 relative (global L2)
+of an FP64 recomputation on the same positions; final HPWL/overflow of a run
+within 0.5 % of the oracle's run.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+F32_01 = float(np.float32(0.1))  # the device's f32 min_dist, exactly
+
+
+def rel_l2(ax, ay, bx, by):
+    return float(np.sqrt(((ax - bx) ** 2 + (ay - by) ** 2).sum() /
+                         max((bx ** 2 + by ** 2).sum(), 1e-300)))
+
+
+@pytest.fixture(scope="module")
+def small_design(fx, ctx, plain_small):
+    d = fx.Design(ctx, plain_small.circuit)
+    d.set_positions(plain_small.placement.gate_x, plain_small.placement.gate_y)
+    yield d
+    d.close()
+
+
+# ---- rows D + F --------------------------------------------------------------
+@pytest.mark.parametrize("cols,rows", [(64, 64), (37, 53), (1, 1), (256, 256), (512, 7)])
+def test_congestion_bit_exact(small_design, plain_small, oracle, cols, rows):
+    c, p = plain_small.circuit, plain_small.placement
+    counts, hpwl, tot, mx = small_design.congestion(cols, rows)
+    h, v = oracle.congestion(c.net_ptr, c.net_gate, p.gate_x, p.gate_y,
+                             c.chip_width, c.chip_height, cols, rows)
+    assert np.array_equal(counts.astype(np.float32), h)
+    assert np.array_equal(h, v)
+    ref = oracle.hpwl_f64(c.net_ptr, c.net_gate, p.gate_x, p.gate_y)
+    assert abs(hpwl - ref) <= 1e-12 * ref
+    _, _, cap = oracle.grid_geometry(c.chip_width, c.chip_height, cols, rows)
+    rt, rm = oracle.overflow(h, v, cols, rows, cap)
+    assert mx == rm
+    assert abs(tot - rt) <= 1e-5 * max(rt, 1.0)
+    # the reference's own f32 running sum stays within 0.5 %
+    assert abs(hpwl - oracle.hpwl_f32(c.net_ptr, c.net_gate, p.gate_x, p.gate_y)) <= 5e-3 * ref
+
+
+def test_congestion_edge_cases(fx, ctx, oracle):
+    # empty and single-pin nets (skipped), a gate named twice, positions below
+    # zero / beyond the die / on cell boundaries / NaN, and a net whose every
+    # position is NaN (min > max: no cells).
+    nets = [[], [3], [0, 0], [1, 2, 3], [4, 5], [6, 7], [8, 9], [0, 9, 5], [10, 11]]
+    circ = fx.Circuit.from_nets(nets, 12, chip_width=100.0, chip_height=100.0)
+    x = np.array([10, -5, 250, 20, 30, 40, np.nan, 50, 1e30, 0.0, np.nan, np.nan], np.float32)
+    y = np.array([10, 50, 60, -1e30, 12.5, 25, 5, np.nan, 99.99, 100, np.nan, np.nan],
+                 np.float32)
+    d = fx.Design(ctx, circ)
+    try:
+        for cols, rows in ((8, 8), (10, 10), (3, 17)):
+            counts, hpwl, tot, mx = d.congestion(cols, rows, x, y)
+            h, v = oracle.congestion(circ.net_ptr, circ.net_gate, x, y, 100.0, 100.0,
+                                     cols, rows)
+            assert np.array_equal(counts.astype(np.float32), h)
+    finally:
+        d.close()
+
+
+def test_congestion_repeat_calls_are_identical(small_design):
+    a = small_design.congestion(64, 64)
+    b = small_design.congestion(64, 64)
+    assert np.array_equal(a[0], b[0]) and a[1:] == b[1:]
+
+
+def test_reference_api_build_and_compute(fx, plain_small, oracle):
+    c, p = plain_small.circuit, plain_small.placement
+    g = fx.build_and_compute(p, c, 64, 64)
+    h, _ = oracle.congestion(c.net_ptr, c.net_gate, p.gate_x, p.gate_y,
+                             c.chip_width, c.chip_height, 64, 64)
+    assert np.array_equal(g.h_congestion, h) and np.array_equal(g.v_congestion, h)
+
+
+# ---- row A ---------------------------------------------------------------------
+def test_adjacency_matches_reference(small_design, plain_small, oracle):
+    c = plain_small.circuit
+    ap, ai = small_design.adjacency()
+    rp, ri = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    assert np.array_equal(ap, rp)
+    for g in range(0, c.num_gates, 7):
+        assert sorted(ai[ap[g]:ap[g + 1]]) == sorted(ri[rp[g]:rp[g + 1]])
+
+
+def test_attraction_vs_fp64(small_design, plain_small, oracle):
+    p = plain_small.placement
+    ap, ai = small_design.adjacency()
+    fx_, fy_ = small_design.attraction(1.0)
+    rx, ry = oracle.attraction_f64(ap, ai, p.gate_x, p.gate_y, 1.0)
+    assert rel_l2(fx_, fy_, rx, ry) < 1e-5
+    sx, sy = oracle.attraction_f32(ap, ai, p.gate_x, p.gate_y, 1.0)
+    assert rel_l2(sx, sy, rx, ry) < 1e-5  # the reference's own f32 order
+
+
+# ---- row B ---------------------------------------------------------------------
+def _bh_check(d, x, y, oracle, k=0.5, theta=0.5):
+    d.set_positions(x, y)
+    bx, by, keys, perm, root = d.barnes_hut(k, theta, 0.1)
+    o = oracle.bh_forces(x, y, k, theta, F32_01)
+    assert np.array_equal(root, o["root"])
+    assert np.array_equal(keys, o["keys"])  # Morton keys bit-exact
+    assert np.array_equal(perm, o["perm"])  # stable sort order exact
+    assert rel_l2(bx, by, o["fx"], o["fy"]) < 1e-5
+    return bx, by
+
+
+def test_barnes_hut_config1(small_design, plain_small, oracle):
+    p = plain_small.placement
+    bx, by = _bh_check(small_design, p.gate_x, p.gate_y, oracle)
+    ref = oracle.bh_reference(p.gate_x, p.gate_y, 0.5, 0.5, 0.1)
+    if ref is not None:  # the reference's own tree, when built here
+        assert rel_l2(bx, by, *ref) < 5e-3
+
+
+@pytest.mark.parametrize("case", ["coincident", "pair", "line", "clumps", "tiny"])
+def test_barnes_hut_degenerate(fx, ctx, oracle, case):
+    rng = np.random.default_rng(3)
+    n = {"coincident": 300, "pair": 2, "line": 2000, "clumps": 5000, "tiny": 3}[case]
+    if case == "coincident":
+        x = np.full(n, 7.25, np.float32); y = np.full(n, 3.5, np.float32)
+    elif case == "pair":
+        x = np.array([1.0, 1.05], np.float32); y = np.array([2.0, 2.0], np.float32)
+    elif case == "line":
+        x = np.linspace(0, 50, n).astype(np.float32); y = np.full(n, 10.0, np.float32)
+    elif case == "clumps":
+        c = rng.integers(0, 20, n)
+        x = (c * 5.0 + rng.integers(0, 3, n) * 1e-3).astype(np.float32)
+        y = (c * 2.0).astype(np.float32)
+    else:
+        x = np.array([0.0, 1e-6, 2e-6], np.float32); y = np.zeros(3, np.float32)
+    circ = fx.Circuit.from_nets([[0, 1]] if n >= 2 else [], n, 100.0, 100.0)
+    d = fx.Design(ctx, circ)
+    try:
+        bx, by = _bh_check(d, x, y, oracle)
+        assert np.all(np.isfinite(bx)) and np.all(np.isfinite(by))
+    finally:
+        d.close()
+
+
+def test_barnes_hut_clustered_large(fx, ctx, oracle):
+    rng = np.random.default_rng(5)
+    n = 200_000
+    centers = rng.random((50, 2)) * 1000
+    pick = rng.integers(0, 50, n)
+    pts = (centers[pick] + rng.normal(0, 8.0, (n, 2))).astype(np.float32)
+    circ = fx.Circuit.from_nets([[0, 1]], n, 1200.0, 1200.0)
+    d = fx.Design(ctx, circ)
+    try:
+        _bh_check(d, pts[:, 0].copy(), pts[:, 1].copy(), oracle)
+    finally:
+        d.close()
+
+
+# ---- row C ---------------------------------------------------------------------
+@pytest.mark.parametrize("G", [128, 256])
+def test_density_simt_vs_fp64(fx, ctx, oracle, G):
+    s = fx.synth_plain(9, 20_000, 24_000, 170.0)
+    c, p = s.circuit, s.placement
+    d = fx.Design(ctx, c)
+    try:
+        d.set_positions(p.gate_x, p.gate_y)
+        out = d.density(G, 0.7, 1.0, fx.FX_DCT_SIMT, grids=True)
+        area = (c.gate_widths * c.gate_heights).astype(np.float64)
+        ref = oracle.density_forces(p.gate_x, p.gate_y, area, c.chip_width, c.chip_height,
+                                    G, 0.7, 1.0)
+        assert np.allclose(out["rho"], ref["rho"], rtol=0, atol=1e-5)
+        phi_err = np.linalg.norm(out["phi"] - ref["phi"]) / np.linalg.norm(ref["phi"])
+        assert phi_err < 1e-5, phi_err
+        e_err = rel_l2(out["ex"].ravel(), out["ey"].ravel(), ref["ex"].ravel(), ref["ey"].ravel())
+        assert e_err < 1e-3, e_err
+        assert rel_l2(out["fx"], out["fy"], ref["fx"], ref["fy"]) < 1e-3
+        assert abs(out["energy"] - ref["energy"]) <= 1e-3 * abs(ref["energy"])
+    finally:
+        d.close()
+
+
+# ---- rows A+B+E+D+F: the plain-small run ------------------------------------------
+def test_plain_small_run_matches_oracle(fx, ctx, plain_small, oracle):
+    """200 iterations of attraction (k=1) + Barnes-Hut (theta 0.5) + damped
+    step on the 10k-gate netlist, 64 x 64 congestion: final HPWL and overflow
+    within 0.5 % of the oracle's own run; congestion bit-exact on the final
+    device positions."""
+    c, p = plain_small.circuit, plain_small.placement
+    iters = 200
+    cfg = fx.iter_cfg(density_bins=0, cong_cols=64, cong_rows=64)
+    d = fx.Design(ctx, c)
+    try:
+        x = p.gate_x.copy(); y = p.gate_y.copy()
+        st = d.force_iterate(cfg, iters, x, y)
+        ap, ai = d.adjacency()
+        counts, hpwl, tot, _ = d.congestion(64, 64, x, y)
+    finally:
+        d.close()
+    assert st.hpwl == hpwl
+    h, _ = oracle.congestion(c.net_ptr, c.net_gate, x, y, c.chip_width, c.chip_height, 64, 64)
+    assert np.array_equal(counts.astype(np.float32), h)
+    # the oracle's own run
+    ox = p.gate_x.copy(); oy = p.gate_y.copy()
+    vx = np.zeros_like(ox); vy = np.zeros_like(oy)
+    for _ in range(iters):
+        fa_x, fa_y = oracle.attraction_f32(ap, ai, ox, oy, 1.0)
+        b = oracle.bh_forces(ox, oy, 0.5, 0.5, F32_01)
+        Fx = fa_x + b["fx"].astype(np.float32)
+        Fy = fa_y + b["fy"].astype(np.float32)
+        oracle.integrate(ox, oy, vx, vy, Fx, Fy, 0.1, 0.9, (0.0, 0.0, 120.0, 120.0))
+    ref_hpwl = oracle.hpwl_f64(c.net_ptr, c.net_gate, ox, oy)
+    assert abs(hpwl - ref_hpwl) <= 5e-3 * ref_hpwl, (hpwl, ref_hpwl)
+    oh, ov = oracle.congestion(c.net_ptr, c.net_gate, ox, oy, c.chip_width, c.chip_height, 64, 64)
+    _, _, cap = oracle.grid_geometry(c.chip_width, c.chip_height, 64, 64)
+    rt, _ = oracle.overflow(oh, ov, 64, 64, cap)
+    assert abs(tot - rt) <= 5e-3 * max(rt, 1.0), (tot, rt)
