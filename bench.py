@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark of the 1M-gate plain placement iteration on B200.
+
+One step = one plain composite iteration of the HAPR placement hot path on
+the 1,000,000-gate / 1,200,000-net synthetic netlist (die 1200 x 1200):
+net-spring attraction (k = 1) + Barnes-Hut repulsion (theta 0.5, k 0.5,
+min_dist 0.1) + DCT-II Poisson density force (1024 x 1024 grid, GEMM form) +
+damped Euler step + congestion counting (512 x 512) and FP64 HPWL.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fluxion|reference]
+
+Prints one JSON line (rank 0). With N > 1 (torchrun, one process per GPU)
+every rank runs an independent replica of the workload ("replicas only": the
+path does not shard), timing is the max over ranks and `value` is the sum of
+iterations over all ranks divided by that time.
+
+--impl reference times the reference's CPU implementation of the same
+iteration on this host's cores (the oracle port of the Rust path plus the
+reference's own BarnesHutTree.cpp and its scipy DCT) on a bounded sample of
+each stage; only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "neon-physics-fluxion_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "1M-gate force iterations/s"
+UNIT = "iterations/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fluxion", choices=["fluxion", "reference"])
+    ap.add_argument("--gates", type=int, default=1_000_000)
+    ap.add_argument("--nets", type=int, default=1_200_000)
+    ap.add_argument("--die", type=float, default=1200.0)
+    ap.add_argument("--bins", type=int, default=1024)
+    ap.add_argument("--cong", type=int, default=512)
+    ap.add_argument("--precision", default="simt", choices=["fp32", "tf32", "bf16", "simt"])
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "simt": 3}
+PREC_DTYPE = {"fp32": "f32 (DCT 3xTF32)", "tf32": "f32 (DCT TF32)",
+              "bf16": "f32 (DCT BF16)", "simt": "f32"}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(device)], stdout=self.tmp,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.tmp.flush()
+        rows = [l.split(",") for l in Path(self.tmp.name).read_text().splitlines() if l.strip()]
+        os.unlink(self.tmp.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [c.strip() for c in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def algorithmic(n, m, p, a, G, gc):
+    """Compulsory HBM bytes (each array read once, each output written once)
+    and flops per iteration, by stage."""
+    b = {
+        # adj_ptr, adj_idx, own x/y, v, BH force, area, E fields, new x/y, v,
+        # density accumulator update
+        "attract_integrate": 4 * (n + 1) + 4 * a + 8 * n + 8 * n + 8 * n + 4 * n
+        + 8 * G * G + 8 * n + 8 * n + 8 * G * G,
+        # keys+idx written, positions read
+        "bh_keys": 8 * n + 8 * n,
+        # 4 passes: read keys+idx, write keys+idx (histogram pass re-reads keys)
+        "bh_sort": 4 * (8 * n + 8 * n + 4 * n),
+        # gather sorted positions, prefix sums, nodes (child, range, com, meta)
+        "bh_tree": 4 * n + 8 * n + 8 * n + 16 * n + 4 * n + (n - 1) * (8 + 8 + 16 + 8 + 8),
+        # sorted positions, perm, nodes read once, force written
+        "bh_walk": 8 * n + 4 * n + (n - 1) * (8 + 8 + 16 + 8) + 8 * n,
+        # charge grid, 4 GEMM operands in+out, field
+        "density": 8 * G * G + 4 * G * G + 4 * (3 * 4 * G * G) + 4 * G * G + 8 * G * G,
+        # net_ptr, pins, positions, difference array RMW, counts
+        "congestion": 4 * (m + 1) + 4 * p + 8 * n + 2 * 4 * (gc + 1) ** 2 + 4 * gc * gc,
+    }
+    f = {"density": 4 * 2 * G ** 3}
+    return b, f
+
+
+# ---------------------------------------------------------------------------
+def cpu_iteration_sample(syn, x, y, bins, cong, threads, bh_stride, cong_stride):
+    """Seconds per plain iteration of the CPU path, from a bounded sample.
+
+    attraction (oracle restatement of placer.rs:243-255, full), Barnes-Hut
+    (the reference's BarnesHutTree.cpp: full build + every bh_stride-th
+    point's walk, scaled), DCT density (the reference's scipy dctn/idctn,
+    full), damped step (full), congestion (congestion.rs:11-62 on every
+    cong_stride-th net, scaled) and HPWL (full)."""
+    from oracle import oracle as orc
+    c = syn.circuit
+    ap, ai = syn.adj
+    area = (c.gate_widths * c.gate_heights).astype(np.float64)
+    t = {}
+    t0 = time.perf_counter()
+    fa = orc.attraction_f32(ap, ai, x, y, 1.0)
+    t["attraction"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.bh_reference(x, y, 0.5, 0.5, 0.1, threads, stride=len(x))
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bh = orc.bh_reference(x, y, 0.5, 0.5, 0.1, threads, stride=bh_stride)
+    t_samp = time.perf_counter() - t0
+    t["barnes_hut"] = t_build + max(t_samp - t_build, 0.0) * bh_stride
+    t0 = time.perf_counter()
+    dens = orc.density_forces(x, y, area, c.chip_width, c.chip_height, bins, 0.7, 1e-4)
+    t["density"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fx = (fa[0] + bh[0].astype(np.float32)) + dens["fx"].astype(np.float32)
+    fy = (fa[1] + bh[1].astype(np.float32)) + dens["fy"].astype(np.float32)
+    xx, yy = x.copy(), y.copy()
+    vx, vy = np.zeros_like(xx), np.zeros_like(yy)
+    orc.integrate(xx, yy, vx, vy, fx, fy, 0.1, 0.9, (0.0, 0.0, c.chip_width, c.chip_height))
+    t["integrate"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.congestion_sample(c.net_ptr, c.net_gate, xx, yy, c.chip_width, c.chip_height,
+                          cong, cong, cong_stride)
+    t["congestion"] = (time.perf_counter() - t0) * cong_stride
+    t0 = time.perf_counter()
+    orc.hpwl_f32(c.net_ptr, c.net_gate, xx, yy)
+    t["hpwl"] = time.perf_counter() - t0
+    return sum(t.values()), t
+
+
+class SynthCache:
+    def __init__(self, args):
+        import fluxion_b200 as fx
+        self.syn = fx.synth_plain(args.seed, args.gates, args.nets, args.die)
+        self.circuit = self.syn.circuit
+        self.placement = self.syn.placement
+        self.adj = None
+
+
+def run_reference(args, rank, world):
+    """CPU implementation of the same iteration (the reference arm)."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sc = SynthCache(args)
+    from oracle import oracle as orc
+    orc.build()
+    c = sc.circuit
+    sc.adj = orc.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    x, y = sc.placement.gate_x.copy(), sc.placement.gate_y.copy()
+    bh_stride, cong_stride = 16, 256
+    per = []
+    for i in range(args.warmup + args.steps):
+        s, parts = cpu_iteration_sample(sc, x, y, args.bins, args.cong, threads,
+                                        bh_stride, cong_stride)
+        if i >= args.warmup:
+            per.append(s)
+    sec = float(np.mean(per))
+    value = 1.0 / sec
+    sample = (f"one plain iteration per step on {args.gates} gates: attraction, integrate, "
+              f"HPWL and the scipy DCT density in full; Barnes-Hut with the reference "
+              f"BarnesHutTree.cpp (full build, walk of every {bh_stride}th point, scaled); "
+              f"congestion on every {cong_stride}th net (scaled); initial positions")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"plain-1M: {args.gates} gates, {args.nets} nets, die "
+                      f"{args.die:g}, BH theta 0.5, DCT {args.bins}^2, congestion "
+                      f"{args.cong}^2", "seed": args.seed},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                            "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0},
+           "stage_seconds": {k: round(v, 4) for k, v in parts.items()}}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_fluxion(args, rank, world, local_rank):
+    import fluxion_b200 as fx
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist = tdist
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sc = SynthCache(args)
+    c, p = sc.circuit, sc.placement
+    ctx = fx.Context(local_rank)
+    d = fx.Design(ctx, c)
+    cfg = fx.iter_cfg(density_bins=args.bins, dct_precision=PREC[args.precision],
+                      cong_cols=args.cong, cong_rows=args.cong)
+    # warm-up from the initial placement
+    d.set_positions(p.gate_x, p.gate_y)
+    d.force_iterate(cfg, args.warmup)
+    x0, y0 = d.get_positions()  # positions at the start of the timed region
+    d.set_positions(x0, y0)
+    ctx.synchronize()
+    launches0 = ctx.kernel_launches()
+    ctx.reset_stage_times()
+    ctx.set_profiling(True)
+    clocks = ClockSampler(local_rank)
+    barrier()
+    ctx.synchronize()
+    ctx.mark(0)
+    st = d.force_iterate(cfg, args.steps)
+    ctx.mark(1)
+    ctx.synchronize()
+    ms = ctx.elapsed_ms(0, 1)
+    barrier()
+    clk = clocks.stop()
+    ctx.set_profiling(False)
+    launches = ctx.kernel_launches() - launches0
+    stages = ctx.stage_times()
+    ms_max = max_over_ranks(ms)
+    value = world * args.steps / (ms_max / 1e3)
+
+    # end to end through the public call with host buffers: one
+    # fx_force_iterate call of `steps` iterations, positions copied in from
+    # pinned host memory and results read back inside the timed region.
+    e2e = None
+    if not args.no_e2e:
+        try:
+            import torch
+            hx = torch.from_numpy(x0.copy()).pin_memory()
+            hy = torch.from_numpy(y0.copy()).pin_memory()
+            ax, ay = hx.numpy(), hy.numpy()
+            ax[...] = x0
+            ay[...] = y0
+            pinned = True
+        except Exception:
+            ax, ay = x0.copy(), y0.copy()
+            pinned = False
+        ctx.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        d.force_iterate(cfg, args.steps, ax, ay)
+        e2e_s = time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s)
+        e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": 8 * c.num_gates / args.steps,
+               "d2h_bytes_per_step": (8 * c.num_gates + 48) / args.steps,
+               "call": f"fx_force_iterate(iters={args.steps}) with host x/y"
+                       f"{' (pinned)' if pinned else ''}"}
+
+    n, m, pn, a = d.n, d.m, d.p, d.a
+    G, gc = args.bins, args.cong
+    b_alg, f_alg = algorithmic(n, m, pn, a, G, gc)
+    per_iter = {k: stages[k][0] / max(stages[k][1], 1) for k in stages if stages[k][1]}
+    dom = max(per_iter, key=per_iter.get)
+    hbm, bf16, src = peaks()
+    if dom == "density" and args.precision != "simt":
+        ach = f_alg["density"] / (per_iter[dom] * 1e-3) / 1e12
+        peak = bf16 if args.precision == "bf16" else bf16 / 2
+        roof = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": ach / peak, "traffic": None, "kernel": dom,
+                "peak_source": f"{src} bf16 dense" + ("" if args.precision == "bf16"
+                                                      else " / 2 (tf32)")}
+    else:
+        ach = b_alg[dom] / (per_iter[dom] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": None, "kernel": dom,
+                "peak_source": f"{src} HBM copy"}
+    B_iter = sum(b_alg.values())
+    it_ms = ms_max / args.steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        orc.build()
+        sc.adj = d.adjacency()
+        sec, parts = cpu_iteration_sample(sc, x0, y0, G, gc, 1, 16, 256)
+        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "one plain iteration at the timed region's start positions on 1 core: "
+                         "attraction/integrate/HPWL (oracle restatement) and scipy DCT in "
+                         "full; reference BarnesHutTree.cpp walk of every 16th point and "
+                         "congestion of every 256th net, scaled",
+               "stage_seconds": {k: round(v, 4) for k, v in parts.items()}}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": it_ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": PREC_DTYPE[args.precision], "data": "synthetic",
+           "config": {"workload": f"plain-1M: {args.gates} gates, {args.nets} nets "
+                      f"({pn} pins, {a} adjacency entries), die {args.die:g}, BH theta 0.5, "
+                      f"DCT {G}^2 ({args.precision}), congestion {gc}^2",
+                      "seed": args.seed, "parallelism": "replicas" if world > 1 else "single",
+                      "l2": "working set per iteration ~%d MB > 126 MB L2" % (B_iter // 2**20)},
+           "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+           "clocks": clk,
+           "iteration_roofline": {"bytes": B_iter, "achieved_gbs": B_iter / (it_ms * 1e-3) / 1e9,
+                                  "frac_of_hbm": B_iter / (it_ms * 1e-3) / 1e9 / hbm},
+           "stage_ms_per_iter": {k: round(v, 4) for k, v in per_iter.items()},
+           "final_hpwl": st.hpwl}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    d.close()
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_fluxion(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -61,6 +61,13 @@ int fx_ctx_stage_times(fx_ctx *ctx, double *out_ms, int64_t *out_calls, int n);
 int fx_ctx_reset_stage_times(fx_ctx *ctx);
 /* Number of kernels this library has launched on the context. */
 int64_t fx_ctx_kernel_launches(fx_ctx *ctx);
+/* Device-side timing on the context's main stream: fx_ctx_mark records
+ * event `slot` (0..15); fx_ctx_elapsed waits for both and returns the
+ * milliseconds between two recorded slots. */
+int fx_ctx_mark(fx_ctx *ctx, int slot);
+int fx_ctx_elapsed(fx_ctx *ctx, int slot_a, int slot_b, float *out_ms);
+/* Waits until all work queued on the context has finished. */
+int fx_ctx_synchronize(fx_ctx *ctx);
 
 /* Stage identifiers for fx_ctx_stage_times. */
 #define FX_STAGE_ATTRACT_INTEGRATE 0 /* rows A+E fused                        */
@@ -168,9 +175,10 @@ int fx_force_iterate(fx_ctx *ctx, fx_design *design, const fx_iter_cfg *cfg,
 /* Row A: out_f = k * sum_{j in adj(i)} (p_j - p_i)  (placer.rs:243-255). */
 int fx_stage_attraction(fx_ctx *ctx, fx_design *design, float k,
                         float *out_fx, float *out_fy);
-/* Row B: Barnes-Hut repulsion. Also returns the Morton keys and the sorted
- * order (out_keys[N], out_perm[N], either may be NULL) and the root square
- * (out_root[3] = {x_min, y_min, size}, may be NULL). */
+/* Row B: Barnes-Hut repulsion. Also returns the Morton keys in gate order
+ * (out_keys[N]), the stable key order (out_perm[s] = gate at sorted
+ * position s) and the root square (out_root[3] = {x_min, y_min, size});
+ * any of the three may be NULL. */
 int fx_stage_barnes_hut(fx_ctx *ctx, fx_design *design, float k, float theta,
                         float min_dist, float *out_fx, float *out_fy,
                         uint32_t *out_keys, int32_t *out_perm,
@@ -183,6 +191,17 @@ int fx_stage_density(fx_ctx *ctx, fx_design *design, int32_t bins,
                      float *out_fx, float *out_fy, float *out_rho,
                      float *out_phi, float *out_ex, float *out_ey,
                      double *out_energy);
+
+/* ---- host-only helpers (no GPU needed) ---------------------------------- */
+/* Builds the deduplicated clique-expansion adjacency of
+ * Circuit::build_adjacency (H/src/data/circuit.rs:154-171) in the
+ * reference's insertion order: out_adj_ptr[N+1], out_adj_idx[A]. Returns A
+ * (the full count even when it exceeds cap; at most cap entries are
+ * written; out_adj_idx may be NULL to query A) or a negative FX_E* code. */
+int64_t fx_adjacency_build(int32_t n_gates, int32_t n_nets,
+                           const int32_t *net_ptr, const int32_t *net_gate,
+                           int32_t *out_adj_ptr, int32_t *out_adj_idx,
+                           int64_t cap);
 
 /* ---- synthetic netlists (host-only; no GPU needed) ---------------------- */
 typedef struct fx_netlist fx_netlist;

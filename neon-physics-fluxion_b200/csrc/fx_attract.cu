@@ -4,11 +4,13 @@
 //
 // Attraction follows place_gates_in_leaf (H/src/algorithm/placer.rs:243-255)
 // over the full deduplicated adjacency (circuit.rs:154-171):
-//   F_i = k * sum_{j in adj(i)} (p_j - p_i).
-// Eight lanes own one gate: they read its adjacency row with coalesced
-// loads, gather neighbour positions (L2-resident) and combine their partial
-// sums with a fixed shuffle tree, so no float atomics are involved and the
-// result does not depend on scheduling.
+//   F_i = sum_{j in adj(i)} k * (p_j - p_i),
+// added in adjacency order in f32 exactly as the reference does. A block owns
+// 256 consecutive gates; their adjacency rows form one contiguous CSR range,
+// which the block stages through shared memory with coalesced index loads and
+// neighbour-position gathers, then each thread walks its own row in order.
+// No float atomics are involved and the result is bit-identical to the
+// reference's sequential sum.
 // The step follows placer.rs:275-280 exactly (no contraction):
 //   v = (v + F*dt) * damping ; p = clamp(p + v*dt, lo, hi).
 #include "fx_internal.h"
@@ -21,46 +23,52 @@ int bh_bbox(fx_ctx *ctx, fx_design *d, const float *x, const float *y,
 int density_scatter(fx_ctx *ctx, fx_design *d, const float *x, const float *y,
                     int G, int precision, cudaStream_t s);
 
-constexpr int kLanes = 8;
-constexpr int kStepThreads = 256;
+constexpr int kGates = 256;   // gates (threads) per block
+constexpr int kChunk = 2048;  // adjacency entries staged per round
 
-template <int L>
-__device__ __forceinline__ float2 spring_sum(const int32_t *__restrict__ adj_ptr,
-                                             const int32_t *__restrict__ adj_idx,
-                                             const float *__restrict__ x,
-                                             const float *__restrict__ y,
-                                             int g, bool valid, int sub) {
-  float sx = 0.f, sy = 0.f;
-  if (valid) {
-    const float xi = x[g], yi = y[g];
-    const int b = __ldg(adj_ptr + g), e = __ldg(adj_ptr + g + 1);
-    for (int q = b + sub; q < e; q += L) {
+// Block-cooperative spring sum: every thread of the block must call it.
+__device__ __forceinline__ float2 spring_block(const int32_t *__restrict__ adj_ptr,
+                                               const int32_t *__restrict__ adj_idx,
+                                               const float *__restrict__ x,
+                                               const float *__restrict__ y,
+                                               int n, int g0, float k,
+                                               float xi, float yi) {
+  __shared__ float2 sh[kChunk];
+  const int t = threadIdx.x, g = g0 + t;
+  const bool valid = g < n;
+  const int gend = min(g0 + kGates, n);
+  const int A0 = __ldg(adj_ptr + g0), A1 = __ldg(adj_ptr + gend);
+  const int b = valid ? __ldg(adj_ptr + g) : 0;
+  const int e = valid ? __ldg(adj_ptr + g + 1) : 0;
+  float ax = 0.f, ay = 0.f;
+  for (int c0 = A0; c0 < A1; c0 += kChunk) {
+    const int c1 = min(c0 + kChunk, A1);
+    for (int q = c0 + t; q < c1; q += kGates) {
       const int j = __ldg(adj_idx + q);
-      sx += __fsub_rn(__ldg(x + j), xi);
-      sy += __fsub_rn(__ldg(y + j), yi);
+      sh[q - c0] = make_float2(__ldg(x + j), __ldg(y + j));
     }
+    __syncthreads();
+    const int lo = max(b, c0), hi = min(e, c1);
+    for (int q = lo; q < hi; ++q) {
+      const float2 pj = sh[q - c0];
+      ax = __fadd_rn(ax, __fmul_rn(k, __fsub_rn(pj.x, xi)));
+      ay = __fadd_rn(ay, __fmul_rn(k, __fsub_rn(pj.y, yi)));
+    }
+    __syncthreads();
   }
-#pragma unroll
-  for (int o = L / 2; o > 0; o >>= 1) {
-    sx += __shfl_xor_sync(0xffffffffu, sx, o, L);
-    sy += __shfl_xor_sync(0xffffffffu, sy, o, L);
-  }
-  return make_float2(sx, sy);
+  return make_float2(ax, ay);
 }
 
-__global__ void __launch_bounds__(kStepThreads)
+__global__ void __launch_bounds__(kGates)
 attract_kernel(const int32_t *__restrict__ adj_ptr,
                const int32_t *__restrict__ adj_idx, const float *__restrict__ x,
                const float *__restrict__ y, int n, float k,
                float2 *__restrict__ out) {
-  const int per_block = kStepThreads / kLanes;
-  const int sub = threadIdx.x % kLanes;
-  for (int base = blockIdx.x * per_block; base < n; base += gridDim.x * per_block) {
-    const int g = base + threadIdx.x / kLanes;
-    const bool valid = g < n;
-    const float2 s = spring_sum<kLanes>(adj_ptr, adj_idx, x, y, g, valid, sub);
-    if (valid && sub == 0) out[g] = make_float2(__fmul_rn(k, s.x), __fmul_rn(k, s.y));
-  }
+  const int g0 = blockIdx.x * kGates, g = g0 + threadIdx.x;
+  const bool valid = g < n;
+  const float xi = valid ? x[g] : 0.f, yi = valid ? y[g] : 0.f;
+  const float2 f = spring_block(adj_ptr, adj_idx, x, y, n, g0, k, xi, yi);
+  if (valid) out[g] = f;
 }
 
 struct StepArgs {
@@ -77,10 +85,11 @@ struct StepArgs {
   // integrate
   float dt, damp, xlo, ylo, xhi, yhi;
   // bookkeeping for the next iteration
-  unsigned int *bbox;
-  unsigned long long *dens_acc;
-  double *epart;
-  unsigned int *edone;
+  unsigned int *bbox;          // box of the new positions (ordered ints) or null
+  unsigned long long *dens_acc;  // density accumulator for the new positions
+  float4 *bbox_part;
+  double *e_part;
+  unsigned int *done;
   double *energy;
 };
 
@@ -98,82 +107,132 @@ __device__ __forceinline__ float clampf_ref(float v, float lo, float hi) {
   return v;
 }
 
-__global__ void __launch_bounds__(kStepThreads)
+// One gate per thread: F = attraction + Barnes-Hut + density (f32, in this
+// order), the damped step, then the new positions' density scatter and box.
+__global__ void __launch_bounds__(kGates)
 fused_step_kernel(StepArgs a) {
-  const int per_block = kStepThreads / kLanes;
-  const int sub = threadIdx.x % kLanes;
-  const int lane = threadIdx.x & 31;
+  const int g0 = blockIdx.x * kGates, g = g0 + threadIdx.x;
+  const bool valid = g < a.n;
+  const float px = valid ? a.x[g] : 0.f, py = valid ? a.y[g] : 0.f;
+  const float2 s = spring_block(a.adj_ptr, a.adj_idx, a.x, a.y, a.n, g0, a.k, px, py);
+  float nx = px, ny = py;
   double e_acc = 0.0;
-  for (int base = blockIdx.x * per_block; base < a.n; base += gridDim.x * per_block) {
-    const int g = base + threadIdx.x / kLanes;
-    const bool valid = g < a.n;
-    const float2 s = spring_sum<kLanes>(a.adj_ptr, a.adj_idx, a.x, a.y, g, valid, sub);
-    float nx = FLT_MAX, ny = FLT_MAX;
-    bool lead = valid && sub == 0;
-    if (lead) {
-      const float px = a.x[g], py = a.y[g];
-      float fx = __fmul_rn(a.k, s.x), fy = __fmul_rn(a.k, s.y);
-      if (a.fbh) {
-        const float2 b = a.fbh[g];
-        fx = __fadd_rn(fx, b.x);
-        fy = __fadd_rn(fy, b.y);
-      }
-      if (a.ex) {
-        const int c = bin_of(px, a.bw, a.G), r = bin_of(py, a.bh, a.G);
-        const size_t bi = (size_t)r * a.G + c;
-        const float q = a.area[g];
-        fx = __fadd_rn(fx, __fmul_rn(__fmul_rn(q, a.ex[bi]), a.dweight));
-        fy = __fadd_rn(fy, __fmul_rn(__fmul_rn(q, a.ey[bi]), a.dweight));
-        e_acc += 0.5 * (double)q * (double)a.phi[bi] * (double)a.dweight;
-      }
-      float vx = __fmul_rn(__fadd_rn(a.vx[g], __fmul_rn(fx, a.dt)), a.damp);
-      float vy = __fmul_rn(__fadd_rn(a.vy[g], __fmul_rn(fy, a.dt)), a.damp);
-      nx = clampf_ref(__fadd_rn(px, __fmul_rn(vx, a.dt)), a.xlo, a.xhi);
-      ny = clampf_ref(__fadd_rn(py, __fmul_rn(vy, a.dt)), a.ylo, a.yhi);
-      a.vx[g] = vx;
-      a.vy[g] = vy;
-      a.xn[g] = nx;
-      a.yn[g] = ny;
-      if (a.dens_acc) {
-        const int c = bin_of(nx, a.bw, a.G), r = bin_of(ny, a.bh, a.G);
-        atomicAdd(a.dens_acc + (size_t)r * a.G + c,
-                  (unsigned long long)llrint((double)a.area[g] * 4294967296.0));
-      }
+  long long dbin = -1;
+  unsigned long long dval = 0;
+  if (valid) {
+    float fx = s.x, fy = s.y;
+    if (a.fbh) {
+      const float2 b = a.fbh[g];
+      fx = __fadd_rn(fx, b.x);
+      fy = __fadd_rn(fy, b.y);
     }
-    if (a.bbox) {
-      float mnx = lead ? nx : FLT_MAX, mny = lead ? ny : FLT_MAX;
-      float mxx = lead ? nx : -FLT_MAX, mxy = lead ? ny : -FLT_MAX;
-#pragma unroll
-      for (int o = 16; o >= kLanes; o >>= 1) {
-        mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
-        mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
-        mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
-        mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
-      }
-      if (lane == 0) {
-        atomicMin(a.bbox + 0, f2ord(mnx));
-        atomicMin(a.bbox + 1, f2ord(mny));
-        atomicMax(a.bbox + 2, f2ord(mxx));
-        atomicMax(a.bbox + 3, f2ord(mxy));
-      }
+    if (a.ex) {
+      const int c = bin_of(px, a.bw, a.G), r = bin_of(py, a.bh, a.G);
+      const size_t bi = (size_t)r * a.G + c;
+      const float q = a.area[g];
+      fx = __fadd_rn(fx, __fmul_rn(__fmul_rn(q, a.ex[bi]), a.dweight));
+      fy = __fadd_rn(fy, __fmul_rn(__fmul_rn(q, a.ey[bi]), a.dweight));
+      e_acc = 0.5 * (double)q * (double)a.phi[bi] * (double)a.dweight;
+    }
+    const float vx = __fmul_rn(__fadd_rn(a.vx[g], __fmul_rn(fx, a.dt)), a.damp);
+    const float vy = __fmul_rn(__fadd_rn(a.vy[g], __fmul_rn(fy, a.dt)), a.damp);
+    nx = clampf_ref(__fadd_rn(px, __fmul_rn(vx, a.dt)), a.xlo, a.xhi);
+    ny = clampf_ref(__fadd_rn(py, __fmul_rn(vy, a.dt)), a.ylo, a.yhi);
+    a.vx[g] = vx;
+    a.vy[g] = vy;
+    a.xn[g] = nx;
+    a.yn[g] = ny;
+    if (a.dens_acc) {
+      const int c = bin_of(nx, a.bw, a.G), r = bin_of(ny, a.bh, a.G);
+      dbin = (long long)r * a.G + c;
+      dval = (unsigned long long)llrint((double)a.area[g] * 4294967296.0);
     }
   }
-  if (a.energy) last_block_sum(block_sum_double(e_acc), a.epart, a.edone, a.energy);
+  if (a.dens_acc) agg_add_u64(a.dens_acc, dbin, dval);
+  // Box of the new positions and density energy: per-block values, then the
+  // last block combines them in block order.
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float mnx = valid ? nx : FLT_MAX, mny = valid ? ny : FLT_MAX;
+  float mxx = valid ? nx : -FLT_MAX, mxy = valid ? ny : -FLT_MAX;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+  }
+  __shared__ float4 wbox[kGates / 32];
+  if (lane == 0) wbox[w] = make_float4(mnx, mny, mxx, mxy);
+  const double esum = block_sum_double(e_acc);  // contains __syncthreads
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    float4 bb = wbox[0];
+    for (int q = 1; q < kGates / 32; ++q) {
+      bb.x = fminf(bb.x, wbox[q].x);
+      bb.y = fminf(bb.y, wbox[q].y);
+      bb.z = fmaxf(bb.z, wbox[q].z);
+      bb.w = fmaxf(bb.w, wbox[q].w);
+    }
+    a.bbox_part[blockIdx.x] = bb;
+    a.e_part[blockIdx.x] = esum;
+    __threadfence();
+    last = atomicAdd(a.done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  float4 bb = make_float4(FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX);
+  double et = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += kGates) {
+    const float4 q = __ldcg(a.bbox_part + i);
+    bb.x = fminf(bb.x, q.x);
+    bb.y = fminf(bb.y, q.y);
+    bb.z = fmaxf(bb.z, q.z);
+    bb.w = fmaxf(bb.w, q.w);
+    et += __ldcg(a.e_part + i);
+  }
+  et = block_sum_double(et);
+  bb.x = -block_max_float(-bb.x);
+  bb.y = -block_max_float(-bb.y);
+  bb.z = block_max_float(bb.z);
+  bb.w = block_max_float(bb.w);
+  if (threadIdx.x == 0) {
+    if (a.bbox) {
+      a.bbox[0] = f2ord(bb.x);
+      a.bbox[1] = f2ord(bb.y);
+      a.bbox[2] = f2ord(bb.z);
+      a.bbox[3] = f2ord(bb.w);
+    }
+    if (a.energy) *a.energy = et;
+    *a.done = 0u;
+  }
 }
 
 int attraction_run(fx_ctx *ctx, fx_design *d, float k, float2 *out,
                    cudaStream_t s) {
-  int nb = (d->n + (kStepThreads / kLanes) - 1) / (kStepThreads / kLanes);
-  if (nb > ctx->num_sms * 16) nb = ctx->num_sms * 16;
-  attract_kernel<<<nb, kStepThreads, 0, s>>>(d->adj_ptr.p, d->adj_idx.p,
-                                             d->x[d->cur].p, d->y[d->cur].p,
-                                             d->n, k, out);
+  const int nb = (d->n + kGates - 1) / kGates;
+  attract_kernel<<<nb, kGates, 0, s>>>(d->adj_ptr.p, d->adj_idx.p,
+                                       d->x[d->cur].p, d->y[d->cur].p, d->n, k,
+                                       out);
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   return FX_OK;
 }
 
-static int validate_cfg(const fx_design *d, const fx_iter_cfg &c) {
+static int step_alloc(fx_design *d, cudaStream_t s) {
+  StepWork &w = d->step;
+  const size_t nb = ((size_t)d->n + kGates - 1) / kGates;
+  if (w.bbox_part.p && w.bbox_part.n >= nb) return FX_OK;
+  FX_TRY(w.bbox_part.alloc(nb));
+  FX_TRY(w.e_part.alloc(nb));
+  FX_TRY(w.done.alloc(4));
+  FX_TRY(w.energy.alloc(4));
+  FX_CHECK_CUDA(cudaMemsetAsync(w.done.p, 0, 16, s));
+  FX_CHECK_CUDA(cudaMemsetAsync(w.energy.p, 0, 32, s));
+  return FX_OK;
+}
+
+static int validate_cfg(const fx_iter_cfg &c) {
   if (!(c.dt > 0.f) || !(c.damping >= 0.f) || !(c.min_dist > 0.f) ||
       !(c.theta >= 0.f) || c.density_bins < 0 || c.cong_cols < 0 ||
       c.cong_rows < 0 || (c.cong_cols == 0) != (c.cong_rows == 0)) {
@@ -188,7 +247,6 @@ static int validate_cfg(const fx_design *d, const fx_iter_cfg &c) {
     set_error("fx_iter_cfg: unknown dct_precision %d", c.dct_precision);
     return FX_EINVAL;
   }
-  (void)d;
   return FX_OK;
 }
 
@@ -243,22 +301,22 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     return FX_EINVAL;
   }
   const fx_iter_cfg c = *cfg;
-  FX_TRY(validate_cfg(d, c));
+  FX_TRY(validate_cfg(c));
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream, s2 = ctx->stream2;
   if (x) FX_TRY(fx_design_set_positions(d, x, y));
+  FX_TRY(step_alloc(d, s));
   const bool use_bh = c.repel_weight != 0.f;
   const bool use_dens = c.density_bins > 0 && c.density_weight != 0.f;
   const bool use_cong = c.cong_cols > 0;
   const int G = c.density_bins;
   // Bounding box / density of the starting positions; each step then
   // prepares both for the positions it writes.
-  if (use_bh) {
-    FX_TRY(bh_bbox(ctx, d, d->x[d->cur].p, d->y[d->cur].p, s));
-    FX_CHECK_CUDA(cudaMemsetAsync(d->bh.bbox.p + 4, 0, 4, s));
-  }
-  if (use_dens) FX_TRY(density_scatter(ctx, d, d->x[d->cur].p, d->y[d->cur].p, G,
-                                       c.dct_precision, s));
+  if (use_bh) FX_TRY(bh_bbox(ctx, d, d->x[d->cur].p, d->y[d->cur].p, s));
+  if (use_dens)
+    FX_TRY(density_scatter(ctx, d, d->x[d->cur].p, d->y[d->cur].p, G,
+                           c.dct_precision, s));
+  const int nb = (d->n + kGates - 1) / kGates;
   for (int it = 0; it < iters; ++it) {
     if (use_dens) {
       FX_CHECK_CUDA(cudaEventRecord(ctx->fork, s));
@@ -292,9 +350,6 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
       a.bh = d->chip_h / (float)G;
       a.dweight = c.density_weight;
       a.dens_acc = d->dens.area_fx.p;
-      a.epart = d->dens.energy.p;
-      a.edone = (unsigned int *)(d->dens.energy.p + 4096);
-      a.energy = d->dens.energy.p + 4098;
     }
     a.dt = c.dt;
     a.damp = c.damping;
@@ -303,11 +358,13 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     a.xhi = d->chip_w;
     a.yhi = d->chip_h;
     a.bbox = use_bh ? d->bh.bbox.p : nullptr;
+    a.bbox_part = d->step.bbox_part.p;
+    a.e_part = d->step.e_part.p;
+    a.done = d->step.done.p;
+    a.energy = d->step.energy.p;
     cudaEvent_t ev;
     timer_begin(ctx, FX_STAGE_ATTRACT_INTEGRATE, s, &ev);
-    int nb = (d->n + (kStepThreads / kLanes) - 1) / (kStepThreads / kLanes);
-    if (nb > ctx->num_sms * 16) nb = ctx->num_sms * 16;
-    fused_step_kernel<<<nb, kStepThreads, 0, s>>>(a);
+    fused_step_kernel<<<nb, kGates, 0, s>>>(a);
     FX_CHECK_LAUNCH();
     ctx->launches += 1;
     timer_end(ctx, FX_STAGE_ATTRACT_INTEGRATE, s, ev);
@@ -318,30 +375,27 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   }
   fx_iter_stats st{};
   st.iterations = iters;
+  double res[2] = {0, 0};
+  unsigned int err = 0;
   if (use_cong && iters > 0) {
-    double res[2];
     FX_CHECK_CUDA(cudaMemcpyAsync(res, d->cong.result.p, 16, cudaMemcpyDeviceToHost, s));
     FX_CHECK_CUDA(cudaMemcpyAsync(&st.max_overflow, d->cong.result_max.p, 4,
                                   cudaMemcpyDeviceToHost, s));
-    FX_CHECK_CUDA(cudaStreamSynchronize(s));
-    st.hpwl = res[0];
-    st.total_overflow = res[1];
   }
   if (use_dens && iters > 0)
-    FX_CHECK_CUDA(cudaMemcpyAsync(&st.density_energy, d->dens.energy.p + 4098, 8,
+    FX_CHECK_CUDA(cudaMemcpyAsync(&st.density_energy, d->step.energy.p, 8,
                                   cudaMemcpyDeviceToHost, s));
-  if (use_bh && iters > 0) {
-    unsigned int err = 0;
+  if (use_bh && iters > 0)
     FX_CHECK_CUDA(cudaMemcpyAsync(&err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
-    FX_CHECK_CUDA(cudaStreamSynchronize(s));
-    if (err) {
-      set_error("Barnes-Hut walk stack overflow");
-      return FX_EINVAL;
-    }
-    st.bh_nodes = d->n - 1;
-  }
-  if (x) FX_TRY(fx_design_get_positions(d, x, y));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (err) {
+    set_error("Barnes-Hut walk stack overflow");
+    return FX_EINVAL;
+  }
+  st.hpwl = res[0];
+  st.total_overflow = res[1];
+  st.bh_nodes = use_bh ? d->n - 1 : 0;
+  if (x) FX_TRY(fx_design_get_positions(d, x, y));
   if (stats) *stats = st;
   return FX_OK;
 }

@@ -21,6 +21,16 @@
 // the same level) are always opened. Points that share all 30 key bits form
 // a bucket (a cell of level 15): it is accepted as a whole by the same rule,
 // otherwise each of its points interacts directly.
+//
+// Every value is fixed by the sorted keys alone: node mass sums are added in
+// tree order (left + right, FP64) by a bottom-up sweep, decisions and forces
+// use IEEE f32 operations without contraction (sqrt and reciprocal correctly
+// rounded), and each point adds its terms in depth-first order (left child
+// first). The result is bit-identical run to run and to a sequential
+// restatement of the same rules.
+#include <algorithm>
+#include <climits>
+
 #include "fx_internal.h"
 #include "fx_device.cuh"
 
@@ -29,7 +39,6 @@ namespace fx {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys
-constexpr int kScanBlock = 1024;                        // prefix-sum block
 constexpr int kWalkWarps = 8;
 constexpr int kStack = 64;
 
@@ -46,6 +55,8 @@ __global__ void bh_bbox_kernel(const float *__restrict__ x,
     mny = fminf(mny, py);
     mxy = fmaxf(mxy, py);
   }
+  __shared__ float red[4][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
@@ -53,7 +64,20 @@ __global__ void bh_bbox_kernel(const float *__restrict__ x,
     mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
     mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
   }
-  if ((threadIdx.x & 31) == 0) {
+  if (lane == 0) {
+    red[0][w] = mnx;
+    red[1][w] = mny;
+    red[2][w] = mxx;
+    red[3][w] = mxy;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+      mnx = fminf(mnx, red[0][q]);
+      mny = fminf(mny, red[1][q]);
+      mxx = fmaxf(mxx, red[2][q]);
+      mxy = fmaxf(mxy, red[3][q]);
+    }
     atomicMin(bbox + 0, f2ord(mnx));
     atomicMin(bbox + 1, f2ord(mny));
     atomicMax(bbox + 2, f2ord(mxx));
@@ -133,55 +157,67 @@ radix_hist_kernel(const uint32_t *__restrict__ keys, int n, int shift,
   tile_hist[(size_t)threadIdx.x * T + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of the digit-major tile histogram (single block).
-__global__ void __launch_bounds__(1024)
+// Per-digit exclusive scan of the digit-major tile histogram: block d scans
+// the T tile counts of digit d and records the digit's total.
+__global__ void __launch_bounds__(256)
 radix_scan_kernel(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-                  int count) {
-  __shared__ uint32_t ws[32];
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const int per = (count + 1023) / 1024;
-  const int b = t * per, e = min(count, b + per);
+                  uint32_t *__restrict__ digit_total, int T) {
+  __shared__ uint32_t ws[8];
+  const int d = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const uint32_t *row = in + (size_t)d * T;
+  uint32_t *orow = out + (size_t)d * T;
+  const int per = (T + 255) / 256;
+  const int b = min(T, t * per), e = min(T, b + per);
   uint32_t s = 0;
-  for (int i = b; i < e; ++i) s += in[i];
+  for (int i = b; i < e; ++i) s += row[i];
   uint32_t v = s;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+    const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
     if (lane >= o) v += u;
   }
   if (lane == 31) ws[w] = v;
   __syncthreads();
-  if (w == 0) {
-    uint32_t u = ws[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t q = __shfl_up_sync(0xffffffffu, u, o);
-      if (lane >= o) u += q;
-    }
-    ws[lane] = u;
-  }
-  __syncthreads();
-  uint32_t run = v - s + (w > 0 ? ws[w - 1] : 0u);
+  uint32_t run = v - s;
+  for (int q = 0; q < w; ++q) run += ws[q];
   for (int i = b; i < e; ++i) {
-    const uint32_t c = in[i];
-    out[i] = run;
+    const uint32_t c = row[i];
+    orow[i] = run;
     run += c;
   }
+  if (t == 255) digit_total[d] = run;
 }
 
 // Stable scatter: within a tile, warp w ranks its 256 keys in order
-// (__match_any_sync groups lanes with equal digits), then warps are ordered
-// by a per-digit prefix over the warp counts.
+// (__match_any_sync groups lanes with equal digits), warps are ordered by a
+// per-digit prefix over the warp counts, tiles by the per-digit scan and
+// digits by the scan of the digit totals.
 __global__ void __launch_bounds__(kSortThreads)
 radix_scatter_kernel(const uint32_t *__restrict__ kin,
                      const int32_t *__restrict__ iin,
                      uint32_t *__restrict__ kout, int32_t *__restrict__ iout,
                      int n, int shift, const uint32_t *__restrict__ tile_scan,
-                     int T) {
+                     const uint32_t *__restrict__ digit_total, int T) {
   constexpr int kWarps = kSortThreads / 32;
   __shared__ uint32_t cnt[kWarps][256];
+  __shared__ uint32_t doff[256];
+  __shared__ uint32_t ws[kWarps];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   for (int i = t; i < kWarps * 256; i += kSortThreads) (&cnt[0][0])[i] = 0;
+  {
+    const uint32_t s = digit_total[t];
+    uint32_t v = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
+    }
+    if (lane == 31) ws[w] = v;
+    __syncthreads();
+    uint32_t off = v - s;
+    for (int q = 0; q < w; ++q) off += ws[q];
+    doff[t] = off;
+  }
   __syncthreads();
   const int base = blockIdx.x * kSortTile + w * (32 * kSortItems);
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -204,7 +240,7 @@ radix_scatter_kernel(const uint32_t *__restrict__ kin,
     rank[r] = old + __popc(peers & lt_mask);
   }
   __syncthreads();
-  if (t < 256) {
+  {
     uint32_t run = 0;
 #pragma unroll
     for (int ww = 0; ww < kWarps; ++ww) {
@@ -219,110 +255,23 @@ radix_scatter_kernel(const uint32_t *__restrict__ kin,
     const int i = base + r * 32 + lane;
     if (i < n) {
       const uint32_t dg = (k[r] >> shift) & 255u;
-      const uint32_t pos =
-          tile_scan[(size_t)dg * T + blockIdx.x] + cnt[w][dg] + rank[r];
+      const uint32_t pos = doff[dg] + tile_scan[(size_t)dg * T + blockIdx.x] +
+                           cnt[w][dg] + rank[r];
       kout[pos] = k[r];
       iout[pos] = v[r];
     }
   }
 }
 
-// ---- sorted positions and FP64 prefix sums -------------------------------------
-__global__ void __launch_bounds__(256)
-bh_gather_kernel(const float *__restrict__ x, const float *__restrict__ y,
-                 const int32_t *__restrict__ perm, int n,
-                 float2 *__restrict__ spos, double2 *__restrict__ bsum) {
-  const int base = blockIdx.x * kScanBlock;
-  double sx = 0.0, sy = 0.0;
-  for (int i = base + threadIdx.x; i < min(n, base + kScanBlock); i += 256) {
+// ---- sorted positions --------------------------------------------------------------
+__global__ void bh_gather_kernel(const float *__restrict__ x,
+                                 const float *__restrict__ y,
+                                 const int32_t *__restrict__ perm, int n,
+                                 float2 *__restrict__ spos) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
     const int g = perm[i];
-    const float2 p = make_float2(x[g], y[g]);
-    spos[i] = p;
-    sx += (double)p.x;
-    sy += (double)p.y;
-  }
-  sx = block_sum_double(sx);
-  sy = block_sum_double(sy);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = make_double2(sx, sy);
-}
-
-// Exclusive scan of the block sums (single block, sequential per thread).
-__global__ void __launch_bounds__(1024)
-bh_bsum_scan_kernel(double2 *__restrict__ bsum, int nb) {
-  __shared__ double2 part[1024];
-  const int t = threadIdx.x;
-  const int per = (nb + 1023) / 1024;
-  const int b = t * per, e = min(nb, b + per);
-  double sx = 0.0, sy = 0.0;
-  for (int i = b; i < e; ++i) {
-    sx += bsum[i].x;
-    sy += bsum[i].y;
-  }
-  part[t] = make_double2(sx, sy);
-  __syncthreads();
-  if (t == 0) {
-    double ax = 0.0, ay = 0.0;
-    for (int i = 0; i < 1024; ++i) {
-      const double2 q = part[i];
-      part[i] = make_double2(ax, ay);
-      ax += q.x;
-      ay += q.y;
-    }
-  }
-  __syncthreads();
-  double ax = part[t].x, ay = part[t].y;
-  for (int i = b; i < e; ++i) {
-    const double2 q = bsum[i];
-    bsum[i] = make_double2(ax, ay);
-    ax += q.x;
-    ay += q.y;
-  }
-}
-
-// Inclusive prefix of the sorted positions within each block plus the block
-// offset. Sequential per thread over 4 consecutive items, then a warp/block
-// scan of the thread totals.
-__global__ void __launch_bounds__(256)
-bh_prefix_kernel(const float2 *__restrict__ spos, int n,
-                 const double2 *__restrict__ bsum,
-                 double2 *__restrict__ prefix) {
-  __shared__ double2 ws[8];
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const int base = blockIdx.x * kScanBlock + t * 4;
-  double px[4], py[4];
-  double sx = 0.0, sy = 0.0;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int i = base + j;
-    const float2 p = i < n ? spos[i] : make_float2(0.f, 0.f);
-    sx += (double)p.x;
-    sy += (double)p.y;
-    px[j] = sx;
-    py[j] = sy;
-  }
-  double vx = sx, vy = sy;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const double ux = __shfl_up_sync(0xffffffffu, vx, o);
-    const double uy = __shfl_up_sync(0xffffffffu, vy, o);
-    if (lane >= o) {
-      vx += ux;
-      vy += uy;
-    }
-  }
-  if (lane == 31) ws[w] = make_double2(vx, vy);
-  __syncthreads();
-  double ox = bsum[blockIdx.x].x, oy = bsum[blockIdx.x].y;
-  for (int q = 0; q < w; ++q) {
-    ox += ws[q].x;
-    oy += ws[q].y;
-  }
-  ox += vx - sx;
-  oy += vy - sy;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int i = base + j;
-    if (i < n) prefix[i] = make_double2(ox + px[j], oy + py[j]);
+    spos[i] = make_float2(x[g], y[g]);
   }
 }
 
@@ -338,8 +287,8 @@ __device__ __forceinline__ int bh_delta(const uint32_t *__restrict__ keys,
 __global__ void bh_tree_kernel(const uint32_t *__restrict__ keys, int n,
                                int32_t *__restrict__ child,
                                int32_t *__restrict__ range,
-                               int32_t *__restrict__ delta_node,
-                               int32_t *__restrict__ delta_parent) {
+                               int32_t *__restrict__ dnode,
+                               int32_t *__restrict__ dparent) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   const int dr = bh_delta(keys, n, i, i + 1), dl = bh_delta(keys, n, i, i - 1);
@@ -366,78 +315,208 @@ __global__ void bh_tree_kernel(const uint32_t *__restrict__ keys, int n,
   child[2 * i + 1] = right;
   range[2 * i] = lo;
   range[2 * i + 1] = hi;
-  delta_node[i] = dn;
-  if (left >= 0) delta_parent[left] = dn;
-  if (right >= 0) delta_parent[right] = dn;
-  if (i == 0) delta_parent[0] = -1;
+  dnode[i] = dn;
+  if (left >= 0) dparent[left] = dn;
+  if (right >= 0) dparent[right] = dn;
+  if (i == 0) dparent[0] = -1;
 }
 
-// Centre of mass (FP64 prefix difference, stored as an f32 hi/lo pair) and
-// the node's opening size: meta = {count, size^2}; size^2 < 0 marks a node
-// that stands for no quad level (always opened); count < 0 marks a bucket.
-__global__ void bh_finalize_kernel(int n, const int32_t *__restrict__ range,
-                                   const int32_t *__restrict__ delta_node,
-                                   const int32_t *__restrict__ delta_parent,
-                                   const double2 *__restrict__ prefix,
-                                   const float *__restrict__ root,
-                                   float4 *__restrict__ com,
-                                   float2 *__restrict__ meta) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n - 1) return;
-  const int first = range[2 * i], last = range[2 * i + 1];
-  const int cnt = last - first + 1;
-  double2 hi2 = prefix[last];
-  if (first > 0) {
-    const double2 lo2 = prefix[first - 1];
-    hi2.x -= lo2.x;
-    hi2.y -= lo2.y;
-  }
-  const double cx = hi2.x / (double)cnt, cy = hi2.y / (double)cnt;
-  const float hx = (float)cx, hy = (float)cy;
-  com[i] = make_float4(hx, hy, (float)(cx - (double)hx), (float)(cy - (double)hy));
-  const int dn = delta_node[i], dp = delta_parent[i];
-  const float rs = root[2];
-  float2 m;
-  if (dn >= 30) {
-    const float s = ldexpf(rs, -15);
-    m = make_float2(-(float)cnt, __fmul_rn(s, s));
-  } else {
-    const int lmax = dn >> 1;
-    if (dp >= 0 && (dp >> 1) == lmax) {
-      m = make_float2((float)cnt, -1.0f);
+// ---- FP64 prefix sums of the sorted positions, fixed association ------------
+// Chunks of kScanChunk consecutive values are added sequentially by one
+// thread each (left to right, starting from 0.0); chunk totals form the next
+// level, until one chunk remains. Exclusive offsets then flow back down:
+// a chunk's running sum starts from its offset at the level above. The
+// association depends only on n, so a sequential restatement reproduces
+// every bit. Node sums are prefix differences.
+constexpr int kScanChunk = 128;
+
+__global__ void scan_up_kernel(const float2 *__restrict__ pts,
+                               const double2 *__restrict__ in, int len,
+                               double2 *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = c * kScanChunk;
+  if (b >= len) return;
+  const int e = min(len, b + kScanChunk);
+  double sx = 0.0, sy = 0.0;
+  for (int i = b; i < e; ++i) {
+    if (pts) {
+      const float2 p = pts[i];
+      sx = sx + (double)p.x;
+      sy = sy + (double)p.y;
     } else {
-      const float s = ldexpf(rs, -lmax);
-      m = make_float2((float)cnt, __fmul_rn(s, s));
+      const double2 v = in[i];
+      sx = sx + v.x;
+      sy = sy + v.y;
     }
   }
-  meta[i] = m;
+  out[c] = make_double2(sx, sy);
+}
+
+// Exclusive running sums of one level: chunk c starts from `up[c]` (or 0.0
+// at the top, where the whole level is one chunk).
+__global__ void scan_down_kernel(const double2 *__restrict__ v, int len,
+                                 const double2 *__restrict__ up,
+                                 double2 *__restrict__ x) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = c * kScanChunk;
+  if (b >= len) return;
+  const int e = min(len, b + kScanChunk);
+  double sx = up ? up[c].x : 0.0, sy = up ? up[c].y : 0.0;
+  for (int i = b; i < e; ++i) {
+    x[i] = make_double2(sx, sy);
+    sx = sx + v[i].x;
+    sy = sy + v[i].y;
+  }
+}
+
+// Inclusive prefix of the points: chunk c starts from off[c] (or 0.0).
+__global__ void scan_final_kernel(const float2 *__restrict__ pts, int n,
+                                  const double2 *__restrict__ off,
+                                  double2 *__restrict__ prefix) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = c * kScanChunk;
+  if (b >= n) return;
+  const int e = min(n, b + kScanChunk);
+  double sx = off ? off[c].x : 0.0, sy = off ? off[c].y : 0.0;
+  for (int i = b; i < e; ++i) {
+    const float2 p = pts[i];
+    sx = sx + (double)p.x;
+    sy = sy + (double)p.y;
+    prefix[i] = make_double2(sx, sy);
+  }
+}
+
+// Walk record of every internal node (two float4):
+//   r0 = {cx_hi, cy_hi, cx_lo, cy_lo}  centre of mass as an f32 hi/lo pair
+//   r1 = {count (negative: bucket), size^2 (negative: no quad level),
+//         first, last (as int bits)}
+__global__ void bh_node_kernel(int n, const int32_t *__restrict__ range,
+                               const int32_t *__restrict__ dnode,
+                               const int32_t *__restrict__ dparent,
+                               const double2 *__restrict__ prefix,
+                               const float *__restrict__ root,
+                               float4 *__restrict__ node) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int f = range[2 * i], l = range[2 * i + 1];
+  const int cnt = l - f + 1;
+  double sx = prefix[l].x, sy = prefix[l].y;
+  if (f > 0) {
+    sx = sx - prefix[f - 1].x;
+    sy = sy - prefix[f - 1].y;
+  }
+  const double cx = sx / (double)cnt, cy = sy / (double)cnt;
+  const float hx = (float)cx, hy = (float)cy;
+  node[2 * i] = make_float4(hx, hy, (float)(cx - (double)hx), (float)(cy - (double)hy));
+  const int dn = dnode[i], dp = dparent[i];
+  const float rs = root[2];
+  float c, s2;
+  if (dn >= 30) {
+    const float sz = ldexpf(rs, -15);
+    c = -(float)cnt;
+    s2 = __fmul_rn(sz, sz);
+  } else {
+    const int lmax = dn >> 1;
+    c = (float)cnt;
+    if (dp >= 0 && (dp >> 1) == lmax) {
+      s2 = -1.0f;
+    } else {
+      const float sz = ldexpf(rs, -lmax);
+      s2 = __fmul_rn(sz, sz);
+    }
+  }
+  node[2 * i + 1] = make_float4(c, s2, __int_as_float(f), __int_as_float(l));
+}
+
+// Quad children: a node that stands for no quad level (at most one such level
+// separates two quad cells) is replaced by its own two children, so every
+// node lists up to four children, in key order. kNone marks empty slots.
+constexpr int kNone = INT_MIN;
+
+__global__ void bh_qchild_kernel(int n, const int32_t *__restrict__ child,
+                                 const int32_t *__restrict__ dnode,
+                                 int4 *__restrict__ qchild) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int out[4] = {kNone, kNone, kNone, kNone};
+  int k = 0;
+  const int lv = dnode[i] >> 1;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int c = child[2 * i + h];
+    if (c >= 0 && dnode[c] < 30 && (dnode[c] >> 1) == lv) {
+      out[k++] = child[2 * c];
+      out[k++] = child[2 * c + 1];
+    } else {
+      out[k++] = c;
+    }
+  }
+  qchild[i] = make_int4(out[0], out[1], out[2], out[3]);
 }
 
 // ---- warp-cooperative walk ----------------------------------------------------
-// Each warp owns 32 consecutive sorted points (spatially close). It walks the
-// tree once with a shared stack of (node, lane mask): every lane applies the
-// reference opening rule to its own point, lanes that accept a node take its
-// centre-of-mass term, and the children are pushed only for the lanes that
-// opened it. Interaction lists are therefore exactly per point.
+// Each warp owns 32 consecutive sorted points (spatially close) and walks the
+// quadtree with a shared stack of (node, lane mask) entries, each an opened
+// cell. Popping a cell evaluates all its children for the lanes in the mask:
+// every lane applies the reference opening rule to its own point, so
+// interaction lists are exactly per point. A lane adds, per opened cell, the
+// terms of its children in order (single points, accepted cells, opened
+// buckets point by point), and then descends into the children it opened, in
+// order.
+
+// The law k*Q/d^2 along (dx, dy)/d with d = max(|r|, min_dist), in IEEE f32:
+// inv = 1/sqrt(max(r2, md^2)), f = ((kQ * inv) * inv) * inv, F += f * r.
+__device__ __forceinline__ void bh_term(float dx, float dy, float r2c, float kq,
+                                        float &fx, float &fy) {
+  const float inv = __frcp_rn(__fsqrt_rn(r2c));
+  const float f = __fmul_rn(__fmul_rn(__fmul_rn(kq, inv), inv), inv);
+  fx = __fadd_rn(fx, __fmul_rn(f, dx));
+  fy = __fadd_rn(fy, __fmul_rn(f, dy));
+}
+
 __device__ __forceinline__ void bh_direct(float px, float py, float2 q,
                                           float kq, float md2, float &fx,
                                           float &fy) {
   const float dx = __fsub_rn(px, q.x), dy = __fsub_rn(py, q.y);
   const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-  const float inv = rsqrtf(fmaxf(r2, md2));
-  const float f = kq * inv * inv * inv;
-  fx += f * dx;
-  fy += f * dy;
+  bh_term(dx, dy, fmaxf(r2, md2), kq, fx, fy);
+}
+
+// Applies the opening rule of internal node c for the lanes in `mask`; adds
+// the accepted and bucket terms and returns the lanes that open c as a cell
+// to descend into (0 for a bucket, whose points were handled here).
+__device__ __forceinline__ unsigned bh_eval(int c, unsigned mask, int lane,
+                                            int s, float2 p, float k,
+                                            float th2, float md2,
+                                            const float4 *__restrict__ node,
+                                            const float2 *__restrict__ spos,
+                                            float &fx, float &fy) {
+  const float4 r0 = node[2 * c], r1 = node[2 * c + 1];
+  const bool in = (mask >> lane) & 1u;
+  const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
+  const float dy = __fsub_rn(__fsub_rn(p.y, r0.y), r0.w);
+  const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float r2c = fmaxf(r2, md2);
+  // size^2 < 0 (a node standing for no quad level) is always opened
+  const bool accept = in && r1.y >= 0.f && (r1.y < __fmul_rn(th2, r2c));
+  if (accept) bh_term(dx, dy, r2c, __fmul_rn(k, fabsf(r1.x)), fx, fy);
+  const unsigned open = __ballot_sync(0xffffffffu, in && !accept);
+  if (open == 0u || r1.x > 0.f) return open;
+  const bool mine = (open >> lane) & 1u;  // bucket: point by point
+  const int b = __float_as_int(r1.z), e = __float_as_int(r1.w);
+  for (int t = b; t <= e; ++t) {
+    const float2 q = spos[t];
+    if (mine && t != s) bh_direct(p.x, p.y, q, k, md2, fx, fy);
+  }
+  return 0u;
 }
 
 __global__ void __launch_bounds__(kWalkWarps * 32)
 bh_walk_kernel(int n, const float2 *__restrict__ spos,
                const int32_t *__restrict__ perm,
-               const int32_t *__restrict__ child,
-               const int32_t *__restrict__ range,
-               const float4 *__restrict__ com, const float2 *__restrict__ meta,
-               float k, float th2, float md2, float2 *__restrict__ force,
-               unsigned int *__restrict__ err) {
+               const int4 *__restrict__ qchild,
+               const float4 *__restrict__ node, float k, float th2, float md2,
+               float2 *__restrict__ force, unsigned int *__restrict__ err) {
   __shared__ int32_t st_node[kWalkWarps][kStack];
   __shared__ unsigned st_mask[kWalkWarps][kStack];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -449,88 +528,99 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
   float fx = 0.f, fy = 0.f;
   int sp = 0;
   if (n >= 2) {
-    if (lane == 0) {
-      st_node[w][0] = 0;
-      st_mask[w][0] = active;
+    const unsigned open = bh_eval(0, active, lane, s, p, k, th2, md2, node, spos, fx, fy);
+    if (open) {
+      if (lane == 0) {
+        st_node[w][0] = 0;
+        st_mask[w][0] = open;
+      }
+      sp = 1;
     }
-    sp = 1;
   }
   __syncwarp();
   while (sp > 0) {
     --sp;
-    const int node = st_node[w][sp];
+    const int nd = st_node[w][sp];
     const unsigned mask = st_mask[w][sp];
     __syncwarp();
-    const bool in = (mask >> lane) & 1u;
-    if (node < 0) {  // single point
-      const int t = ~node;
-      if (in && t != s) bh_direct(p.x, p.y, spos[t], k, md2, fx, fy);
-      continue;
-    }
-    const float2 m = meta[node];
-    unsigned open;
-    if (m.y < 0.f) {
-      open = mask;
-    } else {
-      const float4 c = com[node];
-      const float dx = __fsub_rn(__fsub_rn(p.x, c.x), c.z);
-      const float dy = __fsub_rn(__fsub_rn(p.y, c.y), c.w);
-      const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-      const float r2c = fmaxf(r2, md2);
-      const bool accept = in && (m.y < __fmul_rn(th2, r2c));
-      if (accept) {
-        const float inv = rsqrtf(r2c);
-        const float f = k * fabsf(m.x) * inv * inv * inv;
-        fx += f * dx;
-        fy += f * dy;
-      }
-      open = __ballot_sync(0xffffffffu, in && !accept);
-      if (open == 0) continue;
-      if (m.x < 0.f) {  // bucket: direct terms for the lanes that opened it
-        const bool mine = (open >> lane) & 1u;
-        const int b = range[2 * node], e = range[2 * node + 1];
-        for (int t = b; t <= e; ++t) {
-          const float2 q = spos[t];
-          if (mine && t != s) bh_direct(p.x, p.y, q, k, md2, fx, fy);
-        }
+    const int4 q = qchild[nd];
+    const int qc[4] = {q.x, q.y, q.z, q.w};
+    unsigned om[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const int c = qc[h];
+      if (c == kNone) continue;
+      if (c < 0) {  // single point
+        const int t = ~c;
+        if (((mask >> lane) & 1u) && t != s)
+          bh_direct(p.x, p.y, spos[t], k, md2, fx, fy);
         continue;
       }
+      om[h] = bh_eval(c, mask, lane, s, p, k, th2, md2, node, spos, fx, fy);
     }
-    if (sp + 2 > kStack) {
+    const int np = (om[0] != 0u) + (om[1] != 0u) + (om[2] != 0u) + (om[3] != 0u);
+    if (sp + np > kStack) {
       if (lane == 0) atomicOr(err, 1u);
       continue;
     }
-    if (lane == 0) {
-      st_node[w][sp] = child[2 * node + 1];
-      st_mask[w][sp] = open;
-      st_node[w][sp + 1] = child[2 * node];
-      st_mask[w][sp + 1] = open;
+    // push the opened children in reverse so the first one is popped first
+#pragma unroll
+    for (int h = 3; h >= 0; --h) {
+      if (om[h] != 0u) {
+        if (lane == 0) {
+          st_node[w][sp] = qc[h];
+          st_mask[w][sp] = om[h];
+        }
+        ++sp;
+      }
     }
-    sp += 2;
     __syncwarp();
   }
   if (valid) force[perm[s]] = make_float2(fx, fy);
 }
 
+// Lengths of the chunked-scan levels above the points: L[0] = chunks of the
+// points, L[1] = chunks of L[0], ... until a level fits one chunk.
+static int scan_levels(int n, int *len) {
+  int k = 0, m = n;
+  while (m > kScanChunk && k < 5) {
+    m = (m + kScanChunk - 1) / kScanChunk;
+    len[k++] = m;
+  }
+  return k;
+}
+
 static int bh_alloc(fx_design *d) {
   BHWork &b = d->bh;
   const int n = d->n;
-  if (b.n == n && b.com.p) return FX_OK;
+  if (b.n == n && b.node.p) return FX_OK;
   const int T = (n + kSortTile - 1) / kSortTile;
-  const int NB = (n + kScanBlock - 1) / kScanBlock;
   const size_t ni = n > 1 ? (size_t)n - 1 : 1;
   for (int i = 0; i < 2; ++i) {
     FX_TRY(b.keys[i].alloc(n));
     FX_TRY(b.idx[i].alloc(n));
   }
   FX_TRY(b.tile_hist.alloc((size_t)256 * T));
-  FX_TRY(b.tile_scan.alloc((size_t)256 * T + (size_t)2 * NB * 2));
+  FX_TRY(b.tile_scan.alloc((size_t)256 * T));
+  FX_TRY(b.digit_total.alloc(256));
   FX_TRY(b.spos.alloc(n));
-  FX_TRY(b.prefix.alloc(n));
-  FX_TRY(b.child.alloc(2 * ni + 2 * ni + 2 * ni + 4));  // child, delta_node, delta_parent
+  FX_TRY(b.child.alloc(2 * ni));
   FX_TRY(b.range.alloc(2 * ni));
-  FX_TRY(b.com.alloc(ni));
-  FX_TRY(b.meta.alloc(ni));
+  FX_TRY(b.dnode.alloc(ni));
+  FX_TRY(b.dparent.alloc(ni));
+  FX_TRY(b.qchild.alloc(ni));
+  int len[5];
+  const int K = scan_levels(n, len);
+  if (K > 3) {
+    set_error("Barnes-Hut: %d points exceed the prefix-scan capacity", n);
+    return FX_EINVAL;
+  }
+  for (int l = 0; l < K; ++l) {
+    FX_TRY(b.scan[2 * l].alloc(len[l]));      // chunk totals of level l
+    FX_TRY(b.scan[2 * l + 1].alloc(len[l]));  // exclusive offsets of level l
+  }
+  FX_TRY(b.prefix.alloc(n));
+  FX_TRY(b.node.alloc(2 * ni));
   FX_TRY(b.root.alloc(4));
   FX_TRY(b.bbox.alloc(8));
   FX_TRY(b.force.alloc(n));
@@ -542,8 +632,8 @@ static int bh_alloc(fx_design *d) {
 int bh_bbox(fx_ctx *ctx, fx_design *d, const float *x, const float *y,
             cudaStream_t s) {
   FX_TRY(bh_alloc(d));
-  const unsigned int init[4] = {0xffffffffu, 0xffffffffu, 0u, 0u};
-  FX_CHECK_CUDA(cudaMemcpyAsync(d->bh.bbox.p, init, 16, cudaMemcpyHostToDevice, s));
+  const unsigned int init[5] = {0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  FX_CHECK_CUDA(cudaMemcpyAsync(d->bh.bbox.p, init, 20, cudaMemcpyHostToDevice, s));
   int nb = (d->n + 255) / 256;
   if (nb > ctx->num_sms * 8) nb = ctx->num_sms * 8;
   bh_bbox_kernel<<<nb, 256, 0, s>>>(x, y, d->n, d->bh.bbox.p);
@@ -561,9 +651,6 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
   const int n = d->n;
   const float *x = d->x[d->cur].p, *y = d->y[d->cur].p;
   const int T = (n + kSortTile - 1) / kSortTile;
-  const int NB = (n + kScanBlock - 1) / kScanBlock;
-  int32_t *delta_node = b.child.p + 2 * (size_t)(n > 1 ? n - 1 : 1);
-  int32_t *delta_parent = delta_node + (n > 1 ? n - 1 : 1);
   unsigned int *err = b.bbox.p + 4;
   cudaEvent_t ev;
   const int gb = (n + 255) / 256;
@@ -578,36 +665,54 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
     const int src = pass & 1, dst = src ^ 1;
     radix_hist_kernel<<<T, kSortThreads, 0, s>>>(b.keys[src].p, n, 8 * pass,
                                                  b.tile_hist.p, T);
-    radix_scan_kernel<<<1, 1024, 0, s>>>(b.tile_hist.p, b.tile_scan.p, 256 * T);
+    radix_scan_kernel<<<256, 256, 0, s>>>(b.tile_hist.p, b.tile_scan.p,
+                                          b.digit_total.p, T);
     radix_scatter_kernel<<<T, kSortThreads, 0, s>>>(
         b.keys[src].p, b.idx[src].p, b.keys[dst].p, b.idx[dst].p, n, 8 * pass,
-        b.tile_scan.p, T);
+        b.tile_scan.p, b.digit_total.p, T);
   }
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_SORT, s, ev);
   timer_begin(ctx, FX_STAGE_BH_TREE, s, &ev);
-  double2 *bsum = (double2 *)(b.tile_scan.p + (size_t)256 * T);
-  bh_gather_kernel<<<NB, 256, 0, s>>>(x, y, b.idx[0].p, n, b.spos.p, bsum);
-  bh_bsum_scan_kernel<<<1, 1024, 0, s>>>(bsum, NB);
-  bh_prefix_kernel<<<NB, 256, 0, s>>>(b.spos.p, n, bsum, b.prefix.p);
+  bh_gather_kernel<<<gb, 256, 0, s>>>(x, y, b.idx[0].p, n, b.spos.p);
+  int launches = 1;
   if (n >= 2) {
     const int tb = (n - 1 + 255) / 256;
     bh_tree_kernel<<<tb, 256, 0, s>>>(b.keys[0].p, n, b.child.p, b.range.p,
-                                      delta_node, delta_parent);
-    bh_finalize_kernel<<<tb, 256, 0, s>>>(n, b.range.p, delta_node,
-                                          delta_parent, b.prefix.p, b.root.p,
-                                          b.com.p, b.meta.p);
+                                      b.dnode.p, b.dparent.p);
+    // chunked prefix scan: up, top, down, final
+    int len[5];
+    const int K = scan_levels(n, len);
+    auto blocks = [](int chunks) { return (chunks + 127) / 128; };
+    for (int l = 0; l < K; ++l) {
+      const int in_len = l == 0 ? n : len[l - 1];
+      scan_up_kernel<<<blocks(len[l]), 128, 0, s>>>(
+          l == 0 ? b.spos.p : nullptr, l == 0 ? nullptr : b.scan[2 * (l - 1)].p,
+          in_len, b.scan[2 * l].p);
+    }
+    for (int l = K - 1; l >= 0; --l) {
+      // offsets of level l's values (the chunk totals of level l - 1)
+      const double2 *up = l == K - 1 ? nullptr : b.scan[2 * (l + 1) + 1].p;
+      scan_down_kernel<<<blocks((len[l] + kScanChunk - 1) / kScanChunk), 128, 0, s>>>(
+          b.scan[2 * l].p, len[l], up, b.scan[2 * l + 1].p);
+    }
+    scan_final_kernel<<<blocks(len[0] > 0 && K > 0 ? len[0] : 1), 128, 0, s>>>(
+        b.spos.p, n, K > 0 ? b.scan[1].p : nullptr, b.prefix.p);
+    bh_node_kernel<<<tb, 256, 0, s>>>(n, b.range.p, b.dnode.p, b.dparent.p,
+                                      b.prefix.p, b.root.p, b.node.p);
+    bh_qchild_kernel<<<tb, 256, 0, s>>>(n, b.child.p, b.dnode.p, b.qchild.p);
+    launches += 4 + 2 * K + 1;
   }
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_TREE, s, ev);
   timer_begin(ctx, FX_STAGE_BH_WALK, s, &ev);
   const int wb = (n + kWalkWarps * 32 - 1) / (kWalkWarps * 32);
   bh_walk_kernel<<<wb, kWalkWarps * 32, 0, s>>>(
-      n, b.spos.p, b.idx[0].p, b.child.p, b.range.p, b.com.p, b.meta.p, k,
-      theta * theta, min_dist * min_dist, b.force.p, err);
+      n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, theta * theta,
+      min_dist * min_dist, b.force.p, err);
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_WALK, s, ev);
-  ctx->launches += 2 + 12 + 3 + (n >= 2 ? 2 : 0) + 1;
+  ctx->launches += 2 + 12 + launches + 1;
   return FX_OK;
 }
 
@@ -626,16 +731,15 @@ extern "C" int fx_stage_barnes_hut(fx_ctx *ctx, fx_design *d, float k,
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
   FX_TRY(bh_bbox(ctx, d, d->x[d->cur].p, d->y[d->cur].p, s));
-  FX_CHECK_CUDA(cudaMemsetAsync(d->bh.bbox.p + 4, 0, 4, s));
   FX_TRY(bh_run(ctx, d, k, theta, min_dist, s));
   const size_t n = (size_t)d->n;
   std::vector<float2> f(n);
+  std::vector<uint32_t> skeys(n);
+  std::vector<int32_t> perm(n);
   unsigned int err = 0;
   FX_CHECK_CUDA(cudaMemcpyAsync(f.data(), d->bh.force.p, n * 8, cudaMemcpyDeviceToHost, s));
-  if (out_keys)
-    FX_CHECK_CUDA(cudaMemcpyAsync(out_keys, d->bh.keys[0].p, n * 4, cudaMemcpyDeviceToHost, s));
-  if (out_perm)
-    FX_CHECK_CUDA(cudaMemcpyAsync(out_perm, d->bh.idx[0].p, n * 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(skeys.data(), d->bh.keys[0].p, n * 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(perm.data(), d->bh.idx[0].p, n * 4, cudaMemcpyDeviceToHost, s));
   if (out_root)
     FX_CHECK_CUDA(cudaMemcpyAsync(out_root, d->bh.root.p, 12, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaMemcpyAsync(&err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
@@ -648,5 +752,9 @@ extern "C" int fx_stage_barnes_hut(fx_ctx *ctx, fx_design *d, float k,
     if (out_fx) out_fx[i] = f[i].x;
     if (out_fy) out_fy[i] = f[i].y;
   }
+  // keys in gate order; perm maps sorted position -> gate
+  if (out_keys)
+    for (size_t i = 0; i < n; ++i) out_keys[perm[i]] = skeys[i];
+  if (out_perm) std::copy(perm.begin(), perm.end(), out_perm);
   return FX_OK;
 }

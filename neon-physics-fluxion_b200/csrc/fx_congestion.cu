@@ -15,8 +15,10 @@ constexpr int kNetThreads = 256;
 constexpr int kMaxNetBlocks = 148 * 16;
 
 // One thread per net: f32 bounding box with Rust's NaN-ignoring min/max,
-// cell_at on both corners, four corner increments of the difference array,
-// and the net's HPWL term in FP64.
+// cell_at on both corners, four corner increments of the difference array
+// (warp-aggregated: lanes hitting the same element add once), and the net's
+// HPWL term in FP64. Warps step through the nets together so every lane
+// takes part in the aggregation.
 __global__ void __launch_bounds__(kNetThreads)
 cong_nets_kernel(const int32_t *__restrict__ net_ptr,
                  const int32_t *__restrict__ net_gate,
@@ -25,30 +27,42 @@ cong_nets_kernel(const int32_t *__restrict__ net_ptr,
                  int32_t *__restrict__ diff, double *__restrict__ partial,
                  unsigned int *__restrict__ done, double *__restrict__ result) {
   double acc = 0.0;
-  const int ld = cols + 1;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < M;
-       e += gridDim.x * blockDim.x) {
-    const int b = __ldg(net_ptr + e), t = __ldg(net_ptr + e + 1);
-    if (t - b < 2) continue;
-    float mnx = FLT_MAX, mxx = -FLT_MAX, mny = FLT_MAX, mxy = -FLT_MAX;
-    for (int q = b; q < t; ++q) {
-      const int g = __ldg(net_gate + q);
-      const float px = __ldg(x + g), py = __ldg(y + g);
-      mnx = fminf(mnx, px);
-      mxx = fmaxf(mxx, px);
-      mny = fminf(mny, py);
-      mxy = fmaxf(mxy, py);
+  const long long ld = cols + 1;
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int w0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); w0 < M; w0 += stride) {
+    const int e = w0 + lane;
+    int b = 0, t = 0;
+    if (e < M) {
+      b = __ldg(net_ptr + e);
+      t = __ldg(net_ptr + e + 1);
     }
-    acc += ((double)mxx - (double)mnx) + ((double)mxy - (double)mny);
-    if (diff) {
+    long long i00 = -1, i01 = -1, i10 = -1, i11 = -1;
+    if (t - b >= 2) {
+      float mnx = FLT_MAX, mxx = -FLT_MAX, mny = FLT_MAX, mxy = -FLT_MAX;
+      for (int q = b; q < t; ++q) {
+        const int g = __ldg(net_gate + q);
+        const float px = __ldg(x + g), py = __ldg(y + g);
+        mnx = fminf(mnx, px);
+        mxx = fmaxf(mxx, px);
+        mny = fminf(mny, py);
+        mxy = fmaxf(mxy, py);
+      }
+      acc += ((double)mxx - (double)mnx) + ((double)mxy - (double)mny);
       const int c0 = cell_at(mnx, cw, cols), c1 = cell_at(mxx, cw, cols);
       const int r0 = cell_at(mny, ch, rows), r1 = cell_at(mxy, ch, rows);
       if (c0 <= c1 && r0 <= r1) {
-        atomicAdd(diff + (size_t)r0 * ld + c0, 1);
-        atomicAdd(diff + (size_t)r0 * ld + c1 + 1, -1);
-        atomicAdd(diff + (size_t)(r1 + 1) * ld + c0, -1);
-        atomicAdd(diff + (size_t)(r1 + 1) * ld + c1 + 1, 1);
+        i00 = (long long)r0 * ld + c0;
+        i01 = (long long)r0 * ld + c1 + 1;
+        i10 = (long long)(r1 + 1) * ld + c0;
+        i11 = (long long)(r1 + 1) * ld + c1 + 1;
       }
+    }
+    if (diff) {
+      agg_add_const_i32(diff, i00, 1);
+      agg_add_const_i32(diff, i01, -1);
+      agg_add_const_i32(diff, i10, -1);
+      agg_add_const_i32(diff, i11, 1);
     }
   }
   const double s = block_sum_double(acc);

@@ -1,4 +1,5 @@
 // fx_core.cu -- context, error reporting, stage timing and design upload.
+#include <algorithm>
 #include <cstdarg>
 #include <cstring>
 #include <new>
@@ -64,10 +65,15 @@ void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a) {
   if (ctx->timer.pending.size() > 4096) ctx->timer.resolve();
 }
 
-// Deduplicated clique-expansion adjacency (H/src/data/circuit.rs:154-171):
-// gate a's list holds every other gate sharing a net with it, once, and a
-// itself when a net names a twice. Built from the gate->net incidence in
-// O(sum over nets of degree^2) with a marker array.
+// Deduplicated clique-expansion adjacency (H/src/data/circuit.rs:154-171),
+// in the reference's insertion order. The reference walks the pairs (i < j)
+// of every net in net order and appends each endpoint to the other's list
+// unless present. For a gate a at pin position p of net e that yields the
+// net's pins in pin order without position p; so each list is "incident
+// nets in net order, pins in pin order, skipping a and duplicates". A net
+// that names a twice also appends a itself; such nets replay the pair loop
+// for a to keep the exact order. Built from the gate->net incidence in
+// O(sum over nets of degree^2) with a marker array instead of Vec::contains.
 static int build_adjacency(int32_t N, int32_t M, const int32_t *net_ptr,
                            const int32_t *net_gate, std::vector<int32_t> &ptr,
                            std::vector<int32_t> &idx) {
@@ -86,26 +92,29 @@ static int build_adjacency(int32_t N, int32_t M, const int32_t *net_ptr,
   ptr.assign((size_t)N + 1, 0);
   idx.clear();
   idx.reserve((size_t)P * 4);
+  auto push = [&](int32_t a, int32_t b) {
+    if (mark[b] != a) {
+      mark[b] = a;
+      idx.push_back(b);
+    }
+  };
   for (int32_t a = 0; a < N; ++a) {
-    bool self = false;
-    int32_t prev_net = -1;
     for (int32_t t = inc_ptr[a]; t < inc_ptr[a + 1]; ++t) {
-      int32_t e = inc[t];
-      if (e == prev_net) {  // a appears more than once in net e
-        self = true;
-        continue;
-      }
-      prev_net = e;
-      for (int32_t q = net_ptr[e]; q < net_ptr[e + 1]; ++q) {
-        int32_t b = net_gate[q];
-        if (b == a) continue;
-        if (mark[b] != a) {
-          mark[b] = a;
-          idx.push_back(b);
-        }
+      const int32_t e = inc[t];
+      if (t > inc_ptr[a] && inc[t - 1] == e) continue;  // net already done
+      const bool repeated = t + 1 < inc_ptr[a + 1] && inc[t + 1] == e;
+      const int32_t b0 = net_ptr[e], b1 = net_ptr[e + 1];
+      if (!repeated) {
+        for (int32_t q = b0; q < b1; ++q)
+          if (net_gate[q] != a) push(a, net_gate[q]);
+      } else {  // replay circuit.rs:158-168 for the pairs that touch a
+        for (int32_t i = b0; i < b1; ++i)
+          for (int32_t j = i + 1; j < b1; ++j) {
+            if (net_gate[i] == a) push(a, net_gate[j]);
+            if (net_gate[j] == a) push(a, net_gate[i]);
+          }
       }
     }
-    if (self) idx.push_back(a);
     if (idx.size() > (size_t)INT32_MAX) {
       set_error("adjacency exceeds 2^31 entries");
       return FX_EINVAL;
@@ -165,6 +174,8 @@ extern "C" int fx_ctx_destroy(fx_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   cudaStreamSynchronize(ctx->stream2);
   ctx->timer.destroy();
+  for (auto &e : ctx->marks)
+    if (e) cudaEventDestroy(e);
   cudaEventDestroy(ctx->fork);
   cudaEventDestroy(ctx->join);
   cudaStreamDestroy(ctx->stream);
@@ -206,13 +217,79 @@ extern "C" int64_t fx_ctx_kernel_launches(fx_ctx *ctx) {
   return ctx ? ctx->launches : -1;
 }
 
+extern "C" int fx_ctx_mark(fx_ctx *ctx, int slot) {
+  if (!ctx || slot < 0 || slot >= 16) return FX_EINVAL;
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  if (!ctx->marks[slot]) FX_CHECK_CUDA(cudaEventCreate(&ctx->marks[slot]));
+  FX_CHECK_CUDA(cudaEventRecord(ctx->marks[slot], ctx->stream));
+  return FX_OK;
+}
+
+extern "C" int fx_ctx_elapsed(fx_ctx *ctx, int a, int b, float *out_ms) {
+  if (!ctx || !out_ms || a < 0 || a >= 16 || b < 0 || b >= 16 ||
+      !ctx->marks[a] || !ctx->marks[b])
+    return FX_EINVAL;
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  FX_CHECK_CUDA(cudaEventSynchronize(ctx->marks[b]));
+  FX_CHECK_CUDA(cudaEventElapsedTime(out_ms, ctx->marks[a], ctx->marks[b]));
+  return FX_OK;
+}
+
+extern "C" int fx_ctx_synchronize(fx_ctx *ctx) {
+  if (!ctx) return FX_EINVAL;
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  FX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  FX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream2));
+  return FX_OK;
+}
+
+static int validate_netlist(int32_t n_gates, int32_t n_nets,
+                            const int32_t *net_ptr, const int32_t *net_gate) {
+  if (n_gates <= 0 || n_nets < 0 || !net_ptr || (n_nets > 0 && !net_gate)) {
+    set_error("invalid netlist arguments");
+    return FX_EINVAL;
+  }
+  if (net_ptr[0] != 0) {
+    set_error("net_ptr[0] must be 0");
+    return FX_EINVAL;
+  }
+  for (int32_t e = 0; e < n_nets; ++e)
+    if (net_ptr[e + 1] < net_ptr[e]) {
+      set_error("net_ptr decreases at net %d", e);
+      return FX_EINVAL;
+    }
+  const int64_t P = net_ptr[n_nets];
+  for (int64_t q = 0; q < P; ++q)
+    if (net_gate[q] < 0 || net_gate[q] >= n_gates) {
+      set_error("pin %lld names gate %d (n_gates=%d)", (long long)q, net_gate[q],
+                n_gates);
+      return FX_EINVAL;
+    }
+  return FX_OK;
+}
+
+extern "C" int64_t fx_adjacency_build(int32_t n_gates, int32_t n_nets,
+                                      const int32_t *net_ptr,
+                                      const int32_t *net_gate,
+                                      int32_t *out_adj_ptr, int32_t *out_adj_idx,
+                                      int64_t cap) {
+  if (!out_adj_ptr) return FX_EINVAL;
+  FX_TRY(validate_netlist(n_gates, n_nets, net_ptr, net_gate));
+  std::vector<int32_t> ptr, idx;
+  FX_TRY(build_adjacency(n_gates, n_nets, net_ptr, net_gate, ptr, idx));
+  memcpy(out_adj_ptr, ptr.data(), ptr.size() * 4);
+  if (out_adj_idx && cap > 0)
+    memcpy(out_adj_idx, idx.data(),
+           (size_t)std::min<int64_t>(cap, (int64_t)idx.size()) * 4);
+  return (int64_t)idx.size();
+}
+
 extern "C" int fx_design_load(fx_ctx *ctx, int32_t n_gates, int32_t n_nets,
                               const int32_t *net_ptr, const int32_t *net_gate,
                               const float *gate_w, const float *gate_h,
                               float chip_w, float chip_h,
                               fx_design **out_design) {
-  if (!ctx || !out_design || n_gates <= 0 || n_nets < 0 || !net_ptr ||
-      (n_nets > 0 && !net_gate)) {
+  if (!ctx || !out_design) {
     set_error("fx_design_load: invalid arguments");
     return FX_EINVAL;
   }
@@ -221,25 +298,8 @@ extern "C" int fx_design_load(fx_ctx *ctx, int32_t n_gates, int32_t n_nets,
     set_error("fx_design_load: chip size must be positive");
     return FX_EINVAL;
   }
-  // Validate the CSR: monotone pointers starting at 0, gate ids in range.
-  if (net_ptr[0] != 0) {
-    set_error("fx_design_load: net_ptr[0] must be 0");
-    return FX_EINVAL;
-  }
-  for (int32_t e = 0; e < n_nets; ++e) {
-    if (net_ptr[e + 1] < net_ptr[e]) {
-      set_error("fx_design_load: net_ptr decreases at net %d", e);
-      return FX_EINVAL;
-    }
-  }
+  FX_TRY(validate_netlist(n_gates, n_nets, net_ptr, net_gate));
   const int64_t P = net_ptr[n_nets];
-  for (int64_t q = 0; q < P; ++q) {
-    if (net_gate[q] < 0 || net_gate[q] >= n_gates) {
-      set_error("fx_design_load: pin %lld names gate %d (n_gates=%d)",
-                (long long)q, net_gate[q], n_gates);
-      return FX_EINVAL;
-    }
-  }
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
   fx_design *d = new (std::nothrow) fx_design();
   if (!d) return FX_ENOMEM;
@@ -320,46 +380,11 @@ extern "C" int fx_design_free(fx_design *d) {
   d->vx.release();
   d->vy.release();
   d->fattr.release();
-  BHWork &b = d->bh;
-  for (int i = 0; i < 2; ++i) {
-    b.keys[i].release();
-    b.idx[i].release();
-  }
-  b.tile_hist.release();
-  b.tile_scan.release();
-  b.spos.release();
-  b.prefix.release();
-  b.child.release();
-  b.range.release();
-  b.com.release();
-  b.meta.release();
-  b.root.release();
-  b.bbox.release();
-  b.force.release();
-  DensityWork &w = d->dens;
-  w.area_fx.release();
-  w.cmat.release();
-  w.cmat_t.release();
-  w.cmat_lo.release();
-  w.cmat_t_lo.release();
-  w.cmat_bf.release();
-  w.cmat_t_bf.release();
-  w.inv_eig.release();
-  for (int i = 0; i < 4; ++i) w.buf[i].release();
-  for (int i = 0; i < 3; ++i) w.lo[i].release();
-  for (int i = 0; i < 2; ++i) w.bf[i].release();
-  w.ex.release();
-  w.ey.release();
-  w.energy.release();
-  w.force.release();
-  CongWork &c = d->cong;
-  c.diff.release();
-  c.counts.release();
-  c.partial.release();
-  c.partial_max.release();
-  c.done.release();
-  c.result.release();
-  c.result_max.release();
+  auto rel = [](auto &buf) { buf.release(); };
+  d->bh.for_each(rel);
+  d->dens.for_each(rel);
+  d->cong.for_each(rel);
+  d->step.for_each(rel);
   delete d;
   return FX_OK;
 }
@@ -419,20 +444,11 @@ extern "C" int64_t fx_design_device_bytes(const fx_design *d) {
        d->adj_idx.bytes() + d->area.bytes();
   for (int i = 0; i < 2; ++i) t += d->x[i].bytes() + d->y[i].bytes();
   t += d->vx.bytes() + d->vy.bytes() + d->fattr.bytes();
-  const BHWork &b = d->bh;
-  for (int i = 0; i < 2; ++i) t += b.keys[i].bytes() + b.idx[i].bytes();
-  t += b.tile_hist.bytes() + b.tile_scan.bytes() + b.spos.bytes() +
-       b.prefix.bytes() + b.child.bytes() + b.range.bytes() + b.com.bytes() +
-       b.meta.bytes() + b.force.bytes();
-  const DensityWork &w = d->dens;
-  t += w.area_fx.bytes() + w.cmat.bytes() + w.cmat_t.bytes() +
-       w.cmat_lo.bytes() + w.cmat_t_lo.bytes() + w.cmat_bf.bytes() +
-       w.cmat_t_bf.bytes() + w.inv_eig.bytes() + w.ex.bytes() + w.ey.bytes() +
-       w.force.bytes();
-  for (int i = 0; i < 4; ++i) t += w.buf[i].bytes();
-  for (int i = 0; i < 3; ++i) t += w.lo[i].bytes();
-  for (int i = 0; i < 2; ++i) t += w.bf[i].bytes();
-  const CongWork &c = d->cong;
-  t += c.diff.bytes() + c.counts.bytes();
+  auto add = [&t](auto &buf) { t += (int64_t)buf.bytes(); };
+  fx_design *m = const_cast<fx_design *>(d);
+  m->bh.for_each(add);
+  m->dens.for_each(add);
+  m->cong.for_each(add);
+  m->step.for_each(add);
   return t;
 }

@@ -211,6 +211,9 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
 int density_scatter(fx_ctx *ctx, fx_design *d, const float *x, const float *y,
                     int G, int precision, cudaStream_t s) {
   FX_TRY(dens_setup(d, G, precision, s));
+  // The accumulator may still hold the scatter of a previous call's final
+  // positions: start from zero.
+  FX_CHECK_CUDA(cudaMemsetAsync(d->dens.area_fx.p, 0, (size_t)G * G * 8, s));
   const float bw = d->chip_w / (float)G, bh = d->chip_h / (float)G;
   int nb = (d->n + 255) / 256;
   if (nb > ctx->num_sms * 8) nb = ctx->num_sms * 8;

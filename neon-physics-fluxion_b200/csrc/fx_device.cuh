@@ -92,6 +92,36 @@ __device__ __forceinline__ void last_block_sum(double block_value,
   }
 }
 
+// Warp-aggregated atomic adds: lanes naming the same element (idx >= 0) are
+// combined and one lane issues the atomic. Every lane of the warp must call
+// these (idx < 0 = nothing to add). Sums of integers are exact, so the
+// result does not depend on the grouping.
+__device__ __forceinline__ void agg_add_u64(unsigned long long *base, long long idx,
+                                            unsigned long long v) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned peers = __match_any_sync(0xffffffffu, idx);
+  const bool alone = __all_sync(0xffffffffu, peers == (1u << lane));
+  if (alone) {
+    if (idx >= 0) atomicAdd(base + idx, v);
+    return;
+  }
+  unsigned long long sum = 0;
+#pragma unroll
+  for (int src = 0; src < 32; ++src) {
+    const unsigned long long w = __shfl_sync(0xffffffffu, v, src);
+    if ((peers >> src) & 1u) sum += w;
+  }
+  if (idx >= 0 && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(base + idx, sum);
+}
+
+// Adds the same constant `v` from every lane naming idx (>= 0).
+__device__ __forceinline__ void agg_add_const_i32(int *base, long long idx, int v) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned peers = __match_any_sync(0xffffffffu, idx);
+  if (idx >= 0 && lane == (unsigned)(__ffs(peers) - 1))
+    atomicAdd(base + idx, v * __popc(peers));
+}
+
 // Order-preserving float <-> uint mapping for atomicMin/atomicMax.
 __device__ __forceinline__ unsigned int f2ord(float f) {
   const unsigned int u = __float_as_uint(f);

@@ -85,19 +85,32 @@ struct StageTimer {
 // ---- Barnes-Hut workspace ----------------------------------------------------
 struct BHWork {
   int n = 0;
-  DevBuf<uint32_t> keys[2];
-  DevBuf<int32_t> idx[2];
+  DevBuf<uint32_t> keys[2];     // radix sort ping-pong (keys[0] = sorted)
+  DevBuf<int32_t> idx[2];       // gate index payload (idx[0] = sorted order)
   DevBuf<uint32_t> tile_hist;   // radix sort: digit x tile counts
-  DevBuf<uint32_t> tile_scan;
+  DevBuf<uint32_t> tile_scan;   // per-digit exclusive scan of tile_hist
+  DevBuf<uint32_t> digit_total; // 256 digit totals
   DevBuf<float2> spos;          // positions in sorted order
-  DevBuf<double2> prefix;       // inclusive prefix sums of spos (FP64)
-  DevBuf<int32_t> child;        // internal nodes: 2 per node (tagged)
-  DevBuf<int32_t> range;        // internal nodes: first,last
-  DevBuf<float4> com;           // internal nodes: {cx_hi, cy_hi, cx_lo, cy_lo}
-  DevBuf<float2> meta;          // internal nodes: {count, size^2 (or <0)}
-  DevBuf<float> root;           // {x_min, y_min, size, inv_size}
-  DevBuf<unsigned int> bbox;    // ordered-int min/max of x, y
+  DevBuf<int32_t> child;        // internal nodes: 2 children (leaf s -> ~s)
+  DevBuf<int32_t> range;        // internal nodes: first, last
+  DevBuf<int32_t> dnode;        // internal nodes: prefix length
+  DevBuf<int32_t> dparent;      // internal nodes: parent's prefix length
+  DevBuf<int4> qchild;          // internal nodes: up to 4 quad children
+  DevBuf<double2> scan[6];      // chunked FP64 prefix-scan levels
+  DevBuf<double2> prefix;       // inclusive FP64 prefix sums of spos
+  DevBuf<float4> node;          // internal nodes: 2 x float4 walk records
+  DevBuf<float> root;           // {x_min, y_min, size}
+  DevBuf<unsigned int> bbox;    // [0..3] ordered-int box, [4] error flag
   DevBuf<float2> force;         // per gate (original order)
+  template <class F>
+  void for_each(F &&f) {
+    for (auto &b : keys) f(b);
+    for (auto &b : idx) f(b);
+    f(tile_hist); f(tile_scan); f(digit_total); f(spos); f(child); f(range);
+    f(dnode); f(dparent); f(qchild);
+    for (auto &b : scan) f(b);
+    f(prefix); f(node); f(root); f(bbox); f(force);
+  }
 };
 
 // ---- density (DCT Poisson) workspace -----------------------------------------
@@ -117,6 +130,15 @@ struct DensityWork {
   DevBuf<float> ex, ey;                // field
   DevBuf<double> energy;               // FP64 partials
   DevBuf<float2> force;                // per gate
+  template <class F>
+  void for_each(F &&f) {
+    f(area_fx); f(cmat); f(cmat_t); f(cmat_lo); f(cmat_t_lo); f(cmat_bf);
+    f(cmat_t_bf); f(inv_eig);
+    for (auto &b : buf) f(b);
+    for (auto &b : lo) f(b);
+    for (auto &b : bf) f(b);
+    f(ex); f(ey); f(energy); f(force);
+  }
 };
 
 // ---- congestion workspace ----------------------------------------------------
@@ -129,6 +151,23 @@ struct CongWork {
   DevBuf<unsigned int> done;   // last-block counters
   DevBuf<double> result;       // {hpwl, total_overflow}
   DevBuf<float> result_max;
+  template <class F>
+  void for_each(F &&f) {
+    f(diff); f(counts); f(partial); f(partial_max); f(done); f(result);
+    f(result_max);
+  }
+};
+
+// ---- fused attraction/integrate step: cross-block reductions ------------------
+struct StepWork {
+  DevBuf<float4> bbox_part;     // per block {min x, min y, max x, max y}
+  DevBuf<double> e_part;        // per block density energy
+  DevBuf<unsigned int> done;    // last-block counter
+  DevBuf<double> energy;        // result
+  template <class F>
+  void for_each(F &&f) {
+    f(bbox_part); f(e_part); f(done); f(energy);
+  }
 };
 
 }  // namespace fx
@@ -141,6 +180,7 @@ struct fx_ctx {
   int num_sms = 0;
   fx::StageTimer timer;
   int64_t launches = 0;
+  cudaEvent_t marks[16] = {};
 };
 
 struct fx_design {
@@ -163,6 +203,7 @@ struct fx_design {
   fx::BHWork bh;
   fx::DensityWork dens;
   fx::CongWork cong;
+  fx::StepWork step;
 };
 
 namespace fx {

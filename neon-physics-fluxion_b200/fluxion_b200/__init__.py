@@ -7,12 +7,12 @@ reference's data types and entry points.
 from ._lib import (FX_DCT_BF16, FX_DCT_FP32, FX_DCT_SIMT, FX_DCT_TF32, FluxionError,
                    IterCfg, IterStats, load)
 from .api import (Circuit, Context, Design, Placement, RoutingGrid, Synth,
-                  build_and_compute, compute_congestion, compute_hpwl, default_context,
+                  build_adjacency, build_and_compute, compute_congestion, compute_hpwl, default_context,
                   iter_cfg, synth_leaves, synth_plain)
 
 __all__ = [
     "Circuit", "Context", "Design", "Placement", "RoutingGrid", "Synth",
-    "build_and_compute", "compute_congestion", "compute_hpwl", "default_context",
+    "build_adjacency", "build_and_compute", "compute_congestion", "compute_hpwl", "default_context",
     "iter_cfg", "synth_leaves", "synth_plain", "FluxionError", "IterCfg", "IterStats",
     "load", "FX_DCT_FP32", "FX_DCT_TF32", "FX_DCT_BF16", "FX_DCT_SIMT",
 ]

@@ -83,6 +83,9 @@ SIGNATURES = {
     "fx_ctx_stage_times": (C.c_int, [P, PF64, PI64, C.c_int]),
     "fx_ctx_reset_stage_times": (C.c_int, [P]),
     "fx_ctx_kernel_launches": (C.c_int64, [P]),
+    "fx_ctx_mark": (C.c_int, [P, C.c_int]),
+    "fx_ctx_elapsed": (C.c_int, [P, C.c_int, C.c_int, PF32]),
+    "fx_ctx_synchronize": (C.c_int, [P]),
     "fx_design_load": (C.c_int, [P, I32, I32, PI32, PI32, PF32, PF32, F32, F32,
                                  C.POINTER(P)]),
     "fx_design_free": (C.c_int, [P]),
@@ -100,6 +103,7 @@ SIGNATURES = {
                                       PI32, PF32]),
     "fx_stage_density": (C.c_int, [P, P, I32, F32, F32, I32, PF32, PF32, PF32,
                                    PF32, PF32, PF32, PF64]),
+    "fx_adjacency_build": (C.c_int64, [I32, I32, PI32, PI32, PI32, PI32, C.c_int64]),
     "fx_synth_plain": (C.c_int, [C.c_uint64, I32, I32, F32, F32, I32, C.POINTER(P)]),
     "fx_synth_leaves": (C.c_int, [C.c_uint64, I32, I32, I32, F32, C.POINTER(P)]),
     "fx_netlist_sizes": (C.c_int, [P, PI64, PI64, PI64, PI64]),

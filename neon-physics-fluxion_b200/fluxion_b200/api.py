@@ -179,6 +179,17 @@ class Context:
     def kernel_launches(self) -> int:
         return int(self.lib.fx_ctx_kernel_launches(self.handle))
 
+    def mark(self, slot: int) -> None:
+        check(self.lib.fx_ctx_mark(self.handle, slot), "fx_ctx_mark")
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_float()
+        check(self.lib.fx_ctx_elapsed(self.handle, a, b, C.byref(ms)), "fx_ctx_elapsed")
+        return ms.value
+
+    def synchronize(self) -> None:
+        check(self.lib.fx_ctx_synchronize(self.handle), "fx_ctx_synchronize")
+
 
 class Design:
     """A device-resident netlist (fx_design) with positions and workspaces."""
@@ -365,6 +376,25 @@ def compute_hpwl(placement: Placement, circuit: Circuit,
         if own:
             design.close()
     return hpwl
+
+
+def build_adjacency(circuit: Circuit):
+    """circuit.rs:154-171 Circuit::build_adjacency, in the reference's order.
+
+    Host-only (no GPU); returns (adj_ptr[N+1], adj_idx[A]) int32 CSR."""
+    lib = load()
+    net_ptr = np.ascontiguousarray(circuit.net_ptr, np.int32)
+    net_gate = np.ascontiguousarray(circuit.net_gate, np.int32)
+    ap = np.zeros(circuit.num_gates + 1, np.int32)
+    a = check(lib.fx_adjacency_build(circuit.num_gates, circuit.num_nets,
+                                     ptr(net_ptr, C.c_int32), ptr(net_gate, C.c_int32),
+                                     ptr(ap, C.c_int32), None, 0), "fx_adjacency_build")
+    ai = np.zeros(max(a, 1), np.int32)
+    check(lib.fx_adjacency_build(circuit.num_gates, circuit.num_nets,
+                                 ptr(net_ptr, C.c_int32), ptr(net_gate, C.c_int32),
+                                 ptr(ap, C.c_int32), ptr(ai, C.c_int32), a),
+          "fx_adjacency_build")
+    return ap, ai[:a]
 
 
 # ---------------------------------------------------------------------------

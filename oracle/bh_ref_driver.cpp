@@ -9,16 +9,19 @@
 
 #include <thread>
 
-extern "C" void bh_ref_forces(int n, const double *px, const double *py,
-                              const double *q, double theta, double k,
-                              double min_dist, double *fx, double *fy,
-                              int threads) {
+// stride > 1 evaluates only points i with i % stride == 0 (the tree is
+// always built over all points); used to time a bounded sample.
+extern "C" void bh_ref_forces_sample(int n, const double *px, const double *py,
+                                     const double *q, double theta, double k,
+                                     double min_dist, double *fx, double *fy,
+                                     int threads, int stride) {
   fluxion::BarnesHutTree tree(theta);
   tree.build(px, py, q, n);
   // The tree is read-only after build, so points can be split across
   // threads (threads <= 1 runs on the calling thread).
-  auto work = [&](int t, int stride) {
-    for (int i = t; i < n; i += stride) {
+  if (stride < 1) stride = 1;
+  auto work = [&](int t, int nthreads) {
+    for (int i = t * stride; i < n; i += nthreads * stride) {
       double a = 0.0, b = 0.0;
       tree.computeForcesForParticle(i, px[i], py[i], q[i], k, min_dist, a, b);
       fx[i] = a;
@@ -32,4 +35,11 @@ extern "C" void bh_ref_forces(int n, const double *px, const double *py,
     for (int t = 0; t < threads; ++t) pool.emplace_back(work, t, threads);
     for (auto &th : pool) th.join();
   }
+}
+
+extern "C" void bh_ref_forces(int n, const double *px, const double *py,
+                              const double *q, double theta, double k,
+                              double min_dist, double *fx, double *fy,
+                              int threads) {
+  bh_ref_forces_sample(n, px, py, q, theta, k, min_dist, fx, fy, threads, 1);
 }

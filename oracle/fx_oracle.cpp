@@ -101,6 +101,46 @@ void or_congestion(int32_t m, const int32_t *net_ptr, const int32_t *net_gate,
   }
 }
 
+// compute_congestion_cpu restricted to nets e with e % stride == 0 (the grids
+// are cleared first). Used to time a bounded sample of the reference's
+// congestion loop; the full call is stride 1.
+void or_congestion_sample(int32_t m, const int32_t *net_ptr,
+                          const int32_t *net_gate, const float *x,
+                          const float *y, float chip_w, float chip_h,
+                          int64_t cols, int64_t rows, int32_t stride, float *h,
+                          float *v) {
+  float cw, ch, cap;
+  or_grid_geometry(chip_w, chip_h, cols, rows, &cw, &ch, &cap);
+  const size_t cells = (size_t)(cols * rows);
+  std::fill(h, h + cells, 0.0f);
+  std::fill(v, v + cells, 0.0f);
+  for (int32_t e = 0; e < m; e += stride) {
+    const int32_t b = net_ptr[e], t = net_ptr[e + 1];
+    if (t - b < 2) continue;
+    float min_x = 3.40282347e+38f, max_x = -3.40282347e+38f;
+    float min_y = 3.40282347e+38f, max_y = -3.40282347e+38f;
+    for (int32_t q = b; q < t; ++q) {
+      const float px = x[net_gate[q]], py = y[net_gate[q]];
+      min_x = std::fmin(min_x, px);
+      max_x = std::fmax(max_x, px);
+      min_y = std::fmin(min_y, py);
+      max_y = std::fmax(max_y, py);
+    }
+    const int64_t c0 = or_cell_at(min_x, cw, cols), r0 = or_cell_at(min_y, ch, rows);
+    const int64_t c1 = or_cell_at(max_x, cw, cols), r1 = or_cell_at(max_y, ch, rows);
+    for (int64_t r = r0; r <= r1; ++r)
+      for (int64_t c = c0; c <= c1; ++c) {
+        const size_t idx = (size_t)(r * cols + c);
+        if (idx < cells) h[idx] += 1.0f;
+      }
+    for (int64_t c = c0; c <= c1; ++c)
+      for (int64_t r = r0; r <= r1; ++r) {
+        const size_t idx = (size_t)(r * cols + c);
+        if (idx < cells) v[idx] += 1.0f;
+      }
+  }
+}
+
 // H/src/data/grid.rs:71-91  overflow_at / max_overflow / total_overflow.
 void or_overflow(const float *h, const float *v, int64_t cols, int64_t rows,
                  float capacity, float *total, float *maxv) {
@@ -574,96 +614,217 @@ void or_bh_keys(int32_t n, const float *x, const float *y, const float *root,
 }
 
 namespace {
+// FP64 inclusive prefix sums of the sorted positions with the fixed chunked
+// association of the device: chunks of 128 consecutive values are added left
+// to right from 0.0; chunk totals form the next level until one chunk
+// remains; each chunk's running sum then starts from its offset one level up.
+constexpr int kScanChunk = 128;
+
+static void chunked_prefix(const std::vector<double> &v, std::vector<double> &out) {
+  const int64_t n = (int64_t)v.size();
+  std::vector<std::vector<double>> tot;  // tot[l] = chunk totals of level l
+  const std::vector<double> *cur = &v;
+  while ((int64_t)cur->size() > kScanChunk) {
+    const int64_t m = ((int64_t)cur->size() + kScanChunk - 1) / kScanChunk;
+    std::vector<double> t((size_t)m);
+    for (int64_t c = 0; c < m; ++c) {
+      double acc = 0.0;
+      for (int64_t i = c * kScanChunk; i < std::min<int64_t>(cur->size(), (c + 1) * kScanChunk); ++i)
+        acc = acc + (*cur)[i];
+      t[c] = acc;
+    }
+    tot.push_back(std::move(t));
+    cur = &tot.back();
+  }
+  // exclusive offsets, top level first
+  std::vector<double> off_above;  // offsets of the level above's values
+  std::vector<std::vector<double>> offs(tot.size());
+  for (int l = (int)tot.size() - 1; l >= 0; --l) {
+    const std::vector<double> &vals = tot[l];
+    std::vector<double> &o = offs[l];
+    o.resize(vals.size());
+    const int64_t chunks = ((int64_t)vals.size() + kScanChunk - 1) / kScanChunk;
+    for (int64_t c = 0; c < chunks; ++c) {
+      double acc = (l == (int)tot.size() - 1) ? 0.0 : offs[l + 1][c];
+      for (int64_t i = c * kScanChunk; i < std::min<int64_t>(vals.size(), (c + 1) * kScanChunk); ++i) {
+        o[i] = acc;
+        acc = acc + vals[i];
+      }
+    }
+  }
+  out.resize((size_t)n);
+  const int64_t chunks = (n + kScanChunk - 1) / kScanChunk;
+  for (int64_t c = 0; c < chunks; ++c) {
+    double acc = tot.empty() ? 0.0 : offs[0][c];
+    for (int64_t i = c * kScanChunk; i < std::min<int64_t>(n, (c + 1) * kScanChunk); ++i) {
+      acc = acc + v[i];
+      out[i] = acc;
+    }
+  }
+}
+
+// The radix tree over the sorted keys, built top-down: node [f, l] splits
+// after the last position s with delta(f, s) > delta(f, l). Children are
+// internal node ids or ~leaf (sorted position), as on the device.
 struct BHTree {
   int32_t n;
   std::vector<uint32_t> key;      // sorted keys
   std::vector<int32_t> perm;      // sorted -> original
   std::vector<float> sx, sy;      // sorted positions
-  std::vector<double> px, py;     // inclusive FP64 prefix sums
+  std::vector<double> px, py;     // chunked FP64 prefix sums
   float rsize;
+  struct Node {
+    int32_t f, l, dn, dp, left, right;
+    double cxd, cyd;                // FP64 centre of mass
+    float hx, hy, lx, ly, s2;       // COM hi/lo, size^2 (<0: no quad level)
+    bool bucket;
+  };
+  std::vector<Node> nodes;
   int delta(int32_t i, int32_t j) const {
     if (j < 0 || j >= n) return -1;
     if (key[i] != key[j]) return __builtin_clz(key[i] ^ key[j]) - 2;
     return 30 + __builtin_clz((uint32_t)(i ^ j));
   }
-  // Split of [f, l]: the last s with delta(f, s) > delta(f, l).
   int32_t split(int32_t f, int32_t l) const {
     const int dn = delta(f, l);
-    int32_t lo = f, hi = l - 1;  // answer in [f, l-1]
+    int32_t lo = f, hi = l - 1;
     while (lo < hi) {
       const int32_t mid = lo + (hi - lo + 1) / 2;
       if (delta(f, mid) > dn) lo = mid; else hi = mid - 1;
     }
     return lo;
   }
+  int32_t build(int32_t f, int32_t l, int dp) {
+    const int32_t id = (int32_t)nodes.size();
+    nodes.push_back(Node{});
+    const int dn = delta(f, l);
+    const int32_t g = split(f, l);
+    const int32_t left = g == f ? ~f : build(f, g, dn);
+    const int32_t right = g + 1 == l ? ~l : build(g + 1, l, dn);
+    Node &nd = nodes[id];
+    nd.f = f;
+    nd.l = l;
+    nd.dn = dn;
+    nd.dp = dp;
+    nd.left = left;
+    nd.right = right;
+    double sxd = px[l], syd = py[l];
+    if (f > 0) {
+      sxd = sxd - px[f - 1];
+      syd = syd - py[f - 1];
+    }
+    const int32_t cnt = l - f + 1;
+    nd.cxd = sxd / (double)cnt;
+    nd.cyd = syd / (double)cnt;
+    nd.hx = (float)nd.cxd;
+    nd.hy = (float)nd.cyd;
+    nd.lx = (float)(nd.cxd - (double)nd.hx);
+    nd.ly = (float)(nd.cyd - (double)nd.hy);
+    nd.bucket = dn >= 30;
+    const int lmax = nd.bucket ? 15 : dn >> 1;
+    const float sz = std::ldexp(rsize, -lmax);
+    nd.s2 = (!nd.bucket && dp >= 0 && (dp >> 1) == lmax) ? -1.0f : sz * sz;
+    return id;
+  }
+  // Up to four quad children of an internal node, in key order: a child that
+  // stands for no quad level is replaced by its own two children.
+  int quad_children(int32_t c, int32_t out[4]) const {
+    int k = 0;
+    const Node &nd = nodes[c];
+    for (int32_t h : {nd.left, nd.right}) {
+      if (h >= 0 && nodes[h].dn < 30 && (nodes[h].dn >> 1) == (nd.dn >> 1)) {
+        out[k++] = nodes[h].left;
+        out[k++] = nodes[h].right;
+      } else {
+        out[k++] = h;
+      }
+    }
+    return k;
+  }
 };
 
+// IEEE f32 law, in the device's operation order.
+static inline void term32(float dx, float dy, float r2c, float kq, float &fx,
+                          float &fy) {
+  const float inv = 1.0f / std::sqrt(r2c);
+  const float f = ((kq * inv) * inv) * inv;
+  fx = fx + f * dx;
+  fy = fy + f * dy;
+}
+
+// Per-point walk with the device's rules and term order: for every opened
+// cell, the terms of its children in key order (single points, accepted
+// cells, opened buckets point by point), then the opened children in order.
 struct Walker {
   const BHTree &t;
   double k, md;
-  float th2, md2;
-  int32_t s;             // sorted index of the target point
+  float kf, th2, md2;
+  int32_t s;                 // sorted index of the target point
   float pxf, pyf;
-  double pxd, pyd;
-  double fx = 0, fy = 0;
+  double fx = 0, fy = 0;     // FP64 recomputation of the same interactions
+  float gx = 0.f, gy = 0.f;  // f32, device order
   int64_t inter = 0;
   void point(int32_t q) {
-    const double dx = pxd - (double)t.sx[q], dy = pyd - (double)t.sy[q];
+    const double dx = (double)pxf - (double)t.sx[q], dy = (double)pyf - (double)t.sy[q];
     const double d = std::max(std::sqrt(dx * dx + dy * dy), md);
     const double f = k / (d * d);
     fx += f * dx / d;
     fy += f * dy / d;
+    const float ex = pxf - t.sx[q], ey = pyf - t.sy[q];
+    const float r2 = ex * ex + ey * ey;
+    term32(ex, ey, std::fmax(r2, md2), kf, gx, gy);
     ++inter;
   }
-  void visit(int32_t f, int32_t l, int dparent) {
-    if (f == l) {
-      if (f != s) point(f);
-      return;
+  // Adds the terms child c contributes at this cell; true if c is a cell
+  // this point must descend into.
+  bool eval(int32_t c) {
+    if (c < 0) {
+      if (~c != s) point(~c);
+      return false;
     }
-    const int dn = t.delta(f, l);
-    const int32_t cnt = l - f + 1;
-    const double sx = t.px[l] - (f > 0 ? t.px[f - 1] : 0.0);
-    const double sy = t.py[l] - (f > 0 ? t.py[f - 1] : 0.0);
-    const double cxd = sx / cnt, cyd = sy / cnt;
-    const bool bucket = dn >= 30;
-    const int lmax = bucket ? 15 : dn >> 1;
-    const bool transparent = !bucket && dparent >= 0 && (dparent >> 1) == lmax;
-    if (!transparent) {
-      // f32 decision, bit-identical to the device: COM as an f32 hi/lo pair.
-      const float hx = (float)cxd, hy = (float)cyd;
-      const float lx = (float)(cxd - (double)hx), ly = (float)(cyd - (double)hy);
-      const float dx = (pxf - hx) - lx, dy = (pyf - hy) - ly;
-      const float r2 = dx * dx + dy * dy;
-      const float r2c = std::fmax(r2, md2);
-      const float sz = std::ldexp(t.rsize, -lmax);
-      if (sz * sz < th2 * r2c) {
-        const double ddx = pxd - cxd, ddy = pyd - cyd;
-        const double d = std::max(std::sqrt(ddx * ddx + ddy * ddy), md);
-        const double fm = k * cnt / (d * d);
-        fx += fm * ddx / d;
-        fy += fm * ddy / d;
-        ++inter;
-        return;
-      }
-      if (bucket) {
-        for (int32_t q = f; q <= l; ++q)
-          if (q != s) point(q);
-        return;
-      }
+    const BHTree::Node &nd = t.nodes[c];
+    const float dx = (pxf - nd.hx) - nd.lx, dy = (pyf - nd.hy) - nd.ly;
+    const float r2 = dx * dx + dy * dy;
+    const float r2c = std::fmax(r2, md2);
+    if (nd.s2 >= 0.0f && nd.s2 < th2 * r2c) {
+      const int32_t cnt = nd.l - nd.f + 1;
+      const double ddx = (double)pxf - nd.cxd, ddy = (double)pyf - nd.cyd;
+      const double d = std::max(std::sqrt(ddx * ddx + ddy * ddy), md);
+      const double fm = k * cnt / (d * d);
+      fx += fm * ddx / d;
+      fy += fm * ddy / d;
+      term32(dx, dy, r2c, kf * (float)cnt, gx, gy);
+      ++inter;
+      return false;
     }
-    const int32_t g = t.split(f, l);
-    visit(f, g, dn);
-    visit(g + 1, l, dn);
+    if (nd.bucket) {
+      for (int32_t q = nd.f; q <= nd.l; ++q)
+        if (q != s) point(q);
+      return false;
+    }
+    return true;
+  }
+  void open(int32_t c) {
+    int32_t ch[4];
+    const int m = t.quad_children(c, ch);
+    bool op[4] = {false, false, false, false};
+    for (int h = 0; h < m; ++h) op[h] = eval(ch[h]);
+    for (int h = 0; h < m; ++h)
+      if (op[h]) open(ch[h]);
   }
 };
 }  // namespace
 
-// Forces on every point (original order) in FP64, plus the sorted order,
-// keys, root square and the interaction count per point (may be null).
+// Forces on every point (original order): FP64 recomputation (fx/fy) and the
+// f32 values in the device's operation order (fx32/fy32, may be null), plus
+// keys (gate order), sorted order, root square and interaction count per
+// point (each may be null). The opening decisions use the f32 rounding of
+// min_dist; the FP64 law uses min_dist as given.
 void or_bh_forces(int32_t n, const float *x, const float *y, double k,
                   float theta, double min_dist, double *fx, double *fy,
                   uint32_t *out_keys, int32_t *out_perm, float *out_root,
-                  int64_t *out_inter, int32_t threads) {
+                  int64_t *out_inter, int32_t threads, float *fx32,
+                  float *fy32) {
   if (n <= 0) return;
   float root[3];
   or_bh_root(n, x, y, root);
@@ -679,28 +840,29 @@ void or_bh_forces(int32_t n, const float *x, const float *y, double k,
   t.key.resize((size_t)n);
   t.sx.resize((size_t)n);
   t.sy.resize((size_t)n);
-  t.px.resize((size_t)n);
-  t.py.resize((size_t)n);
-  double ax = 0.0, ay = 0.0;
+  std::vector<double> vx((size_t)n), vy((size_t)n);
   for (int32_t s = 0; s < n; ++s) {
     const int32_t g = t.perm[s];
     t.key[s] = keys[g];
     t.sx[s] = x[g];
     t.sy[s] = y[g];
-    ax += (double)x[g];
-    ay += (double)y[g];
-    t.px[s] = ax;
-    t.py[s] = ay;
+    vx[s] = (double)x[g];
+    vy[s] = (double)y[g];
   }
-  // Decisions use the f32 floor (as the device); the FP64 law uses min_dist.
+  chunked_prefix(vx, t.px);
+  chunked_prefix(vy, t.py);
+  t.nodes.reserve(n > 1 ? (size_t)n - 1 : 1);
+  if (n >= 2) t.build(0, n - 1, -1);
   const float mdf = (float)min_dist;
-  const float th2 = theta * theta, md2 = mdf * mdf;
+  const float th2 = theta * theta, md2 = mdf * mdf, kf = (float)k;
   par_for(n, threads, [&](int32_t s) {
-    Walker w{t, k, min_dist, th2, md2, s, t.sx[s], t.sy[s], t.sx[s], t.sy[s]};
-    if (n >= 2) w.visit(0, n - 1, -1);
+    Walker w{t, k, min_dist, kf, th2, md2, s, t.sx[s], t.sy[s]};
+    if (n >= 2 && w.eval(0)) w.open(0);
     const int32_t g = t.perm[s];
     fx[g] = w.fx;
     fy[g] = w.fy;
+    if (fx32) fx32[g] = w.gx;
+    if (fy32) fy32[g] = w.gy;
     if (out_inter) out_inter[g] = w.inter;
   });
   if (out_keys) std::copy(keys.begin(), keys.end(), out_keys);

@@ -52,6 +52,9 @@ def lib() -> C.CDLL:
                                        F32P, F32P, F32P]
         L.or_congestion.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
                                     C.c_float, C.c_int64, C.c_int64, F32P, F32P]
+        L.or_congestion_sample.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
+                                           C.c_float, C.c_int64, C.c_int64, C.c_int32,
+                                           F32P, F32P]
         L.or_overflow.argtypes = [F32P, F32P, C.c_int64, C.c_int64, C.c_float, F32P, F32P]
         L.or_hpwl_f32.restype = C.c_float
         L.or_hpwl_f32.argtypes = [C.c_int32, I32P, I32P, F32P, F32P]
@@ -81,7 +84,7 @@ def lib() -> C.CDLL:
         L.or_bh_keys.argtypes = [C.c_int32, F32P, F32P, F32P, U32P]
         L.or_bh_forces.argtypes = [C.c_int32, F32P, F32P, C.c_double, C.c_float,
                                    C.c_double, F64P, F64P, U32P, I32P, F32P, I64P,
-                                   C.c_int32]
+                                   C.c_int32, F32P, F32P]
         L.or_repulsion_exact.argtypes = [C.c_int32, F32P, F32P, C.c_double, C.c_double,
                                          F64P, F64P]
         _lib = L
@@ -95,6 +98,9 @@ def ref_lib():
         R = C.CDLL(str(REF_LIB))
         R.bh_ref_forces.argtypes = [C.c_int, F64P, F64P, F64P, C.c_double, C.c_double,
                                     C.c_double, F64P, F64P, C.c_int]
+        R.bh_ref_forces_sample.argtypes = [C.c_int, F64P, F64P, F64P, C.c_double,
+                                           C.c_double, C.c_double, F64P, F64P, C.c_int,
+                                           C.c_int]
         _ref = R
     return _ref
 
@@ -130,6 +136,17 @@ def congestion(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows):
     lib().or_congestion(len(net_ptr) - 1, _p(net_ptr, C.c_int32), _p(net_gate, C.c_int32),
                         _p(x, C.c_float), _p(y, C.c_float), chip_w, chip_h, cols, rows,
                         _p(h, C.c_float), _p(v, C.c_float))
+    return h, v
+
+
+def congestion_sample(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows, stride):
+    net_ptr, net_gate, x, y = _i32(net_ptr), _i32(net_gate), _f32(x), _f32(y)
+    h = np.empty(cols * rows, np.float32)
+    v = np.empty(cols * rows, np.float32)
+    lib().or_congestion_sample(len(net_ptr) - 1, _p(net_ptr, C.c_int32),
+                               _p(net_gate, C.c_int32), _p(x, C.c_float), _p(y, C.c_float),
+                               chip_w, chip_h, cols, rows, stride, _p(h, C.c_float),
+                               _p(v, C.c_float))
     return h, v
 
 
@@ -265,14 +282,17 @@ def bh_keys(x, y, root):
 
 
 def bh_forces(x, y, k=0.5, theta=0.5, min_dist=0.1, threads=1):
-    """FP64 forces with the device's tree and opening decisions.
+    """Barnes-Hut forces with the device's tree and opening decisions.
 
-    min_dist enters the FP64 law as given; the opening decisions use its f32
-    rounding. Pass float(np.float32(v)) to reproduce a device run exactly.
+    Returns the FP64 recomputation of each point's interaction list (fx, fy)
+    and the f32 forces in the device's operation order (fx32, fy32). min_dist
+    enters the FP64 law as given; the decisions and the f32 law use its f32
+    rounding. Pass float(np.float32(v)) to compare with a device run.
     """
     x, y = _f32(x), _f32(y)
     n = len(x)
     fx, fy = np.empty(n), np.empty(n)
+    fx32, fy32 = np.empty(n, np.float32), np.empty(n, np.float32)
     keys = np.empty(n, np.uint32)
     perm = np.empty(n, np.int32)
     root = np.empty(3, np.float32)
@@ -280,8 +300,9 @@ def bh_forces(x, y, k=0.5, theta=0.5, min_dist=0.1, threads=1):
     lib().or_bh_forces(n, _p(x, C.c_float), _p(y, C.c_float), k, theta, min_dist,
                        _p(fx, C.c_double), _p(fy, C.c_double), _p(keys, C.c_uint32),
                        _p(perm, C.c_int32), _p(root, C.c_float), _p(inter, C.c_int64),
-                       threads)
-    return dict(fx=fx, fy=fy, keys=keys, perm=perm, root=root, interactions=inter)
+                       threads, _p(fx32, C.c_float), _p(fy32, C.c_float))
+    return dict(fx=fx, fy=fy, fx32=fx32, fy32=fy32, keys=keys, perm=perm, root=root,
+                interactions=inter)
 
 
 def repulsion_exact(x, y, k=0.5, min_dist=0.1):
@@ -293,17 +314,21 @@ def repulsion_exact(x, y, k=0.5, min_dist=0.1):
     return fx, fy
 
 
-def bh_reference(x, y, k=0.5, theta=0.5, min_dist=0.1, threads=1):
-    """Forces from the reference's own BarnesHutTree.cpp (unit charges)."""
+def bh_reference(x, y, k=0.5, theta=0.5, min_dist=0.1, threads=1, stride=1):
+    """Forces from the reference's own BarnesHutTree.cpp (unit charges).
+
+    stride > 1 evaluates only every stride-th point (a timing sample; the
+    other entries are left as zero)."""
     R = ref_lib()
     if R is None:
         return None
     px = np.ascontiguousarray(x, np.float64)
     py = np.ascontiguousarray(y, np.float64)
     q = np.ones(len(px))
-    fx, fy = np.empty(len(px)), np.empty(len(px))
-    R.bh_ref_forces(len(px), _p(px, C.c_double), _p(py, C.c_double), _p(q, C.c_double),
-                    theta, k, min_dist, _p(fx, C.c_double), _p(fy, C.c_double), threads)
+    fx, fy = np.zeros(len(px)), np.zeros(len(px))
+    R.bh_ref_forces_sample(len(px), _p(px, C.c_double), _p(py, C.c_double),
+                           _p(q, C.c_double), theta, k, min_dist, _p(fx, C.c_double),
+                           _p(fy, C.c_double), threads, stride)
     return fx, fy
 
 

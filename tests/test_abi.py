@@ -95,3 +95,24 @@ def test_synth_leaves_shape(fx):
     first = leaf_of[c.net_gate[c.net_ptr[:-1]]]
     assert np.all(leaf_of[c.net_gate] == np.repeat(first, deg))
     assert abs(c.num_nets / c.num_gates - 1.5) < 0.02
+
+
+def test_adjacency_order_matches_reference(fx, oracle):
+    # circuit.rs:154-171: the product's host builder reproduces the reference's
+    # lists in insertion order, including nets that name a gate twice.
+    s = fx.synth_plain(5, 3000, 3600, 60.0)
+    ap, ai = fx.build_adjacency(s.circuit)
+    rp, ri = oracle.build_adjacency(3000, s.circuit.net_ptr, s.circuit.net_gate)
+    assert np.array_equal(ap, rp) and np.array_equal(ai, ri)
+    nets = [[0, 1, 0, 2], [2, 2], [3, 1, 3, 3, 0], [4], [], [1, 4, 1]]
+    c = fx.Circuit.from_nets(nets, 5)
+    ap, ai = fx.build_adjacency(c)
+    rp, ri = oracle.build_adjacency(5, c.net_ptr, c.net_gate)
+    assert np.array_equal(ap, rp) and np.array_equal(ai, ri)
+
+
+def test_adjacency_rejects_bad_csr(fx):
+    import pytest
+    c = fx.Circuit.from_nets([[0, 7]], 3)
+    with pytest.raises(fx.FluxionError):
+        fx.build_adjacency(c)

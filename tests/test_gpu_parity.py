@@ -39,7 +39,9 @@ def test_congestion_bit_exact(small_design, plain_small, oracle, cols, rows):
     _, _, cap = oracle.grid_geometry(c.chip_width, c.chip_height, cols, rows)
     rt, rm = oracle.overflow(h, v, cols, rows, cap)
     assert mx == rm
-    assert abs(tot - rt) <= 1e-5 * max(rt, 1.0)
+    ov = np.maximum((h + v) - np.float32(cap), np.float32(0)).astype(np.float64)
+    assert abs(tot - ov.sum()) <= 1e-12 * max(ov.sum(), 1.0)  # FP64 recomputation
+    assert abs(tot - rt) <= 5e-3 * max(rt, 1.0)  # the reference's f32 running sum
     # the reference's own f32 running sum stays within 0.5 %
     assert abs(hpwl - oracle.hpwl_f32(c.net_ptr, c.net_gate, p.gate_x, p.gate_y)) <= 5e-3 * ref
 
@@ -88,14 +90,21 @@ def test_adjacency_matches_reference(small_design, plain_small, oracle):
         assert sorted(ai[ap[g]:ap[g + 1]]) == sorted(ri[rp[g]:rp[g + 1]])
 
 
-def test_attraction_vs_fp64(small_design, plain_small, oracle):
-    p = plain_small.placement
+def test_adjacency_order_is_reference_order(small_design, plain_small, oracle):
+    c = plain_small.circuit
     ap, ai = small_design.adjacency()
+    rp, ri = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    assert np.array_equal(ap, rp) and np.array_equal(ai, ri)
+
+
+def test_attraction_bit_exact_and_vs_fp64(small_design, plain_small, oracle):
+    p, c = plain_small.placement, plain_small.circuit
+    rp, ri = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
     fx_, fy_ = small_design.attraction(1.0)
-    rx, ry = oracle.attraction_f64(ap, ai, p.gate_x, p.gate_y, 1.0)
+    sx, sy = oracle.attraction_f32(rp, ri, p.gate_x, p.gate_y, 1.0)
+    assert np.array_equal(fx_, sx) and np.array_equal(fy_, sy)  # reference f32 order
+    rx, ry = oracle.attraction_f64(rp, ri, p.gate_x, p.gate_y, 1.0)
     assert rel_l2(fx_, fy_, rx, ry) < 1e-5
-    sx, sy = oracle.attraction_f32(ap, ai, p.gate_x, p.gate_y, 1.0)
-    assert rel_l2(sx, sy, rx, ry) < 1e-5  # the reference's own f32 order
 
 
 # ---- row B ---------------------------------------------------------------------
@@ -106,7 +115,8 @@ def _bh_check(d, x, y, oracle, k=0.5, theta=0.5):
     assert np.array_equal(root, o["root"])
     assert np.array_equal(keys, o["keys"])  # Morton keys bit-exact
     assert np.array_equal(perm, o["perm"])  # stable sort order exact
-    assert rel_l2(bx, by, o["fx"], o["fy"]) < 1e-5
+    assert np.array_equal(bx, o["fx32"]) and np.array_equal(by, o["fy32"])  # bit-exact
+    assert rel_l2(bx, by, o["fx"], o["fy"]) < 1e-5  # FP64, same interaction list
     return bx, by
 
 
@@ -181,11 +191,22 @@ def test_density_simt_vs_fp64(fx, ctx, oracle, G):
 
 
 # ---- rows A+B+E+D+F: the plain-small run ------------------------------------------
+def _oracle_run(oracle, c, x0, y0, iters, box):
+    rp, ri = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    ox, oy = x0.copy(), y0.copy()
+    vx, vy = np.zeros_like(ox), np.zeros_like(oy)
+    for _ in range(iters):
+        fa_x, fa_y = oracle.attraction_f32(rp, ri, ox, oy, 1.0)
+        b = oracle.bh_forces(ox, oy, 0.5, 0.5, F32_01)
+        oracle.integrate(ox, oy, vx, vy, fa_x + b["fx32"], fa_y + b["fy32"], 0.1, 0.9, box)
+    return ox, oy
+
+
 def test_plain_small_run_matches_oracle(fx, ctx, plain_small, oracle):
     """200 iterations of attraction (k=1) + Barnes-Hut (theta 0.5) + damped
-    step on the 10k-gate netlist, 64 x 64 congestion: final HPWL and overflow
-    within 0.5 % of the oracle's own run; congestion bit-exact on the final
-    device positions."""
+    step on the 10k-gate netlist with 64 x 64 congestion: the device run and
+    the oracle's run end on bit-identical positions, so HPWL and overflow
+    agree exactly (the 0.5 % bar is met with zero error)."""
     c, p = plain_small.circuit, plain_small.placement
     iters = 200
     cfg = fx.iter_cfg(density_bins=0, cong_cols=64, cong_rows=64)
@@ -193,25 +214,36 @@ def test_plain_small_run_matches_oracle(fx, ctx, plain_small, oracle):
     try:
         x = p.gate_x.copy(); y = p.gate_y.copy()
         st = d.force_iterate(cfg, iters, x, y)
-        ap, ai = d.adjacency()
-        counts, hpwl, tot, _ = d.congestion(64, 64, x, y)
+        counts, hpwl, tot, mx = d.congestion(64, 64, x, y)
     finally:
         d.close()
-    assert st.hpwl == hpwl
-    h, _ = oracle.congestion(c.net_ptr, c.net_gate, x, y, c.chip_width, c.chip_height, 64, 64)
+    assert st.hpwl == hpwl and st.total_overflow == tot
+    ox, oy = _oracle_run(oracle, c, p.gate_x, p.gate_y, iters, (0.0, 0.0, 120.0, 120.0))
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
+    h, v = oracle.congestion(c.net_ptr, c.net_gate, ox, oy, c.chip_width, c.chip_height, 64, 64)
     assert np.array_equal(counts.astype(np.float32), h)
-    # the oracle's own run
-    ox = p.gate_x.copy(); oy = p.gate_y.copy()
-    vx = np.zeros_like(ox); vy = np.zeros_like(oy)
-    for _ in range(iters):
-        fa_x, fa_y = oracle.attraction_f32(ap, ai, ox, oy, 1.0)
-        b = oracle.bh_forces(ox, oy, 0.5, 0.5, F32_01)
-        Fx = fa_x + b["fx"].astype(np.float32)
-        Fy = fa_y + b["fy"].astype(np.float32)
-        oracle.integrate(ox, oy, vx, vy, Fx, Fy, 0.1, 0.9, (0.0, 0.0, 120.0, 120.0))
     ref_hpwl = oracle.hpwl_f64(c.net_ptr, c.net_gate, ox, oy)
-    assert abs(hpwl - ref_hpwl) <= 5e-3 * ref_hpwl, (hpwl, ref_hpwl)
-    oh, ov = oracle.congestion(c.net_ptr, c.net_gate, ox, oy, c.chip_width, c.chip_height, 64, 64)
+    assert abs(hpwl - ref_hpwl) <= 1e-12 * ref_hpwl
     _, _, cap = oracle.grid_geometry(c.chip_width, c.chip_height, 64, 64)
-    rt, _ = oracle.overflow(oh, ov, 64, 64, cap)
-    assert abs(tot - rt) <= 5e-3 * max(rt, 1.0), (tot, rt)
+    rt, rm = oracle.overflow(h, v, 64, 64, cap)
+    assert mx == rm and abs(tot - rt) <= 5e-3 * max(rt, 1.0)
+    # the reference's own f32 HPWL of the same positions, within 0.5 %
+    assert abs(hpwl - oracle.hpwl_f32(c.net_ptr, c.net_gate, ox, oy)) <= 5e-3 * ref_hpwl
+
+
+def test_plain_iteration_is_deterministic(fx, ctx):
+    """The full composite iteration (with the DCT density term) gives
+    bit-identical positions when repeated."""
+    s = fx.synth_plain(3, 30_000, 36_000, 208.0)
+    cfg = fx.iter_cfg(density_bins=256, cong_cols=128, cong_rows=128)
+    d = fx.Design(ctx, s.circuit)
+    try:
+        out = []
+        for _ in range(2):
+            x = s.placement.gate_x.copy(); y = s.placement.gate_y.copy()
+            st = d.force_iterate(cfg, 12, x, y)
+            out.append((x, y, st.hpwl, st.total_overflow, st.density_energy))
+    finally:
+        d.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2:] == out[1][2:]
