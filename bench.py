@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--die", type=float, default=1200.0)
     ap.add_argument("--bins", type=int, default=1024)
     ap.add_argument("--cong", type=int, default=512)
-    ap.add_argument("--precision", default="simt", choices=["fp32", "tf32", "bf16", "simt"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "tf32", "bf16", "simt"])
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -59,8 +59,9 @@ def parse():
 
 
 PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "simt": 3}
-PREC_DTYPE = {"fp32": "f32 (DCT 3xTF32)", "tf32": "f32 (DCT TF32)",
-              "bf16": "f32 (DCT BF16)", "simt": "f32"}
+PREC_DTYPE = {"fp32": "f32 (DCT GEMMs 3xTF32, FP32 accumulate)",
+              "tf32": "f32 (DCT GEMMs TF32, FP32 accumulate)",
+              "bf16": "f32 (DCT GEMMs BF16, FP32 accumulate)", "simt": "f32"}
 
 
 # ---------------------------------------------------------------------------

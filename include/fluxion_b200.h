@@ -192,6 +192,39 @@ int fx_stage_density(fx_ctx *ctx, fx_design *design, int32_t bins,
                      float *out_phi, float *out_ex, float *out_ey,
                      double *out_energy);
 
+/* ---- row H: batched leaf placement --------------------------------------- */
+typedef struct fx_leaf_cfg {
+  int32_t force_iterations; /* PlacerConfig::force_iterations (default 50)    */
+  float attract_weight;     /* placer.rs:250 (1.0)                            */
+  float repel_weight;       /* placer.rs:264 (0.5)                            */
+  float damping;            /* placer.rs:276 (0.9)                            */
+  float dt;                 /* placer.rs:276-279 (0.1)                        */
+  int32_t schedule;         /* FX_LEAF_*                                      */
+  int32_t reserved0, reserved1;
+} fx_leaf_cfg;
+
+#define FX_LEAF_AUTO        0 /* time the schedules once, keep the fastest   */
+#define FX_LEAF_WARP        1 /* one warp per leaf, 8 leaves per block        */
+#define FX_LEAF_CTA64       2 /* 64 threads per leaf                          */
+#define FX_LEAF_CTA128      3 /* 128 threads per leaf                         */
+#define FX_LEAF_CTA256      4 /* one 256-thread block per leaf                */
+#define FX_LEAF_PER_CLUSTER 5 /* baseline: one kernel launch per leaf         */
+
+int fx_leaf_cfg_default(fx_leaf_cfg *cfg);
+
+/* Places every leaf with place_gates_in_leaf (H/src/algorithm/placer.rs:
+ * 210-287) -- the leaf loop of hapr_placement (placer.rs:65-69) -- in one
+ * persistent launch. Leaf l holds the gates leaf_gate[leaf_ptr[l] ..
+ * leaf_ptr[l+1]-1] (at most 512) and the region (cx, cy, w, h) =
+ * region[4l..4l+3]. Attraction uses the design's adjacency restricted to the
+ * leaf. Results are bit-identical to the reference's f32 loop. out_x/out_y
+ * (length N) are in/out: leaf gates are overwritten, other gates keep their
+ * values. out_schedule (may be NULL) receives the schedule used. */
+int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *design, int32_t n_leaves,
+                         const int32_t *leaf_ptr, const int32_t *leaf_gate,
+                         const float *region, const fx_leaf_cfg *cfg,
+                         float *out_x, float *out_y, int32_t *out_schedule);
+
 /* ---- host-only helpers (no GPU needed) ---------------------------------- */
 /* Builds the deduplicated clique-expansion adjacency of
  * Circuit::build_adjacency (H/src/data/circuit.rs:154-171) in the

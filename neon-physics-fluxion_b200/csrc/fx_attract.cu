@@ -132,7 +132,7 @@ fused_step_kernel(StepArgs a) {
       const float q = a.area[g];
       fx = __fadd_rn(fx, __fmul_rn(__fmul_rn(q, a.ex[bi]), a.dweight));
       fy = __fadd_rn(fy, __fmul_rn(__fmul_rn(q, a.ey[bi]), a.dweight));
-      e_acc = 0.5 * (double)q * (double)a.phi[bi] * (double)a.dweight;
+      if (a.phi) e_acc = 0.5 * (double)q * (double)a.phi[bi] * (double)a.dweight;
     }
     const float vx = __fmul_rn(__fadd_rn(a.vx[g], __fmul_rn(fx, a.dt)), a.damp);
     const float vy = __fmul_rn(__fadd_rn(a.vy[g], __fmul_rn(fy, a.dt)), a.damp);
@@ -263,7 +263,7 @@ extern "C" int fx_iter_cfg_default(fx_iter_cfg *c) {
   c->density_weight = 1.0e-4f;
   c->target_density = 0.7f;
   c->density_bins = 1024;
-  c->dct_precision = FX_DCT_SIMT;
+  c->dct_precision = FX_DCT_FP32;
   c->cong_cols = 512;
   c->cong_rows = 512;
   c->damping = 0.9f;
@@ -290,7 +290,8 @@ extern "C" int fx_stage_attraction(fx_ctx *ctx, fx_design *d, float k,
 
 namespace fx {
 int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
-                int precision, cudaStream_t s);
+                int precision, bool need_phi, cudaStream_t s);
+int gemm_tc_error(unsigned int *out, cudaStream_t s);
 }
 
 extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
@@ -321,8 +322,9 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     if (use_dens) {
       FX_CHECK_CUDA(cudaEventRecord(ctx->fork, s));
       FX_CHECK_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
+      // the potential only feeds the energy statistic of the last step
       FX_TRY(density_run(ctx, d, G, c.target_density, c.density_weight,
-                         c.dct_precision, s2));
+                         c.dct_precision, it == iters - 1, s2));
       FX_CHECK_CUDA(cudaEventRecord(ctx->join, s2));
     }
     if (use_bh) FX_TRY(bh_run(ctx, d, c.repel_weight, c.theta, c.min_dist, s));
@@ -343,7 +345,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     if (use_dens) {
       a.ex = d->dens.ex.p;
       a.ey = d->dens.ey.p;
-      a.phi = d->dens.buf[3].p;
+      a.phi = it == iters - 1 ? d->dens.buf[3].p : nullptr;
       a.area = d->area.p;
       a.G = G;
       a.bw = d->chip_w / (float)G;
@@ -391,6 +393,14 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   if (err) {
     set_error("Barnes-Hut walk stack overflow");
     return FX_EINVAL;
+  }
+  if (use_dens && c.dct_precision != FX_DCT_SIMT) {
+    unsigned int tc_err = 0;
+    FX_TRY(gemm_tc_error(&tc_err, s));
+    if (tc_err) {
+      set_error("tensor-core GEMM: a bounded wait expired (error word %u)", tc_err);
+      return FX_ETIMEOUT;
+    }
   }
   st.hpwl = res[0];
   st.total_overflow = res[1];

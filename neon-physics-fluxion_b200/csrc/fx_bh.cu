@@ -24,9 +24,9 @@
 //
 // Every value is fixed by the sorted keys alone: node mass sums are added in
 // tree order (left + right, FP64) by a bottom-up sweep, decisions and forces
-// use IEEE f32 operations without contraction (sqrt and reciprocal correctly
-// rounded), and each point adds its terms in depth-first order (left child
-// first). The result is bit-identical run to run and to a sequential
+// use IEEE f32 operations without contraction (the inverse square root is a
+// fixed bit-level estimate plus Newton steps), and each point adds its terms
+// in a fixed order. The result is bit-identical run to run and to a sequential
 // restatement of the same rules.
 #include <algorithm>
 #include <climits>
@@ -464,11 +464,26 @@ __global__ void bh_qchild_kernel(int n, const int32_t *__restrict__ child,
 // buckets point by point), and then descends into the children it opened, in
 // order.
 
-// The law k*Q/d^2 along (dx, dy)/d with d = max(|r|, min_dist), in IEEE f32:
-// inv = 1/sqrt(max(r2, md^2)), f = ((kQ * inv) * inv) * inv, F += f * r.
+// 1/sqrt(x) for x >= min_dist^2 > 0: the bit-level estimate of Lomont
+// ("Fast inverse square root", 2003; constant 0x5f375a86) refined by three
+// Newton steps y <- y * (1.5 - (x/2) * y * y) in IEEE f32 without
+// contraction. Integer ops and correctly rounded products only, so a
+// sequential restatement reproduces it bit for bit; the result is within a
+// couple of ulp of the exact value.
+__device__ __forceinline__ float bh_rsqrt(float x) {
+  float y = __int_as_float(0x5f375a86 - (__float_as_int(x) >> 1));
+  const float h = __fmul_rn(0.5f, x);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    y = __fmul_rn(y, __fsub_rn(1.5f, __fmul_rn(__fmul_rn(h, y), y)));
+  return y;
+}
+
+// The law k*Q/d^2 along (dx, dy)/d with d = max(|r|, min_dist), in f32:
+// inv = rsqrt(max(r2, md^2)), f = ((kQ * inv) * inv) * inv, F += f * r.
 __device__ __forceinline__ void bh_term(float dx, float dy, float r2c, float kq,
                                         float &fx, float &fy) {
-  const float inv = __frcp_rn(__fsqrt_rn(r2c));
+  const float inv = bh_rsqrt(r2c);
   const float f = __fmul_rn(__fmul_rn(__fmul_rn(kq, inv), inv), inv);
   fx = __fadd_rn(fx, __fmul_rn(f, dx));
   fy = __fadd_rn(fy, __fmul_rn(f, dy));

@@ -9,13 +9,12 @@
 //                [0,0] := 1, phi_hat = -rho_hat / lambda, phi_hat[0,0] := 0
 //                                                                (:72-86)
 //   potential    phi = IDCT_ortho(phi_hat) = C^T phi_hat C       (:89)
-//   field        centred differences inside, one-sided at edges  (:91-103)
+//   field        centred differences inside, one-sided at edges  (:91-103),
+//                applied as the operator products Dx C^T / Dy C^T
 //   force        F_i = area_i * E[row, col] * weight             (:134-150)
-// C is the orthonormal DCT-II matrix (G x G). The four transforms are NT
-// GEMMs D = A * B^T with A in {C, C^T} (constant) and B the data produced by
-// the previous stage:
-//   T1^T = C * rho^T ; rho_hat = C * T1 (epilogue: * -1/lambda) ;
-//   T3^T = C^T * phi_hat^T ; phi = C^T * T3.
+// C is the orthonormal DCT-II matrix (G x G). The transforms are NT GEMMs
+// D = A * B^T with A a constant operator and B the data produced by the
+// previous GEMM (see density_run).
 // Bin areas are accumulated as 64-bit fixed point so the density is exact
 // and independent of the scatter order.
 #include <cmath>
@@ -25,6 +24,8 @@
 #include "fx_gemm.cuh"
 
 namespace fx {
+
+int gemm_tc_error(unsigned int *out, cudaStream_t s);
 
 constexpr double kAreaScale = 4294967296.0;  // 2^32
 
@@ -67,33 +68,6 @@ __global__ void dens_charge_kernel(unsigned long long *__restrict__ acc,
   }
 }
 
-// E = -grad(phi) with the reference's stencils (force_electrostatic.py:
-// 96-103), evaluated in f32 in the same operation order.
-__global__ void dens_field_kernel(const float *__restrict__ phi, int G,
-                                  float wx, float wy, float *__restrict__ ex,
-                                  float *__restrict__ ey) {
-  const int cells = G * G;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cells;
-       i += gridDim.x * blockDim.x) {
-    const int r = i / G, c = i - r * G;
-    float e;
-    if (c == 0)
-      e = -__fmul_rn(__fsub_rn(phi[i + 1], phi[i]), wx);
-    else if (c == G - 1)
-      e = -__fmul_rn(__fsub_rn(phi[i], phi[i - 1]), wx);
-    else
-      e = __fmul_rn(__fmul_rn(-__fsub_rn(phi[i + 1], phi[i - 1]), wx), 0.5f);
-    ex[i] = e;
-    if (r == 0)
-      e = -__fmul_rn(__fsub_rn(phi[i + G], phi[i]), wy);
-    else if (r == G - 1)
-      e = -__fmul_rn(__fsub_rn(phi[i], phi[i - G]), wy);
-    else
-      e = __fmul_rn(__fmul_rn(-__fsub_rn(phi[i + G], phi[i - G]), wy), 0.5f);
-    ey[i] = e;
-  }
-}
-
 // Per-gate force and the FP64 energy 0.5 * sum q * phi (force_electrostatic.
 // py:134-150).
 __global__ void dens_gather_kernel(const float *__restrict__ x,
@@ -120,7 +94,40 @@ __global__ void dens_gather_kernel(const float *__restrict__ x,
   last_block_sum(block_sum_double(e) * (double)weight, partial, done, energy);
 }
 
-// Host: DCT matrices and the inverse eigenvalues, in FP64 then rounded.
+// Uploads a constant G x G operand computed in FP64 in the formats of
+// `precision`: f32 values (SIMT, TF32), TF32 head + residual (3xTF32), bf16.
+static int upload_operand(const std::vector<double> &m, int precision, float *f32,
+                          float *lo, uint16_t *bf, cudaStream_t s) {
+  const size_t cells = m.size();
+  std::vector<float> hi(cells), rl;
+  std::vector<uint16_t> hb;
+  if (precision == FX_DCT_FP32) rl.resize(cells);
+  if (precision == FX_DCT_BF16) hb.resize(cells);
+  for (size_t i = 0; i < cells; ++i) {
+    const float v = (float)m[i];
+    if (precision == FX_DCT_FP32) {
+      hi[i] = tf32_hi_host(v);
+      rl[i] = v - hi[i];
+    } else {
+      hi[i] = v;
+    }
+    if (precision == FX_DCT_BF16) hb[i] = bf16_host(v);
+  }
+  FX_CHECK_CUDA(cudaMemcpyAsync(f32, hi.data(), cells * 4, cudaMemcpyHostToDevice, s));
+  if (lo) FX_CHECK_CUDA(cudaMemcpyAsync(lo, rl.data(), cells * 4, cudaMemcpyHostToDevice, s));
+  if (bf) FX_CHECK_CUDA(cudaMemcpyAsync(bf, hb.data(), cells * 2, cudaMemcpyHostToDevice, s));
+  return cudaStreamSynchronize(s) == cudaSuccess ? FX_OK : FX_ECUDA;
+}
+
+// Host: DCT matrix C, the inverse eigenvalues and the field operators
+// Dx C^T, Dy C^T, in FP64 then rounded. Dx is the reference's x stencil
+// (force_electrostatic.py:96-103) as a matrix on a row of phi:
+// E_x[r][c] = sum_c' phi[r][c'] Dx[c][c'] with -wx/2 (phi[c+1] - phi[c-1])
+// inside and -wx (phi[1] - phi[0]), -wx (phi[G-1] - phi[G-2]) at the edges;
+// Dy likewise on columns. Since phi = C^T phi_hat C, the field is
+//   E_x = C^T (phi_hat (Dx C^T)^T),   E_y = (Dy C^T) (phi_hat C),
+// the same linear map as differencing phi, without forming the difference
+// of a large smooth potential in f32.
 static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   DensityWork &w = d->dens;
   if (w.G == G && w.precision == precision && w.cmat.p) return FX_OK;
@@ -128,31 +135,35 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   FX_TRY(w.area_fx.alloc(cells));
   FX_TRY(w.cmat.alloc(cells));
   FX_TRY(w.cmat_t.alloc(cells));
+  FX_TRY(w.dxct.alloc(cells));
+  FX_TRY(w.dyct.alloc(cells));
   FX_TRY(w.inv_eig.alloc(cells));
-  for (int i = 0; i < 4; ++i) FX_TRY(w.buf[i].alloc(cells));
+  for (int i = 0; i < 5; ++i) FX_TRY(w.buf[i].alloc(cells));
   FX_TRY(w.ex.alloc(cells));
   FX_TRY(w.ey.alloc(cells));
   FX_TRY(w.energy.alloc(4096 + 8));
   FX_TRY(w.force.alloc((size_t)d->n));
-  if (precision == FX_DCT_FP32) {
+  const bool split = precision == FX_DCT_FP32, half = precision == FX_DCT_BF16;
+  if (split) {
     FX_TRY(w.cmat_lo.alloc(cells));
     FX_TRY(w.cmat_t_lo.alloc(cells));
-    for (int i = 0; i < 3; ++i) FX_TRY(w.lo[i].alloc(cells));
+    FX_TRY(w.dxct_lo.alloc(cells));
+    FX_TRY(w.dyct_lo.alloc(cells));
+    for (int i = 0; i < 4; ++i) FX_TRY(w.lo[i].alloc(cells));
   }
-  if (precision == FX_DCT_BF16) {
+  if (half) {
     FX_TRY(w.cmat_bf.alloc(cells));
     FX_TRY(w.cmat_t_bf.alloc(cells));
-    FX_TRY(w.bf[0].alloc(cells));
-    FX_TRY(w.bf[1].alloc(cells));
+    FX_TRY(w.dxct_bf.alloc(cells));
+    FX_TRY(w.dyct_bf.alloc(cells));
+    for (int i = 0; i < 3; ++i) FX_TRY(w.bf[i].alloc(cells));
   }
-  std::vector<float> c(cells), ct(cells), ie(cells);
-  std::vector<float> clo, ctlo;
-  std::vector<uint16_t> cbf, ctbf;
   const double pi = 3.14159265358979323846;
+  std::vector<double> c(cells), ct(cells), dx(cells), dy(cells);
   for (int k = 0; k < G; ++k) {
     const double sk = k == 0 ? std::sqrt(1.0 / G) : std::sqrt(2.0 / G);
     for (int n = 0; n < G; ++n) {
-      const float v = (float)(sk * std::cos(pi * (2.0 * n + 1.0) * k / (2.0 * G)));
+      const double v = sk * std::cos(pi * (2.0 * n + 1.0) * k / (2.0 * G));
       c[(size_t)k * G + n] = v;
       ct[(size_t)n * G + k] = v;
     }
@@ -160,6 +171,24 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   // wx = 1/bw with bw = die/G (force_electrostatic.py:126-128).
   const double bw = (double)(d->chip_w / (float)G), bh = (double)(d->chip_h / (float)G);
   const double wx = 1.0 / bw, wy = 1.0 / bh;
+  // (D C^T)[i][k] = sum_j D[i][j] C[k][j] with the two-point stencils.
+  auto stencil = [&](double wgt, std::vector<double> &out) {
+    for (int i = 0; i < G; ++i)
+      for (int k = 0; k < G; ++k) {
+        const double *ck = &c[(size_t)k * G];
+        double v;
+        if (i == 0)
+          v = -(ck[1] - ck[0]) * wgt;
+        else if (i == G - 1)
+          v = -(ck[G - 1] - ck[G - 2]) * wgt;
+        else
+          v = -(ck[i + 1] - ck[i - 1]) * wgt * 0.5;
+        out[(size_t)i * G + k] = v;
+      }
+  };
+  stencil(wx, dx);
+  stencil(wy, dy);
+  std::vector<float> ie(cells);
   for (int ky = 0; ky < G; ++ky)
     for (int kx = 0; kx < G; ++kx) {
       const double ax = wx * std::cos(pi * kx / G) - wx;
@@ -168,37 +197,15 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
       if (kx == 0 && ky == 0) lam = 1.0;
       ie[(size_t)ky * G + kx] = (kx == 0 && ky == 0) ? 0.0f : (float)(-1.0 / lam);
     }
-  FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat.p, c.data(), cells * 4, cudaMemcpyHostToDevice, s));
-  FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat_t.p, ct.data(), cells * 4, cudaMemcpyHostToDevice, s));
   FX_CHECK_CUDA(cudaMemcpyAsync(w.inv_eig.p, ie.data(), cells * 4, cudaMemcpyHostToDevice, s));
-  if (precision == FX_DCT_FP32) {
-    // 3xTF32: cmat holds the TF32 head of C, cmat_lo the exact residual.
-    clo.resize(cells);
-    ctlo.resize(cells);
-    for (int k = 0; k < G; ++k)
-      for (int n = 0; n < G; ++n) {
-        const float v = c[(size_t)k * G + n];
-        const float h = tf32_hi_host(v);
-        c[(size_t)k * G + n] = h;
-        ct[(size_t)n * G + k] = h;
-        clo[(size_t)k * G + n] = v - h;
-        ctlo[(size_t)n * G + k] = v - h;
-      }
-    FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat.p, c.data(), cells * 4, cudaMemcpyHostToDevice, s));
-    FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat_t.p, ct.data(), cells * 4, cudaMemcpyHostToDevice, s));
-    FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat_lo.p, clo.data(), cells * 4, cudaMemcpyHostToDevice, s));
-    FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat_t_lo.p, ctlo.data(), cells * 4, cudaMemcpyHostToDevice, s));
-  }
-  if (precision == FX_DCT_BF16) {
-    cbf.resize(cells);
-    ctbf.resize(cells);
-    for (size_t i = 0; i < cells; ++i) {
-      cbf[i] = bf16_host(c[i]);
-      ctbf[i] = bf16_host(ct[i]);
-    }
-    FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat_bf.p, cbf.data(), cells * 2, cudaMemcpyHostToDevice, s));
-    FX_CHECK_CUDA(cudaMemcpyAsync(w.cmat_t_bf.p, ctbf.data(), cells * 2, cudaMemcpyHostToDevice, s));
-  }
+  FX_TRY(upload_operand(c, precision, w.cmat.p, split ? w.cmat_lo.p : nullptr,
+                        half ? w.cmat_bf.p : nullptr, s));
+  FX_TRY(upload_operand(ct, precision, w.cmat_t.p, split ? w.cmat_t_lo.p : nullptr,
+                        half ? w.cmat_t_bf.p : nullptr, s));
+  FX_TRY(upload_operand(dx, precision, w.dxct.p, split ? w.dxct_lo.p : nullptr,
+                        half ? w.dxct_bf.p : nullptr, s));
+  FX_TRY(upload_operand(dy, precision, w.dyct.p, split ? w.dyct_lo.p : nullptr,
+                        half ? w.dyct_bf.p : nullptr, s));
   FX_CHECK_CUDA(cudaMemsetAsync(w.area_fx.p, 0, cells * 8, s));
   FX_CHECK_CUDA(cudaMemsetAsync(w.energy.p, 0, (4096 + 8) * 8, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
@@ -224,10 +231,14 @@ int density_scatter(fx_ctx *ctx, fx_design *d, const float *x, const float *y,
   return FX_OK;
 }
 
-// Charge grid -> phi -> field, from the accumulated areas (which are
-// consumed and re-armed).
+// Charge grid -> spectrum -> field (and the potential when need_phi), from
+// the accumulated areas (which are consumed and re-armed). Seven NT GEMMs
+// D = A B^T on G x G matrices, A always a constant operator:
+//   T1^T = C rho^T ; phi_hat = (C T1) * (-1/lambda) ;
+//   T3^T = C^T phi_hat^T ; E_y = (Dy C^T) T3 ;
+//   T4^T = (Dx C^T) phi_hat^T ; E_x = C^T T4 ; [phi = C^T T3].
 int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
-                int precision, cudaStream_t s) {
+                int precision, bool need_phi, cudaStream_t s) {
   (void)weight;
   FX_TRY(dens_setup(d, G, precision, s));
   DensityWork &w = d->dens;
@@ -237,35 +248,36 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
   cudaEvent_t ev;
   timer_begin(ctx, FX_STAGE_DENSITY, s, &ev);
   const int eb = ctx->num_sms * 8;
-  float *rho = w.buf[0].p, *t1 = w.buf[1].p, *phat = w.buf[2].p, *t3 = w.buf[1].p;
-  float *phi = w.buf[3].p;
   // Split (3xTF32) and bf16 operand copies exist only for their precision.
   const bool split = precision == FX_DCT_FP32, half = precision == FX_DCT_BF16;
   auto LO = [&](int i) { return split ? w.lo[i].p : nullptr; };
   auto BF = [&](int i) { return half ? w.bf[i].p : nullptr; };
+  auto K = [&](float *f, float *l, uint16_t *b) {
+    return GemmOperands{f, split ? l : nullptr, half ? b : nullptr};
+  };
   dens_charge_kernel<<<eb, 256, 0, s>>>(w.area_fx.p, cells, inv_bin_area, target,
-                                        rho, LO(2), BF(0));
+                                        w.buf[0].p, LO(2), BF(0));
   FX_CHECK_LAUNCH();
-  GemmOperands A{w.cmat.p, split ? w.cmat_lo.p : nullptr, half ? w.cmat_bf.p : nullptr};
-  GemmOperands At{w.cmat_t.p, split ? w.cmat_t_lo.p : nullptr,
-                  half ? w.cmat_t_bf.p : nullptr};
-  GemmOperands B0{rho, LO(2), BF(0)};
-  GemmOperands B1{t1, LO(1), BF(1)};
-  GemmOperands B2{phat, LO(0), BF(0)};
-  GemmOperands B3{t3, LO(1), BF(1)};
-  // T1^T = C rho^T
-  FX_TRY(gemm_nt(ctx, precision, G, A, B0, nullptr, B1, s));
-  // rho_hat = C T1, epilogue * (-1/lambda) -> phi_hat
-  FX_TRY(gemm_nt(ctx, precision, G, A, B1, w.inv_eig.p, B2, s));
-  // T3^T = C^T phi_hat^T
-  FX_TRY(gemm_nt(ctx, precision, G, At, B2, nullptr, B3, s));
-  // phi = C^T T3
-  GemmOperands P{phi, nullptr, nullptr};
-  FX_TRY(gemm_nt(ctx, precision, G, At, B3, nullptr, P, s));
-  dens_field_kernel<<<eb, 256, 0, s>>>(phi, G, (float)(1.0 / (double)bw),
-                                       (float)(1.0 / (double)bh), w.ex.p, w.ey.p);
-  FX_CHECK_LAUNCH();
-  ctx->launches += 2;
+  ctx->launches += 1;
+  const GemmOperands C = K(w.cmat.p, w.cmat_lo.p, w.cmat_bf.p);
+  const GemmOperands Ct = K(w.cmat_t.p, w.cmat_t_lo.p, w.cmat_t_bf.p);
+  const GemmOperands DxCt = K(w.dxct.p, w.dxct_lo.p, w.dxct_bf.p);
+  const GemmOperands DyCt = K(w.dyct.p, w.dyct_lo.p, w.dyct_bf.p);
+  const GemmOperands rho{w.buf[0].p, LO(2), BF(0)};
+  const GemmOperands t1{w.buf[1].p, LO(1), BF(1)};
+  const GemmOperands phat{w.buf[2].p, LO(0), BF(0)};
+  const GemmOperands t3{w.buf[1].p, LO(1), BF(1)};
+  const GemmOperands t4{w.buf[4].p, LO(3), BF(2)};
+  const GemmOperands ex{w.ex.p, nullptr, nullptr};
+  const GemmOperands ey{w.ey.p, nullptr, nullptr};
+  const GemmOperands phi{w.buf[3].p, nullptr, nullptr};
+  FX_TRY(gemm_nt(ctx, precision, G, C, rho, nullptr, t1, s));
+  FX_TRY(gemm_nt(ctx, precision, G, C, t1, w.inv_eig.p, phat, s));
+  FX_TRY(gemm_nt(ctx, precision, G, Ct, phat, nullptr, t3, s));
+  FX_TRY(gemm_nt(ctx, precision, G, DyCt, t3, nullptr, ey, s));
+  if (need_phi) FX_TRY(gemm_nt(ctx, precision, G, Ct, t3, nullptr, phi, s));
+  FX_TRY(gemm_nt(ctx, precision, G, DxCt, phat, nullptr, t4, s));
+  FX_TRY(gemm_nt(ctx, precision, G, Ct, t4, nullptr, ex, s));
   timer_end(ctx, FX_STAGE_DENSITY, s, ev);
   return FX_OK;
 }
@@ -304,23 +316,35 @@ extern "C" int fx_stage_density(fx_ctx *ctx, fx_design *d, int32_t bins,
   cudaStream_t s = ctx->stream;
   const float *x = d->x[d->cur].p, *y = d->y[d->cur].p;
   FX_TRY(density_scatter(ctx, d, x, y, bins, precision, s));
-  FX_TRY(density_run(ctx, d, bins, target_density, weight, precision, s));
+  FX_TRY(density_run(ctx, d, bins, target_density, weight, precision, true, s));
   FX_TRY(density_gather(ctx, d, x, y, bins, weight, s));
   DensityWork &w = d->dens;
   const size_t cells = (size_t)bins * bins, n = (size_t)d->n;
   std::vector<float2> f(n);
   double e = 0.0;
   FX_CHECK_CUDA(cudaMemcpyAsync(f.data(), w.force.p, n * 8, cudaMemcpyDeviceToHost, s));
+  std::vector<float> rho_lo;
   if (out_rho) FX_CHECK_CUDA(cudaMemcpyAsync(out_rho, w.buf[0].p, cells * 4, cudaMemcpyDeviceToHost, s));
+  if (out_rho && precision == FX_DCT_FP32) {
+    rho_lo.resize(cells);
+    FX_CHECK_CUDA(cudaMemcpyAsync(rho_lo.data(), w.lo[2].p, cells * 4, cudaMemcpyDeviceToHost, s));
+  }
   if (out_phi) FX_CHECK_CUDA(cudaMemcpyAsync(out_phi, w.buf[3].p, cells * 4, cudaMemcpyDeviceToHost, s));
   if (out_ex) FX_CHECK_CUDA(cudaMemcpyAsync(out_ex, w.ex.p, cells * 4, cudaMemcpyDeviceToHost, s));
   if (out_ey) FX_CHECK_CUDA(cudaMemcpyAsync(out_ey, w.ey.p, cells * 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaMemcpyAsync(&e, w.energy.p + 4097, 8, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  unsigned int tc_err = 0;
+  FX_TRY(gemm_tc_error(&tc_err, s));
+  if (tc_err) {
+    set_error("tensor-core GEMM: a bounded wait expired (error word %u)", tc_err);
+    return FX_ETIMEOUT;
+  }
   for (size_t i = 0; i < n; ++i) {
     if (out_fx) out_fx[i] = f[i].x;
     if (out_fy) out_fy[i] = f[i].y;
   }
+  for (size_t i = 0; i < rho_lo.size(); ++i) out_rho[i] += rho_lo[i];
   if (out_energy) *out_energy = e;
   return FX_OK;
 }

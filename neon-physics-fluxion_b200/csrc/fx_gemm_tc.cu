@@ -1,15 +1,425 @@
 // fx_gemm_tc.cu -- tensor-core (tcgen05) NT GEMMs for the DCT stage.
+//
+// D[i][j] = sum_k A[i][k] * B[j][k] for G x G row-major f32/bf16 matrices,
+// both operands K-major. One CTA computes a 128 x 128 tile of D:
+//   * warp 0 (one elected thread) streams 128 x 128-byte K slices of A and B
+//     into a ring of shared-memory stages with TMA (128B swizzle, no
+//     multicast), signalling a per-stage mbarrier with the transaction bytes;
+//   * warp 1 (one thread) issues tcgen05.mma (M = 128, N = 128, K = 32 bytes
+//     per instruction) into a 128-column TMEM accumulator and releases each
+//     stage with tcgen05.commit;
+//   * warp 2 owns the TMEM allocation;
+//   * all four warps drain TMEM with tcgen05.ld (warp w holds rows 32w..32w+31)
+//     and apply the optional element-wise scale S before storing.
+// Precisions: TF32 (kind::tf32, one product), BF16 (kind::f16 with bf16
+// operands, one product) and FP32 as 3xTF32: A = Ah + Al, B = Bh + Bl with the
+// heads rounded to TF32, D = Ah Bh + Ah Bl + Al Bh accumulated in FP32 (the
+// Al Bl term is below f32 resolution).
+// Every mbarrier wait is bounded: on expiry the CTA records an error, waits
+// (bounded) for its own TMA copies, frees TMEM and returns.
+#include <cuda.h>
+
+#include <mutex>
+#include <unordered_map>
+
 #include "fx_internal.h"
 #include "fx_gemm.cuh"
 
 namespace fx {
 
+constexpr int kTcBM = 128, kTcBN = 128, kTcThreads = 128;
+constexpr int kTileBytes = 128 * 128;  // one 128-row x 128-byte operand tile
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+// ---- PTX helpers ----------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of the given parity; false on expiry.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map,
+                                            uint32_t bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// K-major operand tile, 128-byte rows packed, 128B swizzle: SBO = 1024 bytes
+// (8-row swizzle atoms), LBO unused (16), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3ffffu) >> 4);
+  d |= (uint64_t)(16u >> 4) << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+template <int KIND>
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t a, uint64_t b,
+                                     uint32_t idesc, uint32_t accum) {
+  if (KIND == 0)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accum));
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accum));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          bar)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, "
+      "%9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, "
+      "%24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+        "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+        "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+        "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]),
+        "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// PREC: 0 = 3xTF32, 1 = TF32, 2 = BF16.
+template <int PREC>
+struct TcCfg {
+  static constexpr int kKind = PREC == 2 ? 1 : 0;          // 0 tf32, 1 f16
+  static constexpr int kElem = PREC == 2 ? 2 : 4;          // operand bytes
+  static constexpr int kKBlock = 128 / kElem;              // elements per slice
+  static constexpr int kTiles = PREC == 0 ? 4 : 2;         // tiles per stage
+  static constexpr int kStages = PREC == 0 ? 3 : 6;
+  static constexpr int kStageBytes = kTiles * kTileBytes;
+  static constexpr uint32_t kFmt = PREC == 2 ? 1u : 2u;    // bf16 : tf32
+  static constexpr uint32_t kIdesc = (1u << 4) | (kFmt << 7) | (kFmt << 10) |
+                                     ((uint32_t)(kTcBN >> 3) << 17) |
+                                     ((uint32_t)(kTcBM >> 4) << 24);
+  static constexpr int kSmem = 1024 + kStages * kStageBytes + 256;
+};
+
+template <int PREC>
+__global__ void __launch_bounds__(kTcThreads, 1)
+tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
+               const __grid_constant__ CUtensorMap tAlo,
+               const __grid_constant__ CUtensorMap tB,
+               const __grid_constant__ CUtensorMap tBlo, int G,
+               const float *__restrict__ S, float *__restrict__ D,
+               float *__restrict__ Dlo, uint16_t *__restrict__ Dbf,
+               unsigned int *__restrict__ err) {
+  using Cfg = TcCfg<PREC>;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-aligned stages
+  const uint32_t bar0 = base + Cfg::kStages * Cfg::kStageBytes;
+  // barriers: full[s] at bar0 + 8s, empty[s] at bar0 + 64 + 8s, done at +128
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 64u + 8u * s; };
+  const uint32_t done_bar = bar0 + 128u;
+  const uint32_t tmem_slot = bar0 + 136u;
+  const uint32_t abort_slot = bar0 + 140u;
+  uint8_t *gen_base = smem_raw + (base - raw);
+  volatile uint32_t *tmem_ptr = (volatile uint32_t *)(gen_base + (tmem_slot - base));
+  volatile uint32_t *abort_flag = (volatile uint32_t *)(gen_base + (abort_slot - base));
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bm = blockIdx.y * kTcBM, bn = blockIdx.x * kTcBN;
+  const int KB = G / Cfg::kKBlock;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < Cfg::kStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0u;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tmem_slot),
+                 "r"(kTcBN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_ptr;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer --------------------------------------------------------
+    int issued = 0;
+    for (int kb = 0; kb < KB; ++kb) {
+      const int s = kb % Cfg::kStages;
+      const uint32_t ph = (uint32_t)(kb / Cfg::kStages) & 1u;
+      if (kb >= Cfg::kStages && !mbar_wait(empty_bar(s), ph ^ 1u)) {
+        *abort_flag = 1u;
+        atomicOr(err, 2u);
+        break;
+      }
+      if (*abort_flag) break;
+      const uint32_t st = base + s * Cfg::kStageBytes;
+      mbar_expect_tx(full_bar(s), Cfg::kStageBytes);
+      const int x = kb * Cfg::kKBlock;
+      tma_load_2d(st, &tA, full_bar(s), x, bm);
+      tma_load_2d(st + kTileBytes, &tB, full_bar(s), x, bn);
+      if (PREC == 0) {
+        tma_load_2d(st + 2 * kTileBytes, &tAlo, full_bar(s), x, bm);
+        tma_load_2d(st + 3 * kTileBytes, &tBlo, full_bar(s), x, bn);
+      }
+      issued = kb + 1;
+    }
+    // Before leaving, make sure none of this CTA's copies is still in flight.
+    const int first = issued > Cfg::kStages ? issued - Cfg::kStages : 0;
+    for (int kb = first; kb < issued; ++kb)
+      mbar_wait(full_bar(kb % Cfg::kStages), (uint32_t)(kb / Cfg::kStages) & 1u);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----------------------------------------------------------
+    bool ok = true;
+    for (int kb = 0; kb < KB; ++kb) {
+      const int s = kb % Cfg::kStages;
+      const uint32_t ph = (uint32_t)(kb / Cfg::kStages) & 1u;
+      if (!mbar_wait(full_bar(s), ph) || *abort_flag) {
+        *abort_flag = 1u;
+        atomicOr(err, 2u);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t st = base + s * Cfg::kStageBytes;
+      const uint64_t a = umma_desc(st), b = umma_desc(st + kTileBytes);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+        umma<Cfg::kKind>(tmem, a + 2u * k, b + 2u * k, Cfg::kIdesc, acc);
+        if (PREC == 0) {
+          const uint64_t alo = umma_desc(st + 2 * kTileBytes);
+          const uint64_t blo = umma_desc(st + 3 * kTileBytes);
+          umma<Cfg::kKind>(tmem, a + 2u * k, blo + 2u * k, Cfg::kIdesc, 1u);
+          umma<Cfg::kKind>(tmem, alo + 2u * k, b + 2u * k, Cfg::kIdesc, 1u);
+        }
+      }
+      umma_commit(empty_bar(s));
+    }
+    umma_commit(done_bar);
+    (void)ok;
+  }
+  // ---- epilogue: all warps ------------------------------------------------------
+  // tcgen05.ld is warp-collective: lane 0 waits and the warp follows its
+  // verdict.
+  __syncwarp();
+  uint32_t go = 0u;
+  if (lane == 0) {
+    const bool done_ok = mbar_wait(done_bar, 0u);
+    if (!done_ok) {
+      *abort_flag = 1u;
+      atomicOr(err, 2u);
+    }
+    go = (done_ok && !*abort_flag) ? 1u : 0u;
+  }
+  go = __shfl_sync(0xffffffffu, go, 0);
+  tc_fence_after();
+  if (go) {
+    const int r = bm + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      const size_t o = (size_t)r * G + bn + c0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        float x = __uint_as_float(v[j]);
+        if (S) x *= S[o + j];
+        store_operand(x, o + j, D, Dlo, Dbf);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcBN));
+  }
+}
+
+// ---- host: tensor maps -------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
+                                  void *, const cuuint64_t *, const cuuint64_t *,
+                                  const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  });
+  return fn;
+}
+
+// A G x G row-major operand as a 2-D tensor map with 128 x 128-byte boxes.
+static int make_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is unavailable");
+    return FX_ECUDA;
+  }
+  if (((uintptr_t)ptr & 15u) != 0) {
+    set_error("tensor map base not 16-byte aligned");
+    return FX_EINVAL;
+  }
+  const int esz = bf16 ? 2 : 4;
+  const cuuint64_t dims[2] = {(cuuint64_t)G, (cuuint64_t)G};
+  const cuuint64_t strides[1] = {(cuuint64_t)G * esz};
+  const cuuint32_t box[2] = {(cuuint32_t)(128 / esz), 128u};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r =
+      fn(out, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+         const_cast<void *>(ptr), dims, strides, box, estr,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return FX_ECUDA;
+  }
+  return FX_OK;
+}
+
+struct MapKey {
+  const void *p;
+  int G;
+  bool bf;
+  bool operator==(const MapKey &o) const { return p == o.p && G == o.G && bf == o.bf; }
+};
+struct MapKeyHash {
+  size_t operator()(const MapKey &k) const {
+    return std::hash<const void *>()(k.p) ^ ((size_t)k.G << 1) ^ (size_t)k.bf;
+  }
+};
+
+static int get_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
+  static std::mutex mu;
+  static std::unordered_map<MapKey, CUtensorMap, MapKeyHash> cache;
+  std::lock_guard<std::mutex> g(mu);
+  const MapKey k{ptr, G, bf16};
+  auto it = cache.find(k);
+  if (it != cache.end()) {
+    *out = it->second;
+    return FX_OK;
+  }
+  FX_TRY(make_map(ptr, G, bf16, out));
+  cache.emplace(k, *out);
+  return FX_OK;
+}
+
+static DevBuf<unsigned int> g_tc_err;
+
+template <int PREC>
+static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands &B,
+                  const float *S, const GemmOperands &D, cudaStream_t s) {
+  using Cfg = TcCfg<PREC>;
+  const bool bf = PREC == 2;
+  CUtensorMap ta, talo, tb, tblo;
+  const void *pa = bf ? (const void *)A.bf : (const void *)A.f32;
+  const void *pb = bf ? (const void *)B.bf : (const void *)B.f32;
+  if (!pa || !pb || (PREC == 0 && (!A.lo || !B.lo))) {
+    set_error("gemm_nt: operand format missing for precision %d", PREC);
+    return FX_EINVAL;
+  }
+  FX_TRY(get_map(pa, G, bf, &ta));
+  FX_TRY(get_map(pb, G, bf, &tb));
+  if (PREC == 0) {
+    FX_TRY(get_map(A.lo, G, false, &talo));
+    FX_TRY(get_map(B.lo, G, false, &tblo));
+  } else {
+    talo = ta;
+    tblo = tb;
+  }
+  static bool attr_set = false;
+  if (!attr_set) {
+    FX_CHECK_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<PREC>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       Cfg::kSmem));
+    attr_set = true;
+  }
+  if (!g_tc_err.p) {
+    FX_TRY(g_tc_err.alloc(1));
+    FX_CHECK_CUDA(cudaMemset(g_tc_err.p, 0, 4));
+  }
+  dim3 grid(G / kTcBN, G / kTcBM);
+  tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(ta, talo, tb, tblo, G, S, D.f32,
+                                                            D.lo, D.bf, g_tc_err.p);
+  FX_CHECK_LAUNCH();
+  ctx->launches += 1;
+  return FX_OK;
+}
+
 int gemm_nt_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
                const GemmOperands &B, const float *S, const GemmOperands &D,
                cudaStream_t s) {
-  (void)ctx; (void)G; (void)A; (void)B; (void)S; (void)D; (void)s;
-  set_error("gemm_nt: precision %d is not available in this build", precision);
+  switch (precision) {
+    case FX_DCT_FP32: return launch<0>(ctx, G, A, B, S, D, s);
+    case FX_DCT_TF32: return launch<1>(ctx, G, A, B, S, D, s);
+    case FX_DCT_BF16: return launch<2>(ctx, G, A, B, S, D, s);
+  }
+  set_error("gemm_nt: unknown precision %d", precision);
   return FX_EINVAL;
+}
+
+// Error word of the tensor-core GEMMs (bit 1: a bounded wait expired).
+int gemm_tc_error(unsigned int *out, cudaStream_t s) {
+  *out = 0;
+  if (!g_tc_err.p) return FX_OK;
+  FX_CHECK_CUDA(cudaMemcpyAsync(out, g_tc_err.p, 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  return FX_OK;
 }
 
 }  // namespace fx

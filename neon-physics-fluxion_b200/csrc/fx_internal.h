@@ -124,16 +124,20 @@ struct DensityWork {
   DevBuf<float> cmat_t_lo;
   DevBuf<uint16_t> cmat_bf, cmat_t_bf; // bf16 copies
   DevBuf<float> inv_eig;               // -1/lambda with DC = 0 (G*G)
-  DevBuf<float> buf[4];                // rho, t1, t2, phi
-  DevBuf<float> lo[3];                 // low parts for 3xTF32 operands
-  DevBuf<uint16_t> bf[2];              // bf16 operand staging
+  DevBuf<float> dxct, dyct;            // stencil x C^T (field operators)
+  DevBuf<float> dxct_lo, dyct_lo;
+  DevBuf<uint16_t> dxct_bf, dyct_bf;
+  DevBuf<float> buf[5];                // rho, T1^T/T3^T, phi_hat, phi, T4^T
+  DevBuf<float> lo[4];                 // low parts for 3xTF32 operands
+  DevBuf<uint16_t> bf[3];              // bf16 operand staging
   DevBuf<float> ex, ey;                // field
   DevBuf<double> energy;               // FP64 partials
   DevBuf<float2> force;                // per gate
   template <class F>
   void for_each(F &&f) {
     f(area_fx); f(cmat); f(cmat_t); f(cmat_lo); f(cmat_t_lo); f(cmat_bf);
-    f(cmat_t_bf); f(inv_eig);
+    f(cmat_t_bf); f(inv_eig); f(dxct); f(dyct); f(dxct_lo); f(dyct_lo);
+    f(dxct_bf); f(dyct_bf);
     for (auto &b : buf) f(b);
     for (auto &b : lo) f(b);
     for (auto &b : bf) f(b);
@@ -181,6 +185,7 @@ struct fx_ctx {
   fx::StageTimer timer;
   int64_t launches = 0;
   cudaEvent_t marks[16] = {};
+  int leaf_schedule = 0;           // last autotuned leaf schedule
 };
 
 struct fx_design {
@@ -214,7 +219,7 @@ int attraction_run(fx_ctx *ctx, fx_design *d, float k, float2 *out, cudaStream_t
 int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
            cudaStream_t s);
 int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
-                int precision, cudaStream_t s);
+                int precision, bool need_phi, cudaStream_t s);
 int fused_step(fx_ctx *ctx, fx_design *d, const fx_iter_cfg &cfg,
                cudaStream_t s);
 void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a);

@@ -1,0 +1,362 @@
+// fx_leaf.cu -- row H: batched leaf placement (place_gates_in_leaf for
+// thousands of independent leaf clusters in one persistent launch).
+//
+// Semantics are those of place_gates_in_leaf (H/src/algorithm/placer.rs:
+// 210-287), reproduced bit for bit:
+//   * init (placer.rs:226-227): x_i = min_x + (i/n) w,
+//     y_i = min_y + ((7i mod n)/n) h, velocities 0;
+//   * attraction (:243-255): for each neighbour of gate i in adjacency order
+//     that lies in the leaf, F_i += k (p_j - p_i);
+//   * repulsion (:258-272): the reference walks pairs i < j and adds the pair
+//     force to i and subtracts it from j, so gate j receives its terms in
+//     partner order m = 0..n-1. Each thread owns one gate and adds, in that
+//     order, f_jm = force * (p_j - p_m) / dist, which equals the reference's
+//     "-= fx_ij" exactly (IEEE subtraction of t equals addition of -t, and the
+//     products are sign-symmetric); sqrt and divisions are IEEE as in Rust;
+//   * damped step with clamp to the leaf box (:275-280).
+// Schedules: a group of T threads (T = 32, 64, 128 or 256) owns one leaf at a
+// time, looping over gates when n > T; groups pull leaves (largest first)
+// from an atomic work counter until the batch is done, running all
+// iterations of a leaf in shared memory. Every schedule gives identical
+// results, so the autotuner is free to pick the fastest.
+#include <algorithm>
+#include <numeric>
+#include <unordered_map>
+
+#include "fx_internal.h"
+
+namespace fx {
+
+constexpr int kLeafMax = 512;  // gates per leaf held in shared memory
+constexpr int kLeafArrays = 6;  // x, y, vx, vy, fx, fy
+
+struct LeafBatch {
+  const int32_t *gptr;     // [L+1] offsets into the gate list (leaf order)
+  const int32_t *gate;     // [G] global gate ids
+  const int32_t *aptr;     // [G+1] in-leaf adjacency row offsets
+  const int16_t *aidx;     // in-leaf neighbour local indices (reference order)
+  const float4 *region;    // [L] (cx, cy, w, h)
+  const int32_t *order;    // [L] leaves in processing order
+  int n_leaves;
+  int iters;
+  float k, repel, damping, dt;
+  float *out_x, *out_y;    // global positions (written for leaf gates)
+  unsigned int *counter;   // work counter
+};
+
+__device__ __forceinline__ float rclamp(float v, float lo, float hi) {
+  if (v < lo) v = lo;
+  if (v > hi) v = hi;
+  return v;
+}
+
+// Barrier of one T-thread group: the warp, the whole block, or a named
+// barrier (ids 1.. per group) for intermediate sizes.
+template <int T>
+__device__ __forceinline__ void group_sync(int id) {
+  if (T == 32)
+    __syncwarp();
+  else if (T == 256)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(T) : "memory");
+}
+
+// One leaf on a group of T threads (tid in [0, T)); sm: the group's shared
+// arrays x, y, vx, vy, fx, fy (kLeafMax each).
+template <int T>
+__device__ void place_leaf(const LeafBatch &b, int leaf, int tid, float *sm, int sid) {
+  float *sx = sm, *sy = sm + kLeafMax, *svx = sm + 2 * kLeafMax;
+  float *svy = sm + 3 * kLeafMax, *sfx = sm + 4 * kLeafMax, *sfy = sm + 5 * kLeafMax;
+  const int g0 = b.gptr[leaf];
+  const int n = b.gptr[leaf + 1] - g0;
+  if (n <= 0) return;
+  const float4 r = b.region[leaf];
+  const float half_w = r.z / 2.0f, half_h = r.w / 2.0f;
+  const float min_x = __fsub_rn(r.x, half_w), min_y = __fsub_rn(r.y, half_h);
+  const float max_x = __fadd_rn(min_x, r.z), max_y = __fadd_rn(min_y, r.w);
+  const float nf = (float)n;
+  for (int i = tid; i < n; i += T) {
+    sx[i] = __fadd_rn(min_x, __fmul_rn(__fdiv_rn((float)i, nf), r.z));
+    sy[i] = __fadd_rn(min_y, __fmul_rn(__fdiv_rn((float)((i * 7) % n), nf), r.w));
+    svx[i] = 0.f;
+    svy[i] = 0.f;
+  }
+  group_sync<T>(sid);
+  for (int it = 0; it < b.iters; ++it) {
+    for (int i = tid; i < n; i += T) {
+      const float xi = sx[i], yi = sy[i];
+      float ax = 0.f, ay = 0.f;
+      const int a0 = b.aptr[g0 + i], a1 = b.aptr[g0 + i + 1];
+      for (int e = a0; e < a1; ++e) {
+        const int j = b.aidx[e];
+        ax = __fadd_rn(ax, __fmul_rn(b.k, __fsub_rn(sx[j], xi)));
+        ay = __fadd_rn(ay, __fmul_rn(b.k, __fsub_rn(sy[j], yi)));
+      }
+      for (int m = 0; m < n; ++m) {
+        if (m == i) continue;
+        const float dx = __fsub_rn(xi, sx[m]), dy = __fsub_rn(yi, sy[m]);
+        const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
+        const float force = __fdiv_rn(b.repel, __fmul_rn(dist, dist));
+        ax = __fadd_rn(ax, __fdiv_rn(__fmul_rn(force, dx), dist));
+        ay = __fadd_rn(ay, __fdiv_rn(__fmul_rn(force, dy), dist));
+      }
+      sfx[i] = ax;
+      sfy[i] = ay;
+    }
+    group_sync<T>(sid);
+    for (int i = tid; i < n; i += T) {
+      const float vx = __fmul_rn(__fadd_rn(svx[i], __fmul_rn(sfx[i], b.dt)), b.damping);
+      const float vy = __fmul_rn(__fadd_rn(svy[i], __fmul_rn(sfy[i], b.dt)), b.damping);
+      svx[i] = vx;
+      svy[i] = vy;
+      sx[i] = rclamp(__fadd_rn(sx[i], __fmul_rn(vx, b.dt)), min_x, max_x);
+      sy[i] = rclamp(__fadd_rn(sy[i], __fmul_rn(vy, b.dt)), min_y, max_y);
+    }
+    group_sync<T>(sid);
+  }
+  for (int i = tid; i < n; i += T) {
+    const int g = b.gate[g0 + i];
+    b.out_x[g] = sx[i];
+    b.out_y[g] = sy[i];
+  }
+  group_sync<T>(sid);
+}
+
+// T threads per leaf; the 256-thread block holds 256 / T groups.
+template <int T>
+__global__ void __launch_bounds__(256)
+leaf_batch_kernel(LeafBatch b, int per_cluster_leaf) {
+  extern __shared__ float lsm[];
+  constexpr int kGroups = 256 / T;
+  const int grp = threadIdx.x / T, tid = threadIdx.x % T;
+  float *sm = lsm + grp * kLeafArrays * kLeafMax;
+  const int sid = 1 + grp;
+  if (per_cluster_leaf >= 0) {  // the one-launch-per-leaf baseline
+    if (grp == 0) place_leaf<T>(b, per_cluster_leaf, tid, sm, sid);
+    return;
+  }
+  __shared__ int next[kGroups];
+  while (true) {
+    if (tid == 0) {
+      const unsigned int w = atomicAdd(b.counter, 1u);
+      next[grp] = w < (unsigned)b.n_leaves ? b.order[w] : -1;
+    }
+    group_sync<T>(sid);
+    const int leaf = next[grp];
+    group_sync<T>(sid);
+    if (leaf < 0) break;
+    place_leaf<T>(b, leaf, tid, sm, sid);
+  }
+}
+
+// Host-side leaf structures: in-leaf adjacency in the reference's order and
+// a largest-first processing order.
+struct LeafHost {
+  std::vector<int32_t> aptr;
+  std::vector<int16_t> aidx;
+  std::vector<int32_t> order;
+};
+
+static int build_leaf_host(const fx_design *d, int L, const int32_t *leaf_ptr,
+                           const int32_t *leaf_gate, LeafHost &h) {
+  const int32_t G = leaf_ptr[L];
+  h.aptr.assign((size_t)G + 1, 0);
+  h.aidx.clear();
+  std::vector<int32_t> local((size_t)d->n, -1);
+  for (int l = 0; l < L; ++l) {
+    const int32_t b = leaf_ptr[l], e = leaf_ptr[l + 1];
+    if (e - b > kLeafMax) {
+      set_error("leaf %d has %d gates (limit %d)", l, e - b, kLeafMax);
+      return FX_EINVAL;
+    }
+    for (int32_t i = b; i < e; ++i) {
+      const int32_t g = leaf_gate[i];
+      if (g < 0 || g >= d->n) {
+        set_error("leaf gate %d out of range", g);
+        return FX_EINVAL;
+      }
+      local[g] = i - b;  // HashMap insert: a repeated gate keeps the last slot
+    }
+    for (int32_t i = b; i < e; ++i) {
+      const int32_t g = leaf_gate[i];
+      for (int32_t q = d->h_adj_ptr[g]; q < d->h_adj_ptr[g + 1]; ++q) {
+        const int32_t j = d->h_adj_idx[q];
+        if (local[j] >= 0) h.aidx.push_back((int16_t)local[j]);
+      }
+      h.aptr[(size_t)i + 1] = (int32_t)h.aidx.size();
+    }
+    for (int32_t i = b; i < e; ++i) local[leaf_gate[i]] = -1;
+  }
+  h.order.resize(L);
+  std::iota(h.order.begin(), h.order.end(), 0);
+  std::stable_sort(h.order.begin(), h.order.end(), [&](int a, int c) {
+    return leaf_ptr[a + 1] - leaf_ptr[a] > leaf_ptr[c + 1] - leaf_ptr[c];
+  });
+  return FX_OK;
+}
+
+template <int T>
+static int launch_leaf(fx_ctx *ctx, const LeafBatch &b, bool per_cluster,
+                       cudaStream_t s) {
+  constexpr int kGroups = 256 / T;
+  const size_t smem = (size_t)kGroups * kLeafArrays * kLeafMax * sizeof(float);
+  static bool attr = false;
+  if (!attr) {
+    FX_CHECK_CUDA(cudaFuncSetAttribute(leaf_batch_kernel<T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    attr = true;
+  }
+  if (per_cluster) {
+    for (int l = 0; l < b.n_leaves; ++l)
+      leaf_batch_kernel<T><<<1, 256, smem, s>>>(b, l);
+    FX_CHECK_LAUNCH();
+    ctx->launches += b.n_leaves;
+    return FX_OK;
+  }
+  int per_sm = 0;
+  FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_batch_kernel<T>,
+                                                               256, smem));
+  if (per_sm < 1) per_sm = 1;
+  int grid = ctx->num_sms * per_sm;
+  const int need = (b.n_leaves + kGroups - 1) / kGroups;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  FX_CHECK_CUDA(cudaMemsetAsync(b.counter, 0, 4, s));
+  leaf_batch_kernel<T><<<grid, 256, smem, s>>>(b, -1);
+  FX_CHECK_LAUNCH();
+  ctx->launches += 1;
+  return FX_OK;
+}
+
+static int run_schedule(fx_ctx *ctx, const LeafBatch &b, int schedule,
+                        cudaStream_t s) {
+  switch (schedule) {
+    case FX_LEAF_WARP: return launch_leaf<32>(ctx, b, false, s);
+    case FX_LEAF_CTA64: return launch_leaf<64>(ctx, b, false, s);
+    case FX_LEAF_CTA128: return launch_leaf<128>(ctx, b, false, s);
+    case FX_LEAF_CTA256: return launch_leaf<256>(ctx, b, false, s);
+    case FX_LEAF_PER_CLUSTER: return launch_leaf<128>(ctx, b, true, s);
+  }
+  set_error("unknown leaf schedule %d", schedule);
+  return FX_EINVAL;
+}
+
+}  // namespace fx
+
+using namespace fx;
+
+extern "C" int fx_leaf_cfg_default(fx_leaf_cfg *c) {
+  if (!c) return FX_EINVAL;
+  c->force_iterations = 50;
+  c->attract_weight = 1.0f;
+  c->repel_weight = 0.5f;
+  c->damping = 0.9f;
+  c->dt = 0.1f;
+  c->schedule = FX_LEAF_AUTO;
+  c->reserved0 = 0;
+  c->reserved1 = 0;
+  return FX_OK;
+}
+
+extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
+                                    const int32_t *leaf_ptr, const int32_t *leaf_gate,
+                                    const float *region, const fx_leaf_cfg *cfg,
+                                    float *out_x, float *out_y, int32_t *out_schedule) {
+  if (!ctx || !d || n_leaves < 0 || (n_leaves > 0 && (!leaf_ptr || !leaf_gate || !region)) ||
+      !cfg || !out_x || !out_y || cfg->force_iterations < 0) {
+    set_error("fx_hapr_place_leaves: invalid arguments");
+    return FX_EINVAL;
+  }
+  if (n_leaves == 0) return FX_OK;
+  if (leaf_ptr[0] != 0) {
+    set_error("fx_hapr_place_leaves: leaf_ptr[0] must be 0");
+    return FX_EINVAL;
+  }
+  for (int l = 0; l < n_leaves; ++l)
+    if (leaf_ptr[l + 1] < leaf_ptr[l]) {
+      set_error("fx_hapr_place_leaves: leaf_ptr decreases at %d", l);
+      return FX_EINVAL;
+    }
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  LeafHost h;
+  FX_TRY(build_leaf_host(d, n_leaves, leaf_ptr, leaf_gate, h));
+  const int32_t G = leaf_ptr[n_leaves];
+  DevBuf<int32_t> gptr, gate, aptr, order;
+  DevBuf<int16_t> aidx;
+  DevBuf<float4> reg;
+  DevBuf<float> ox, oy;
+  DevBuf<unsigned int> counter;
+  FX_TRY(gptr.alloc((size_t)n_leaves + 1));
+  FX_TRY(gate.alloc(G > 0 ? (size_t)G : 1));
+  FX_TRY(aptr.alloc((size_t)G + 1));
+  FX_TRY(aidx.alloc(h.aidx.empty() ? 1 : h.aidx.size()));
+  FX_TRY(order.alloc((size_t)n_leaves));
+  FX_TRY(reg.alloc((size_t)n_leaves));
+  FX_TRY(ox.alloc((size_t)d->n));
+  FX_TRY(oy.alloc((size_t)d->n));
+  FX_TRY(counter.alloc(2));
+  auto up = [&](void *dst, const void *src, size_t bytes) {
+    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s) : cudaSuccess;
+  };
+  FX_CHECK_CUDA(up(gptr.p, leaf_ptr, ((size_t)n_leaves + 1) * 4));
+  FX_CHECK_CUDA(up(gate.p, leaf_gate, (size_t)G * 4));
+  FX_CHECK_CUDA(up(aptr.p, h.aptr.data(), h.aptr.size() * 4));
+  FX_CHECK_CUDA(up(aidx.p, h.aidx.data(), h.aidx.size() * 2));
+  FX_CHECK_CUDA(up(order.p, h.order.data(), h.order.size() * 4));
+  FX_CHECK_CUDA(up(reg.p, region, (size_t)n_leaves * 16));
+  FX_CHECK_CUDA(up(ox.p, out_x, (size_t)d->n * 4));
+  FX_CHECK_CUDA(up(oy.p, out_y, (size_t)d->n * 4));
+  LeafBatch b{gptr.p, gate.p, aptr.p, aidx.p, reg.p, order.p, n_leaves,
+              cfg->force_iterations, cfg->attract_weight, cfg->repel_weight,
+              cfg->damping, cfg->dt, ox.p, oy.p, counter.p};
+  int schedule = cfg->schedule;
+  if (schedule == FX_LEAF_AUTO) {
+    // Autotune: time each schedule once on this batch (results are identical)
+    // and keep the fastest for this context.
+    float best = 1e30f;
+    int best_s = FX_LEAF_CTA128;
+    cudaEvent_t e0, e1;
+    FX_CHECK_CUDA(cudaEventCreate(&e0));
+    FX_CHECK_CUDA(cudaEventCreate(&e1));
+    for (int sc : {FX_LEAF_WARP, FX_LEAF_CTA64, FX_LEAF_CTA128, FX_LEAF_CTA256}) {
+      FX_CHECK_CUDA(cudaEventRecord(e0, s));
+      int rc = run_schedule(ctx, b, sc, s);
+      if (rc != FX_OK) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+      }
+      FX_CHECK_CUDA(cudaEventRecord(e1, s));
+      FX_CHECK_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      FX_CHECK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        best_s = sc;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->leaf_schedule = best_s;
+    schedule = best_s;
+  }
+  cudaEvent_t ev;
+  timer_begin(ctx, FX_STAGE_LEAF, s, &ev);
+  FX_TRY(run_schedule(ctx, b, schedule, s));
+  timer_end(ctx, FX_STAGE_LEAF, s, ev);
+  FX_CHECK_CUDA(cudaMemcpyAsync(out_x, ox.p, (size_t)d->n * 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(out_y, oy.p, (size_t)d->n * 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (out_schedule) *out_schedule = schedule;
+  for (auto *p : {&gptr, &gate, &aptr, &order}) p->release();
+  aidx.release();
+  reg.release();
+  ox.release();
+  oy.release();
+  counter.release();
+  return FX_OK;
+}

@@ -60,7 +60,15 @@ class LeafCfg(C.Structure):
     _fields_ = [("force_iterations", C.c_int32), ("attract_weight", C.c_float),
                 ("repel_weight", C.c_float), ("damping", C.c_float),
                 ("dt", C.c_float), ("schedule", C.c_int32),
-                ("threads_per_cluster", C.c_int32), ("use_graph", C.c_int32)]
+                ("reserved0", C.c_int32), ("reserved1", C.c_int32)]
+
+
+FX_LEAF_AUTO = 0
+FX_LEAF_WARP = 1
+FX_LEAF_CTA64 = 2
+FX_LEAF_CTA128 = 3
+FX_LEAF_CTA256 = 4
+FX_LEAF_PER_CLUSTER = 5
 
 
 P = C.c_void_p
@@ -104,6 +112,9 @@ SIGNATURES = {
     "fx_stage_density": (C.c_int, [P, P, I32, F32, F32, I32, PF32, PF32, PF32,
                                    PF32, PF32, PF32, PF64]),
     "fx_adjacency_build": (C.c_int64, [I32, I32, PI32, PI32, PI32, PI32, C.c_int64]),
+    "fx_leaf_cfg_default": (C.c_int, [C.POINTER(LeafCfg)]),
+    "fx_hapr_place_leaves": (C.c_int, [P, P, I32, PI32, PI32, PF32, C.POINTER(LeafCfg),
+                                       PF32, PF32, PI32]),
     "fx_synth_plain": (C.c_int, [C.c_uint64, I32, I32, F32, F32, I32, C.POINTER(P)]),
     "fx_synth_leaves": (C.c_int, [C.c_uint64, I32, I32, I32, F32, C.POINTER(P)]),
     "fx_netlist_sizes": (C.c_int, [P, PI64, PI64, PI64, PI64]),

@@ -299,6 +299,26 @@ class Design:
                        ex=g[2].reshape(bins, bins), ey=g[3].reshape(bins, bins))
         return out
 
+    # -- row H: batched leaf placement ------------------------------------------
+    def place_leaves(self, leaf_ptr, leaf_gate, region, cfg=None, x=None, y=None):
+        """placer.rs:65-69 + place_gates_in_leaf for every leaf in one launch.
+
+        Returns (x, y, schedule): positions of all gates (leaf gates placed,
+        others taken from x/y or zero) and the schedule the call used."""
+        cfg = cfg if cfg is not None else leaf_cfg()
+        lp = np.ascontiguousarray(leaf_ptr, np.int32)
+        lg = np.ascontiguousarray(leaf_gate, np.int32)
+        rg = np.ascontiguousarray(region, np.float32).reshape(-1)
+        ox = np.zeros(self.n, np.float32) if x is None else np.array(x, np.float32)
+        oy = np.zeros(self.n, np.float32) if y is None else np.array(y, np.float32)
+        sched = C.c_int32()
+        check(self.lib.fx_hapr_place_leaves(self.ctx.handle, self.handle, len(lp) - 1,
+                                            ptr(lp, C.c_int32), ptr(lg, C.c_int32),
+                                            ptr(rg, C.c_float), C.byref(cfg),
+                                            ptr(ox, C.c_float), ptr(oy, C.c_float),
+                                            C.byref(sched)), "fx_hapr_place_leaves")
+        return ox, oy, sched.value
+
     # -- the plain composite iteration -------------------------------------
     def force_iterate(self, cfg: "IterCfg", iters: int, x=None, y=None) -> IterStats:
         st = IterStats()
@@ -311,6 +331,16 @@ class Design:
             x[...] = xa
             y[...] = ya
         return st
+
+
+def leaf_cfg(**overrides) -> "_lib.LeafCfg":
+    cfg = _lib.LeafCfg()
+    check(load().fx_leaf_cfg_default(C.byref(cfg)), "fx_leaf_cfg_default")
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
 
 
 def iter_cfg(**overrides) -> IterCfg:

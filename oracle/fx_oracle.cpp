@@ -743,10 +743,23 @@ struct BHTree {
   }
 };
 
-// IEEE f32 law, in the device's operation order.
+// The device's inverse square root: Lomont's bit-level estimate
+// (0x5f375a86) and three Newton steps, IEEE f32 without contraction.
+static inline float rsqrt32(float x) {
+  int32_t i;
+  std::memcpy(&i, &x, 4);
+  i = 0x5f375a86 - (i >> 1);
+  float y;
+  std::memcpy(&y, &i, 4);
+  const float h = 0.5f * x;
+  for (int k = 0; k < 3; ++k) y = y * (1.5f - (h * y) * y);
+  return y;
+}
+
+// f32 law, in the device's operation order.
 static inline void term32(float dx, float dy, float r2c, float kq, float &fx,
                           float &fy) {
-  const float inv = 1.0f / std::sqrt(r2c);
+  const float inv = rsqrt32(r2c);
   const float f = ((kq * inv) * inv) * inv;
   fx = fx + f * dx;
   fy = fy + f * dy;

@@ -37,7 +37,13 @@ F64P = C.POINTER(C.c_double)
 
 
 def build() -> None:
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    """Builds the oracle libraries (output goes to stderr, never stdout)."""
+    import sys
+    r = subprocess.run(["make", "-s", "-C", str(HERE)], stdout=subprocess.PIPE,
+                       stderr=subprocess.STDOUT, text=True)
+    if r.stdout:
+        sys.stderr.write(r.stdout)
+    r.check_returncode()
 
 
 def lib() -> C.CDLL:
@@ -216,10 +222,12 @@ def integrate(x, y, vx, vy, fx, fy, dt, damping, box):
 def place_leaf(gates, adj_ptr, adj_idx, region, iters, attract=1.0, repel=0.5,
                damping=0.9, dt=0.1, out_x=None, out_y=None, n_total=None):
     gates = _i32(gates)
-    n_total = n_total if n_total is not None else int(gates.max()) + 1
     if out_x is None:
+        n_total = n_total if n_total is not None else int(gates.max()) + 1
         out_x = np.zeros(n_total, np.float32)
         out_y = np.zeros(n_total, np.float32)
+    if len(gates) == 0:
+        return out_x, out_y
     adj_ptr, adj_idx = _i32(adj_ptr), _i32(adj_idx)
     lib().or_place_leaf(len(gates), _p(gates, C.c_int32), _p(adj_ptr, C.c_int32),
                         _p(adj_idx, C.c_int32), *[float(r) for r in region], iters,

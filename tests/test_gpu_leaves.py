@@ -1,0 +1,96 @@
+"""Row H: the batched leaf placer against the oracle's literal restatement of
+place_gates_in_leaf (HAPR_fluxion_v4/src/algorithm/placer.rs:210-287)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_leaves(oracle, s, iters):
+    c = s.circuit
+    ap, ai = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    ox = np.zeros(c.num_gates, np.float32)
+    oy = np.zeros(c.num_gates, np.float32)
+    lp, reg = s.leaf_ptr, s.region.reshape(-1, 4)
+    gates = np.arange(c.num_gates, dtype=np.int32)
+    for l in range(len(lp) - 1):
+        oracle.place_leaf(gates[lp[l]:lp[l + 1]], ap, ai, reg[l], iters, 1.0, 0.5, 0.9, 0.1,
+                          ox, oy)
+    return ox, oy
+
+
+@pytest.fixture(scope="module")
+def batch(fx):
+    return fx.synth_leaves(7, 192, 16, 128, 1.5)
+
+
+@pytest.mark.parametrize("schedule", ["warp", "cta64", "cta128", "cta256", "per_cluster"])
+def test_leaf_schedules_bit_exact(fx, ctx, oracle, batch, schedule):
+    code = {"warp": fx.FX_LEAF_WARP, "cta64": fx.FX_LEAF_CTA64, "cta128": fx.FX_LEAF_CTA128,
+            "cta256": fx.FX_LEAF_CTA256, "per_cluster": fx.FX_LEAF_PER_CLUSTER}[schedule]
+    d = fx.Design(ctx, batch.circuit)
+    try:
+        cfg = fx.leaf_cfg(force_iterations=60, schedule=code)
+        gates = np.arange(batch.circuit.num_gates, dtype=np.int32)
+        x, y, used = d.place_leaves(batch.leaf_ptr, gates, batch.region, cfg)
+    finally:
+        d.close()
+    assert used == code
+    ox, oy = _oracle_leaves(oracle, batch, 60)
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
+
+
+def test_leaf_autotune_and_full_run(fx, ctx, oracle):
+    """300 iterations (the batched-leaf workload's count) on 48 clusters,
+    autotuned schedule: bit-identical to the reference loop."""
+    s = fx.synth_leaves(11, 48, 16, 128, 1.5)
+    d = fx.Design(ctx, s.circuit)
+    try:
+        gates = np.arange(s.circuit.num_gates, dtype=np.int32)
+        x, y, used = d.place_leaves(s.leaf_ptr, gates, s.region,
+                                    fx.leaf_cfg(force_iterations=300))
+    finally:
+        d.close()
+    assert used in (fx.FX_LEAF_WARP, fx.FX_LEAF_CTA64, fx.FX_LEAF_CTA128, fx.FX_LEAF_CTA256)
+    ox, oy = _oracle_leaves(oracle, s, 300)
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
+
+
+def test_leaf_regions_and_untouched_gates(fx, ctx, oracle):
+    """Leaves on distinct regions (the hierarchy's vertical strips), a leaf of
+    one gate, an empty leaf, and gates outside every leaf keeping their input
+    positions."""
+    s = fx.synth_plain(4, 600, 700, 40.0)
+    c = s.circuit
+    ap, ai = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    h = oracle.build_hierarchy(c.num_gates, ap, ai, c.chip_width, c.chip_height)
+    lp, lg, reg = h["leaf_ptr"].copy(), h["leaf_gate"].copy(), h["region"].copy()
+    # drop the last leaf's gates from the batch and add a 1-gate and an empty leaf
+    keep = lp[-2]
+    dropped = lg[keep:].copy()
+    lg2 = np.concatenate([lg[:keep], dropped[:1]])
+    lp2 = np.concatenate([lp[:-1], [keep + 1, keep + 1]]).astype(np.int32)
+    reg2 = np.concatenate([reg[:-1], reg[-1:], reg[-1:]])
+    x0 = np.full(c.num_gates, 7.0, np.float32)
+    d = fx.Design(ctx, c)
+    try:
+        x, y, _ = d.place_leaves(lp2, lg2, reg2, fx.leaf_cfg(force_iterations=50),
+                                 x0, x0.copy())
+    finally:
+        d.close()
+    ox, oy = x0.copy(), x0.copy()
+    for l in range(len(lp2) - 1):
+        oracle.place_leaf(lg2[lp2[l]:lp2[l + 1]], ap, ai, reg2[l], 50, 1.0, 0.5, 0.9, 0.1,
+                          ox, oy)
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
+    assert np.all(x[dropped[1:]] == 7.0)
+
+
+def test_leaf_too_large_is_rejected(fx, ctx):
+    s = fx.synth_plain(4, 600, 700, 40.0)
+    d = fx.Design(ctx, s.circuit)
+    try:
+        with pytest.raises(fx.FluxionError):
+            d.place_leaves([0, 600], np.arange(600), [20, 20, 40, 40])
+    finally:
+        d.close()

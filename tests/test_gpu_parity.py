@@ -168,24 +168,37 @@ def test_barnes_hut_clustered_large(fx, ctx, oracle):
 
 
 # ---- row C ---------------------------------------------------------------------
+# Relative L2 error bars of the potential / field / force against the FP64
+# FFT oracle, per GEMM precision: FP32 CUDA-core GEMMs, 3xTF32 and single-pass
+# TF32 / BF16 tensor-core GEMMs (all accumulate in FP32).
+PREC_TOL = {"simt": (1e-5, 2e-5), "fp32": (2e-4, 2e-4), "tf32": (1e-2, 1e-2),
+            "bf16": (5e-2, 5e-2)}
+
+
 @pytest.mark.parametrize("G", [128, 256])
-def test_density_simt_vs_fp64(fx, ctx, oracle, G):
+@pytest.mark.parametrize("prec", ["simt", "fp32", "tf32", "bf16"])
+def test_density_vs_fp64(fx, ctx, oracle, G, prec):
     s = fx.synth_plain(9, 20_000, 24_000, 170.0)
     c, p = s.circuit, s.placement
+    code = {"simt": fx.FX_DCT_SIMT, "fp32": fx.FX_DCT_FP32, "tf32": fx.FX_DCT_TF32,
+            "bf16": fx.FX_DCT_BF16}[prec]
+    tol_phi, tol_e = PREC_TOL[prec]
     d = fx.Design(ctx, c)
     try:
         d.set_positions(p.gate_x, p.gate_y)
-        out = d.density(G, 0.7, 1.0, fx.FX_DCT_SIMT, grids=True)
+        out = d.density(G, 0.7, 1.0, code, grids=True)
         area = (c.gate_widths * c.gate_heights).astype(np.float64)
         ref = oracle.density_forces(p.gate_x, p.gate_y, area, c.chip_width, c.chip_height,
                                     G, 0.7, 1.0)
         assert np.allclose(out["rho"], ref["rho"], rtol=0, atol=1e-5)
         phi_err = np.linalg.norm(out["phi"] - ref["phi"]) / np.linalg.norm(ref["phi"])
-        assert phi_err < 1e-5, phi_err
         e_err = rel_l2(out["ex"].ravel(), out["ey"].ravel(), ref["ex"].ravel(), ref["ey"].ravel())
-        assert e_err < 1e-3, e_err
-        assert rel_l2(out["fx"], out["fy"], ref["fx"], ref["fy"]) < 1e-3
-        assert abs(out["energy"] - ref["energy"]) <= 1e-3 * abs(ref["energy"])
+        f_err = rel_l2(out["fx"], out["fy"], ref["fx"], ref["fy"])
+        print(f"density G={G} {prec}: phi {phi_err:.3e} field {e_err:.3e} force {f_err:.3e}")
+        assert phi_err < tol_phi, phi_err
+        assert e_err < tol_e, e_err
+        assert f_err < tol_e
+        assert abs(out["energy"] - ref["energy"]) <= 10 * tol_phi * abs(ref["energy"])
     finally:
         d.close()
 
