@@ -225,6 +225,54 @@ int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *design, int32_t n_leaves,
                          const float *region, const fx_leaf_cfg *cfg,
                          float *out_x, float *out_y, int32_t *out_schedule);
 
+/* ---- row G: batched power iteration ------------------------------------- */
+/* Runs compute_fiedler_vector (H/src/algorithm/partitioner.rs:106-185) for
+ * every cluster at once: cluster c is the gate list cluster_gate[
+ * cluster_ptr[c] .. cluster_ptr[c+1]-1] (clusters must not share gates);
+ * its induced Laplacian uses the design's adjacency. The start vector is the
+ * reference's sin(i * 2.71828), normalised; each iteration applies L, removes
+ * the mean (deflation against the constant vector) and normalises, with FP64
+ * reductions. tol = 0 runs exactly max_iters iterations (the reference uses
+ * 30, H/src/main.rs:80); tol > 0 stops a cluster once its Rayleigh quotient
+ * changes by at most tol relative. out_v[G] receives each cluster's vector
+ * (same order as cluster_gate); out_iters[C] and out_lambda[C] (may be NULL)
+ * the iterations run and the final Rayleigh quotient v^T L v. */
+int fx_fiedler(fx_ctx *ctx, fx_design *design, int32_t n_clusters,
+               const int32_t *cluster_ptr, const int32_t *cluster_gate,
+               int32_t max_iters, double tol, float *out_v,
+               int32_t *out_iters, double *out_lambda);
+
+/* ---- congestion refinement (the loop of the next pipeline stage) -------- */
+typedef struct fx_refine_cfg {
+  int32_t max_iterations;   /* RefineConfig::max_iterations (100)            */
+  float move_distance;      /* max move per step (5.0)                       */
+  float overflow_threshold; /* hot-cell threshold and stop level (1.0 in the
+                               default YAML, H/config/default.yaml:37)       */
+  int32_t grid_cols;        /* routing grid (256 x 256)                       */
+  int32_t grid_rows;
+  int32_t reserved0;
+} fx_refine_cfg;
+
+typedef struct fx_refine_stats {
+  int64_t iterations;       /* iterations that moved gates                   */
+  int64_t moves;            /* gate moves in total                           */
+  float total_overflow;     /* final f32 total overflow (grid.rs:86-91)      */
+  float max_overflow;       /* final max overflow -> Placement::max_congestion */
+  double hpwl;              /* final HPWL (FP64)                             */
+} fx_refine_stats;
+
+int fx_refine_cfg_default(fx_refine_cfg *cfg);
+
+/* refine_placement (H/src/algorithm/refiner.rs:34-126): repeat congestion ->
+ * f32 total overflow -> stop when <= threshold or after 10 stalled
+ * iterations (change < 1 %) -> move every gate of a hot cell toward the
+ * first least-congested cell within radius 3, clamped to move_distance and
+ * the die. Positions end bit-identical to the reference loop. x/y: in/out
+ * host positions, or NULL to refine the resident positions. out_counts
+ * (rows x cols, may be NULL) receives the final congestion counts. */
+int fx_refine(fx_ctx *ctx, fx_design *design, const fx_refine_cfg *cfg,
+              float *x, float *y, fx_refine_stats *stats, uint32_t *out_counts);
+
 /* ---- host-only helpers (no GPU needed) ---------------------------------- */
 /* Builds the deduplicated clique-expansion adjacency of
  * Circuit::build_adjacency (H/src/data/circuit.rs:154-171) in the

@@ -9,7 +9,7 @@ from ._lib import (FX_DCT_BF16, FX_DCT_FP32, FX_DCT_SIMT, FX_DCT_TF32, FX_LEAF_A
                    FX_LEAF_WARP, FluxionError, IterCfg, IterStats, LeafCfg, load)
 from .api import (Circuit, Context, Design, Placement, RoutingGrid, Synth,
                   build_adjacency, build_and_compute, compute_congestion, compute_hpwl, default_context,
-                  iter_cfg, leaf_cfg, synth_leaves, synth_plain)
+                  iter_cfg, leaf_cfg, refine_cfg, synth_leaves, synth_plain)
 
 __all__ = [
     "Circuit", "Context", "Design", "Placement", "RoutingGrid", "Synth",
@@ -17,5 +17,5 @@ __all__ = [
     "iter_cfg", "synth_leaves", "synth_plain", "FluxionError", "IterCfg", "IterStats",
     "load", "FX_DCT_FP32", "FX_DCT_TF32", "FX_DCT_BF16", "FX_DCT_SIMT", "leaf_cfg",
     "LeafCfg", "FX_LEAF_AUTO", "FX_LEAF_WARP", "FX_LEAF_CTA64", "FX_LEAF_CTA128",
-    "FX_LEAF_CTA256", "FX_LEAF_PER_CLUSTER",
+    "FX_LEAF_CTA256", "FX_LEAF_PER_CLUSTER", "refine_cfg",
 ]

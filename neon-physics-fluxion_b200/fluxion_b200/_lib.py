@@ -71,6 +71,18 @@ FX_LEAF_CTA256 = 4
 FX_LEAF_PER_CLUSTER = 5
 
 
+class RefineCfg(C.Structure):
+    _fields_ = [("max_iterations", C.c_int32), ("move_distance", C.c_float),
+                ("overflow_threshold", C.c_float), ("grid_cols", C.c_int32),
+                ("grid_rows", C.c_int32), ("reserved0", C.c_int32)]
+
+
+class RefineStats(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("moves", C.c_int64),
+                ("total_overflow", C.c_float), ("max_overflow", C.c_float),
+                ("hpwl", C.c_double)]
+
+
 P = C.c_void_p
 I32 = C.c_int32
 I64 = C.c_int64
@@ -115,6 +127,10 @@ SIGNATURES = {
     "fx_leaf_cfg_default": (C.c_int, [C.POINTER(LeafCfg)]),
     "fx_hapr_place_leaves": (C.c_int, [P, P, I32, PI32, PI32, PF32, C.POINTER(LeafCfg),
                                        PF32, PF32, PI32]),
+    "fx_fiedler": (C.c_int, [P, P, I32, PI32, PI32, I32, C.c_double, PF32, PI32, PF64]),
+    "fx_refine_cfg_default": (C.c_int, [C.POINTER(RefineCfg)]),
+    "fx_refine": (C.c_int, [P, P, C.POINTER(RefineCfg), PF32, PF32, C.POINTER(RefineStats),
+                            PU32]),
     "fx_synth_plain": (C.c_int, [C.c_uint64, I32, I32, F32, F32, I32, C.POINTER(P)]),
     "fx_synth_leaves": (C.c_int, [C.c_uint64, I32, I32, I32, F32, C.POINTER(P)]),
     "fx_netlist_sizes": (C.c_int, [P, PI64, PI64, PI64, PI64]),

@@ -319,6 +319,40 @@ class Design:
                                             C.byref(sched)), "fx_hapr_place_leaves")
         return ox, oy, sched.value
 
+    # -- row G: batched power iteration -----------------------------------------
+    def fiedler(self, cluster_ptr, cluster_gate, max_iters: int = 30, tol: float = 0.0):
+        """partitioner.rs:106-185 for every cluster at once.
+
+        Returns (v[G] f32 in cluster_gate order, iterations[C], lambda[C])."""
+        cp = np.ascontiguousarray(cluster_ptr, np.int32)
+        cg = np.ascontiguousarray(cluster_gate, np.int32)
+        C_ = len(cp) - 1
+        v = np.empty(len(cg), np.float32)
+        its = np.empty(C_, np.int32)
+        lam = np.empty(C_, np.float64)
+        check(self.lib.fx_fiedler(self.ctx.handle, self.handle, C_, ptr(cp, C.c_int32),
+                                  ptr(cg, C.c_int32), max_iters, tol, ptr(v, C.c_float),
+                                  ptr(its, C.c_int32), ptr(lam, C.c_double)), "fx_fiedler")
+        return v, its, lam
+
+    # -- congestion refinement ----------------------------------------------------
+    def refine(self, cfg=None, x=None, y=None, counts: bool = False):
+        """refiner.rs:34-126 refine_placement. With x/y (host arrays, updated
+        in place) or on the resident positions. Returns RefineStats (and the
+        final counts when counts=True)."""
+        cfg = cfg if cfg is not None else refine_cfg()
+        st = _lib.RefineStats()
+        xa = None if x is None else np.ascontiguousarray(x, np.float32)
+        ya = None if y is None else np.ascontiguousarray(y, np.float32)
+        cnt = np.empty(cfg.grid_cols * cfg.grid_rows, np.uint32) if counts else None
+        check(self.lib.fx_refine(self.ctx.handle, self.handle, C.byref(cfg),
+                                 ptr(xa, C.c_float), ptr(ya, C.c_float), C.byref(st),
+                                 ptr(cnt, C.c_uint32)), "fx_refine")
+        if x is not None:
+            x[...] = xa
+            y[...] = ya
+        return (st, cnt) if counts else st
+
     # -- the plain composite iteration -------------------------------------
     def force_iterate(self, cfg: "IterCfg", iters: int, x=None, y=None) -> IterStats:
         st = IterStats()
@@ -336,6 +370,16 @@ class Design:
 def leaf_cfg(**overrides) -> "_lib.LeafCfg":
     cfg = _lib.LeafCfg()
     check(load().fx_leaf_cfg_default(C.byref(cfg)), "fx_leaf_cfg_default")
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
+
+
+def refine_cfg(**overrides) -> "_lib.RefineCfg":
+    cfg = _lib.RefineCfg()
+    check(load().fx_refine_cfg_default(C.byref(cfg)), "fx_refine_cfg_default")
     for k, v in overrides.items():
         if not hasattr(cfg, k):
             raise KeyError(k)

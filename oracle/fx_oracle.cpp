@@ -33,6 +33,13 @@ static void par_for(int32_t n, int32_t threads, F f) {
   for (auto &th : pool) th.join();
 }
 
+// Rust f32::clamp (NaN passes through).
+static inline float rust_clamp(float v, float lo, float hi) {
+  if (v < lo) v = lo;
+  if (v > hi) v = hi;
+  return v;
+}
+
 extern "C" {
 
 // ---------------------------------------------------------------------------
@@ -200,6 +207,78 @@ double or_hpwl_f64(int32_t m, const int32_t *net_ptr, const int32_t *net_gate,
   return total;
 }
 
+// H/src/algorithm/refiner.rs:34-126  refine_placement, literally: congestion,
+// f32 total overflow, stop / stall rules, then every gate in a hot cell
+// (gates_in_hot_cells, congestion.rs:77-93) moves toward the first
+// least-congested cell within radius 3 (move_gate_from_hot_cell), against
+// the grid of that iteration. x/y are updated in place. Returns the
+// iterations that moved gates; out[0..2] = final total overflow, max
+// overflow, f32 HPWL (placement.rs:48-74).
+int32_t or_refine(int32_t n, int32_t m, const int32_t *net_ptr,
+                  const int32_t *net_gate, float *x, float *y, float chip_w,
+                  float chip_h, int32_t max_iters, float move_distance,
+                  float threshold, int64_t cols, int64_t rows, float *out) {
+  float cw, ch, cap;
+  or_grid_geometry(chip_w, chip_h, cols, rows, &cw, &ch, &cap);
+  const size_t cells = (size_t)(cols * rows);
+  std::vector<float> h(cells), v(cells);
+  std::vector<char> hot(cells);
+  float prev = 3.40282347e+38f;
+  int32_t stall = 0, moved_iters = 0;
+  for (int32_t it = 0; it < max_iters; ++it) {
+    or_congestion(m, net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows, h.data(),
+                  v.data());
+    float total, mx;
+    or_overflow(h.data(), v.data(), cols, rows, cap, &total, &mx);
+    if (total <= threshold) break;
+    if (std::fabs(prev - total) < 0.01f * std::fmax(prev, 1.0f)) {
+      if (++stall >= 10) break;
+    } else {
+      stall = 0;
+    }
+    prev = total;
+    for (size_t i = 0; i < cells; ++i) {
+      float ov = (h[i] + v[i]) - cap;
+      ov = std::fmax(ov, 0.0f);
+      hot[i] = ov > threshold;
+    }
+    for (int32_t g = 0; g < n; ++g) {
+      const float gx = x[g], gy = y[g];
+      const int64_t col = or_cell_at(gx, cw, cols), row = or_cell_at(gy, ch, rows);
+      if (!hot[(size_t)(row * cols + col)]) continue;
+      bool found = false;
+      int64_t bc = 0, br = 0;
+      float best = 0.0f;
+      for (int64_t dr = -3; dr <= 3; ++dr)
+        for (int64_t dc = -3; dc <= 3; ++dc) {
+          if (dr == 0 && dc == 0) continue;
+          const int64_t nc = col + dc, nr = row + dr;
+          if (nc < 0 || nc >= cols || nr < 0 || nr >= rows) continue;
+          const size_t idx = (size_t)(nr * cols + nc);
+          const float tot = h[idx] + v[idx];
+          if (!found || tot < best) {  // min_by keeps the first minimum
+            found = true;
+            best = tot;
+            bc = nc;
+            br = nr;
+          }
+        }
+      if (!found) continue;
+      const float tx = ((float)bc + 0.5f) * cw, ty = ((float)br + 0.5f) * ch;
+      const float dx = rust_clamp(tx - gx, -move_distance, move_distance);
+      const float dy = rust_clamp(ty - gy, -move_distance, move_distance);
+      x[g] = rust_clamp(gx + dx, 0.0f, chip_w);
+      y[g] = rust_clamp(gy + dy, 0.0f, chip_h);
+    }
+    ++moved_iters;
+  }
+  or_congestion(m, net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows, h.data(),
+                v.data());
+  or_overflow(h.data(), v.data(), cols, rows, cap, &out[0], &out[1]);
+  out[2] = or_hpwl_f32(m, net_ptr, net_gate, x, y);
+  return moved_iters;
+}
+
 // H/src/data/circuit.rs:154-171  build_adjacency, literally: for every net,
 // every pair i < j, push each endpoint into the other's list unless it is
 // already there (Vec::contains). Returns the entry count; writes at most
@@ -268,11 +347,6 @@ void or_attraction_f64(int32_t n, const int32_t *adj_ptr, const int32_t *adj_idx
 
 // H/src/algorithm/placer.rs:275-280  damped Euler step with clamp to the
 // box [xlo, xhi] x [ylo, yhi] (Rust clamp: NaN passes through).
-static inline float rust_clamp(float v, float lo, float hi) {
-  if (v < lo) v = lo;
-  if (v > hi) v = hi;
-  return v;
-}
 
 void or_integrate(int32_t n, float *x, float *y, float *vx, float *vy,
                   const float *fx, const float *fy, float dt, float damping,

@@ -61,6 +61,10 @@ def lib() -> C.CDLL:
         L.or_congestion_sample.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
                                            C.c_float, C.c_int64, C.c_int64, C.c_int32,
                                            F32P, F32P]
+        L.or_refine.restype = C.c_int32
+        L.or_refine.argtypes = [C.c_int32, C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
+                                C.c_float, C.c_int32, C.c_float, C.c_float, C.c_int64,
+                                C.c_int64, F32P]
         L.or_overflow.argtypes = [F32P, F32P, C.c_int64, C.c_int64, C.c_float, F32P, F32P]
         L.or_hpwl_f32.restype = C.c_float
         L.or_hpwl_f32.argtypes = [C.c_int32, I32P, I32P, F32P, F32P]
@@ -154,6 +158,20 @@ def congestion_sample(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows, strid
                                chip_w, chip_h, cols, rows, stride, _p(h, C.c_float),
                                _p(v, C.c_float))
     return h, v
+
+
+def refine(net_ptr, net_gate, x, y, chip_w, chip_h, max_iters=100, move_distance=5.0,
+           threshold=1.0, cols=256, rows=256):
+    """refiner.rs:34-126 on float32 copies of x/y; returns (x, y, iters, stats)."""
+    net_ptr, net_gate = _i32(net_ptr), _i32(net_gate)
+    x, y = np.array(x, np.float32), np.array(y, np.float32)
+    out = np.zeros(3, np.float32)
+    it = lib().or_refine(len(x), len(net_ptr) - 1, _p(net_ptr, C.c_int32),
+                         _p(net_gate, C.c_int32), _p(x, C.c_float), _p(y, C.c_float),
+                         chip_w, chip_h, max_iters, move_distance, threshold, cols, rows,
+                         _p(out, C.c_float))
+    return x, y, int(it), dict(total_overflow=float(out[0]), max_overflow=float(out[1]),
+                               hpwl_f32=float(out[2]))
 
 
 def overflow(h, v, cols, rows, capacity):
