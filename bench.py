@@ -5,7 +5,12 @@ One step = one plain composite iteration of the HAPR placement hot path on
 the 1,000,000-gate / 1,200,000-net synthetic netlist (die 1200 x 1200):
 net-spring attraction (k = 1) + Barnes-Hut repulsion (theta 0.5, k 0.5,
 min_dist 0.1) + DCT-II Poisson density force (1024 x 1024 grid, GEMM form) +
-damped Euler step + congestion counting (512 x 512) and FP64 HPWL.
+damped Euler step + congestion counting (512 x 512) and FP64 HPWL. Every
+step starts from the same device-resident state (the seeded uniform
+placement after the warm-up iterations, checkpointed with
+fx_design_save_state and restored inside the step), so each timed step does
+the same work; the configured 500-iteration run is reported beside it
+("trajectory").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fluxion|reference]
 
@@ -38,12 +43,15 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "1M-gate force iterations/s"
 UNIT = "iterations/s"
+# fx_force_iterate reads back HPWL + total overflow (16 B), max overflow (4),
+# density energy (8) and the walk's error word (4) after the last iteration
+ITER_STATS_D2H = 32
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fluxion", choices=["fluxion", "reference"])
     ap.add_argument("--gates", type=int, default=1_000_000)
@@ -55,6 +63,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--trajectory", type=int, default=500,
+                    help="iterations of the full run reported beside the steps (0: skip)")
     return ap.parse_args()
 
 
@@ -66,7 +76,7 @@ PREC_DTYPE = {"fp32": "f32 (DCT GEMMs 3xTF32, FP32 accumulate)",
 
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -77,7 +87,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(device)], stdout=self.tmp,
+                 "-lms", "100", "-i", str(device)], stdout=self.tmp,
                 stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -267,20 +277,31 @@ def run_fluxion(args, rank, world, local_rank):
     d = fx.Design(ctx, c)
     cfg = fx.iter_cfg(density_bins=args.bins, dct_precision=PREC[args.precision],
                       cong_cols=args.cong, cong_rows=args.cong)
-    # warm-up from the initial placement
+    # The start state of every step: the seeded uniform placement advanced by
+    # `warmup` iterations, velocities zero, checkpointed on the device.
     d.set_positions(p.gate_x, p.gate_y)
     d.force_iterate(cfg, args.warmup)
-    x0, y0 = d.get_positions()  # positions at the start of the timed region
+    x0, y0 = d.get_positions()
     d.set_positions(x0, y0)
+    d.save_state()
+
+    def step():
+        d.restore_state()
+        return d.force_iterate(cfg, 1)
+
+    for _ in range(args.warmup):
+        step()
     ctx.synchronize()
     launches0 = ctx.kernel_launches()
     ctx.reset_stage_times()
     ctx.set_profiling(True)
     clocks = ClockSampler(local_rank)
+    time.sleep(0.3)
     barrier()
     ctx.synchronize()
     ctx.mark(0)
-    st = d.force_iterate(cfg, args.steps)
+    for _ in range(args.steps):
+        st = step()
     ctx.mark(1)
     ctx.synchronize()
     ms = ctx.elapsed_ms(0, 1)
@@ -292,33 +313,53 @@ def run_fluxion(args, rank, world, local_rank):
     ms_max = max_over_ranks(ms)
     value = world * args.steps / (ms_max / 1e3)
 
-    # end to end through the public call with host buffers: one
-    # fx_force_iterate call of `steps` iterations, positions copied in from
-    # pinned host memory and results read back inside the timed region.
+    # End to end through the public call with host buffers: every step
+    # copies the start positions in from pinned host memory, runs the
+    # iteration and reads the new positions and statistics back. The host
+    # refill of the buffers between steps is outside the timed intervals.
     e2e = None
     if not args.no_e2e:
         try:
             import torch
-            hx = torch.from_numpy(x0.copy()).pin_memory()
-            hy = torch.from_numpy(y0.copy()).pin_memory()
-            ax, ay = hx.numpy(), hy.numpy()
-            ax[...] = x0
-            ay[...] = y0
+            ax = torch.empty(c.num_gates, dtype=torch.float32).pin_memory().numpy()
+            ay = torch.empty(c.num_gates, dtype=torch.float32).pin_memory().numpy()
             pinned = True
         except Exception:
-            ax, ay = x0.copy(), y0.copy()
+            ax = np.empty(c.num_gates, np.float32)
+            ay = np.empty(c.num_gates, np.float32)
             pinned = False
-        ctx.synchronize()
-        barrier()
-        t0 = time.perf_counter()
-        d.force_iterate(cfg, args.steps, ax, ay)
-        e2e_s = time.perf_counter() - t0
+        e2e_s = 0.0
+        for i in range(args.warmup + args.steps):
+            ax[...] = x0
+            ay[...] = y0
+            ctx.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            d.force_iterate(cfg, 1, ax, ay)
+            if i >= args.warmup:
+                e2e_s += time.perf_counter() - t0
         e2e_s = max_over_ranks(e2e_s)
         e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": 8 * c.num_gates / args.steps,
-               "d2h_bytes_per_step": (8 * c.num_gates + 48) / args.steps,
-               "call": f"fx_force_iterate(iters={args.steps}) with host x/y"
-                       f"{' (pinned)' if pinned else ''}"}
+               "h2d_bytes_per_step": 8 * c.num_gates,
+               "d2h_bytes_per_step": 8 * c.num_gates + ITER_STATS_D2H,
+               "call": "fx_force_iterate(iters=1) with host x/y"
+                       f"{' (pinned)' if pinned else ''} per step"}
+
+    # The whole configured run: `trajectory` iterations from the seeded
+    # uniform placement in one call (the reference's math contracts the
+    # netlist, so later iterations are cheaper than the timed steps).
+    traj = None
+    if args.trajectory > 0:
+        d.set_positions(p.gate_x, p.gate_y)
+        ctx.synchronize()
+        ctx.mark(2)
+        tst = d.force_iterate(cfg, args.trajectory)
+        ctx.mark(3)
+        ctx.synchronize()
+        tms = ctx.elapsed_ms(2, 3)
+        traj = {"iterations": args.trajectory, "value": args.trajectory / (tms / 1e3),
+                "unit": UNIT, "final_hpwl": tst.hpwl,
+                "final_total_overflow": tst.total_overflow}
 
     n, m, pn, a = d.n, d.m, d.p, d.a
     G, gc = args.bins, args.cong
@@ -368,7 +409,7 @@ def run_fluxion(args, rank, world, local_rank):
            "iteration_roofline": {"bytes": B_iter, "achieved_gbs": B_iter / (it_ms * 1e-3) / 1e9,
                                   "frac_of_hbm": B_iter / (it_ms * 1e-3) / 1e9 / hbm},
            "stage_ms_per_iter": {k: round(v, 4) for k, v in per_iter.items()},
-           "final_hpwl": st.hpwl}
+           "step_hpwl": st.hpwl, "trajectory": traj}
     if rank == 0:
         print(json.dumps(out), flush=True)
     d.close()

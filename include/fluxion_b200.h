@@ -105,6 +105,14 @@ int fx_design_adjacency(const fx_design *design, int32_t *out_adj_ptr,
  * are zeroed by set_positions). */
 int fx_design_set_positions(fx_design *design, const float *x, const float *y);
 int fx_design_get_positions(fx_design *design, float *out_x, float *out_y);
+/* Device-side checkpoint of the placement state (positions and velocities):
+ * save_state copies the current state into a second device buffer set
+ * (allocated on the first call), restore_state copies it back. Both are
+ * stream-ordered device copies on the context's stream; restore before a
+ * save fails with FX_EINVAL. No counterpart in the reference (its state
+ * lives in host Vec<f32>s that the caller clones). */
+int fx_design_save_state(fx_design *design);
+int fx_design_restore_state(fx_design *design);
 /* Device bytes held by the design (netlist + positions + workspaces). */
 int64_t fx_design_device_bytes(const fx_design *design);
 

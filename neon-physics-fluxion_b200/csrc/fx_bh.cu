@@ -466,34 +466,36 @@ __global__ void bh_qchild_kernel(int n, const int32_t *__restrict__ child,
 
 // 1/sqrt(x) for x >= min_dist^2 > 0: the bit-level estimate of Lomont
 // ("Fast inverse square root", 2003; constant 0x5f375a86) refined by three
-// Newton steps y <- y * (1.5 - (x/2) * y * y) in IEEE f32 without
-// contraction. Integer ops and correctly rounded products only, so a
-// sequential restatement reproduces it bit for bit; the result is within a
-// couple of ulp of the exact value.
+// Newton steps y <- y * fma(-(x/2) * y, y, 1.5) in IEEE f32. Integer ops,
+// correctly rounded products and fused multiply-adds only (each written out
+// explicitly, nothing left to contraction), so a sequential restatement with
+// fmaf reproduces it bit for bit; the result is within a couple of ulp of the
+// exact value.
 __device__ __forceinline__ float bh_rsqrt(float x) {
   float y = __int_as_float(0x5f375a86 - (__float_as_int(x) >> 1));
   const float h = __fmul_rn(0.5f, x);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
-    y = __fmul_rn(y, __fsub_rn(1.5f, __fmul_rn(__fmul_rn(h, y), y)));
+    y = __fmul_rn(y, __fmaf_rn(-__fmul_rn(h, y), y, 1.5f));
   return y;
 }
 
 // The law k*Q/d^2 along (dx, dy)/d with d = max(|r|, min_dist), in f32:
-// inv = rsqrt(max(r2, md^2)), f = ((kQ * inv) * inv) * inv, F += f * r.
+// inv = rsqrt(max(r2, md^2)), f = ((kQ * inv) * inv) * inv,
+// F = fma(f, r, F); r2 = fma(dx, dx, dy * dy).
 __device__ __forceinline__ void bh_term(float dx, float dy, float r2c, float kq,
                                         float &fx, float &fy) {
   const float inv = bh_rsqrt(r2c);
   const float f = __fmul_rn(__fmul_rn(__fmul_rn(kq, inv), inv), inv);
-  fx = __fadd_rn(fx, __fmul_rn(f, dx));
-  fy = __fadd_rn(fy, __fmul_rn(f, dy));
+  fx = __fmaf_rn(f, dx, fx);
+  fy = __fmaf_rn(f, dy, fy);
 }
 
 __device__ __forceinline__ void bh_direct(float px, float py, float2 q,
                                           float kq, float md2, float &fx,
                                           float &fy) {
   const float dx = __fsub_rn(px, q.x), dy = __fsub_rn(py, q.y);
-  const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
   bh_term(dx, dy, fmaxf(r2, md2), kq, fx, fy);
 }
 
@@ -510,7 +512,7 @@ __device__ __forceinline__ unsigned bh_eval(int c, unsigned mask, int lane,
   const bool in = (mask >> lane) & 1u;
   const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
   const float dy = __fsub_rn(__fsub_rn(p.y, r0.y), r0.w);
-  const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
   const float r2c = fmaxf(r2, md2);
   // size^2 < 0 (a node standing for no quad level) is always opened
   const bool accept = in && r1.y >= 0.f && (r1.y < __fmul_rn(th2, r2c));

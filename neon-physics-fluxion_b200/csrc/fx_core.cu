@@ -437,6 +437,34 @@ extern "C" int fx_design_get_positions(fx_design *d, float *out_x,
   return FX_OK;
 }
 
+extern "C" int fx_design_save_state(fx_design *d) {
+  if (!d) return FX_EINVAL;
+  FX_CHECK_CUDA(cudaSetDevice(d->ctx->device));
+  cudaStream_t s = d->ctx->stream;
+  const size_t b = (size_t)d->n * 4;
+  const float *src[4] = {d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p};
+  for (int i = 0; i < 4; ++i) {
+    if (!d->saved[i].p) FX_TRY(d->saved[i].alloc(d->n));
+    FX_CHECK_CUDA(cudaMemcpyAsync(d->saved[i].p, src[i], b, cudaMemcpyDeviceToDevice, s));
+  }
+  return FX_OK;
+}
+
+extern "C" int fx_design_restore_state(fx_design *d) {
+  if (!d) return FX_EINVAL;
+  if (!d->saved[0].p) {
+    set_error("fx_design_restore_state: no saved state");
+    return FX_EINVAL;
+  }
+  FX_CHECK_CUDA(cudaSetDevice(d->ctx->device));
+  cudaStream_t s = d->ctx->stream;
+  const size_t b = (size_t)d->n * 4;
+  float *dst[4] = {d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p};
+  for (int i = 0; i < 4; ++i)
+    FX_CHECK_CUDA(cudaMemcpyAsync(dst[i], d->saved[i].p, b, cudaMemcpyDeviceToDevice, s));
+  return FX_OK;
+}
+
 extern "C" int64_t fx_design_device_bytes(const fx_design *d) {
   if (!d) return -1;
   int64_t t = 0;
@@ -444,6 +472,7 @@ extern "C" int64_t fx_design_device_bytes(const fx_design *d) {
        d->adj_idx.bytes() + d->area.bytes();
   for (int i = 0; i < 2; ++i) t += d->x[i].bytes() + d->y[i].bytes();
   t += d->vx.bytes() + d->vy.bytes() + d->fattr.bytes();
+  for (int i = 0; i < 4; ++i) t += d->saved[i].bytes();
   auto add = [&t](auto &buf) { t += (int64_t)buf.bytes(); };
   fx_design *m = const_cast<fx_design *>(d);
   m->bh.for_each(add);

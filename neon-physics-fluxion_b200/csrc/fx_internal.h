@@ -203,6 +203,7 @@ struct fx_design {
   fx::DevBuf<float> x[2], y[2];
   int cur = 0;
   fx::DevBuf<float> vx, vy;
+  fx::DevBuf<float> saved[4];    // checkpoint: x, y, vx, vy
   fx::DevBuf<float2> fattr;      // attraction-only force output (stage API)
   // workspaces
   fx::BHWork bh;

@@ -113,6 +113,8 @@ SIGNATURES = {
     "fx_design_adjacency": (C.c_int, [P, PI32, PI32]),
     "fx_design_set_positions": (C.c_int, [P, PF32, PF32]),
     "fx_design_get_positions": (C.c_int, [P, PF32, PF32]),
+    "fx_design_save_state": (C.c_int, [P]),
+    "fx_design_restore_state": (C.c_int, [P]),
     "fx_design_device_bytes": (C.c_int64, [P]),
     "fx_congestion": (C.c_int, [P, P, PF32, PF32, I32, I32, PU32, PF64, PF64, PF32]),
     "fx_iter_cfg_default": (C.c_int, [C.POINTER(IterCfg)]),

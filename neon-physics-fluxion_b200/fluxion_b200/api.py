@@ -245,6 +245,14 @@ class Design:
                                                ptr(y, C.c_float)), "get_positions")
         return x, y
 
+    def save_state(self) -> None:
+        """Device-side checkpoint of positions and velocities."""
+        check(self.lib.fx_design_save_state(self.handle), "save_state")
+
+    def restore_state(self) -> None:
+        """Restores the last save_state (stream-ordered, no host sync)."""
+        check(self.lib.fx_design_restore_state(self.handle), "restore_state")
+
     def device_bytes(self) -> int:
         return int(self.lib.fx_design_device_bytes(self.handle))
 
@@ -361,8 +369,9 @@ class Design:
         check(self.lib.fx_force_iterate(self.ctx.handle, self.handle, C.byref(cfg), iters,
                                         ptr(xa, C.c_float), ptr(ya, C.c_float),
                                         C.byref(st)), "fx_force_iterate")
-        if x is not None:
+        if x is not None and xa is not x:
             x[...] = xa
+        if y is not None and ya is not y:
             y[...] = ya
         return st
 

@@ -818,7 +818,8 @@ struct BHTree {
 };
 
 // The device's inverse square root: Lomont's bit-level estimate
-// (0x5f375a86) and three Newton steps, IEEE f32 without contraction.
+// (0x5f375a86) and three Newton steps y * fma(-(h * y), y, 1.5), IEEE f32
+// with the device's explicit fused multiply-adds and no other contraction.
 static inline float rsqrt32(float x) {
   int32_t i;
   std::memcpy(&i, &x, 4);
@@ -826,7 +827,7 @@ static inline float rsqrt32(float x) {
   float y;
   std::memcpy(&y, &i, 4);
   const float h = 0.5f * x;
-  for (int k = 0; k < 3; ++k) y = y * (1.5f - (h * y) * y);
+  for (int k = 0; k < 3; ++k) y = y * std::fmaf(-(h * y), y, 1.5f);
   return y;
 }
 
@@ -835,8 +836,8 @@ static inline void term32(float dx, float dy, float r2c, float kq, float &fx,
                           float &fy) {
   const float inv = rsqrt32(r2c);
   const float f = ((kq * inv) * inv) * inv;
-  fx = fx + f * dx;
-  fy = fy + f * dy;
+  fx = std::fmaf(f, dx, fx);
+  fy = std::fmaf(f, dy, fy);
 }
 
 // Per-point walk with the device's rules and term order: for every opened
@@ -858,7 +859,7 @@ struct Walker {
     fx += f * dx / d;
     fy += f * dy / d;
     const float ex = pxf - t.sx[q], ey = pyf - t.sy[q];
-    const float r2 = ex * ex + ey * ey;
+    const float r2 = std::fmaf(ex, ex, ey * ey);
     term32(ex, ey, std::fmax(r2, md2), kf, gx, gy);
     ++inter;
   }
@@ -871,7 +872,7 @@ struct Walker {
     }
     const BHTree::Node &nd = t.nodes[c];
     const float dx = (pxf - nd.hx) - nd.lx, dy = (pyf - nd.hy) - nd.ly;
-    const float r2 = dx * dx + dy * dy;
+    const float r2 = std::fmaf(dx, dx, dy * dy);
     const float r2c = std::fmax(r2, md2);
     if (nd.s2 >= 0.0f && nd.s2 < th2 * r2c) {
       const int32_t cnt = nd.l - nd.f + 1;

@@ -260,3 +260,28 @@ def test_plain_iteration_is_deterministic(fx, ctx):
         d.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert out[0][2:] == out[1][2:]
+
+
+def test_saved_state_restores_the_step(fx, ctx):
+    """save_state / restore_state: an iteration from the restored state (with
+    non-zero velocities) repeats the first one bit for bit, and restore
+    without a save is rejected."""
+    s = fx.synth_plain(5, 20_000, 24_000, 170.0)
+    cfg = fx.iter_cfg(density_bins=128, cong_cols=64, cong_rows=64)
+    d = fx.Design(ctx, s.circuit)
+    try:
+        with pytest.raises(fx.FluxionError):
+            d.restore_state()
+        d.set_positions(s.placement.gate_x, s.placement.gate_y)
+        d.force_iterate(cfg, 2)        # velocities are non-zero from here on
+        d.save_state()
+        out = []
+        for _ in range(2):
+            d.restore_state()
+            st = d.force_iterate(cfg, 3)
+            x, y = d.get_positions()
+            out.append((x, y, st.hpwl, st.total_overflow))
+    finally:
+        d.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2:] == out[1][2:]
