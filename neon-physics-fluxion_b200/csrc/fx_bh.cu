@@ -455,14 +455,17 @@ __global__ void bh_qchild_kernel(int n, const int32_t *__restrict__ child,
 }
 
 // ---- warp-cooperative walk ----------------------------------------------------
-// Each warp owns 32 consecutive sorted points (spatially close) and walks the
-// quadtree with a shared stack of (node, lane mask) entries, each an opened
-// cell. Popping a cell evaluates all its children for the lanes in the mask:
+// Each warp owns 32 consecutive sorted points (spatially close), split into
+// groups of kWalkGroup lanes. Each group walks the quadtree with its own
+// shared stack of (node, lane mask) entries, each an opened cell; the groups
+// of a warp pop in lockstep, so one pass of the loop serves up to 32/kWalkGroup
+// cells. Popping a cell evaluates all its children for the lanes in the mask:
 // every lane applies the reference opening rule to its own point, so
 // interaction lists are exactly per point. A lane adds, per opened cell, the
 // terms of its children in order (single points, accepted cells, opened
 // buckets point by point), and then descends into the children it opened, in
-// order.
+// order. A group's stack holds the union of its points' opened cells, which
+// near the leaves is much smaller than the union over the whole warp.
 
 // 1/sqrt(x) for x >= min_dist^2 > 0: the bit-level estimate of Lomont
 // ("Fast inverse square root", 2003; constant 0x5f375a86) refined by three
@@ -499,34 +502,43 @@ __device__ __forceinline__ void bh_direct(float px, float py, float2 q,
   bh_term(dx, dy, fmaxf(r2, md2), kq, fx, fy);
 }
 
-// Applies the opening rule of internal node c for the lanes in `mask`; adds
-// the accepted and bucket terms and returns the lanes that open c as a cell
-// to descend into (0 for a bucket, whose points were handled here).
-__device__ __forceinline__ unsigned bh_eval(int c, unsigned mask, int lane,
-                                            int s, float2 p, float k,
-                                            float th2, float md2,
+// Applies the opening rule of child c (an internal node when `cell`) to the
+// lane's point when `in`; adds accepted-cell, single-point and bucket terms.
+// Called by all 32 lanes together (the ballot); returns the lanes that open
+// c as a cell to descend into.
+__device__ __forceinline__ unsigned bh_eval(int c, bool in, bool cell, int s,
+                                            float2 p, float k, float th2,
+                                            float md2,
                                             const float4 *__restrict__ node,
                                             const float2 *__restrict__ spos,
                                             float &fx, float &fy) {
-  const float4 r0 = node[2 * c], r1 = node[2 * c + 1];
-  const bool in = (mask >> lane) & 1u;
-  const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
-  const float dy = __fsub_rn(__fsub_rn(p.y, r0.y), r0.w);
-  const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-  const float r2c = fmaxf(r2, md2);
-  // size^2 < 0 (a node standing for no quad level) is always opened
-  const bool accept = in && r1.y >= 0.f && (r1.y < __fmul_rn(th2, r2c));
-  if (accept) bh_term(dx, dy, r2c, __fmul_rn(k, fabsf(r1.x)), fx, fy);
-  const unsigned open = __ballot_sync(0xffffffffu, in && !accept);
-  if (open == 0u || r1.x > 0.f) return open;
-  const bool mine = (open >> lane) & 1u;  // bucket: point by point
-  const int b = __float_as_int(r1.z), e = __float_as_int(r1.w);
-  for (int t = b; t <= e; ++t) {
-    const float2 q = spos[t];
-    if (mine && t != s) bh_direct(p.x, p.y, q, k, md2, fx, fy);
+  bool op = false;
+  if (in) {
+    if (!cell) {  // single point ~c
+      if (~c != s) bh_direct(p.x, p.y, spos[~c], k, md2, fx, fy);
+    } else {
+      const float4 r0 = node[2 * c], r1 = node[2 * c + 1];
+      const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
+      const float dy = __fsub_rn(__fsub_rn(p.y, r0.y), r0.w);
+      const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+      const float r2c = fmaxf(r2, md2);
+      // size^2 < 0 (a node standing for no quad level) is always opened
+      if (r1.y >= 0.f && r1.y < __fmul_rn(th2, r2c)) {
+        bh_term(dx, dy, r2c, __fmul_rn(k, fabsf(r1.x)), fx, fy);
+      } else if (r1.x > 0.f) {
+        op = true;
+      } else {  // bucket: point by point
+        const int b = __float_as_int(r1.z), e = __float_as_int(r1.w);
+        for (int t = b; t <= e; ++t)
+          if (t != s) bh_direct(p.x, p.y, spos[t], k, md2, fx, fy);
+      }
+    }
   }
-  return 0u;
+  return __ballot_sync(0xffffffffu, op);
 }
+
+constexpr int kWalkGroup = 8;                    // lanes per group
+constexpr int kWalkGroups = 32 / kWalkGroup;     // groups per warp
 
 __global__ void __launch_bounds__(kWalkWarps * 32)
 bh_walk_kernel(int n, const float2 *__restrict__ spos,
@@ -534,61 +546,65 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
                const int4 *__restrict__ qchild,
                const float4 *__restrict__ node, float k, float th2, float md2,
                float2 *__restrict__ force, unsigned int *__restrict__ err) {
-  __shared__ int32_t st_node[kWalkWarps][kStack];
-  __shared__ unsigned st_mask[kWalkWarps][kStack];
+  __shared__ int32_t st_node[kWalkWarps][kWalkGroups][kStack];
+  __shared__ unsigned st_mask[kWalkWarps][kWalkGroups][kStack];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane / kWalkGroup;
+  const bool leader = (lane % kWalkGroup) == 0;
+  const unsigned gmask = (kWalkGroup == 32 ? 0xffffffffu
+                                           : ((1u << kWalkGroup) - 1u) << (g * kWalkGroup));
   const int s = (blockIdx.x * kWalkWarps + w) * 32 + lane;
   const bool valid = s < n;
-  const unsigned active = __ballot_sync(0xffffffffu, valid);
-  if (active == 0) return;
+  if (__ballot_sync(0xffffffffu, valid) == 0u) return;
   const float2 p = valid ? spos[s] : make_float2(0.f, 0.f);
   float fx = 0.f, fy = 0.f;
-  int sp = 0;
+  int sp = 0;  // this group's stack depth (uniform in the group)
   if (n >= 2) {
-    const unsigned open = bh_eval(0, active, lane, s, p, k, th2, md2, node, spos, fx, fy);
+    const unsigned open = bh_eval(0, valid, true, s, p, k, th2, md2, node, spos, fx, fy) & gmask;
     if (open) {
-      if (lane == 0) {
-        st_node[w][0] = 0;
-        st_mask[w][0] = open;
+      if (leader) {
+        st_node[w][g][0] = 0;
+        st_mask[w][g][0] = open;
       }
       sp = 1;
     }
   }
   __syncwarp();
-  while (sp > 0) {
-    --sp;
-    const int nd = st_node[w][sp];
-    const unsigned mask = st_mask[w][sp];
+  while (__any_sync(0xffffffffu, sp > 0)) {
+    const bool has = sp > 0;
+    int nd = 0;
+    unsigned mask = 0u;
+    if (has) {
+      --sp;
+      nd = st_node[w][g][sp];
+      mask = st_mask[w][g][sp];
+    }
     __syncwarp();
-    const int4 q = qchild[nd];
+    int4 q = make_int4(kNone, kNone, kNone, kNone);
+    if (has) q = qchild[nd];
     const int qc[4] = {q.x, q.y, q.z, q.w};
-    unsigned om[4] = {0u, 0u, 0u, 0u};
+    const bool in = (mask >> lane) & 1u;
+    unsigned om[4];
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
       const int c = qc[h];
-      if (c == kNone) continue;
-      if (c < 0) {  // single point
-        const int t = ~c;
-        if (((mask >> lane) & 1u) && t != s)
-          bh_direct(p.x, p.y, spos[t], k, md2, fx, fy);
-        continue;
-      }
-      om[h] = bh_eval(c, mask, lane, s, p, k, th2, md2, node, spos, fx, fy);
+      om[h] = bh_eval(c, in && c != kNone, c >= 0, s, p, k, th2, md2, node, spos, fx, fy) &
+              gmask;
     }
     const int np = (om[0] != 0u) + (om[1] != 0u) + (om[2] != 0u) + (om[3] != 0u);
     if (sp + np > kStack) {
-      if (lane == 0) atomicOr(err, 1u);
-      continue;
-    }
-    // push the opened children in reverse so the first one is popped first
+      if (leader) atomicOr(err, 1u);
+    } else {
+      // push the opened children in reverse so the first one is popped first
 #pragma unroll
-    for (int h = 3; h >= 0; --h) {
-      if (om[h] != 0u) {
-        if (lane == 0) {
-          st_node[w][sp] = qc[h];
-          st_mask[w][sp] = om[h];
+      for (int h = 3; h >= 0; --h) {
+        if (om[h] != 0u) {
+          if (leader) {
+            st_node[w][g][sp] = qc[h];
+            st_mask[w][g][sp] = om[h];
+          }
+          ++sp;
         }
-        ++sp;
       }
     }
     __syncwarp();
