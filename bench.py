@@ -129,6 +129,23 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
+# stage's kernels at the default 1M-gate workload, from single ncu captures
+# (`--set full -s 1 -c 1` of the bench command with --steps 2 --warmup 3;
+# summaries under profiles/). A stage missing here reports traffic null.
+NCU_DRAM_BYTES = {
+    # bh_walk_kernel: 59.568 MB read + 2.309 MB written
+    "bh_walk": 61_876_736,
+    # 6 x tc_gemm_kernel<0> (21.000 MB + 0.011 MB each) + dens_charge_kernel
+    # (8.393 MB); dens_scatter runs in the previous step's fused kernel
+    "density": 6 * 21_010_944 + 8_393_472,
+}
+# What bounds each stage when it is not HBM or the tensor pipe (ncu).
+NCU_LIMITER = {
+    "bh_walk": "instruction issue: 87% issue-active, 0.5% of DRAM peak, 81% warps active",
+}
+
+
 # ---------------------------------------------------------------------------
 def algorithmic(n, m, p, a, G, gc):
     """Compulsory HBM bytes (each array read once, each output written once)
@@ -371,14 +388,18 @@ def run_fluxion(args, rank, world, local_rank):
         ach = f_alg["density"] / (per_iter[dom] * 1e-3) / 1e12
         peak = bf16 if args.precision == "bf16" else bf16 / 2
         roof = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                "frac": ach / peak, "traffic": None, "kernel": dom,
+                "frac": ach / peak, "traffic": NCU_DRAM_BYTES.get(dom), "kernel": dom,
                 "peak_source": f"{src} bf16 dense" + ("" if args.precision == "bf16"
                                                       else " / 2 (tf32)")}
     else:
         ach = b_alg[dom] / (per_iter[dom] * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": None, "kernel": dom,
-                "peak_source": f"{src} HBM copy"}
+                "frac": ach / hbm, "traffic": NCU_DRAM_BYTES.get(dom), "kernel": dom,
+                "algorithmic_bytes": b_alg[dom], "peak_source": f"{src} HBM copy"}
+    if dom in NCU_LIMITER:
+        roof["limiter"] = NCU_LIMITER[dom]
+    if args.gates != 1_000_000 or args.bins != 1024 or args.precision != "fp32":
+        roof["traffic"] = None  # the captures are of the default workload
     B_iter = sum(b_alg.values())
     it_ms = ms_max / args.steps
 
