@@ -132,6 +132,36 @@ int fx_congestion(fx_ctx *ctx, fx_design *design, const float *x,
                   uint32_t *out_counts, double *out_hpwl,
                   double *out_total_overflow, float *out_max_overflow);
 
+/* Congestion without any device allocation. No counterpart in the reference
+ * (its congestion runs on host Vecs); this is an extra entry point beside
+ * fx_congestion for callers that may not allocate device memory during the
+ * call: fx_congestion allocates its workspace on first use and again when
+ * the grid changes size, which can fail when the caller's own memory pool
+ * holds the HBM, and cudaFree waits for the whole device. Same kernels and
+ * results as fx_congestion (bit-identical counts, HPWL and overflow).
+ *
+ * Scratch: one fixed 8 MiB device array per device inside the library;
+ * the difference array needs (rows+1)*(cols+1)*4 bytes of it, so grids up to
+ * 2,080,000 such entries (about 1440 x 1440) are accepted and larger ones
+ * are rejected with FX_EINVAL (use fx_congestion for those).
+ * Inputs and outputs are DEVICE pointers owned by the caller:
+ *   d_x, d_y           positions (n_gates floats each), or both NULL to use
+ *                      the design's resident positions;
+ *   d_counts           rows*cols uint32 (required);
+ *   d_hpwl_overflow    2 doubles {HPWL, total overflow}, or NULL;
+ *   d_max_overflow     1 float, or NULL.
+ * The work is enqueued on the context's stream and the call returns without
+ * waiting; results are ready after fx_ctx_synchronize (or anything ordered
+ * after that stream). The first call on a device sets the scratch up
+ * (cudaGetSymbolAddress, then a synchronous zeroing), so make that first
+ * call before any stream capture begins. Calls share the scratch: two calls
+ * that overlap on one device (different contexts, streams or host threads)
+ * race and corrupt each other's counts; order them. */
+int fx_congestion_noalloc(fx_ctx *ctx, const fx_design *design, const float *d_x,
+                          const float *d_y, int32_t cols, int32_t rows,
+                          uint32_t *d_counts, double *d_hpwl_overflow,
+                          float *d_max_overflow);
+
 /* ---- rows A..F: the plain composite force iteration -------------------- */
 typedef struct fx_iter_cfg {
   float attract_weight;  /* spring k (placer.rs:250, default 1.0)            */

@@ -6,6 +6,8 @@
 // Placement::compute_hpwl (H/src/data/placement.rs:48-74). The reference adds
 // 1.0f to every covered cell of two identical f32 grids; counts stay below
 // 2^24, so one exact uint32 grid carries both.
+#include <mutex>
+
 #include "fx_internal.h"
 #include "fx_device.cuh"
 
@@ -268,5 +270,127 @@ extern "C" int fx_congestion(fx_ctx *ctx, fx_design *d, const float *x,
   if (out_hpwl) *out_hpwl = res[0];
   if (out_total_overflow) *out_total_overflow = res[1];
   if (out_max_overflow) *out_max_overflow = mx;
+  return FX_OK;
+}
+
+// ---- congestion without allocation --------------------------------------------
+// fx_congestion sizes its workspace on first use and again whenever the grid
+// changes. Some callers may not allocate device memory at that point: a host
+// framework whose own pool already holds the HBM (a fresh cudaMalloc can then
+// fail mid-run), or a loop that cannot accept the device-wide wait that
+// cudaFree implies while other streams are busy. fx_congestion_noalloc runs
+// the same three kernels with all their scratch in one fixed array declared
+// below, and writes its results to device buffers the caller already owns.
+namespace fx {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Layout of the scratch array (byte offsets, each 256-aligned):
+//   [0]      two last-block counters        -- must be zero when a call starts
+//   [256]    result slots for NULL outputs  (2 doubles + 1 float)
+//   [512]    FP64 block partials            (kMaxNetBlocks + 4096 doubles)
+//   [..]     f32 block maxima               (4096 floats)
+//   [..]     difference array               -- must be zero when a call starts
+// Each successful call leaves both zero-required regions zero again: the
+// column scan clears every difference entry it reads and the last block of
+// each reduction resets its counter. The first call on a device zeroes the
+// whole array; a call that fails after launching marks the device so the
+// next call zeroes it again before use.
+constexpr size_t kNaDone = 0;
+constexpr size_t kNaResult = 256;
+constexpr size_t kNaPartial = 512;
+constexpr size_t kNaPartialMax = kNaPartial + (size_t)(kMaxNetBlocks + 4096) * 8;
+constexpr size_t kNaDiff = kNaPartialMax + 4096 * 4;
+constexpr size_t kNaDiffEntries = (kNoAllocScratchBytes - kNaDiff) / 4;
+static_assert(kNaPartialMax % 256 == 0 && kNaDiff % 256 == 0, "scratch alignment");
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mu;
+unsigned char *g_na_ptr[kNaMaxDevices] = {};
+bool g_na_dirty[kNaMaxDevices] = {};
+
+// Once per device: the device address of the scratch array, zeroed.
+int noalloc_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= kNaMaxDevices) {
+    set_error("fx_congestion_noalloc: device %d out of range", device);
+    return FX_EINVAL;
+  }
+  if (!g_na_ptr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error("fx_congestion_noalloc: cudaGetSymbolAddress failed: %s",
+                cudaGetErrorString(e));
+      return FX_ECUDA;
+    }
+    FX_CHECK_CUDA(cudaMemset(p, 0, kNoAllocScratchBytes));
+    g_na_ptr[device] = static_cast<unsigned char *>(p);
+    g_na_dirty[device] = false;
+  }
+  *out = g_na_ptr[device];
+  return FX_OK;
+}
+
+}  // namespace
+}  // namespace fx
+
+extern "C" int fx_congestion_noalloc(fx_ctx *ctx, const fx_design *d, const float *d_x,
+                                     const float *d_y, int32_t cols, int32_t rows,
+                                     uint32_t *d_counts, double *d_hpwl_overflow,
+                                     float *d_max_overflow) {
+  if (!ctx || !d || !d_counts || cols <= 0 || rows <= 0 ||
+      (d_x == nullptr) != (d_y == nullptr)) {
+    set_error("fx_congestion_noalloc: invalid arguments");
+    return FX_EINVAL;
+  }
+  const int64_t entries = (int64_t)(cols + 1) * (rows + 1);
+  if (entries > (int64_t)kNaDiffEntries || (cols + 31) / 32 > 4096) {
+    set_error("fx_congestion_noalloc: a %d x %d grid needs %lld bytes of scratch, the "
+              "fixed array holds %zu; use fx_congestion for this grid",
+              cols, rows, (long long)(entries * 4), (size_t)(kNaDiffEntries * 4));
+    return FX_EINVAL;
+  }
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  unsigned char *sc = nullptr;
+  FX_TRY(noalloc_scratch(ctx->device, &sc));
+  cudaStream_t s = ctx->stream;
+  if (g_na_dirty[ctx->device]) {
+    FX_CHECK_CUDA(cudaMemsetAsync(sc, 0, kNoAllocScratchBytes, s));
+    g_na_dirty[ctx->device] = false;
+  }
+  unsigned int *done = reinterpret_cast<unsigned int *>(sc + kNaDone);
+  double *partial = reinterpret_cast<double *>(sc + kNaPartial);
+  float *pmax = reinterpret_cast<float *>(sc + kNaPartialMax);
+  int32_t *diff = reinterpret_cast<int32_t *>(sc + kNaDiff);
+  double *result = d_hpwl_overflow ? d_hpwl_overflow
+                                   : reinterpret_cast<double *>(sc + kNaResult);
+  float *result_max = d_max_overflow ? d_max_overflow
+                                     : reinterpret_cast<float *>(sc + kNaResult + 16);
+  const float *px = d_x ? d_x : d->x[d->cur].p;
+  const float *py = d_y ? d_y : d->y[d->cur].p;
+  // RoutingGrid::new (grid.rs:27-31), as in congestion_run
+  const float cw = d->chip_w / (float)cols;
+  const float ch = d->chip_h / (float)rows;
+  const float cap = (cw + ch) * 0.5f;
+  int nb = (d->m + kNetThreads - 1) / kNetThreads;
+  if (nb > kMaxNetBlocks) nb = kMaxNetBlocks;
+  if (nb < 1) nb = 1;
+  cong_nets_kernel<<<nb, kNetThreads, 0, s>>>(d->net_ptr.p, d->net_gate.p, px, py, d->m,
+                                               cw, ch, cols, rows, diff, partial, done,
+                                               result);
+  cong_scan_rows_kernel<<<rows, 1024, 0, s>>>(diff, cols, rows);
+  cong_scan_cols_kernel<<<(cols + 31) / 32, dim3(32, 32), 0, s>>>(
+      diff, d_counts, cols, rows, cap, partial + kMaxNetBlocks, pmax, done + 1, result,
+      result_max);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_na_dirty[ctx->device] = true;
+    set_error("fx_congestion_noalloc: launch failed: %s", cudaGetErrorString(e));
+    return FX_ECUDA;
+  }
+  ctx->launches += 3;
   return FX_OK;
 }

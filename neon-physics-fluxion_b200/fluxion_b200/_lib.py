@@ -117,6 +117,8 @@ SIGNATURES = {
     "fx_design_restore_state": (C.c_int, [P]),
     "fx_design_device_bytes": (C.c_int64, [P]),
     "fx_congestion": (C.c_int, [P, P, PF32, PF32, I32, I32, PU32, PF64, PF64, PF32]),
+    # device pointers throughout
+    "fx_congestion_noalloc": (C.c_int, [P, P, P, P, I32, I32, P, P, P]),
     "fx_iter_cfg_default": (C.c_int, [C.POINTER(IterCfg)]),
     "fx_force_iterate": (C.c_int, [P, P, C.POINTER(IterCfg), I32, PF32, PF32,
                                    C.POINTER(IterStats)]),

@@ -343,6 +343,17 @@ class Design:
                                   ptr(its, C.c_int32), ptr(lam, C.c_double)), "fx_fiedler")
         return v, its, lam
 
+    def congestion_noalloc(self, cols: int, rows: int, d_counts: int, d_x: int = 0,
+                           d_y: int = 0, d_hpwl_overflow: int = 0,
+                           d_max_overflow: int = 0) -> None:
+        """fx_congestion_noalloc: device pointers (ints, 0 = NULL) in and out,
+        enqueued on the context's stream without allocating; synchronize the
+        context before reading the outputs."""
+        vp = lambda a: C.c_void_p(a) if a else None
+        check(self.lib.fx_congestion_noalloc(self.ctx.handle, self.handle, vp(d_x), vp(d_y),
+                                             cols, rows, vp(d_counts), vp(d_hpwl_overflow),
+                                             vp(d_max_overflow)), "fx_congestion_noalloc")
+
     # -- congestion refinement ----------------------------------------------------
     def refine(self, cfg=None, x=None, y=None, counts: bool = False):
         """refiner.rs:34-126 refine_placement. With x/y (host arrays, updated
