@@ -162,6 +162,37 @@ int fx_congestion_noalloc(fx_ctx *ctx, const fx_design *design, const float *d_x
                           uint32_t *d_counts, double *d_hpwl_overflow,
                           float *d_max_overflow);
 
+/* ---- (f.2) hierarchy build: recursive spectral bisection ---------------- */
+/* Mirrors build_hierarchy (H/src/algorithm/partitioner.rs:36-100, with
+ * compute_fiedler_vector :106-185 and split_by_fiedler :189-213) and the
+ * region pass of hapr_placement (H/src/algorithm/placer.rs:40-63,111-141):
+ * returns the leaves in HierarchyTree::leaves() order (hierarchy.rs:176-190)
+ * with their gates, regions (cx, cy, w, h) and depths. All clusters of one
+ * depth run on the device together. */
+#define FX_PART_EXACT 0 /* the reference's f32 iteration; identical leaves       */
+#define FX_PART_FP64 1  /* FP64 norms / Rayleigh quotient, stop at tol           */
+typedef struct fx_part_cfg {
+  int32_t max_leaf_size;    /* PartitionConfig (partitioner.rs:24-32): 64        */
+  int32_t min_cluster_size; /* 8                                                 */
+  float balance_factor;     /* 0.4, in [0, 0.5]                                  */
+  int32_t power_iterations; /* 30 (main.rs:80); EXACT runs exactly this many,    */
+                            /* FP64 at most this many                            */
+  int32_t mode;             /* FX_PART_*                                         */
+  int32_t reserved0;
+  double tol;               /* FP64: relative change of the Rayleigh quotient    */
+} fx_part_cfg;
+typedef struct fx_part_stats {
+  int32_t n_leaves, n_nodes, max_depth, levels;
+  int64_t power_iterations; /* summed over the bisected clusters                 */
+} fx_part_stats;
+int fx_part_cfg_default(fx_part_cfg *cfg);
+/* out_leaf_ptr[leaf_capacity+1], out_leaf_gate[n_gates],
+ * out_region[4*leaf_capacity], out_leaf_depth[leaf_capacity]; any may be NULL.
+ * FX_EINVAL if the tree has more leaves than leaf_capacity. */
+int fx_partition(fx_ctx *ctx, fx_design *design, const fx_part_cfg *cfg,
+                 int32_t leaf_capacity, int32_t *out_leaf_ptr, int32_t *out_leaf_gate,
+                 float *out_region, int32_t *out_leaf_depth, fx_part_stats *out_stats);
+
 /* ---- rows A..F: the plain composite force iteration -------------------- */
 typedef struct fx_iter_cfg {
   float attract_weight;  /* spring k (placer.rs:250, default 1.0)            */

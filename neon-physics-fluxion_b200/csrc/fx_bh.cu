@@ -263,6 +263,28 @@ radix_scatter_kernel(const uint32_t *__restrict__ kin,
   }
 }
 
+// Stable LSD sort of (key, value) pairs on the low 8*passes key bits. The
+// pairs start in (k[0], v[0]); the result is in (k[passes & 1], v[passes & 1]).
+// Workspace: tile_hist / tile_scan of 256 * radix_sort_tiles(n) words each
+// and digit_total of 256 words.
+int radix_sort_pairs(uint32_t *k[2], int32_t *v[2], int n, int passes,
+                     uint32_t *tile_hist, uint32_t *tile_scan, uint32_t *digit_total,
+                     cudaStream_t s) {
+  if (n <= 0) return FX_OK;
+  const int T = (n + kSortTile - 1) / kSortTile;
+  for (int pass = 0; pass < passes; ++pass) {
+    const int src = pass & 1, dst = src ^ 1;
+    radix_hist_kernel<<<T, kSortThreads, 0, s>>>(k[src], n, 8 * pass, tile_hist, T);
+    radix_scan_kernel<<<256, 256, 0, s>>>(tile_hist, tile_scan, digit_total, T);
+    radix_scatter_kernel<<<T, kSortThreads, 0, s>>>(k[src], v[src], k[dst], v[dst], n,
+                                                    8 * pass, tile_scan, digit_total, T);
+  }
+  FX_CHECK_LAUNCH();
+  return FX_OK;
+}
+
+int radix_sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
+
 // ---- sorted positions --------------------------------------------------------------
 __global__ void bh_gather_kernel(const float *__restrict__ x,
                                  const float *__restrict__ y,

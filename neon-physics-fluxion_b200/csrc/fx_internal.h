@@ -223,6 +223,11 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
                 int precision, bool need_phi, cudaStream_t s);
 int fused_step(fx_ctx *ctx, fx_design *d, const fx_iter_cfg &cfg,
                cudaStream_t s);
+// Stable LSD radix sort of (key, value) pairs (fx_bh.cu).
+int radix_sort_pairs(uint32_t *k[2], int32_t *v[2], int n, int passes,
+                     uint32_t *tile_hist, uint32_t *tile_scan, uint32_t *digit_total,
+                     cudaStream_t s);
+int radix_sort_tiles(int n);
 void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a);
 void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a);
 }  // namespace fx

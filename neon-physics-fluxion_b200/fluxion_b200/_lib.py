@@ -83,6 +83,20 @@ class RefineStats(C.Structure):
                 ("hpwl", C.c_double)]
 
 
+class PartCfg(C.Structure):
+    _fields_ = [("max_leaf_size", C.c_int32), ("min_cluster_size", C.c_int32),
+                ("balance_factor", C.c_float), ("power_iterations", C.c_int32),
+                ("mode", C.c_int32), ("reserved0", C.c_int32), ("tol", C.c_double)]
+
+
+class PartStats(C.Structure):
+    _fields_ = [("n_leaves", C.c_int32), ("n_nodes", C.c_int32), ("max_depth", C.c_int32),
+                ("levels", C.c_int32), ("power_iterations", C.c_int64)]
+
+
+FX_PART_EXACT = 0
+FX_PART_FP64 = 1
+
 P = C.c_void_p
 I32 = C.c_int32
 I64 = C.c_int64
@@ -133,6 +147,9 @@ SIGNATURES = {
                                        PF32, PF32, PI32]),
     "fx_fiedler": (C.c_int, [P, P, I32, PI32, PI32, I32, C.c_double, PF32, PI32, PF64]),
     "fx_refine_cfg_default": (C.c_int, [C.POINTER(RefineCfg)]),
+    "fx_part_cfg_default": (C.c_int, [C.POINTER(PartCfg)]),
+    "fx_partition": (C.c_int, [P, P, C.POINTER(PartCfg), I32, PI32, PI32, PF32, PI32,
+                               C.POINTER(PartStats)]),
     "fx_refine": (C.c_int, [P, P, C.POINTER(RefineCfg), PF32, PF32, C.POINTER(RefineStats),
                             PU32]),
     "fx_synth_plain": (C.c_int, [C.c_uint64, I32, I32, F32, F32, I32, C.POINTER(P)]),

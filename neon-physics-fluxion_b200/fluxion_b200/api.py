@@ -354,6 +354,27 @@ class Design:
                                              cols, rows, vp(d_counts), vp(d_hpwl_overflow),
                                              vp(d_max_overflow)), "fx_congestion_noalloc")
 
+    # -- hierarchy build ---------------------------------------------------------
+    def partition(self, cfg=None) -> dict:
+        """build_hierarchy (partitioner.rs:36-100) + leaf regions (placer.rs:40-63):
+        leaf_ptr[L+1], leaf_gate[N], region[L, 4] = (cx, cy, w, h), leaf_depth[L],
+        and the fx_part_stats fields."""
+        cfg = cfg if cfg is not None else part_cfg()
+        cap = self.n + 1
+        lp = np.zeros(cap + 1, np.int32)
+        lg = np.zeros(max(self.n, 1), np.int32)
+        rg = np.zeros(4 * cap, np.float32)
+        ld = np.zeros(cap, np.int32)
+        st = _lib.PartStats()
+        check(self.lib.fx_partition(self.ctx.handle, self.handle, C.byref(cfg), cap,
+                                    ptr(lp, C.c_int32), ptr(lg, C.c_int32),
+                                    ptr(rg, C.c_float), ptr(ld, C.c_int32), C.byref(st)),
+              "fx_partition")
+        L = st.n_leaves
+        return dict(leaf_ptr=lp[:L + 1], leaf_gate=lg[:self.n], region=rg[:4 * L].reshape(L, 4),
+                    leaf_depth=ld[:L], num_nodes=st.n_nodes, max_depth=st.max_depth,
+                    levels=st.levels, power_iterations=st.power_iterations)
+
     # -- congestion refinement ----------------------------------------------------
     def refine(self, cfg=None, x=None, y=None, counts: bool = False):
         """refiner.rs:34-126 refine_placement. With x/y (host arrays, updated
@@ -390,6 +411,16 @@ class Design:
 def leaf_cfg(**overrides) -> "_lib.LeafCfg":
     cfg = _lib.LeafCfg()
     check(load().fx_leaf_cfg_default(C.byref(cfg)), "fx_leaf_cfg_default")
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
+
+
+def part_cfg(**overrides) -> "_lib.PartCfg":
+    cfg = _lib.PartCfg()
+    check(load().fx_part_cfg_default(C.byref(cfg)), "fx_part_cfg_default")
     for k, v in overrides.items():
         if not hasattr(cfg, k):
             raise KeyError(k)
