@@ -275,6 +275,7 @@ extern "C" int fx_stage_attraction(fx_ctx *ctx, fx_design *d, float k,
                                    float *out_fx, float *out_fy) {
   if (!ctx || !d) return FX_EINVAL;
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   FX_TRY(attraction_run(ctx, d, k, d->fattr.p, s));
   std::vector<float2> f((size_t)d->n);
@@ -304,6 +305,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   const fx_iter_cfg c = *cfg;
   FX_TRY(validate_cfg(c));
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream, s2 = ctx->stream2;
   if (x) FX_TRY(fx_design_set_positions(d, x, y));
   FX_TRY(step_alloc(d, s));

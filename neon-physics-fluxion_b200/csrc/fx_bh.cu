@@ -784,6 +784,7 @@ extern "C" int fx_stage_barnes_hut(fx_ctx *ctx, fx_design *d, float k,
     return FX_EINVAL;
   }
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   FX_TRY(bh_bbox(ctx, d, d->x[d->cur].p, d->y[d->cur].p, s));
   FX_TRY(bh_run(ctx, d, k, theta, min_dist, s));

@@ -244,6 +244,7 @@ extern "C" int fx_congestion(fx_ctx *ctx, fx_design *d, const float *x,
     return FX_EINVAL;
   }
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   const float *dx = d->x[d->cur].p, *dy = d->y[d->cur].p;
   if (x) {

@@ -9,6 +9,7 @@
 namespace fx {
 
 static thread_local char g_err[512] = "";
+thread_local cudaStream_t g_alloc_stream = nullptr;
 
 void set_error(const char *fmt, ...) {
   va_list ap;
@@ -164,6 +165,14 @@ extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
     delete c;
     return FX_ECUDA;
   }
+  // Freed stream-ordered allocations stay in the device's pool for reuse,
+  // so a call's temporaries cost no driver allocation after the first.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   *out_ctx = c;
   return FX_OK;
 }
@@ -301,6 +310,7 @@ extern "C" int fx_design_load(fx_ctx *ctx, int32_t n_gates, int32_t n_nets,
   FX_TRY(validate_netlist(n_gates, n_nets, net_ptr, net_gate));
   const int64_t P = net_ptr[n_nets];
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   fx_design *d = new (std::nothrow) fx_design();
   if (!d) return FX_ENOMEM;
   d->ctx = ctx;
@@ -440,6 +450,7 @@ extern "C" int fx_design_get_positions(fx_design *d, float *out_x,
 extern "C" int fx_design_save_state(fx_design *d) {
   if (!d) return FX_EINVAL;
   FX_CHECK_CUDA(cudaSetDevice(d->ctx->device));
+  AllocScope alloc_scope(d->ctx->stream);
   cudaStream_t s = d->ctx->stream;
   const size_t b = (size_t)d->n * 4;
   const float *src[4] = {d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p};

@@ -313,6 +313,7 @@ extern "C" int fx_stage_density(fx_ctx *ctx, fx_design *d, int32_t bins,
     return FX_EINVAL;
   }
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   const float *x = d->x[d->cur].p, *y = d->y[d->cur].p;
   FX_TRY(density_scatter(ctx, d, x, y, bins, precision, s));

@@ -191,6 +191,7 @@ extern "C" int fx_fiedler(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   chunk_start.push_back(G);
   const int K = (int)chunk_cluster.size();
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   DevBuf<int32_t> d_rptr, d_ridx, d_cs, d_cc, d_clp, d_clc, d_act, d_it;
   DevBuf<float> d_deg, d_v, d_lv, d_mean, d_inv;

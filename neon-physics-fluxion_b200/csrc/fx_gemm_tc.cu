@@ -382,16 +382,22 @@ static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands 
     talo = ta;
     tblo = tb;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    FX_CHECK_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<PREC>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       Cfg::kSmem));
-    attr_set = true;
-  }
-  if (!g_tc_err.p) {
-    FX_TRY(g_tc_err.alloc(1));
-    FX_CHECK_CUDA(cudaMemset(g_tc_err.p, 0, 4));
+  {
+    // one-time set-up, shared by all contexts and host threads
+    static std::mutex mu;
+    static bool attr_set = false;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!attr_set) {
+      FX_CHECK_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<PREC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Cfg::kSmem));
+      attr_set = true;
+    }
+    if (!g_tc_err.p) {
+      AllocScope global_alloc(nullptr);  // a library global: plain cudaMalloc
+      FX_TRY(g_tc_err.alloc(1));
+      FX_CHECK_CUDA(cudaMemset(g_tc_err.p, 0, 4));
+    }
   }
   dim3 grid(G / kTcBN, G / kTcBM);
   tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(ta, talo, tb, tblo, G, S, D.f32,

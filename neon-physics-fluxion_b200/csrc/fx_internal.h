@@ -38,19 +38,52 @@ struct Status {
 #define FX_CHECK_LAUNCH() FX_CHECK_CUDA(cudaGetLastError())
 
 // ---- device buffers --------------------------------------------------------
-// A typed device allocation owned by a design or context.
+// Allocation stream of the calling thread. Inside an API call it is the
+// context's primary stream (set by AllocScope), and DevBufs are then
+// stream-ordered (cudaMallocAsync / cudaFreeAsync from the device's pool,
+// whose memory is retained): allocating or freeing does not wait for the
+// whole device, so jobs on other contexts keep running. Memory allocated
+// this way is used on that stream, or on another stream only after an
+// event recorded on it later. Without a scope (library globals) DevBuf uses
+// cudaMalloc / cudaFree.
+extern thread_local cudaStream_t g_alloc_stream;
+
+struct AllocScope {
+  cudaStream_t prev;
+  explicit AllocScope(cudaStream_t s) : prev(g_alloc_stream) { g_alloc_stream = s; }
+  ~AllocScope() { g_alloc_stream = prev; }
+  AllocScope(const AllocScope &) = delete;
+  AllocScope &operator=(const AllocScope &) = delete;
+};
+
+// A typed device allocation owned by a design, a context or a call.
 template <typename T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  cudaStream_t owner = nullptr;  // stream of a pooled allocation
+  bool pooled = false;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
   int alloc(size_t count) {
     if (count <= n && p) return FX_OK;
     release();
     if (count == 0) return FX_OK;
-    cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+    cudaError_t e;
+    if (g_alloc_stream) {
+      e = cudaMallocAsync((void **)&p, count * sizeof(T), g_alloc_stream);
+      pooled = true;
+      owner = g_alloc_stream;
+    } else {
+      e = cudaMalloc((void **)&p, count * sizeof(T));
+      pooled = false;
+      owner = nullptr;
+    }
     if (e != cudaSuccess) {
       p = nullptr;
-      set_error("cudaMalloc(%zu bytes): %s", count * sizeof(T),
+      set_error("device allocation of %zu bytes: %s", count * sizeof(T),
                 cudaGetErrorString(e));
       return FX_ENOMEM;
     }
@@ -58,9 +91,14 @@ struct DevBuf {
     return FX_OK;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (pooled) cudaFreeAsync(p, owner);
+      else cudaFree(p);
+    }
     p = nullptr;
     n = 0;
+    pooled = false;
+    owner = nullptr;
   }
   size_t bytes() const { return n * sizeof(T); }
 };

@@ -281,6 +281,7 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
       return FX_EINVAL;
     }
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   LeafHost h;
   FX_TRY(build_leaf_host(d, n_leaves, leaf_ptr, leaf_gate, h));

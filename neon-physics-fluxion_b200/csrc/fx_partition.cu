@@ -411,6 +411,7 @@ extern "C" int fx_partition(fx_ctx *ctx, fx_design *d, const fx_part_cfg *cfg,
     return FX_EINVAL;
   }
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   const bool exact = cfg->mode == FX_PART_EXACT;
   int64_t total_iters = 0;

@@ -102,6 +102,7 @@ extern "C" int fx_refine(fx_ctx *ctx, fx_design *d, const fx_refine_cfg *cfg,
     return FX_EINVAL;
   }
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
   if (x) FX_TRY(fx_design_set_positions(d, x, y));
   const int cols = cfg->grid_cols, rows = cfg->grid_rows, cells = cols * rows;
