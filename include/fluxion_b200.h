@@ -342,6 +342,80 @@ int fx_refine_cfg_default(fx_refine_cfg *cfg);
 int fx_refine(fx_ctx *ctx, fx_design *design, const fx_refine_cfg *cfg,
               float *x, float *y, fx_refine_stats *stats, uint32_t *out_counts);
 
+/* ---- serving: continuous batching of placement and ECO jobs ------------- */
+/* A request server on one GPU (the survey's serving pattern; the reference
+ * has no server: FluxionEngine.place runs one placement per process,
+ * H/python/fluxion/engine.py:25-50). Jobs:
+ *   FX_JOB_PLACE  the reference's main.rs flow (H/src/main.rs:74-111) on a
+ *                 netlist: fx_partition -> fx_hapr_place_leaves -> fx_refine;
+ *                 the placed design can stay resident for later ECO jobs;
+ *   FX_JOB_ECO    on a resident design: move the given gates (clamped to the
+ *                 die), then `iterations` plain iterations (fx_force_iterate).
+ * Up to `slots` jobs run at once, each on its own worker thread and context
+ * (own streams), so their kernels overlap on the device. A queued job is
+ * admitted when a slot is free and its estimated device footprint fits in
+ * what the budget has left (resident designs count at their actual size);
+ * jobs that fit may pass a larger one waiting at the head of the queue, but
+ * jobs on one design run in submission order. A job whose estimate exceeds
+ * the whole budget, or a full queue, is refused at submit with FX_EADMIT.
+ * Every job computes exactly what it would compute alone (own buffers and
+ * streams, fixed reduction orders, no atomics shared between jobs). */
+typedef struct fx_server fx_server;
+#define FX_JOB_PLACE 0
+#define FX_JOB_ECO 1
+typedef struct fx_serve_cfg {
+  int32_t device;
+  int32_t slots;            /* jobs on the GPU at once (default 8)                */
+  int32_t queue_capacity;   /* queued jobs before FX_EADMIT (default 65536)       */
+  int32_t reserved0;
+  int64_t hbm_budget_bytes; /* admission budget; 0 = 80 % of free memory at start */
+} fx_serve_cfg;
+typedef struct fx_job_desc {
+  int32_t kind;             /* FX_JOB_*                                            */
+  int32_t keep_resident;    /* PLACE: keep the placed design for ECO jobs          */
+  int64_t design_id;        /* ECO: job id of the PLACE job that made the design   */
+  int32_t n_gates, n_nets;  /* PLACE: the netlist, copied at submit                */
+  const int32_t *net_ptr, *net_gate;
+  const float *gate_w, *gate_h;
+  float chip_w, chip_h;
+  int32_t n_moves;          /* ECO: gate moves, copied at submit                   */
+  int32_t iterations;       /* ECO: plain iterations after the moves               */
+  const int32_t *move_gate;
+  const float *move_dx, *move_dy;
+  const fx_part_cfg *part;  /* stage configurations; NULL = defaults (ECO: the     */
+  const fx_leaf_cfg *leaf;  /* iteration default with a G x G density grid, G the  */
+  const fx_refine_cfg *refine; /* multiple of 128 nearest sqrt(n) in [128, 1024],  */
+  const fx_iter_cfg *iter;  /* and a 256 x 256 congestion grid)                    */
+} fx_job_desc;
+typedef struct fx_job_result {
+  int64_t job_id, design_id;
+  int32_t kind, status;     /* status: FX_OK or the failing FX_* code              */
+  int32_t n_gates, n_leaves;
+  int32_t iterations;       /* refine (PLACE) or plain (ECO) iterations run        */
+  float max_overflow;
+  double hpwl;              /* FP64 HPWL of the final positions                    */
+  double total_overflow;
+  double submit_s, start_s, end_s; /* server clock, seconds since creation         */
+  int64_t est_bytes;        /* admission estimate                                  */
+  char error[160];
+} fx_job_result;
+int fx_serve_cfg_default(fx_serve_cfg *cfg);
+/* Host-only admission estimate of a job (ECO: uses n_gates of the design). */
+int fx_serve_estimate(const fx_job_desc *job, int64_t *out_bytes);
+int fx_serve_create(const fx_serve_cfg *cfg, fx_server **out);
+/* Waits for the running jobs; queued jobs are dropped; frees resident designs. */
+int fx_serve_destroy(fx_server *server);
+int fx_serve_submit(fx_server *server, const fx_job_desc *job, int64_t *out_job_id);
+/* Next finished job in completion order: 1 when *out was filled, 0 when none
+ * finished within wait_ms (wait_ms < 0 waits until one does or nothing is
+ * queued or running). */
+int fx_serve_poll(fx_server *server, int32_t wait_ms, fx_job_result *out);
+/* Positions of a resident design (waits while a job runs on it). */
+int fx_serve_positions(fx_server *server, int64_t design_id, float *out_x, float *out_y);
+int fx_serve_release(fx_server *server, int64_t design_id);
+int fx_serve_stats(fx_server *server, int64_t *out_reserved_bytes, int32_t *out_queued,
+                   int32_t *out_running, int32_t *out_resident);
+
 /* ---- host-only helpers (no GPU needed) ---------------------------------- */
 /* Builds the deduplicated clique-expansion adjacency of
  * Circuit::build_adjacency (H/src/data/circuit.rs:154-171) in the

@@ -355,6 +355,7 @@ static int get_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
     return FX_OK;
   }
   FX_TRY(make_map(ptr, G, bf16, out));
+  if (cache.size() >= 4096) cache.clear();  // bounded: designs come and go
   cache.emplace(k, *out);
   return FX_OK;
 }

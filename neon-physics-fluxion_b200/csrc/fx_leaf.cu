@@ -23,6 +23,8 @@
 #include <numeric>
 #include <unordered_map>
 
+#include <mutex>
+
 #include "fx_internal.h"
 
 namespace fx {
@@ -202,12 +204,16 @@ static int launch_leaf(fx_ctx *ctx, const LeafBatch &b, bool per_cluster,
                        cudaStream_t s) {
   constexpr int kGroups = 256 / T;
   const size_t smem = (size_t)kGroups * kLeafArrays * kLeafMax * sizeof(float);
-  static bool attr = false;
-  if (!attr) {
-    FX_CHECK_CUDA(cudaFuncSetAttribute(leaf_batch_kernel<T>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-    attr = true;
+  {
+    static std::mutex mu;  // concurrent host threads (serving workers)
+    static bool attr = false;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!attr) {
+      FX_CHECK_CUDA(cudaFuncSetAttribute(leaf_batch_kernel<T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+      attr = true;
+    }
   }
   if (per_cluster) {
     for (int l = 0; l < b.n_leaves; ++l)

@@ -8,9 +8,10 @@ from ._lib import (FX_DCT_BF16, FX_DCT_FP32, FX_DCT_SIMT, FX_DCT_TF32, FX_LEAF_A
                    FX_LEAF_CTA64, FX_LEAF_CTA128, FX_LEAF_CTA256, FX_LEAF_PER_CLUSTER,
                    FX_LEAF_WARP, FX_PART_EXACT, FX_PART_FP64, FluxionError, IterCfg,
                    IterStats, LeafCfg, PartCfg, load)
-from .api import (Circuit, Context, Design, Placement, RoutingGrid, Synth,
+from .api import (Circuit, Context, Design, Placement, RoutingGrid, Server, Synth,
                   build_adjacency, build_and_compute, compute_congestion, compute_hpwl, default_context,
-                  iter_cfg, leaf_cfg, part_cfg, refine_cfg, synth_leaves, synth_plain)
+                  iter_cfg, leaf_cfg, part_cfg, refine_cfg, serve_estimate, synth_leaves,
+                  synth_plain)
 
 __all__ = [
     "Circuit", "Context", "Design", "Placement", "RoutingGrid", "Synth",
@@ -19,5 +20,5 @@ __all__ = [
     "load", "FX_DCT_FP32", "FX_DCT_TF32", "FX_DCT_BF16", "FX_DCT_SIMT", "leaf_cfg",
     "LeafCfg", "FX_LEAF_AUTO", "FX_LEAF_WARP", "FX_LEAF_CTA64", "FX_LEAF_CTA128",
     "FX_LEAF_CTA256", "FX_LEAF_PER_CLUSTER", "refine_cfg", "part_cfg", "PartCfg",
-    "FX_PART_EXACT", "FX_PART_FP64",
+    "FX_PART_EXACT", "FX_PART_FP64", "Server", "serve_estimate",
 ]

@@ -97,6 +97,35 @@ class PartStats(C.Structure):
 FX_PART_EXACT = 0
 FX_PART_FP64 = 1
 
+FX_JOB_PLACE = 0
+FX_JOB_ECO = 1
+
+
+class ServeCfg(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slots", C.c_int32), ("queue_capacity", C.c_int32),
+                ("reserved0", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("keep_resident", C.c_int32), ("design_id", C.c_int64),
+                ("n_gates", C.c_int32), ("n_nets", C.c_int32),
+                ("net_ptr", C.c_void_p), ("net_gate", C.c_void_p),
+                ("gate_w", C.c_void_p), ("gate_h", C.c_void_p),
+                ("chip_w", C.c_float), ("chip_h", C.c_float),
+                ("n_moves", C.c_int32), ("iterations", C.c_int32),
+                ("move_gate", C.c_void_p), ("move_dx", C.c_void_p), ("move_dy", C.c_void_p),
+                ("part", C.c_void_p), ("leaf", C.c_void_p), ("refine", C.c_void_p),
+                ("iter", C.c_void_p)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("job_id", C.c_int64), ("design_id", C.c_int64), ("kind", C.c_int32),
+                ("status", C.c_int32), ("n_gates", C.c_int32), ("n_leaves", C.c_int32),
+                ("iterations", C.c_int32), ("max_overflow", C.c_float), ("hpwl", C.c_double),
+                ("total_overflow", C.c_double), ("submit_s", C.c_double),
+                ("start_s", C.c_double), ("end_s", C.c_double), ("est_bytes", C.c_int64),
+                ("error", C.c_char * 160)]
+
 P = C.c_void_p
 I32 = C.c_int32
 I64 = C.c_int64
@@ -148,6 +177,15 @@ SIGNATURES = {
     "fx_fiedler": (C.c_int, [P, P, I32, PI32, PI32, I32, C.c_double, PF32, PI32, PF64]),
     "fx_refine_cfg_default": (C.c_int, [C.POINTER(RefineCfg)]),
     "fx_part_cfg_default": (C.c_int, [C.POINTER(PartCfg)]),
+    "fx_serve_cfg_default": (C.c_int, [C.POINTER(ServeCfg)]),
+    "fx_serve_estimate": (C.c_int, [C.POINTER(JobDesc), PI64]),
+    "fx_serve_create": (C.c_int, [C.POINTER(ServeCfg), C.POINTER(C.c_void_p)]),
+    "fx_serve_destroy": (C.c_int, [P]),
+    "fx_serve_submit": (C.c_int, [P, C.POINTER(JobDesc), PI64]),
+    "fx_serve_poll": (C.c_int, [P, I32, C.POINTER(JobResult)]),
+    "fx_serve_positions": (C.c_int, [P, I64, PF32, PF32]),
+    "fx_serve_release": (C.c_int, [P, I64]),
+    "fx_serve_stats": (C.c_int, [P, PI64, PI32, PI32, PI32]),
     "fx_partition": (C.c_int, [P, P, C.POINTER(PartCfg), I32, PI32, PI32, PF32, PI32,
                                C.POINTER(PartStats)]),
     "fx_refine": (C.c_int, [P, P, C.POINTER(RefineCfg), PF32, PF32, C.POINTER(RefineStats),

@@ -418,6 +418,120 @@ def leaf_cfg(**overrides) -> "_lib.LeafCfg":
     return cfg
 
 
+# ---------------------------------------------------------------------------
+# serving
+def _addr(a) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+class Server:
+    """fx_server: placement (PLACE) and ECO jobs admitted by device footprint
+    and run `slots` at a time, each on its own worker context."""
+
+    def __init__(self, device: int = 0, slots: int = 8, hbm_budget_bytes: int = 0,
+                 queue_capacity: int = 65536):
+        self.lib = load()
+        cfg = _lib.ServeCfg()
+        check(self.lib.fx_serve_cfg_default(C.byref(cfg)), "fx_serve_cfg_default")
+        cfg.device, cfg.slots = device, slots
+        cfg.hbm_budget_bytes, cfg.queue_capacity = hbm_budget_bytes, queue_capacity
+        h = C.c_void_p()
+        check(self.lib.fx_serve_create(C.byref(cfg), C.byref(h)), "fx_serve_create")
+        self.handle = h
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.fx_serve_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def place_desc(circuit: Circuit, keep_resident: bool = False, part=None, leaf=None,
+                   refine=None):
+        """(JobDesc, arrays it points to) for a PLACE job."""
+        arrs = [np.ascontiguousarray(circuit.net_ptr, np.int32),
+                np.ascontiguousarray(circuit.net_gate, np.int32),
+                np.ascontiguousarray(circuit.gate_widths, np.float32),
+                np.ascontiguousarray(circuit.gate_heights, np.float32)]
+        cfgs = [part, leaf, refine]
+        d = _lib.JobDesc(kind=_lib.FX_JOB_PLACE, keep_resident=int(keep_resident),
+                         n_gates=circuit.num_gates, n_nets=circuit.num_nets,
+                         net_ptr=_addr(arrs[0]), net_gate=_addr(arrs[1]),
+                         gate_w=_addr(arrs[2]), gate_h=_addr(arrs[3]),
+                         chip_w=circuit.chip_width, chip_h=circuit.chip_height,
+                         part=C.addressof(part) if part is not None else None,
+                         leaf=C.addressof(leaf) if leaf is not None else None,
+                         refine=C.addressof(refine) if refine is not None else None)
+        return d, (arrs, cfgs)
+
+    @staticmethod
+    def eco_desc(design_id: int, gates, dx, dy, iterations: int = 50, iter_cfg=None,
+                 n_gates: int = 0):
+        arrs = [np.ascontiguousarray(gates, np.int32), np.ascontiguousarray(dx, np.float32),
+                np.ascontiguousarray(dy, np.float32)]
+        d = _lib.JobDesc(kind=_lib.FX_JOB_ECO, design_id=design_id, n_gates=n_gates,
+                         n_moves=len(arrs[0]), iterations=iterations,
+                         move_gate=_addr(arrs[0]), move_dx=_addr(arrs[1]),
+                         move_dy=_addr(arrs[2]),
+                         iter=C.addressof(iter_cfg) if iter_cfg is not None else None)
+        return d, (arrs, [iter_cfg])
+
+    def submit(self, desc_and_keep) -> int:
+        desc, _keep = desc_and_keep
+        jid = C.c_int64()
+        check(self.lib.fx_serve_submit(self.handle, C.byref(desc), C.byref(jid)),
+              "fx_serve_submit")
+        return jid.value
+
+    def submit_place(self, circuit: Circuit, keep_resident: bool = False, **cfgs) -> int:
+        return self.submit(self.place_desc(circuit, keep_resident, **cfgs))
+
+    def submit_eco(self, design_id: int, gates, dx, dy, iterations: int = 50,
+                   iter_cfg=None) -> int:
+        return self.submit(self.eco_desc(design_id, gates, dx, dy, iterations, iter_cfg))
+
+    def poll(self, wait_ms: int = -1) -> Optional[dict]:
+        r = _lib.JobResult()
+        got = self.lib.fx_serve_poll(self.handle, wait_ms, C.byref(r))
+        if got < 0:
+            check(got, "fx_serve_poll")
+        if got == 0:
+            return None
+        out = {k: getattr(r, k) for k, _ in _lib.JobResult._fields_ if k != "error"}
+        out["error"] = r.error.decode(errors="replace")
+        return out
+
+    def positions(self, design_id: int, n: int):
+        x = np.empty(n, np.float32)
+        y = np.empty(n, np.float32)
+        check(self.lib.fx_serve_positions(self.handle, design_id, ptr(x, C.c_float),
+                                          ptr(y, C.c_float)), "fx_serve_positions")
+        return x, y
+
+    def release(self, design_id: int) -> None:
+        check(self.lib.fx_serve_release(self.handle, design_id), "fx_serve_release")
+
+    def stats(self) -> dict:
+        rb, q, r, res = C.c_int64(), C.c_int32(), C.c_int32(), C.c_int32()
+        check(self.lib.fx_serve_stats(self.handle, C.byref(rb), C.byref(q), C.byref(r),
+                                      C.byref(res)), "fx_serve_stats")
+        return dict(reserved_bytes=rb.value, queued=q.value, running=r.value,
+                    resident=res.value)
+
+
+def serve_estimate(desc_and_keep) -> int:
+    """Host-only admission estimate (bytes) of a job description."""
+    desc, _ = desc_and_keep
+    out = C.c_int64()
+    check(load().fx_serve_estimate(C.byref(desc), C.byref(out)), "fx_serve_estimate")
+    return out.value
+
+
 def part_cfg(**overrides) -> "_lib.PartCfg":
     cfg = _lib.PartCfg()
     check(load().fx_part_cfg_default(C.byref(cfg)), "fx_part_cfg_default")
