@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/fluxion_b200.h"
@@ -224,6 +225,9 @@ struct fx_ctx {
   int64_t launches = 0;
   cudaEvent_t marks[16] = {};
   int leaf_schedule = 0;           // last autotuned leaf schedule
+  // FX_LEAF_AUTO decisions by batch shape (leaf count, mean leaf size and
+  // iteration count, each as a power-of-two bucket)
+  std::unordered_map<uint32_t, int> leaf_tuned;
 };
 
 struct fx_design {

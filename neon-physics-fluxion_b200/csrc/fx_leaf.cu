@@ -321,9 +321,25 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
               cfg->force_iterations, cfg->attract_weight, cfg->repel_weight,
               cfg->damping, cfg->dt, ox.p, oy.p, counter.p};
   int schedule = cfg->schedule;
+  bool done = false;
+  auto lg2 = [](int64_t v) {
+    int b = 0;
+    while (v > 1) {
+      v >>= 1;
+      ++b;
+    }
+    return b;
+  };
+  const uint32_t shape = (uint32_t)lg2(n_leaves) | ((uint32_t)lg2(G / std::max(1, n_leaves)) << 8) |
+                         ((uint32_t)lg2(cfg->force_iterations) << 16);
   if (schedule == FX_LEAF_AUTO) {
-    // Autotune: time each schedule once on this batch (results are identical)
-    // and keep the fastest for this context.
+    auto it = ctx->leaf_tuned.find(shape);
+    if (it != ctx->leaf_tuned.end()) schedule = it->second;
+  }
+  if (schedule == FX_LEAF_AUTO) {
+    // Autotune: time each schedule once on this batch (results are identical,
+    // so the last run's output stands) and keep the fastest for batches of
+    // this shape on this context.
     float best = 1e30f;
     int best_s = FX_LEAF_CTA128;
     cudaEvent_t e0, e1;
@@ -348,13 +364,17 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->leaf_schedule = best_s;
+    ctx->leaf_tuned[shape] = best_s;
     schedule = best_s;
+    done = true;
   }
-  cudaEvent_t ev;
-  timer_begin(ctx, FX_STAGE_LEAF, s, &ev);
-  FX_TRY(run_schedule(ctx, b, schedule, s));
-  timer_end(ctx, FX_STAGE_LEAF, s, ev);
+  ctx->leaf_schedule = schedule;
+  if (!done) {
+    cudaEvent_t ev;
+    timer_begin(ctx, FX_STAGE_LEAF, s, &ev);
+    FX_TRY(run_schedule(ctx, b, schedule, s));
+    timer_end(ctx, FX_STAGE_LEAF, s, ev);
+  }
   FX_CHECK_CUDA(cudaMemcpyAsync(out_x, ox.p, (size_t)d->n * 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaMemcpyAsync(out_y, oy.p, (size_t)d->n * 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));

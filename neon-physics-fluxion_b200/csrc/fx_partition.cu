@@ -526,11 +526,14 @@ extern "C" int fx_partition(fx_ctx *ctx, fx_design *d, const fx_part_cfg *cfg,
         part_combine_kernel<<<cb, 64, 0, s>>>(C, beg.p, end.p, cl_ck.p, part.p, 1, cfg->tol,
                                               act.p, mean.p, nrm.p, lambda.p, iters.p);
         part_div_kernel<<<nb, 256, 0, s>>>(N, clp.p, act.p, lv.p, mean.p, nrm.p, v.p);
+        FX_CHECK_LAUNCH();
+        ctx->launches += 4;
+        if (cfg->tol <= 0.0) continue;  // fixed iteration count: nothing converges early
         FX_CHECK_CUDA(cudaMemsetAsync(any.p, 0, 4, s));
         part_retire_kernel<<<cb, 64, 0, s>>>(C, act.p, any.p);
         FX_CHECK_LAUNCH();
-        ctx->launches += 5;
-        if (cfg->tol > 0.0 && (it & 7) == 0) {  // every 8 iterations: all converged?
+        ctx->launches += 1;
+        if ((it & 7) == 0) {  // every 8 iterations: all converged?
           int32_t h_any = 0;
           FX_CHECK_CUDA(cudaMemcpyAsync(&h_any, any.p, 4, cudaMemcpyDeviceToHost, s));
           FX_CHECK_CUDA(cudaStreamSynchronize(s));

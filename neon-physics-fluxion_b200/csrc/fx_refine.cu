@@ -2,8 +2,9 @@
 // H/src/algorithm/refiner.rs:34-126) on the device.
 //
 // Each iteration: congestion counts (rows D+F kernels), the total overflow as
-// the reference's f32 running sum over cells in row-major order (one thread:
-// the stop and stall rules compare this exact value), then every gate whose
+// the reference's f32 running sum over cells in row-major order (one warp
+// stages tiles, one lane adds them in order: the stop and stall rules compare
+// this exact value), then every gate whose
 // cell is hot (overflow > threshold, gates_in_hot_cells, congestion.rs:77-93)
 // moves toward the first least-congested cell within radius 3
 // (move_gate_from_hot_cell, refiner.rs:92-126; Iterator::min_by keeps the
@@ -23,19 +24,39 @@ __device__ __forceinline__ float rclampf(float v, float lo, float hi) {
   return v;
 }
 
-// grid.rs:86-91 total_overflow: f32 running sum, row-major.
-__global__ void refine_total_kernel(const uint32_t *__restrict__ counts, int cells,
-                                    float cap, float *__restrict__ out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// grid.rs:86-91 total_overflow: f32 running sum, row-major. One warp: the
+// lanes compute a tile of overflows into shared memory, then lane 0 adds the
+// tile in cell order (the loads from shared memory run ahead of the adds, so
+// the fold costs about one add latency per cell). The maximum is order-free.
+constexpr int kTotalTile = 4096;
+
+__global__ void __launch_bounds__(32)
+refine_total_kernel(const uint32_t *__restrict__ counts, int cells, float cap,
+                    float *__restrict__ out) {
+  __shared__ float tile[kTotalTile];
+  const int lane = threadIdx.x;
   float t = 0.0f, mx = 0.0f;
-  for (int i = 0; i < cells; ++i) {
-    const float c = (float)counts[i];
-    const float ov = fmaxf(__fsub_rn(__fadd_rn(c, c), cap), 0.0f);
-    t = __fadd_rn(t, ov);
-    mx = fmaxf(mx, ov);
+  for (int base = 0; base < cells; base += kTotalTile) {
+    const int m = min(kTotalTile, cells - base);
+    for (int i = lane; i < m; i += 32) {
+      const float c = (float)counts[base + i];
+      const float ov = fmaxf(__fsub_rn(__fadd_rn(c, c), cap), 0.0f);
+      tile[i] = ov;
+      mx = fmaxf(mx, ov);
+    }
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll 16
+      for (int i = 0; i < m; ++i) t = __fadd_rn(t, tile[i]);
+    }
+    __syncwarp();
   }
-  out[0] = t;
-  out[1] = mx;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) {
+    out[0] = t;
+    out[1] = mx;
+  }
 }
 
 __global__ void refine_move_kernel(float *__restrict__ x, float *__restrict__ y, int n,
@@ -114,6 +135,7 @@ extern "C" int fx_refine(fx_ctx *ctx, fx_design *d, const fx_refine_cfg *cfg,
   DevBuf<unsigned int> moved;
   FX_TRY(tot.alloc(2));
   FX_TRY(moved.alloc(1));
+  FX_CHECK_CUDA(cudaMemsetAsync(moved.p, 0, 4, s));  // moves summed over iterations
   float prev = 3.40282347e+38f;
   int stall = 0, iters = 0;
   int64_t moves = 0;
@@ -132,16 +154,11 @@ extern "C" int fx_refine(fx_ctx *ctx, fx_design *d, const fx_refine_cfg *cfg,
       stall = 0;
     }
     prev = total;
-    FX_CHECK_CUDA(cudaMemsetAsync(moved.p, 0, 4, s));
     refine_move_kernel<<<(d->n + 255) / 256, 256, 0, s>>>(
         px, py, d->n, d->cong.counts.p, cols, rows, cw, ch, cap, cfg->overflow_threshold,
         cfg->move_distance, d->chip_w, d->chip_h, moved.p);
     FX_CHECK_LAUNCH();
     ctx->launches += 1;
-    unsigned int mv = 0;
-    FX_CHECK_CUDA(cudaMemcpyAsync(&mv, moved.p, 4, cudaMemcpyDeviceToHost, s));
-    FX_CHECK_CUDA(cudaStreamSynchronize(s));
-    moves += mv;
     ++iters;
   }
   FX_TRY(congestion_run(ctx, d, px, py, cols, rows, s));
@@ -151,11 +168,14 @@ extern "C" int fx_refine(fx_ctx *ctx, fx_design *d, const fx_refine_cfg *cfg,
   double hp = 0.0;
   FX_CHECK_CUDA(cudaMemcpyAsync(h, tot.p, 8, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaMemcpyAsync(&hp, d->cong.result.p, 8, cudaMemcpyDeviceToHost, s));
+  unsigned int mv = 0;
+  FX_CHECK_CUDA(cudaMemcpyAsync(&mv, moved.p, 4, cudaMemcpyDeviceToHost, s));
   if (out_counts)
     FX_CHECK_CUDA(cudaMemcpyAsync(out_counts, d->cong.counts.p, (size_t)cells * 4,
                                   cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
   if (x) FX_TRY(fx_design_get_positions(d, x, y));
+  moves = mv;
   if (stats) {
     stats->iterations = iters;
     stats->moves = moves;
