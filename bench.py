@@ -65,6 +65,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--trajectory", type=int, default=500,
                     help="iterations of the full run reported beside the steps (0: skip)")
+    ap.add_argument("--workload", default="plain", choices=["plain", "serve"],
+                    help="plain: the 1M-gate iteration; serve: the request stream")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
+    ap.add_argument("--slots", type=int, default=8, help="serve: concurrent jobs")
+    ap.add_argument("--pool", type=int, default=16, help="serve: distinct netlists")
     return ap.parse_args()
 
 
@@ -440,11 +446,253 @@ def run_fluxion(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+SERVE_METRIC = "served placement/ECO jobs/s (p50/p99 latency)"
+
+
+class ServeWorkload:
+    """The serving request stream: Poisson arrivals at `rate` for `duration`
+    seconds; 70 % PLACE jobs on netlists of log-uniform 5k-500k gates (die side
+    1.2 sqrt(N), drawn from a pool of `pool` seeded netlists), 30 % ECO jobs
+    that move 1 % of a resident design's gates by N(0, 2 density bins) and run
+    50 plain iterations. The first `pool` PLACE jobs keep their designs
+    resident as ECO targets."""
+
+    def __init__(self, args, fx):
+        rng = np.random.default_rng(args.seed + 1)
+        lo, hi = np.log(5_000), np.log(500_000)
+        sizes = sorted(int(np.exp(rng.uniform(lo, hi))) for _ in range(args.pool))
+        self.circuits = [fx.synth_plain(args.seed + 7 * i, n, int(1.2 * n), 1.2 * float(np.sqrt(n))).circuit
+                         for i, n in enumerate(sizes)]
+        self.part = fx.part_cfg(mode=fx.FX_PART_FP64, power_iterations=30, tol=0.0)
+        t, self.jobs = 0.0, []
+        resident = []  # (job index, circuit index)
+        while True:
+            t += rng.exponential(1.0 / args.rate)
+            if t > args.duration:
+                break
+            if rng.random() < 0.7 or not resident:
+                ci = int(rng.integers(len(self.circuits)))
+                keep = len(resident) < args.pool
+                if keep:
+                    resident.append((len(self.jobs), ci))
+                self.jobs.append(dict(t=t, kind="place", ci=ci, keep=keep))
+            else:
+                ji, ci = resident[int(rng.integers(len(resident)))]
+                c = self.circuits[ci]
+                k = max(1, c.num_gates // 100)
+                g = rng.choice(c.num_gates, k, replace=False).astype(np.int32)
+                G = min(1024, max(128, int(round(np.sqrt(c.num_gates) / 128.0)) * 128))
+                sig = 2.0 * c.chip_width / G
+                self.jobs.append(dict(t=t, kind="eco", target=ji, ci=ci, gates=g,
+                                      dx=rng.normal(0, sig, k).astype(np.float32),
+                                      dy=rng.normal(0, sig, k).astype(np.float32)))
+
+    def desc(self, fx, j, ids):
+        if j["kind"] == "place":
+            return fx.Server.place_desc(self.circuits[j["ci"]], keep_resident=j["keep"],
+                                        part=self.part)
+        return fx.Server.eco_desc(ids[j["target"]], j["gates"], j["dx"], j["dy"], iterations=50)
+
+    def bytes_in(self, j):
+        c = self.circuits[j["ci"]]
+        if j["kind"] == "place":
+            return 4 * (c.num_nets + 1) + 4 * c.num_pins + 8 * c.num_gates
+        return 12 * len(j["gates"])
+
+
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def run_serve(args, rank, world, local_rank):
+    """Open-loop serving run (arrivals at their Poisson times, results polled
+    as they finish), then the same jobs one at a time on one slot (the serial
+    GPU baseline); each job's HPWL must agree between the two."""
+    import threading
+    import fluxion_b200 as fx
+    if world > 1:
+        args.seed += 1000 * rank
+    wl = ServeWorkload(args, fx)
+    n_jobs = len(wl.jobs)
+
+    def served(slots, open_loop):
+        sv = fx.Server(device=local_rank, slots=slots)
+        ids, res = {}, {}
+        try:
+            # warm-up: one PLACE per pool netlist size class is not needed;
+            # load the kernels once with a small job outside the timing
+            sv.submit(fx.Server.place_desc(wl.circuits[0], part=wl.part))
+            sv.poll(-1)
+            launches0 = sv.stats()["launches"]
+            t0 = time.perf_counter()
+            if open_loop:
+                err = []
+
+                def submitter():
+                    try:
+                        for i, j in enumerate(wl.jobs):
+                            delay = t0 + j["t"] - time.perf_counter()
+                            if delay > 0:
+                                time.sleep(delay)
+                            ids[i] = sv.submit(wl.desc(fx, j, ids))
+                    except Exception as e:  # reported after the run
+                        err.append(e)
+
+                th = threading.Thread(target=submitter)
+                th.start()
+                while len(res) < n_jobs and not (err and not th.is_alive() and
+                                                 len(res) >= len(ids)):
+                    r = sv.poll(100)
+                    if r is not None:
+                        res[r["job_id"]] = r
+                th.join()
+                if err:
+                    raise err[0]
+            else:
+                for i, j in enumerate(wl.jobs):
+                    ids[i] = sv.submit(wl.desc(fx, j, ids))
+                    r = sv.poll(-1)
+                    res[r["job_id"]] = r
+            wall = time.perf_counter() - t0
+            launches = sv.stats()["launches"] - launches0
+        finally:
+            sv.close()
+        out = [res[ids[i]] for i in range(n_jobs)]
+        return out, wall, launches
+
+    clocks = ClockSampler(local_rank)
+    mix, wall_mix, launches = served(args.slots, True)
+    clk = clocks.stop()
+    ser, wall_ser, _ = served(1, False)
+    bad = [r for r in mix + ser if r["status"] != 0]
+    if bad:
+        raise RuntimeError(f"{len(bad)} serving jobs failed: {bad[0]['error']}")
+    lat = [1e3 * (r["end_s"] - r["submit_s"]) for r in mix]
+    svc = [1e3 * (r["end_s"] - r["start_s"]) for r in ser]
+    rel = max(abs(a["hpwl"] - b["hpwl"]) / max(abs(b["hpwl"]), 1e-30) for a, b in zip(mix, ser))
+    jobs_s = n_jobs / wall_mix
+    serial_s = n_jobs / wall_ser
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        t = torch.tensor([n_jobs, wall_mix], dtype=torch.float64, device=f"cuda:{local_rank}")
+        tdist.all_reduce(t[:1], op=tdist.ReduceOp.SUM)
+        w = t[1:].clone()
+        tdist.all_reduce(w, op=tdist.ReduceOp.MAX)
+        jobs_s = float(t[0]) / float(w[0])
+    kinds = [j["kind"] for j in wl.jobs]
+    bin_ = sum(wl.bytes_in(j) for j in wl.jobs) / n_jobs
+    out = {"metric": SERVE_METRIC, "value": jobs_s, "unit": "jobs/s", "n_gpus": world,
+           "steps": n_jobs, "warmup": 1, "ms_per_step": 1e3 * wall_mix / n_jobs,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 (FP64 HPWL/reductions)", "data": "synthetic",
+           "config": {"workload": f"serve: Poisson {args.rate:g} req/s for {args.duration:g} s, "
+                      f"70% PLACE (partition FP64-30 + leaves + refine) on {args.pool} netlists "
+                      f"of 5k-500k gates, 30% ECO (1% moves, 50 plain iterations)",
+                      "slots": args.slots, "jobs": n_jobs, "place": kinds.count("place"),
+                      "eco": kinds.count("eco"), "seed": args.seed,
+                      "pool_gates": [c.num_gates for c in wl.circuits]},
+           "latency_ms": {"p50": _pct(lat, 50), "p90": _pct(lat, 90), "p99": _pct(lat, 99),
+                          "max": max(lat)},
+           "offered_rate": n_jobs / args.duration,
+           "serial": {"value": serial_s, "unit": "jobs/s",
+                      "service_ms": {"p50": _pct(svc, 50), "p99": _pct(svc, 99)},
+                      "how": "same jobs, one at a time on one slot (closed loop)"},
+           "speedup_vs_serial": jobs_s / serial_s,
+           "hpwl_max_rel_diff_vs_serial": rel,
+           "e2e": {"value": jobs_s, "unit": "jobs/s", "h2d_bytes_per_step": bin_,
+                   "d2h_bytes_per_step": 248,
+                   "call": "fx_serve_submit/fx_serve_poll with host netlists and moves"},
+           "gpu_launches": launches, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_serve_reference(args, rank, world):
+    """The reference's CPU flow for the same jobs on a bounded sample: PLACE =
+    build_adjacency + build_hierarchy + place_gates_in_leaf per leaf + refine
+    (the oracle's restatements of main.rs:74-111); ECO = one plain iteration
+    on the CPU path (attraction, Barnes-Hut via BarnesHutTree.cpp, scipy DCT,
+    congestion) scaled to 50. Jobs are taken in order until ~20 s."""
+    if rank != 0:
+        return
+    import fluxion_b200 as fx
+    from oracle import oracle as orc
+    orc.build()
+    wl = ServeWorkload(args, fx)
+    threads = os.cpu_count() or 1
+    done, spent, adj = 0, 0.0, {}
+    for j in wl.jobs:
+        if spent > 20.0 and done > 0:
+            break
+        c = wl.circuits[j["ci"]]
+        t0 = time.perf_counter()
+        if j["ci"] not in adj:
+            adj[j["ci"]] = orc.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+        ap, ai = adj[j["ci"]]
+        if j["kind"] == "place":
+            tr = orc.build_hierarchy(c.num_gates, ap, ai, c.chip_width, c.chip_height)
+            x = np.zeros(c.num_gates, np.float32)
+            y = np.zeros(c.num_gates, np.float32)
+            lp, lg = tr["leaf_ptr"], tr["leaf_gate"]
+            for l in range(len(lp) - 1):
+                orc.place_leaf(lg[lp[l]:lp[l + 1]], ap, ai, tr["region"][l], 50,
+                               out_x=x, out_y=y)
+            # one refine iteration (two congestion passes), scaled to the 30
+            # the GPU runs typically take: the reference counts every cell of
+            # every net's bounding box, seconds per pass at 100k gates
+            t1 = time.perf_counter()
+            orc.refine(c.net_ptr, c.net_gate, x, y, c.chip_width, c.chip_height, max_iters=1)
+            spent += (time.perf_counter() - t1) * (30.0 / 2.0 - 1.0)
+        else:
+            x = np.random.default_rng(0).uniform(0, c.chip_width, c.num_gates).astype(np.float32)
+            y = np.random.default_rng(1).uniform(0, c.chip_height, c.num_gates).astype(np.float32)
+
+            class S:
+                pass
+            sc = S()
+            sc.circuit, sc.adj = c, (ap, ai)
+            G = min(1024, max(128, int(round(np.sqrt(c.num_gates) / 128.0)) * 128))
+            sec, _ = cpu_iteration_sample(sc, x, y, G, 256, threads, 16, 64)
+            spent += 49 * sec  # 50 iterations, one measured
+        spent += time.perf_counter() - t0
+        done += 1
+    value = done / spent
+    out = {"metric": SERVE_METRIC, "value": value, "unit": "jobs/s", "impl": "reference",
+           "n_gpus": world, "steps": done, "warmup": 0, "ms_per_step": 1e3 * spent / done,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic",
+           "config": {"workload": "serve (same job stream as --impl fluxion)", "seed": args.seed},
+           "cpu_baseline": {"value": value, "unit": "jobs/s", "cores": threads, "kind": "port",
+                            "sample": f"the first {done} jobs of the stream, run one after "
+                                      "another on the CPU (PLACE: hierarchy and leaves in "
+                                      "full, refine as 1 iteration scaled to 30; ECO: 1 of "
+                                      "50 plain iterations timed, scaled)"},
+           "e2e": {"value": value, "unit": "jobs/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.workload == "serve":
+        if args.impl == "reference":
+            run_serve_reference(args, rank, world)
+        else:
+            if world > 1:
+                import torch
+                import torch.distributed as tdist
+                torch.cuda.set_device(local_rank)
+                tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+            run_serve(args, rank, world, local_rank)
+            if world > 1:
+                tdist.barrier()
+                tdist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -414,7 +414,7 @@ int fx_serve_poll(fx_server *server, int32_t wait_ms, fx_job_result *out);
 int fx_serve_positions(fx_server *server, int64_t design_id, float *out_x, float *out_y);
 int fx_serve_release(fx_server *server, int64_t design_id);
 int fx_serve_stats(fx_server *server, int64_t *out_reserved_bytes, int32_t *out_queued,
-                   int32_t *out_running, int32_t *out_resident);
+                   int32_t *out_running, int32_t *out_resident, int64_t *out_launches);
 
 /* ---- host-only helpers (no GPU needed) ---------------------------------- */
 /* Builds the deduplicated clique-expansion adjacency of

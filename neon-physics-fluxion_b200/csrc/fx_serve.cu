@@ -549,9 +549,14 @@ extern "C" int fx_serve_release(fx_server *sv, int64_t design_id) {
 }
 
 extern "C" int fx_serve_stats(fx_server *sv, int64_t *reserved, int32_t *queued,
-                              int32_t *running, int32_t *resident) {
+                              int32_t *running, int32_t *resident, int64_t *launches) {
   if (!sv) return FX_EINVAL;
   std::lock_guard<std::mutex> lock(sv->mu);
+  if (launches) {  // kernels launched by all worker contexts so far
+    int64_t l = 0;
+    for (fx_ctx *c : sv->ctxs) l += c->launches;
+    *launches = l;
+  }
   if (reserved) *reserved = sv->reserved;
   if (queued) *queued = (int32_t)sv->queue.size();
   if (running) *running = sv->running;

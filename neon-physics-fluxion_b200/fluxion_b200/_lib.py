@@ -185,7 +185,7 @@ SIGNATURES = {
     "fx_serve_poll": (C.c_int, [P, I32, C.POINTER(JobResult)]),
     "fx_serve_positions": (C.c_int, [P, I64, PF32, PF32]),
     "fx_serve_release": (C.c_int, [P, I64]),
-    "fx_serve_stats": (C.c_int, [P, PI64, PI32, PI32, PI32]),
+    "fx_serve_stats": (C.c_int, [P, PI64, PI32, PI32, PI32, PI64]),
     "fx_partition": (C.c_int, [P, P, C.POINTER(PartCfg), I32, PI32, PI32, PF32, PI32,
                                C.POINTER(PartStats)]),
     "fx_refine": (C.c_int, [P, P, C.POINTER(RefineCfg), PF32, PF32, C.POINTER(RefineStats),

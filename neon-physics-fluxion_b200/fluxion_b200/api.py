@@ -517,11 +517,11 @@ class Server:
         check(self.lib.fx_serve_release(self.handle, design_id), "fx_serve_release")
 
     def stats(self) -> dict:
-        rb, q, r, res = C.c_int64(), C.c_int32(), C.c_int32(), C.c_int32()
+        rb, q, r, res, ln = C.c_int64(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64()
         check(self.lib.fx_serve_stats(self.handle, C.byref(rb), C.byref(q), C.byref(r),
-                                      C.byref(res)), "fx_serve_stats")
+                                      C.byref(res), C.byref(ln)), "fx_serve_stats")
         return dict(reserved_bytes=rb.value, queued=q.value, running=r.value,
-                    resident=res.value)
+                    resident=res.value, launches=ln.value)
 
 
 def serve_estimate(desc_and_keep) -> int:
