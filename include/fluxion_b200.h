@@ -453,6 +453,26 @@ int fx_netlist_copy(const fx_netlist *nl, int32_t *out_net_ptr,
                     int32_t *out_leaf_ptr, float *out_region);
 int fx_netlist_free(fx_netlist *nl);
 
+/* ---- (f.3) netlist ingestion and DEF output (host-only) ----------------- */
+/* Mirrors parser::blif::parse (H/src/parser/blif.rs:12-116): one gate per
+ * .names / .latch / .gate line, named g0, g1, ... (width 2, height 10; die
+ * 1000 x 1000); a net joins the driver of a signal (the last token of
+ * .names, the output of .latch, the O= / Y= pin of .gate) and its readers,
+ * in reading order; signals read by several gates but driven by none
+ * (primary inputs) form nets of their readers; one-gate nets are dropped.
+ * The reference collects nets by iterating HashMaps, whose order is seeded
+ * randomly per process; here nets come in first-appearance order of their
+ * signal names (driven signals first, then undriven ones), which fixes the
+ * netlist for a file. design_name (may be NULL) receives the file stem
+ * (Circuit::name) truncated to name_cap - 1 bytes. */
+int fx_blif_read(const char *path, fx_netlist **out, char *design_name, int32_t name_cap);
+/* Mirrors parser::def::write_def (H/src/parser/def.rs:11-43): DIEAREA and
+ * PLACED coordinates are (v * 1000.0f32) as i64 (truncation, saturating,
+ * NaN -> 0). names: n NUL-terminated gate names laid end to end, or NULL for
+ * g0, g1, ... */
+int fx_def_write(const char *path, const char *design_name, int32_t n, const float *x,
+                 const float *y, float chip_w, float chip_h, const char *names);
+
 #ifdef __cplusplus
 }
 #endif

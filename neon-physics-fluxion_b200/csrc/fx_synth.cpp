@@ -12,14 +12,7 @@
 
 #include "fx_internal.h"
 
-struct fx_netlist {
-  int32_t n = 0, m = 0;
-  std::vector<int32_t> net_ptr, net_gate;
-  std::vector<float> w, h, x, y;
-  float die_w = 0.f, die_h = 0.f;
-  std::vector<int32_t> leaf_ptr;
-  std::vector<float> region;
-};
+#include "fx_netlist.h"
 
 namespace {
 

@@ -177,6 +177,8 @@ SIGNATURES = {
     "fx_fiedler": (C.c_int, [P, P, I32, PI32, PI32, I32, C.c_double, PF32, PI32, PF64]),
     "fx_refine_cfg_default": (C.c_int, [C.POINTER(RefineCfg)]),
     "fx_part_cfg_default": (C.c_int, [C.POINTER(PartCfg)]),
+    "fx_blif_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, I32]),
+    "fx_def_write": (C.c_int, [C.c_char_p, C.c_char_p, I32, PF32, PF32, F32, F32, C.c_char_p]),
     "fx_serve_cfg_default": (C.c_int, [C.POINTER(ServeCfg)]),
     "fx_serve_estimate": (C.c_int, [C.POINTER(JobDesc), PI64]),
     "fx_serve_create": (C.c_int, [C.POINTER(ServeCfg), C.POINTER(C.c_void_p)]),

@@ -672,6 +672,31 @@ def _netlist_out(h) -> Synth:
     return Synth(circ, Placement(x, y), leaf_ptr, region[:4 * L])
 
 
+def read_blif(path) -> Circuit:
+    """parser::blif::parse (H/src/parser/blif.rs:12-116) -> Circuit (gates g0..,
+    width 2, height 10, die 1000 x 1000, named after the file stem)."""
+    h = C.c_void_p()
+    name = C.create_string_buffer(256)
+    check(load().fx_blif_read(str(path).encode(), C.byref(h), name, 256), "fx_blif_read")
+    s = _netlist_out(h)
+    c = s.circuit
+    c.name = name.value.decode()
+    c.gate_names = [f"g{i}" for i in range(c.num_gates)]
+    return c
+
+
+def write_def(path, circuit: Circuit, placement: Placement) -> None:
+    """parser::def::write_def (H/src/parser/def.rs:11-43)."""
+    names = None
+    if circuit.gate_names is not None:
+        names = b"".join(n.encode() + b"\0" for n in circuit.gate_names)
+    x = np.ascontiguousarray(placement.gate_x, np.float32)
+    y = np.ascontiguousarray(placement.gate_y, np.float32)
+    check(load().fx_def_write(str(path).encode(), circuit.name.encode(), circuit.num_gates,
+                              ptr(x, C.c_float), ptr(y, C.c_float), circuit.chip_width,
+                              circuit.chip_height, names), "fx_def_write")
+
+
 def synth_plain(seed: int, n_gates: int, n_nets: int, die: float,
                 leaf_size: int = 64) -> Synth:
     """Seeded plain netlist (see fx_synth_plain in include/fluxion_b200.h)."""
