@@ -59,14 +59,20 @@ def parse():
     ap.add_argument("--die", type=float, default=1200.0)
     ap.add_argument("--bins", type=int, default=1024)
     ap.add_argument("--cong", type=int, default=512)
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "tf32", "bf16", "simt"])
+    ap.add_argument("--precision", default="fp32",
+                    choices=["fp32", "3xtf32", "tf32", "bf16", "simt"],
+                    help="DCT GEMMs: fp32 (= simt, CUDA cores), 3xtf32, tf32, bf16 (tensor cores)")
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--trajectory", type=int, default=500,
                     help="iterations of the full run reported beside the steps (0: skip)")
-    ap.add_argument("--workload", default="plain", choices=["plain", "serve"],
-                    help="plain: the 1M-gate iteration; serve: the request stream")
+    ap.add_argument("--workload", default="plain",
+                    choices=["plain", "serve", "leaves", "precision"],
+                    help="plain: the 1M-gate iteration; serve: the request stream; "
+                         "leaves: the batched leaf placement; precision: the DCT sweep")
+    ap.add_argument("--clusters", type=int, default=16_384, help="leaves: clusters")
+    ap.add_argument("--leaf-iters", type=int, default=300, help="leaves: force iterations")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent jobs")
@@ -74,8 +80,9 @@ def parse():
     return ap.parse_args()
 
 
-PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "simt": 3}
-PREC_DTYPE = {"fp32": "f32 (DCT GEMMs 3xTF32, FP32 accumulate)",
+PREC = {"fp32": 3, "simt": 3, "3xtf32": 0, "tf32": 1, "bf16": 2}
+PREC_DTYPE = {"fp32": "f32 (DCT GEMMs FP32 on CUDA cores)",
+              "3xtf32": "f32 (DCT GEMMs 3xTF32, FP32 accumulate)",
               "tf32": "f32 (DCT GEMMs TF32, FP32 accumulate)",
               "bf16": "f32 (DCT GEMMs BF16, FP32 accumulate)", "simt": "f32"}
 
@@ -142,8 +149,9 @@ def peaks():
 NCU_DRAM_BYTES = {
     # bh_walk_kernel: 59.568 MB read + 2.309 MB written
     "bh_walk": 61_876_736,
-    # 6 x tc_gemm_kernel<0> (21.000 MB + 0.011 MB each) + dens_charge_kernel
-    # (8.393 MB); dens_scatter runs in the previous step's fused kernel
+    # with --precision 3xtf32: 6 x tc_gemm_kernel<0> (21.000 MB + 0.011 MB
+    # each) + dens_charge_kernel (8.393 MB); dens_scatter runs in the
+    # previous step's fused kernel
     "density": 6 * 21_010_944 + 8_393_472,
 }
 # What bounds each stage when it is not HBM or the tensor pipe (ncu).
@@ -390,7 +398,7 @@ def run_fluxion(args, rank, world, local_rank):
     per_iter = {k: stages[k][0] / max(stages[k][1], 1) for k in stages if stages[k][1]}
     dom = max(per_iter, key=per_iter.get)
     hbm, bf16, src = peaks()
-    if dom == "density" and args.precision != "simt":
+    if dom == "density" and PREC[args.precision] != 3:
         ach = f_alg["density"] / (per_iter[dom] * 1e-3) / 1e12
         peak = bf16 if args.precision == "bf16" else bf16 / 2
         roof = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
@@ -404,7 +412,8 @@ def run_fluxion(args, rank, world, local_rank):
                 "algorithmic_bytes": b_alg[dom], "peak_source": f"{src} HBM copy"}
     if dom in NCU_LIMITER:
         roof["limiter"] = NCU_LIMITER[dom]
-    if args.gates != 1_000_000 or args.bins != 1024 or args.precision != "fp32":
+    if args.gates != 1_000_000 or args.bins != 1024 or (dom == "density" and
+                                                        args.precision != "3xtf32"):
         roof["traffic"] = None  # the captures are of the default workload
     B_iter = sum(b_alg.values())
     it_ms = ms_max / args.steps
@@ -674,11 +683,260 @@ def run_serve_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+LEAF_METRIC = "batched leaf placement: cluster-iterations/s"
+
+
+def run_leaves(args, rank, world, local_rank):
+    """Batched leaf placement (16,384 clusters of log-uniform 16-128 gates,
+    1.5 nets/gate of degree 2-8, unit boxes, 300 iterations): one step = one
+    fx_hapr_place_leaves call over all clusters. `value` from the kernel's
+    device time (CUDA events on its stream), `e2e` from the whole call (host
+    leaf lists in, positions out); the per-cluster-launch schedule and the
+    CPU restatement of place_gates_in_leaf (placer.rs:210-287) beside it."""
+    import fluxion_b200 as fx
+    syn = fx.synth_leaves(args.seed + rank, args.clusters, 16, 128, 1.5)
+    c = syn.circuit
+    lp, region = syn.leaf_ptr, syn.region
+    lg = np.arange(c.num_gates, dtype=np.int32)
+    sizes = np.diff(lp).astype(np.int64)
+    pairs = int((sizes * (sizes - 1) // 2).sum())
+    ctx = fx.Context(local_rank)
+    d = fx.Design(ctx, c)
+    cfg = fx.leaf_cfg(force_iterations=args.leaf_iters)
+    x, y, sched = d.place_leaves(lp, lg, region, cfg)  # tunes the schedule
+    cfg.schedule = sched
+    for _ in range(max(0, args.warmup - 1)):
+        d.place_leaves(lp, lg, region, cfg)
+    ctx.synchronize()
+    ctx.reset_stage_times()
+    ctx.set_profiling(True)
+    launches0 = ctx.kernel_launches()
+    clocks = ClockSampler(local_rank)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        x2, y2, _ = d.place_leaves(lp, lg, region, cfg)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    ctx.set_profiling(False)
+    launches = ctx.kernel_launches() - launches0
+    kms = ctx.stage_times()["leaf"][0] / args.steps
+    assert np.array_equal(x, x2) and np.array_equal(y, y2)
+    # per-cluster launches (one launch per leaf), once
+    pc = fx.leaf_cfg(force_iterations=args.leaf_iters, schedule=fx.FX_LEAF_PER_CLUSTER)
+    ctx.reset_stage_times()
+    ctx.set_profiling(True)
+    xp, yp, _ = d.place_leaves(lp, lg, region, pc)
+    ctx.set_profiling(False)
+    pc_ms = ctx.stage_times()["leaf"][0]
+    same = bool(np.array_equal(xp, x) and np.array_equal(yp, y))
+    d.close()
+    ctx.close()
+    units = args.clusters * args.leaf_iters
+    ops = 17.0 * pairs * args.leaf_iters  # placer.rs:259-270, per unordered pair
+    achieved = ops / (kms * 1e-3) / 1e12
+    lane_peak = 148 * 128 * 1.965e9 / 1e12
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        orc.build()
+        ap, ai = fx.build_adjacency(c)
+        k = min(args.clusters, 256)
+        t1 = time.perf_counter()
+        ox = np.zeros(c.num_gates, np.float32)
+        oy = np.zeros(c.num_gates, np.float32)
+        for l in range(k):
+            orc.place_leaf(lg[lp[l]:lp[l + 1]], ap, ai, region[4 * l:4 * l + 4],
+                           args.leaf_iters, out_x=ox, out_y=oy)
+        sec = (time.perf_counter() - t1) * args.clusters / k
+        cpu = {"value": units / sec, "unit": "cluster-iterations/s", "cores": 1, "kind": "port",
+               "sample": f"place_gates_in_leaf restated, first {k} of {args.clusters} clusters "
+                         "on 1 core, scaled"}
+    out = {"metric": LEAF_METRIC, "value": world * units / (kms * 1e-3),
+           "unit": "cluster-iterations/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": kms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"leaves: {args.clusters} clusters of 16-128 gates "
+                      f"({c.num_gates} gates, {pairs} pairs), {args.leaf_iters} iterations",
+                      "schedule": int(sched), "seed": args.seed},
+           "roofline": {"bound": "fp32-pipe", "achieved": achieved, "peak": lane_peak,
+                        "unit": "Tops/s", "frac": achieved / lane_peak, "traffic": None,
+                        "kernel": "leaf_batch_kernel",
+                        "peak_source": "nominal 148 SMs x 128 FP32 lanes x 1.965 GHz, 17 ops "
+                                       "per unordered pair"},
+           "per_cluster_launches_ms": pc_ms, "speedup_vs_per_cluster": pc_ms / kms,
+           "same_result_as_per_cluster": same, "cpu_baseline": cpu,
+           "e2e": {"value": world * units * args.steps / wall, "unit": "cluster-iterations/s",
+                   "h2d_bytes_per_step": 4 * (len(lp) + c.num_gates) + 16 * args.clusters
+                   + 8 * c.num_gates,
+                   "d2h_bytes_per_step": 8 * c.num_gates,
+                   "call": "fx_hapr_place_leaves with host leaf lists and regions"},
+           "gpu_launches": launches, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+PREC_METRIC = "density solve precision sweep (field/force rel. L2 vs FP64, tensor TFLOP/s)"
+# plain iterations behind the HPWL delta: few enough that the placement has
+# not contracted (a contracted placement crowds the Barnes-Hut buckets)
+HPWL_ITERS = 3
+
+
+def run_precision(args, rank, world, local_rank):
+    """The density step's precision sweep on a 4M-gate netlist from the same
+    generator (die 2400 x 2400): for G = 2048 and 4096 and each DCT precision
+    (BF16, TF32, 3xTF32, SIMT FP32; FP32 accumulation throughout), the
+    field / force / potential relative L2 error against the FP64 FFT oracle
+    (scipy dctn/idctn of force_electrostatic.py), the density stage's device
+    time and GEMM throughput, and the HPWL after HPWL_ITERS plain iterations
+    against the SIMT FP32 run. HPWL and energy are FP64 reductions on the
+    device."""
+    if rank != 0:
+        return
+    import fluxion_b200 as fx
+    from oracle import oracle as orc
+    t_start = time.perf_counter()
+    n = 4_000_000
+    s = fx.synth_plain(args.seed, n, int(1.2 * n), 2400.0)
+    c, p = s.circuit, s.placement
+    ctx = fx.Context(local_rank)
+    d = fx.Design(ctx, c)
+    d.set_positions(p.gate_x, p.gate_y)
+    area = (c.gate_widths * c.gate_heights).astype(np.float64)
+    codes = {"bf16": fx.FX_DCT_BF16, "tf32": fx.FX_DCT_TF32, "3xtf32": fx.FX_DCT_FP32,
+             "fp32_simt": fx.FX_DCT_SIMT}
+    _, bf16_peak, src = peaks()
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+    rows = []
+    print(f"precision sweep: set-up {time.perf_counter() - t_start:.1f} s", file=sys.stderr,
+          flush=True)
+    for G in (2048, 4096):
+        ref = orc.density_forces(p.gate_x, p.gate_y, area, c.chip_width, c.chip_height, G,
+                                 0.7, 1.0)
+        hp = {}
+        for name, code in codes.items():
+            t_phase = time.perf_counter()
+            d.set_positions(p.gate_x, p.gate_y)  # the oracle's positions
+            out = d.density(G, 0.7, 1.0, code, grids=True)
+            ctx.reset_stage_times()
+            ctx.set_profiling(True)
+            reps = 3
+            for _ in range(reps):
+                d.density(G, 0.7, 1.0, code)
+            ctx.set_profiling(False)
+            ms = ctx.stage_times()["density"][0] / reps
+            flops = 6 * 2.0 * G ** 3 * (3 if code == fx.FX_DCT_FP32 else 1)
+            fld = float(np.sqrt((np.linalg.norm(out["ex"] - ref["ex"]) ** 2 +
+                                 np.linalg.norm(out["ey"] - ref["ey"]) ** 2) /
+                                (np.linalg.norm(ref["ex"]) ** 2 + np.linalg.norm(ref["ey"]) ** 2)))
+            frc = float(np.sqrt((np.linalg.norm(out["fx"] - ref["fx"]) ** 2 +
+                                 np.linalg.norm(out["fy"] - ref["fy"]) ** 2) /
+                                (np.linalg.norm(ref["fx"]) ** 2 + np.linalg.norm(ref["fy"]) ** 2)))
+            cfg = fx.iter_cfg(density_bins=G, dct_precision=code, density_weight=1e-4,
+                              cong_cols=512, cong_rows=512)
+            x0, y0 = p.gate_x.copy(), p.gate_y.copy()
+            st = d.force_iterate(cfg, HPWL_ITERS, x0, y0)
+            hp[name] = st.hpwl
+            print(f"precision sweep: G={G} {name}: {time.perf_counter() - t_phase:.1f} s",
+                  file=sys.stderr, flush=True)
+            peak = bf16_peak if code == fx.FX_DCT_BF16 else bf16_peak / 2
+            rows.append({"G": G, "precision": name, "field_rel_l2": fld, "force_rel_l2": frc,
+                         "phi_rel_l2": rel(out["phi"], ref["phi"]),
+                         "energy_rel": abs(out["energy"] - ref["energy"]) / abs(ref["energy"]),
+                         "density_ms": ms,
+                         "tensor_tflops_executed": (flops / (ms * 1e-3) / 1e12
+                                                    if code != fx.FX_DCT_SIMT else None),
+                         "tensor_frac_of_measured": (flops / (ms * 1e-3) / 1e12 / peak
+                                                     if code != fx.FX_DCT_SIMT else None),
+                         "hpwl_after_iters": st.hpwl})
+        for r in rows:
+            if r["G"] == G:
+                r["hpwl_delta_vs_fp32"] = ((r["hpwl_after_iters"] - hp["fp32_simt"]) /
+                                           hp["fp32_simt"])
+    d.close()
+    ctx.close()
+    best = max((r for r in rows if r["G"] == 4096 and r["tensor_tflops_executed"]),
+               key=lambda r: r["tensor_tflops_executed"])
+    out = {"metric": PREC_METRIC, "value": best["tensor_tflops_executed"], "unit": "TFLOP/s",
+           "n_gpus": 1, "steps": 3, "warmup": 1, "ms_per_step": best["density_ms"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "bf16/tf32/3xtf32/fp32, FP32 accumulate", "data": "synthetic",
+           "config": {"workload": f"precision: {n} gates, die 2400, G in (2048, 4096), "
+                                  "target density 0.7, weight 1", "seed": args.seed,
+                      "peak_source": f"{src} bf16 dense (tf32: half)"},
+           "value_is": f"{best['precision']} at G=4096, executed tensor FLOP/s of the 6 GEMMs",
+           "sweep": rows}
+    print(json.dumps(out), flush=True)
+
+
+def run_leaves_reference(args, rank, world):
+    """place_gates_in_leaf (placer.rs:210-287, the oracle's restatement) over
+    the same clusters on all host threads, on a bounded sample of clusters."""
+    if rank != 0:
+        return
+    from concurrent.futures import ThreadPoolExecutor
+    import fluxion_b200 as fx
+    from oracle import oracle as orc
+    orc.build()
+    syn = fx.synth_leaves(args.seed, args.clusters, 16, 128, 1.5)
+    c, lp, region = syn.circuit, syn.leaf_ptr, syn.region
+    lg = np.arange(c.num_gates, dtype=np.int32)
+    ap, ai = fx.build_adjacency(c)
+    threads = os.cpu_count() or 1
+    ox = np.zeros(c.num_gates, np.float32)
+    oy = np.zeros(c.num_gates, np.float32)
+
+    def one(l):  # ctypes releases the GIL during the call
+        orc.place_leaf(lg[lp[l]:lp[l + 1]], ap, ai, region[4 * l:4 * l + 4], args.leaf_iters,
+                       out_x=ox, out_y=oy)
+
+    k = min(args.clusters, 64 * threads)
+    per = []
+    with ThreadPoolExecutor(threads) as ex:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            list(ex.map(one, range(k)))
+            if i >= args.warmup:
+                per.append((time.perf_counter() - t0) * args.clusters / k)
+    sec = float(np.mean(per))
+    value = args.clusters * args.leaf_iters / sec
+    out = {"metric": LEAF_METRIC, "value": value, "unit": "cluster-iterations/s",
+           "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"leaves: {args.clusters} clusters, {args.leaf_iters} "
+                                  "iterations", "seed": args.seed},
+           "cpu_baseline": {"value": value, "unit": "cluster-iterations/s", "cores": threads,
+                            "kind": "port", "sample": f"first {k} clusters per step on "
+                                                      f"{threads} threads, scaled"},
+           "e2e": {"value": value, "unit": "cluster-iterations/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.workload == "precision":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "metric": PREC_METRIC,
+                              "unavailable": "the FP64 oracle is part of the fluxion arm's "
+                                             "line (error baseline, not a timed arm)"}))
+            return
+        run_precision(args, rank, world, local_rank)
+        return
+    if args.workload == "leaves":
+        args.steps = max(1, min(args.steps, 20))  # a step is a whole 300-iteration batch
+        if args.impl == "reference":
+            run_leaves_reference(args, rank, world)
+            return
+        run_leaves(args, rank, world, local_rank)
+        return
     if args.workload == "serve":
         if args.impl == "reference":
             run_serve_reference(args, rank, world)

@@ -209,10 +209,13 @@ typedef struct fx_iter_cfg {
   float dt;              /* placer.rs:276-279 (0.1)                          */
 } fx_iter_cfg;
 
-#define FX_DCT_FP32  0 /* 3xTF32 split on the tensor cores (FP32 accuracy)   */
+#define FX_DCT_FP32  0 /* 3xTF32 split on the tensor cores; its error grows   */
+                       /* with G (6.6e-4 at 256, 4.4e-3 at 2048 measured):  */
+                       /* FP32 inputs, not FP32 accuracy                     */
 #define FX_DCT_TF32  1 /* single-pass TF32 inputs, FP32 accumulate           */
 #define FX_DCT_BF16  2 /* BF16 inputs, FP32 accumulate                       */
-#define FX_DCT_SIMT  3 /* FP32 CUDA-core GEMM (no tensor cores)              */
+#define FX_DCT_SIMT  3 /* FP32 CUDA-core GEMM (no tensor cores): the FP32-    */
+                       /* accurate solve, the iteration's default            */
 
 typedef struct fx_iter_stats {
   double hpwl;            /* FP64 HPWL after the last iteration              */

@@ -143,6 +143,10 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   FX_TRY(w.ey.alloc(cells));
   FX_TRY(w.energy.alloc(4096 + 8));
   FX_TRY(w.force.alloc((size_t)d->n));
+  if (precision == FX_DCT_SIMT) {
+    const int sp = sgemm_splits(G, d->ctx->num_sms);
+    if (sp > 1) FX_TRY(w.split_ws.alloc((size_t)sp * cells));
+  }
   const bool split = precision == FX_DCT_FP32, half = precision == FX_DCT_BF16;
   if (split) {
     FX_TRY(w.cmat_lo.alloc(cells));
@@ -259,6 +263,7 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
                                         w.buf[0].p, LO(2), BF(0));
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
+  float *WS = precision == FX_DCT_SIMT ? w.split_ws.p : nullptr;
   const GemmOperands C = K(w.cmat.p, w.cmat_lo.p, w.cmat_bf.p);
   const GemmOperands Ct = K(w.cmat_t.p, w.cmat_t_lo.p, w.cmat_t_bf.p);
   const GemmOperands DxCt = K(w.dxct.p, w.dxct_lo.p, w.dxct_bf.p);
@@ -271,13 +276,13 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
   const GemmOperands ex{w.ex.p, nullptr, nullptr};
   const GemmOperands ey{w.ey.p, nullptr, nullptr};
   const GemmOperands phi{w.buf[3].p, nullptr, nullptr};
-  FX_TRY(gemm_nt(ctx, precision, G, C, rho, nullptr, t1, s));
-  FX_TRY(gemm_nt(ctx, precision, G, C, t1, w.inv_eig.p, phat, s));
-  FX_TRY(gemm_nt(ctx, precision, G, Ct, phat, nullptr, t3, s));
-  FX_TRY(gemm_nt(ctx, precision, G, DyCt, t3, nullptr, ey, s));
-  if (need_phi) FX_TRY(gemm_nt(ctx, precision, G, Ct, t3, nullptr, phi, s));
-  FX_TRY(gemm_nt(ctx, precision, G, DxCt, phat, nullptr, t4, s));
-  FX_TRY(gemm_nt(ctx, precision, G, Ct, t4, nullptr, ex, s));
+  FX_TRY(gemm_nt(ctx, precision, G, C, rho, nullptr, t1, s, WS));
+  FX_TRY(gemm_nt(ctx, precision, G, C, t1, w.inv_eig.p, phat, s, WS));
+  FX_TRY(gemm_nt(ctx, precision, G, Ct, phat, nullptr, t3, s, WS));
+  FX_TRY(gemm_nt(ctx, precision, G, DyCt, t3, nullptr, ey, s, WS));
+  if (need_phi) FX_TRY(gemm_nt(ctx, precision, G, Ct, t3, nullptr, phi, s, WS));
+  FX_TRY(gemm_nt(ctx, precision, G, DxCt, phat, nullptr, t4, s, WS));
+  FX_TRY(gemm_nt(ctx, precision, G, Ct, t4, nullptr, ex, s, WS));
   timer_end(ctx, FX_STAGE_DENSITY, s, ev);
   return FX_OK;
 }

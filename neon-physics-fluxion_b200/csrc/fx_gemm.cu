@@ -13,11 +13,14 @@ constexpr int kBM = 128, kBN = 128, kBK = 16;
 
 // 128 x 128 tile per CTA, 8 x 8 outputs per thread in two 4-wide strips per
 // axis (conflict-free shared reads), K staged 16 at a time and stored
-// k-major in shared memory.
+// k-major in shared memory. With `part` the CTA covers K range
+// [z*Ks, (z+1)*Ks) of split z = blockIdx.z and writes its raw partial tile to
+// part[z]; sgemm_reduce_kernel then adds the splits in order.
 __global__ void __launch_bounds__(256)
 sgemm_nt_kernel(const float *__restrict__ A, const float *__restrict__ B,
-                int G, const float *__restrict__ S, float *__restrict__ D,
-                float *__restrict__ Dlo, uint16_t *__restrict__ Dbf) {
+                int G, int Ks, const float *__restrict__ S, float *__restrict__ D,
+                float *__restrict__ Dlo, uint16_t *__restrict__ Dbf,
+                float *__restrict__ part) {
   __shared__ __align__(16) float As[kBK][kBM + 4];
   __shared__ __align__(16) float Bs[kBK][kBN + 4];
   const int t = threadIdx.x;
@@ -29,13 +32,14 @@ sgemm_nt_kernel(const float *__restrict__ A, const float *__restrict__ B,
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
-  const float *a0 = A + (size_t)(bm + lr) * G + lk;
+  const int kb = blockIdx.z * Ks;
+  const float *a0 = A + (size_t)(bm + lr) * G + kb + lk;
   const float *a1 = a0 + (size_t)64 * G;
-  const float *b0 = B + (size_t)(bn + lr) * G + lk;
+  const float *b0 = B + (size_t)(bn + lr) * G + kb + lk;
   const float *b1 = b0 + (size_t)64 * G;
   float4 ra0 = *(const float4 *)a0, ra1 = *(const float4 *)a1;
   float4 rb0 = *(const float4 *)b0, rb1 = *(const float4 *)b1;
-  for (int k0 = 0; k0 < G; k0 += kBK) {
+  for (int k0 = 0; k0 < Ks; k0 += kBK) {
     As[lk + 0][lr] = ra0.x; As[lk + 1][lr] = ra0.y;
     As[lk + 2][lr] = ra0.z; As[lk + 3][lr] = ra0.w;
     As[lk + 0][lr + 64] = ra1.x; As[lk + 1][lr + 64] = ra1.y;
@@ -45,7 +49,7 @@ sgemm_nt_kernel(const float *__restrict__ A, const float *__restrict__ B,
     Bs[lk + 0][lr + 64] = rb1.x; Bs[lk + 1][lr + 64] = rb1.y;
     Bs[lk + 2][lr + 64] = rb1.z; Bs[lk + 3][lr + 64] = rb1.w;
     __syncthreads();
-    if (k0 + kBK < G) {
+    if (k0 + kBK < Ks) {
       ra0 = *(const float4 *)(a0 + k0 + kBK);
       ra1 = *(const float4 *)(a1 + k0 + kBK);
       rb0 = *(const float4 *)(b0 + k0 + kBK);
@@ -74,24 +78,57 @@ sgemm_nt_kernel(const float *__restrict__ A, const float *__restrict__ B,
       const int c = bn + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
       const size_t o = (size_t)r * G + c;
       float v = acc[i][j];
+      if (part) {
+        part[(size_t)blockIdx.z * G * G + o] = v;
+        continue;
+      }
       if (S) v *= S[o];
       store_operand(v, o, D, Dlo, Dbf);
     }
   }
 }
 
+// Adds the split-K partial tiles in split order, then the epilogue.
+__global__ void sgemm_reduce_kernel(const float *__restrict__ part, int splits, int G,
+                                    const float *__restrict__ S, float *__restrict__ D,
+                                    float *__restrict__ Dlo, uint16_t *__restrict__ Dbf) {
+  const size_t cells = (size_t)G * G;
+  for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < cells;
+       o += (size_t)gridDim.x * blockDim.x) {
+    float v = part[o];
+    for (int z = 1; z < splits; ++z) v += part[z * cells + o];
+    if (S) v *= S[o];
+    store_operand(v, o, D, Dlo, Dbf);
+  }
+}
+
+// Split-K factor of the SIMT GEMM: the largest power of two (<= 8) whose
+// CTAs still fit in one wave (two 256-thread CTAs are resident per SM), K
+// per split a multiple of 16.
+int sgemm_splits(int G, int num_sms) {
+  const int tiles = (G / kBM) * (G / kBN);
+  int s = 1;
+  while (tiles * 2 * s <= 2 * num_sms && s < 8 && (G / (2 * s)) % kBK == 0) s *= 2;
+  return s;
+}
+
 int gemm_nt(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
             const GemmOperands &B, const float *S, const GemmOperands &D,
-            cudaStream_t s) {
+            cudaStream_t s, float *split_ws) {
   if (G % 128 != 0) {
     set_error("gemm_nt: G=%d is not a multiple of 128", G);
     return FX_EINVAL;
   }
   if (precision == FX_DCT_SIMT) {
-    dim3 grid(G / kBN, G / kBM);
-    sgemm_nt_kernel<<<grid, 256, 0, s>>>(A.f32, B.f32, G, S, D.f32, D.lo, D.bf);
+    const int splits = split_ws ? sgemm_splits(G, ctx->num_sms) : 1;
+    dim3 grid(G / kBN, G / kBM, splits);
+    sgemm_nt_kernel<<<grid, 256, 0, s>>>(A.f32, B.f32, G, G / splits, S, D.f32, D.lo, D.bf,
+                                         splits > 1 ? split_ws : nullptr);
+    if (splits > 1)
+      sgemm_reduce_kernel<<<ctx->num_sms * 8, 256, 0, s>>>(split_ws, splits, G, S, D.f32,
+                                                           D.lo, D.bf);
     FX_CHECK_LAUNCH();
-    ctx->launches += 1;
+    ctx->launches += splits > 1 ? 2 : 1;
     return FX_OK;
   }
   return gemm_nt_tc(ctx, precision, G, A, B, S, D, s);

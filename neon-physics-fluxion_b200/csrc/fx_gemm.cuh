@@ -61,8 +61,11 @@ __device__ __forceinline__ void store_operand(float v, size_t i, float *f32,
 
 // D[i][j] = sum_k A[i][k] * B[j][k] (* S[i][j] when S != nullptr) for G x G
 // row-major matrices, written to D in the formats of `precision`.
+// split_ws: SIMT split-K workspace of sgemm_splits(G, sms) * G * G floats, or
+// nullptr for no split.
 int gemm_nt(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
             const GemmOperands &B, const float *S, const GemmOperands &D,
-            cudaStream_t s);
+            cudaStream_t s, float *split_ws = nullptr);
+int sgemm_splits(int G, int num_sms);
 
 }  // namespace fx

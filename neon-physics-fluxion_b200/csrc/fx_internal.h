@@ -172,6 +172,7 @@ struct DensityWork {
   DevBuf<float> ex, ey;                // field
   DevBuf<double> energy;               // FP64 partials
   DevBuf<float2> force;                // per gate
+  DevBuf<float> split_ws;              // SIMT split-K partial tiles
   template <class F>
   void for_each(F &&f) {
     f(area_fx); f(cmat); f(cmat_t); f(cmat_lo); f(cmat_t_lo); f(cmat_bf);
@@ -180,7 +181,7 @@ struct DensityWork {
     for (auto &b : buf) f(b);
     for (auto &b : lo) f(b);
     for (auto &b : bf) f(b);
-    f(ex); f(ey); f(energy); f(force);
+    f(ex); f(ey); f(energy); f(force); f(split_ws);
   }
 };
 

@@ -171,16 +171,19 @@ def test_barnes_hut_clustered_large(fx, ctx, oracle):
 # Relative L2 error bars of the potential / field / force against the FP64
 # FFT oracle, per GEMM precision: FP32 CUDA-core GEMMs, 3xTF32 and single-pass
 # TF32 / BF16 tensor-core GEMMs (all accumulate in FP32).
-PREC_TOL = {"simt": (1e-5, 2e-5), "fp32": (2e-4, 2e-4), "tf32": (1e-2, 1e-2),
+# "3xtf32" (FX_DCT_FP32) is the tensor-core split: FP32 inputs, but its error
+# grows with G (the accumulation on the tensor cores); "simt" is FP32 on the
+# CUDA cores, the iteration's default.
+PREC_TOL = {"simt": (1e-5, 2e-5), "3xtf32": (2e-4, 2e-4), "tf32": (1e-2, 1e-2),
             "bf16": (5e-2, 5e-2)}
 
 
 @pytest.mark.parametrize("G", [128, 256])
-@pytest.mark.parametrize("prec", ["simt", "fp32", "tf32", "bf16"])
+@pytest.mark.parametrize("prec", ["simt", "3xtf32", "tf32", "bf16"])
 def test_density_vs_fp64(fx, ctx, oracle, G, prec):
     s = fx.synth_plain(9, 20_000, 24_000, 170.0)
     c, p = s.circuit, s.placement
-    code = {"simt": fx.FX_DCT_SIMT, "fp32": fx.FX_DCT_FP32, "tf32": fx.FX_DCT_TF32,
+    code = {"simt": fx.FX_DCT_SIMT, "3xtf32": fx.FX_DCT_FP32, "tf32": fx.FX_DCT_TF32,
             "bf16": fx.FX_DCT_BF16}[prec]
     tol_phi, tol_e = PREC_TOL[prec]
     d = fx.Design(ctx, c)
