@@ -608,6 +608,16 @@ def run_serve(args, rank, world, local_rank):
            "serial": {"value": serial_s, "unit": "jobs/s",
                       "service_ms": {"p50": _pct(svc, 50), "p99": _pct(svc, 99)},
                       "how": "same jobs, one at a time on one slot (closed loop)"},
+           "service_ms_by_kind": {
+               k: {"n": sum(1 for j in wl.jobs if j["kind"] == k),
+                   "serial_p50": _pct([1e3 * (r["end_s"] - r["start_s"]) for r, j in
+                                       zip(ser, wl.jobs) if j["kind"] == k], 50),
+                   "serial_mean": float(np.mean([1e3 * (r["end_s"] - r["start_s"])
+                                                 for r, j in zip(ser, wl.jobs)
+                                                 if j["kind"] == k] or [0.0])),
+                   "served_p50": _pct([1e3 * (r["end_s"] - r["start_s"]) for r, j in
+                                       zip(mix, wl.jobs) if j["kind"] == k], 50)}
+               for k in ("place", "eco")},
            "speedup_vs_serial": jobs_s / serial_s,
            "hpwl_max_rel_diff_vs_serial": rel,
            "e2e": {"value": jobs_s, "unit": "jobs/s", "h2d_bytes_per_step": bin_,

@@ -568,8 +568,10 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
                const int4 *__restrict__ qchild,
                const float4 *__restrict__ node, float k, float th2, float md2,
                float2 *__restrict__ force, unsigned int *__restrict__ err) {
-  __shared__ int32_t st_node[kWalkWarps][kWalkGroups][kStack];
-  __shared__ unsigned st_mask[kWalkWarps][kWalkGroups][kStack];
+  // one stack per group; the odd stride puts the groups' tops (often at the
+  // same depth) in different banks
+  __shared__ int32_t st_node[kWalkWarps][kWalkGroups][kStack + 1];
+  __shared__ unsigned st_mask[kWalkWarps][kWalkGroups][kStack + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int g = lane / kWalkGroup;
   const bool leader = (lane % kWalkGroup) == 0;

@@ -157,8 +157,14 @@ extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
   if (!c) return FX_ENOMEM;
   c->device = device;
   c->num_sms = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+  // The primary stream (the Barnes-Hut chain and everything serial) gets the
+  // highest priority, the side stream (the density solve that overlaps it)
+  // the lowest, so the short sort and tree kernels are not held back by GEMM
+  // blocks.
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  if (cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) != cudaSuccess) {
     set_error("stream/event creation failed");

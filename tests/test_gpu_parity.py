@@ -288,3 +288,24 @@ def test_saved_state_restores_the_step(fx, ctx):
         d.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert out[0][2:] == out[1][2:]
+
+
+def test_graph_replay_matches_eager_iterations(fx, ctx):
+    """Runs of >= 8 iterations replay a captured CUDA graph of two iterations
+    (stage timing off); with stage timing on every iteration is launched
+    eagerly. Both give the same positions and statistics bit for bit."""
+    s = fx.synth_plain(11, 30_000, 36_000, 208.0)
+    cfg = fx.iter_cfg(density_bins=256, cong_cols=128, cong_rows=128)
+    d = fx.Design(ctx, s.circuit)
+    try:
+        out = []
+        for profiling in (False, True):
+            ctx.set_profiling(profiling)
+            x = s.placement.gate_x.copy(); y = s.placement.gate_y.copy()
+            st = d.force_iterate(cfg, 21, x, y)
+            out.append((x, y, st.hpwl, st.total_overflow, st.density_energy))
+    finally:
+        ctx.set_profiling(False)
+        d.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2:] == out[1][2:]
