@@ -4,6 +4,9 @@
 #include <cstring>
 #include <new>
 
+#include <algorithm>
+#include <thread>
+
 #include "fx_internal.h"
 
 namespace fx {
@@ -89,38 +92,70 @@ static int build_adjacency(int32_t N, int32_t M, const int32_t *net_ptr,
       for (int32_t q = net_ptr[e]; q < net_ptr[e + 1]; ++q)
         inc[fill[net_gate[q]]++] = e;
   }
-  std::vector<int32_t> mark((size_t)N, -1);
-  ptr.assign((size_t)N + 1, 0);
-  idx.clear();
-  idx.reserve((size_t)P * 4);
-  auto push = [&](int32_t a, int32_t b) {
-    if (mark[b] != a) {
-      mark[b] = a;
-      idx.push_back(b);
+  // Each gate's list depends only on its own nets, so gate ranges are built
+  // independently (a stamp array per range) and concatenated in gate order.
+  auto build_range = [&](int32_t g0, int32_t g1, std::vector<int32_t> &cnt,
+                         std::vector<int32_t> &out) {
+    std::vector<int32_t> mark((size_t)N, -1);
+    auto push = [&](int32_t a, int32_t b) {
+      if (mark[b] != a) {
+        mark[b] = a;
+        out.push_back(b);
+      }
+    };
+    for (int32_t a = g0; a < g1; ++a) {
+      const size_t before = out.size();
+      for (int32_t t = inc_ptr[a]; t < inc_ptr[a + 1]; ++t) {
+        const int32_t e = inc[t];
+        if (t > inc_ptr[a] && inc[t - 1] == e) continue;  // net already done
+        const bool repeated = t + 1 < inc_ptr[a + 1] && inc[t + 1] == e;
+        const int32_t b0 = net_ptr[e], b1 = net_ptr[e + 1];
+        if (!repeated) {
+          for (int32_t q = b0; q < b1; ++q)
+            if (net_gate[q] != a) push(a, net_gate[q]);
+        } else {  // replay circuit.rs:158-168 for the pairs that touch a
+          for (int32_t i = b0; i < b1; ++i)
+            for (int32_t j = i + 1; j < b1; ++j) {
+              if (net_gate[i] == a) push(a, net_gate[j]);
+              if (net_gate[j] == a) push(a, net_gate[i]);
+            }
+        }
+      }
+      cnt[(size_t)(a - g0)] = (int32_t)(out.size() - before);
     }
   };
-  for (int32_t a = 0; a < N; ++a) {
-    for (int32_t t = inc_ptr[a]; t < inc_ptr[a + 1]; ++t) {
-      const int32_t e = inc[t];
-      if (t > inc_ptr[a] && inc[t - 1] == e) continue;  // net already done
-      const bool repeated = t + 1 < inc_ptr[a + 1] && inc[t + 1] == e;
-      const int32_t b0 = net_ptr[e], b1 = net_ptr[e + 1];
-      if (!repeated) {
-        for (int32_t q = b0; q < b1; ++q)
-          if (net_gate[q] != a) push(a, net_gate[q]);
-      } else {  // replay circuit.rs:158-168 for the pairs that touch a
-        for (int32_t i = b0; i < b1; ++i)
-          for (int32_t j = i + 1; j < b1; ++j) {
-            if (net_gate[i] == a) push(a, net_gate[j]);
-            if (net_gate[j] == a) push(a, net_gate[i]);
-          }
-      }
-    }
-    if (idx.size() > (size_t)INT32_MAX) {
-      set_error("adjacency exceeds 2^31 entries");
-      return FX_EINVAL;
-    }
-    ptr[(size_t)a + 1] = (int32_t)idx.size();
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int T = N >= 200000 ? (int)std::min<unsigned>(8, hw) : 1;
+  std::vector<std::vector<int32_t>> cnt((size_t)T), part((size_t)T);
+  std::vector<int32_t> lo((size_t)T + 1);
+  for (int t = 0; t <= T; ++t) lo[(size_t)t] = (int32_t)((int64_t)N * t / T);
+  for (int t = 0; t < T; ++t) {
+    cnt[(size_t)t].assign((size_t)(lo[t + 1] - lo[t]), 0);
+    part[(size_t)t].reserve((size_t)((int64_t)P * 4 / T));
+  }
+  if (T == 1) {
+    build_range(0, N, cnt[0], part[0]);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t)
+      th.emplace_back(build_range, lo[t], lo[t + 1], std::ref(cnt[(size_t)t]),
+                      std::ref(part[(size_t)t]));
+    for (auto &x : th) x.join();
+  }
+  size_t total = 0;
+  for (auto &v : part) total += v.size();
+  if (total > (size_t)INT32_MAX) {
+    set_error("adjacency exceeds 2^31 entries");
+    return FX_EINVAL;
+  }
+  ptr.assign((size_t)N + 1, 0);
+  idx.resize(total);
+  size_t off = 0;
+  for (int t = 0; t < T; ++t) {
+    for (int32_t a = lo[t]; a < lo[t + 1]; ++a)
+      ptr[(size_t)a + 1] = ptr[(size_t)a] + cnt[(size_t)t][(size_t)(a - lo[t])];
+    std::copy(part[(size_t)t].begin(), part[(size_t)t].end(), idx.begin() + (int64_t)off);
+    off += part[(size_t)t].size();
   }
   return FX_OK;
 }
