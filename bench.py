@@ -160,6 +160,28 @@ NCU_LIMITER = {
 
 
 # ---------------------------------------------------------------------------
+# Replicas (N > 1, "replicas only"): every rank runs the whole workload on its
+# own GPU; the job's time is the slowest rank's and its throughput the work of
+# all ranks over that time.
+def max_over_ranks(v: float, dist=None, device: str = "cpu") -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units: float, seconds: float, dist=None, device: str = "cpu") -> float:
+    """sum of units over ranks / max of seconds over ranks"""
+    if dist is None:
+        return units / seconds
+    import torch
+    u = torch.tensor([units], dtype=torch.float64, device=device)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(u.item()) / max_over_ranks(seconds, dist, device)
+
+
 def algorithmic(n, m, p, a, G, gc):
     """Compulsory HBM bytes (each array read once, each output written once)
     and flops per iteration, by stage."""
@@ -293,13 +315,7 @@ def run_fluxion(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(v):
-        if dist is None:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    dev = f"cuda:{local_rank}"
 
     sc = SynthCache(args)
     c, p = sc.circuit, sc.placement
@@ -339,7 +355,7 @@ def run_fluxion(args, rank, world, local_rank):
     ctx.set_profiling(False)
     launches = ctx.kernel_launches() - launches0
     stages = ctx.stage_times()
-    ms_max = max_over_ranks(ms)
+    ms_max = max_over_ranks(ms, dist, dev)
     value = world * args.steps / (ms_max / 1e3)
 
     # End to end through the public call with host buffers: every step
@@ -367,7 +383,7 @@ def run_fluxion(args, rank, world, local_rank):
             d.force_iterate(cfg, 1, ax, ay)
             if i >= args.warmup:
                 e2e_s += time.perf_counter() - t0
-        e2e_s = max_over_ranks(e2e_s)
+        e2e_s = max_over_ranks(e2e_s, dist, dev)
         e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": 8 * c.num_gates,
                "d2h_bytes_per_step": 8 * c.num_gates + ITER_STATS_D2H,
@@ -597,13 +613,8 @@ def run_serve(args, rank, world, local_rank):
     jobs_s = n_jobs / wall_mix
     serial_s = n_jobs / wall_ser
     if world > 1:
-        import torch
         import torch.distributed as tdist
-        t = torch.tensor([n_jobs, wall_mix], dtype=torch.float64, device=f"cuda:{local_rank}")
-        tdist.all_reduce(t[:1], op=tdist.ReduceOp.SUM)
-        w = t[1:].clone()
-        tdist.all_reduce(w, op=tdist.ReduceOp.MAX)
-        jobs_s = float(t[0]) / float(w[0])
+        jobs_s = replica_throughput(n_jobs, wall_mix, tdist, f"cuda:{local_rank}")
     kinds = [j["kind"] for j in wl.jobs]
     bin_ = sum(wl.bytes_in(j) for j in wl.jobs) / n_jobs
     out = {"metric": SERVE_METRIC, "value": jobs_s, "unit": "jobs/s", "n_gpus": world,
