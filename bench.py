@@ -146,16 +146,21 @@ def peaks():
 # (`--set full -s 1 -c 1` of the bench command with --steps 2 --warmup 3;
 # summaries under profiles/). A stage missing here reports traffic null.
 NCU_DRAM_BYTES = {
-    # bh_walk_kernel: 59.568 MB read + 2.309 MB written
-    "bh_walk": 61_876_736,
+    # bh_walk_kernel: 59.513 MB read + 2.212 MB written
+    "bh_walk": 61_725_696,
     # with --precision 3xtf32: 6 x tc_gemm_kernel<0> (21.000 MB + 0.011 MB
     # each) + dens_charge_kernel (8.393 MB); dens_scatter runs in the
     # previous step's fused kernel
     "density": 6 * 21_010_944 + 8_393_472,
 }
+# Warp instructions per launch (smsp__inst_executed.sum) and threads per warp
+# instruction (smsp__thread_inst_executed_per_inst_executed.ratio) of the
+# issue-bound walk, from the same kind of capture: its roofline is the issue
+# rate, 4 warp instructions per SM per cycle.
+NCU_WALK_INST = (1_390_529_927, 20.07)
 # What bounds each stage when it is not HBM or the tensor pipe (ncu).
 NCU_LIMITER = {
-    "bh_walk": "instruction issue: 87% issue-active, 0.5% of DRAM peak, 81% warps active",
+    "bh_walk": "instruction issue: 87% issue-active, 0.5% of DRAM peak, 82% warps active",
 }
 
 
@@ -428,6 +433,16 @@ def run_fluxion(args, rank, world, local_rank):
                 "algorithmic_bytes": b_alg[dom], "peak_source": f"{src} HBM copy"}
     if dom in NCU_LIMITER:
         roof["limiter"] = NCU_LIMITER[dom]
+    if dom == "bh_walk" and args.gates == 1_000_000:
+        inst, tpi = NCU_WALK_INST
+        mhz = (clk.get("sm_mhz") or 1965.0) if isinstance(clk, dict) else 1965.0
+        peak_i = 4 * 148 * mhz * 1e6
+        ach_i = inst / (per_iter[dom] * 1e-3)
+        roof["issue"] = {"achieved": ach_i, "peak": peak_i, "unit": "warp inst/s",
+                         "frac": ach_i / peak_i, "inst_per_launch": inst,
+                         "simt_efficiency": tpi / 32.0,
+                         "peak_source": "4 warp instructions per SM per cycle x 148 SMs x "
+                                        "median SM clock during the timed region"}
     if args.gates != 1_000_000 or args.bins != 1024 or (dom == "density" and
                                                         args.precision != "3xtf32"):
         roof["traffic"] = None  # the captures are of the default workload

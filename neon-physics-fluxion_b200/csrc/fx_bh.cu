@@ -343,69 +343,149 @@ __global__ void bh_tree_kernel(const uint32_t *__restrict__ keys, int n,
   if (i == 0) dparent[0] = -1;
 }
 
-// ---- FP64 prefix sums of the sorted positions, fixed association ------------
-// Chunks of kScanChunk consecutive values are added sequentially by one
-// thread each (left to right, starting from 0.0); chunk totals form the next
-// level, until one chunk remains. Exclusive offsets then flow back down:
-// a chunk's running sum starts from its offset at the level above. The
-// association depends only on n, so a sequential restatement reproduces
-// every bit. Node sums are prefix differences.
-constexpr int kScanChunk = 128;
+// ---- exact prefix sums of the sorted positions ---------------------------------
+// Every position becomes the 128-bit integer trunc(v * 2^64) (exact for
+// |v| >= 2^-41; smaller magnitudes lose their bits below 2^-64, non-finite
+// values count as 0). Integer sums do not depend on the order of addition,
+// so the prefix is computed tile-parallel and a node's sum, a prefix
+// difference, is exact. Its centre of mass is then
+//   ((double)hi * 2^64 + (double)lo) * 2^-64 / count
+// with hi/lo the upper (signed) and lower (unsigned) 64 bits, each step
+// rounded to nearest.
+constexpr int kFixThreads = 256, kFixItems = 8, kFixTile = kFixThreads * kFixItems;
 
-__global__ void scan_up_kernel(const float2 *__restrict__ pts,
-                               const double2 *__restrict__ in, int len,
-                               double2 *__restrict__ out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = c * kScanChunk;
-  if (b >= len) return;
-  const int e = min(len, b + kScanChunk);
-  double sx = 0.0, sy = 0.0;
-  for (int i = b; i < e; ++i) {
-    if (pts) {
-      const float2 p = pts[i];
-      sx = sx + (double)p.x;
-      sy = sy + (double)p.y;
-    } else {
-      const double2 v = in[i];
-      sx = sx + v.x;
-      sy = sy + v.y;
+__device__ __forceinline__ __int128 fixed64(float v) {
+  const uint32_t u = __float_as_uint(v);
+  const int e = (int)((u >> 23) & 255u);
+  if (e == 0 || e == 255) return 0;
+  const unsigned long long m = (u & 0x7fffffu) | 0x800000u;  // v = m * 2^(e - 150)
+  const int sh = e - 86;                                     // v * 2^64 = m * 2^(e - 86)
+  unsigned __int128 r = 0;
+  if (sh >= 0) r = (unsigned __int128)m << sh;
+  else if (sh > -64) r = m >> (-sh);
+  return (u >> 31) ? -(__int128)r : (__int128)r;
+}
+
+__device__ __forceinline__ ulonglong2 pack128(__int128 v) {
+  return make_ulonglong2((unsigned long long)v, (unsigned long long)((unsigned __int128)v >> 64));
+}
+__device__ __forceinline__ __int128 unpack128(ulonglong2 p) {
+  return (__int128)(((unsigned __int128)p.y << 64) | p.x);
+}
+__device__ __forceinline__ __int128 shfl_up128(__int128 v, int d) {
+  const ulonglong2 p = pack128(v);
+  return unpack128(make_ulonglong2(__shfl_up_sync(0xffffffffu, p.x, d),
+                                   __shfl_up_sync(0xffffffffu, p.y, d)));
+}
+
+// Inclusive scan of one int128 per thread over the block; also returns the
+// block total.
+__device__ __forceinline__ __int128 block_scan128(__int128 v, __int128 &total) {
+  __shared__ ulonglong2 wtot[kFixThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const __int128 u = shfl_up128(v, o);
+    if (lane >= o) v += u;
+  }
+  if (lane == 31) wtot[w] = pack128(v);
+  __syncthreads();
+  __int128 off = 0, tot = 0;
+  for (int q = 0; q < kFixThreads / 32; ++q) {
+    const __int128 t = unpack128(wtot[q]);
+    if (q < w) off += t;
+    tot += t;
+  }
+  __syncthreads();
+  total = tot;
+  return v + off;
+}
+
+// Pass 1: the (x, y) sums of each tile of kFixTile sorted points.
+__global__ void __launch_bounds__(kFixThreads)
+fix_tile_kernel(const float2 *__restrict__ spos, int n, ulonglong4 *__restrict__ tile_sum) {
+  const int b0 = blockIdx.x * kFixTile + threadIdx.x * kFixItems;
+  __int128 sx = 0, sy = 0;
+#pragma unroll
+  for (int k = 0; k < kFixItems; ++k) {
+    const int i = b0 + k;
+    if (i < n) {
+      const float2 p = spos[i];
+      sx += fixed64(p.x);
+      sy += fixed64(p.y);
     }
   }
-  out[c] = make_double2(sx, sy);
-}
-
-// Exclusive running sums of one level: chunk c starts from `up[c]` (or 0.0
-// at the top, where the whole level is one chunk).
-__global__ void scan_down_kernel(const double2 *__restrict__ v, int len,
-                                 const double2 *__restrict__ up,
-                                 double2 *__restrict__ x) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = c * kScanChunk;
-  if (b >= len) return;
-  const int e = min(len, b + kScanChunk);
-  double sx = up ? up[c].x : 0.0, sy = up ? up[c].y : 0.0;
-  for (int i = b; i < e; ++i) {
-    x[i] = make_double2(sx, sy);
-    sx = sx + v[i].x;
-    sy = sy + v[i].y;
+  __int128 tx, ty;
+  block_scan128(sx, tx);
+  block_scan128(sy, ty);
+  if (threadIdx.x == 0) {
+    const ulonglong2 a = pack128(tx), c = pack128(ty);
+    tile_sum[blockIdx.x] = make_ulonglong4(a.x, a.y, c.x, c.y);
   }
 }
 
-// Inclusive prefix of the points: chunk c starts from off[c] (or 0.0).
-__global__ void scan_final_kernel(const float2 *__restrict__ pts, int n,
-                                  const double2 *__restrict__ off,
-                                  double2 *__restrict__ prefix) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = c * kScanChunk;
-  if (b >= n) return;
-  const int e = min(n, b + kScanChunk);
-  double sx = off ? off[c].x : 0.0, sy = off ? off[c].y : 0.0;
-  for (int i = b; i < e; ++i) {
-    const float2 p = pts[i];
-    sx = sx + (double)p.x;
-    sy = sy + (double)p.y;
-    prefix[i] = make_double2(sx, sy);
+// Pass 2: exclusive offsets of the tiles (one block, kFixThreads tiles at a
+// time, carrying the running total; exact, so the grouping is free).
+__global__ void __launch_bounds__(kFixThreads)
+fix_top_kernel(ulonglong4 *__restrict__ tile_sum, int tiles) {
+  __int128 cx = 0, cy = 0;
+  for (int base = 0; base < tiles; base += kFixThreads) {
+    const int t = base + threadIdx.x;
+    __int128 vx = 0, vy = 0;
+    if (t < tiles) {
+      const ulonglong4 v = tile_sum[t];
+      vx = unpack128(make_ulonglong2(v.x, v.y));
+      vy = unpack128(make_ulonglong2(v.z, v.w));
+    }
+    __int128 tx, ty;
+    const __int128 ix = block_scan128(vx, tx);
+    const __int128 iy = block_scan128(vy, ty);
+    if (t < tiles) {
+      const ulonglong2 a = pack128(cx + ix - vx), c = pack128(cy + iy - vy);
+      tile_sum[t] = make_ulonglong4(a.x, a.y, c.x, c.y);
+    }
+    cx += tx;
+    cy += ty;
   }
+}
+
+// Pass 3: inclusive prefix of every point (x lo/hi, y lo/hi).
+__global__ void __launch_bounds__(kFixThreads)
+fix_prefix_kernel(const float2 *__restrict__ spos, int n,
+                  const ulonglong4 *__restrict__ tile_off, ulonglong4 *__restrict__ prefix) {
+  const int b0 = blockIdx.x * kFixTile + threadIdx.x * kFixItems;
+  __int128 sx = 0, sy = 0;
+#pragma unroll
+  for (int k = 0; k < kFixItems; ++k) {
+    const int i = b0 + k;
+    if (i < n) {
+      const float2 p = spos[i];
+      sx += fixed64(p.x);
+      sy += fixed64(p.y);
+    }
+  }
+  __int128 tx, ty;
+  const ulonglong4 to = tile_off[blockIdx.x];
+  __int128 rx = block_scan128(sx, tx) - sx + unpack128(make_ulonglong2(to.x, to.y));
+  __int128 ry = block_scan128(sy, ty) - sy + unpack128(make_ulonglong2(to.z, to.w));
+  for (int k = 0; k < kFixItems; ++k) {  // the points again (cached), in order
+    const int i = b0 + k;
+    if (i >= n) break;
+    const float2 p = spos[i];
+    rx += fixed64(p.x);
+    ry += fixed64(p.y);
+    const ulonglong2 a = pack128(rx), c = pack128(ry);
+    prefix[i] = make_ulonglong4(a.x, a.y, c.x, c.y);
+  }
+}
+
+// ((double)hi * 2^64 + (double)lo) * 2^-64, each step rounded to nearest.
+__device__ __forceinline__ double fixed_to_double(__int128 v) {
+  const long long hi = (long long)(v >> 64);
+  const unsigned long long lo = (unsigned long long)v;
+  return __dmul_rn(__dadd_rn(__dmul_rn(__ll2double_rn(hi), 18446744073709551616.0),
+                             __ull2double_rn(lo)),
+                   5.42101086242752217003726400434970855712890625e-20);
 }
 
 // Walk record of every internal node (two float4):
@@ -415,19 +495,23 @@ __global__ void scan_final_kernel(const float2 *__restrict__ pts, int n,
 __global__ void bh_node_kernel(int n, const int32_t *__restrict__ range,
                                const int32_t *__restrict__ dnode,
                                const int32_t *__restrict__ dparent,
-                               const double2 *__restrict__ prefix,
+                               const ulonglong4 *__restrict__ prefix,
                                const float *__restrict__ root,
                                float4 *__restrict__ node) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   const int f = range[2 * i], l = range[2 * i + 1];
   const int cnt = l - f + 1;
-  double sx = prefix[l].x, sy = prefix[l].y;
+  const ulonglong4 pl = prefix[l];
+  __int128 sx = unpack128(make_ulonglong2(pl.x, pl.y));
+  __int128 sy = unpack128(make_ulonglong2(pl.z, pl.w));
   if (f > 0) {
-    sx = sx - prefix[f - 1].x;
-    sy = sy - prefix[f - 1].y;
+    const ulonglong4 pf = prefix[f - 1];
+    sx -= unpack128(make_ulonglong2(pf.x, pf.y));
+    sy -= unpack128(make_ulonglong2(pf.z, pf.w));
   }
-  const double cx = sx / (double)cnt, cy = sy / (double)cnt;
+  const double cx = __ddiv_rn(fixed_to_double(sx), (double)cnt);
+  const double cy = __ddiv_rn(fixed_to_double(sy), (double)cnt);
   const float hx = (float)cx, hy = (float)cy;
   node[2 * i] = make_float4(hx, hy, (float)(cx - (double)hx), (float)(cy - (double)hy));
   const int dn = dnode[i], dp = dparent[i];
@@ -636,17 +720,6 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
   if (valid) force[perm[s]] = make_float2(fx, fy);
 }
 
-// Lengths of the chunked-scan levels above the points: L[0] = chunks of the
-// points, L[1] = chunks of L[0], ... until a level fits one chunk.
-static int scan_levels(int n, int *len) {
-  int k = 0, m = n;
-  while (m > kScanChunk && k < 5) {
-    m = (m + kScanChunk - 1) / kScanChunk;
-    len[k++] = m;
-  }
-  return k;
-}
-
 static int bh_alloc(fx_design *d) {
   BHWork &b = d->bh;
   const int n = d->n;
@@ -666,16 +739,7 @@ static int bh_alloc(fx_design *d) {
   FX_TRY(b.dnode.alloc(ni));
   FX_TRY(b.dparent.alloc(ni));
   FX_TRY(b.qchild.alloc(ni));
-  int len[5];
-  const int K = scan_levels(n, len);
-  if (K > 3) {
-    set_error("Barnes-Hut: %d points exceed the prefix-scan capacity", n);
-    return FX_EINVAL;
-  }
-  for (int l = 0; l < K; ++l) {
-    FX_TRY(b.scan[2 * l].alloc(len[l]));      // chunk totals of level l
-    FX_TRY(b.scan[2 * l + 1].alloc(len[l]));  // exclusive offsets of level l
-  }
+  FX_TRY(b.tile_fix.alloc((size_t)(n + kFixTile - 1) / kFixTile));
   FX_TRY(b.prefix.alloc(n));
   FX_TRY(b.node.alloc(2 * ni));
   FX_TRY(b.root.alloc(4));
@@ -737,28 +801,15 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
     const int tb = (n - 1 + 255) / 256;
     bh_tree_kernel<<<tb, 256, 0, s>>>(b.keys[0].p, n, b.child.p, b.range.p,
                                       b.dnode.p, b.dparent.p);
-    // chunked prefix scan: up, top, down, final
-    int len[5];
-    const int K = scan_levels(n, len);
-    auto blocks = [](int chunks) { return (chunks + 127) / 128; };
-    for (int l = 0; l < K; ++l) {
-      const int in_len = l == 0 ? n : len[l - 1];
-      scan_up_kernel<<<blocks(len[l]), 128, 0, s>>>(
-          l == 0 ? b.spos.p : nullptr, l == 0 ? nullptr : b.scan[2 * (l - 1)].p,
-          in_len, b.scan[2 * l].p);
-    }
-    for (int l = K - 1; l >= 0; --l) {
-      // offsets of level l's values (the chunk totals of level l - 1)
-      const double2 *up = l == K - 1 ? nullptr : b.scan[2 * (l + 1) + 1].p;
-      scan_down_kernel<<<blocks((len[l] + kScanChunk - 1) / kScanChunk), 128, 0, s>>>(
-          b.scan[2 * l].p, len[l], up, b.scan[2 * l + 1].p);
-    }
-    scan_final_kernel<<<blocks(len[0] > 0 && K > 0 ? len[0] : 1), 128, 0, s>>>(
-        b.spos.p, n, K > 0 ? b.scan[1].p : nullptr, b.prefix.p);
+    // exact prefix sums: tile sums, tile offsets, point prefixes
+    const int tiles = (n + kFixTile - 1) / kFixTile;
+    fix_tile_kernel<<<tiles, kFixThreads, 0, s>>>(b.spos.p, n, b.tile_fix.p);
+    fix_top_kernel<<<1, kFixThreads, 0, s>>>(b.tile_fix.p, tiles);
+    fix_prefix_kernel<<<tiles, kFixThreads, 0, s>>>(b.spos.p, n, b.tile_fix.p, b.prefix.p);
     bh_node_kernel<<<tb, 256, 0, s>>>(n, b.range.p, b.dnode.p, b.dparent.p,
                                       b.prefix.p, b.root.p, b.node.p);
     bh_qchild_kernel<<<tb, 256, 0, s>>>(n, b.child.p, b.dnode.p, b.qchild.p);
-    launches += 4 + 2 * K + 1;
+    launches += 6;
   }
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_TREE, s, ev);

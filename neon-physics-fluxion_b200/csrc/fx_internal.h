@@ -135,8 +135,8 @@ struct BHWork {
   DevBuf<int32_t> dnode;        // internal nodes: prefix length
   DevBuf<int32_t> dparent;      // internal nodes: parent's prefix length
   DevBuf<int4> qchild;          // internal nodes: up to 4 quad children
-  DevBuf<double2> scan[6];      // chunked FP64 prefix-scan levels
-  DevBuf<double2> prefix;       // inclusive FP64 prefix sums of spos
+  DevBuf<ulonglong4> tile_fix;  // per-tile exact (x, y) sums, then offsets
+  DevBuf<ulonglong4> prefix;    // inclusive exact prefix sums of spos (2 x int128)
   DevBuf<float4> node;          // internal nodes: 2 x float4 walk records
   DevBuf<float> root;           // {x_min, y_min, size}
   DevBuf<unsigned int> bbox;    // [0..3] ordered-int box, [4] error flag
@@ -147,8 +147,7 @@ struct BHWork {
     for (auto &b : idx) f(b);
     f(tile_hist); f(tile_scan); f(digit_total); f(spos); f(child); f(range);
     f(dnode); f(dparent); f(qchild);
-    for (auto &b : scan) f(b);
-    f(prefix); f(node); f(root); f(bbox); f(force);
+    f(tile_fix); f(prefix); f(node); f(root); f(bbox); f(force);
   }
 };
 

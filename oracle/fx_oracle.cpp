@@ -688,53 +688,31 @@ void or_bh_keys(int32_t n, const float *x, const float *y, const float *root,
 }
 
 namespace {
-// FP64 inclusive prefix sums of the sorted positions with the fixed chunked
-// association of the device: chunks of 128 consecutive values are added left
-// to right from 0.0; chunk totals form the next level until one chunk
-// remains; each chunk's running sum then starts from its offset one level up.
-constexpr int kScanChunk = 128;
+// Exact prefix sums of the sorted positions, as the device computes them:
+// each position becomes the 128-bit integer trunc(v * 2^64) (exact for
+// |v| >= 2^-41, non-finite values count as 0), node sums are differences of
+// integer prefixes, and a centre of mass is
+// ((double)hi * 2^64 + (double)lo) * 2^-64 / count (hi/lo: the upper signed and
+// lower unsigned 64 bits), each step rounded to nearest.
+static __int128 fixed64(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, 4);
+  const int e = (int)((u >> 23) & 255u);
+  if (e == 0 || e == 255) return 0;
+  const unsigned long long m = (u & 0x7fffffu) | 0x800000u;
+  const int sh = e - 86;
+  unsigned __int128 r = 0;
+  if (sh >= 0) r = (unsigned __int128)m << sh;
+  else if (sh > -64) r = m >> (-sh);
+  return (u >> 31) ? -(__int128)r : (__int128)r;
+}
 
-static void chunked_prefix(const std::vector<double> &v, std::vector<double> &out) {
-  const int64_t n = (int64_t)v.size();
-  std::vector<std::vector<double>> tot;  // tot[l] = chunk totals of level l
-  const std::vector<double> *cur = &v;
-  while ((int64_t)cur->size() > kScanChunk) {
-    const int64_t m = ((int64_t)cur->size() + kScanChunk - 1) / kScanChunk;
-    std::vector<double> t((size_t)m);
-    for (int64_t c = 0; c < m; ++c) {
-      double acc = 0.0;
-      for (int64_t i = c * kScanChunk; i < std::min<int64_t>(cur->size(), (c + 1) * kScanChunk); ++i)
-        acc = acc + (*cur)[i];
-      t[c] = acc;
-    }
-    tot.push_back(std::move(t));
-    cur = &tot.back();
-  }
-  // exclusive offsets, top level first
-  std::vector<double> off_above;  // offsets of the level above's values
-  std::vector<std::vector<double>> offs(tot.size());
-  for (int l = (int)tot.size() - 1; l >= 0; --l) {
-    const std::vector<double> &vals = tot[l];
-    std::vector<double> &o = offs[l];
-    o.resize(vals.size());
-    const int64_t chunks = ((int64_t)vals.size() + kScanChunk - 1) / kScanChunk;
-    for (int64_t c = 0; c < chunks; ++c) {
-      double acc = (l == (int)tot.size() - 1) ? 0.0 : offs[l + 1][c];
-      for (int64_t i = c * kScanChunk; i < std::min<int64_t>(vals.size(), (c + 1) * kScanChunk); ++i) {
-        o[i] = acc;
-        acc = acc + vals[i];
-      }
-    }
-  }
-  out.resize((size_t)n);
-  const int64_t chunks = (n + kScanChunk - 1) / kScanChunk;
-  for (int64_t c = 0; c < chunks; ++c) {
-    double acc = tot.empty() ? 0.0 : offs[0][c];
-    for (int64_t i = c * kScanChunk; i < std::min<int64_t>(n, (c + 1) * kScanChunk); ++i) {
-      acc = acc + v[i];
-      out[i] = acc;
-    }
-  }
+static double fixed_to_double(__int128 v) {
+  const long long hi = (long long)(v >> 64);
+  const unsigned long long lo = (unsigned long long)v;
+  const double a = (double)hi * 18446744073709551616.0;
+  const double b = a + (double)lo;
+  return b * 5.42101086242752217003726400434970855712890625e-20;
 }
 
 // The radix tree over the sorted keys, built top-down: node [f, l] splits
@@ -745,7 +723,7 @@ struct BHTree {
   std::vector<uint32_t> key;      // sorted keys
   std::vector<int32_t> perm;      // sorted -> original
   std::vector<float> sx, sy;      // sorted positions
-  std::vector<double> px, py;     // chunked FP64 prefix sums
+  std::vector<__int128> px, py;   // exact fixed-point prefix sums
   float rsize;
   struct Node {
     int32_t f, l, dn, dp, left, right;
@@ -782,14 +760,14 @@ struct BHTree {
     nd.dp = dp;
     nd.left = left;
     nd.right = right;
-    double sxd = px[l], syd = py[l];
+    __int128 sxi = px[l], syi = py[l];
     if (f > 0) {
-      sxd = sxd - px[f - 1];
-      syd = syd - py[f - 1];
+      sxi -= px[f - 1];
+      syi -= py[f - 1];
     }
     const int32_t cnt = l - f + 1;
-    nd.cxd = sxd / (double)cnt;
-    nd.cyd = syd / (double)cnt;
+    nd.cxd = fixed_to_double(sxi) / (double)cnt;
+    nd.cyd = fixed_to_double(syi) / (double)cnt;
     nd.hx = (float)nd.cxd;
     nd.hy = (float)nd.cyd;
     nd.lx = (float)(nd.cxd - (double)nd.hx);
@@ -928,17 +906,19 @@ void or_bh_forces(int32_t n, const float *x, const float *y, double k,
   t.key.resize((size_t)n);
   t.sx.resize((size_t)n);
   t.sy.resize((size_t)n);
-  std::vector<double> vx((size_t)n), vy((size_t)n);
+  t.px.resize((size_t)n);
+  t.py.resize((size_t)n);
+  __int128 ax = 0, ay = 0;
   for (int32_t s = 0; s < n; ++s) {
     const int32_t g = t.perm[s];
     t.key[s] = keys[g];
     t.sx[s] = x[g];
     t.sy[s] = y[g];
-    vx[s] = (double)x[g];
-    vy[s] = (double)y[g];
+    ax += fixed64(x[g]);
+    ay += fixed64(y[g]);
+    t.px[s] = ax;
+    t.py[s] = ay;
   }
-  chunked_prefix(vx, t.px);
-  chunked_prefix(vy, t.py);
   t.nodes.reserve(n > 1 ? (size_t)n - 1 : 1);
   if (n >= 2) t.build(0, n - 1, -1);
   const float mdf = (float)min_dist;
