@@ -240,6 +240,10 @@ radix_scatter_kernel(const uint32_t *__restrict__ kin,
     rank[r] = old + __popc(peers & lt_mask);
   }
   __syncthreads();
+  // thread t = digit t: offsets of the warps within the digit, and the
+  // digit's start within the tile (exclusive scan over digits)
+  __shared__ uint32_t tstart[256];
+  __shared__ uint32_t gbase[256];
   {
     uint32_t run = 0;
 #pragma unroll
@@ -248,18 +252,43 @@ radix_scatter_kernel(const uint32_t *__restrict__ kin,
       cnt[ww][t] = run;
       run += c;
     }
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
+    }
+    __syncthreads();
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    uint32_t st = x - run;
+    for (int q = 0; q < w; ++q) st += ws[q];
+    tstart[t] = st;
+    // output index of tile position j of digit t: gbase[t] + j
+    gbase[t] = doff[t] + tile_scan[(size_t)t * T + blockIdx.x] - st;
   }
   __syncthreads();
+  // stage the tile in sorted order, then write it out: consecutive threads
+  // cover consecutive positions of a digit's run, so the stores coalesce
+  __shared__ uint32_t sk[kSortTile];
+  __shared__ int32_t sv[kSortTile];
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
     const int i = base + r * 32 + lane;
     if (i < n) {
       const uint32_t dg = (k[r] >> shift) & 255u;
-      const uint32_t pos = doff[dg] + tile_scan[(size_t)dg * T + blockIdx.x] +
-                           cnt[w][dg] + rank[r];
-      kout[pos] = k[r];
-      iout[pos] = v[r];
+      const uint32_t j = tstart[dg] + cnt[w][dg] + rank[r];
+      sk[j] = k[r];
+      sv[j] = v[r];
     }
+  }
+  __syncthreads();
+  const int m = min(kSortTile, n - (int)(blockIdx.x * kSortTile));
+  for (int j = t; j < m; j += kSortThreads) {
+    const uint32_t key = sk[j];
+    const uint32_t pos = gbase[(key >> shift) & 255u] + (uint32_t)j;
+    kout[pos] = key;
+    iout[pos] = sv[j];
   }
 }
 
