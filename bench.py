@@ -67,9 +67,10 @@ def parse():
     ap.add_argument("--trajectory", type=int, default=500,
                     help="iterations of the full run reported beside the steps (0: skip)")
     ap.add_argument("--workload", default="plain",
-                    choices=["plain", "small", "serve", "leaves", "precision"],
+                    choices=["plain", "small", "serve", "leaves", "precision", "attention"],
                     help="plain: the 1M-gate iteration; serve: the request stream; "
-                         "leaves: the batched leaf placement; precision: the DCT sweep")
+                         "leaves: the batched leaf placement; precision: the DCT sweep; "
+                         "attention: every level of the 1M-gate hierarchy")
     ap.add_argument("--clusters", type=int, default=16_384, help="leaves: clusters")
     ap.add_argument("--leaf-iters", type=int, default=300, help="leaves: force iterations")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
@@ -982,6 +983,141 @@ def run_small(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+ATTN_METRIC = "attention passes/s (compute_all_attention over the hierarchy, top-10)"
+ATTN_TOP_K = 10
+
+
+def attention_setup(args, rank):
+    """The plain netlist, its device hierarchy (default partition config) and
+    the levels with at least two clusters, as host CSR lists."""
+    import fluxion_b200 as fx
+    syn = fx.synth_plain(args.seed + rank, args.gates, args.nets, args.die)
+    return syn, fx
+
+
+def attention_levels(fx, d):
+    tree = d.partition(fx.part_cfg())
+    lv = fx.hierarchy_levels(tree["leaf_ptr"], tree["leaf_gate"], tree["leaf_depth"])
+    return [(t, cp, cg) for t, (cp, cg) in enumerate(lv) if len(cp) - 1 >= 2]
+
+
+def attention_cpu_sample(c, levels, k_max=16):
+    """compute_level_attention restated in C++ with hash sets, on k sampled
+    clusters per level, scaled to the whole level by the cost of each phase:
+    net sets (one scan of every net per cluster) x n/k, intersections x
+    n(n-1)/(k(k-1)), top-k sorts x n/k. Returns (seconds per pass, sample)."""
+    from oracle import oracle as orc
+    orc.build()
+    total, samp = 0.0, 0
+    for _, cp, cg in levels:
+        n = len(cp) - 1
+        k = min(n, k_max)
+        rows = np.linspace(0, n - 1, k).round().astype(np.int32)
+        rows = np.unique(rows)
+        k = len(rows)
+        _, _, t = orc.attention_sample(c.net_ptr, c.net_gate, cp, cg, rows, ATTN_TOP_K)
+        total += t[0] * n / k + t[1] * (n * (n - 1)) / max(k * (k - 1), 1) + t[2] * n / k
+        samp += k
+    return total, samp
+
+
+def run_attention(args, rank, world, local_rank):
+    """(f.4) attention scores, compute_all_attention (attention.rs:33-48),
+    over every level of the plain netlist's hierarchy: one step = one
+    fx_attention call per level with host cluster lists in and top-10 lists
+    out. `value` from the device time of the calls (stage events), `e2e` from
+    the calls' wall time; the dense n x n score matrices are not requested
+    (fx_attention returns them on request)."""
+    syn, fx = attention_setup(args, rank)
+    c = syn.circuit
+    ctx = fx.Context(local_rank)
+    d = fx.Design(ctx, c)
+    levels = attention_levels(fx, d)
+    first = [d.attention_level(cp, cg, ATTN_TOP_K)[0] for _, cp, cg in levels]
+    for _ in range(max(0, args.warmup - 1)):
+        for _, cp, cg in levels:
+            d.attention_level(cp, cg, ATTN_TOP_K)
+    ctx.synchronize()
+    ctx.reset_stage_times()
+    ctx.set_profiling(True)
+    launches0 = ctx.kernel_launches()
+    clocks = ClockSampler(local_rank)
+    t0 = time.perf_counter()
+    same = True
+    for _ in range(args.steps):
+        for (_, cp, cg), f in zip(levels, first):
+            top, _ = d.attention_level(cp, cg, ATTN_TOP_K)
+            same = same and np.array_equal(top, f)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    ctx.set_profiling(False)
+    launches = ctx.kernel_launches() - launches0
+    dev_ms = ctx.stage_times()["attention"][0] / args.steps
+    n_cl = [len(cp) - 1 for _, cp, _ in levels]
+    d.close()
+    ctx.close()
+    # algorithmic bytes of one pass: per level the netlist's pin lists and each
+    # pin's cluster (net_ptr, net_gate, cluster id), each ordered pair key
+    # once, the unique pairs' keys and scores once, and the top-k lists
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sec, k = attention_cpu_sample(c, levels)
+        cpu = {"value": 1.0 / sec, "unit": "passes/s", "cores": 1, "kind": "port",
+               "sample": f"{k} sampled clusters over {len(levels)} levels through the C++ "
+                         "hash-set restatement of compute_level_attention, each phase scaled "
+                         "to the whole level"}
+    h2d = sum(4 * (len(cp) + len(cg)) for _, cp, cg in levels)
+    d2h = sum(4 * n * ATTN_TOP_K for n in n_cl)
+    out = {"metric": ATTN_METRIC, "value": world * 1e3 / dev_ms, "unit": "passes/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+           "data": "synthetic",
+           "config": {"workload": f"attention: {args.gates} gates, {args.nets} nets, "
+                                  f"{len(levels)} levels of 2..{max(n_cl)} clusters, top "
+                                  f"{ATTN_TOP_K}", "seed": args.seed,
+                      "l2": "inputs (pins, pair keys) larger than L2 at the deep levels"},
+           "levels": n_cl, "same_result_every_step": bool(same), "cpu_baseline": cpu,
+           "e2e": {"value": world * args.steps / wall, "unit": "passes/s",
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "call": "fx_attention per level with host cluster lists"},
+           "gpu_launches": launches, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_attention_reference(args, rank, world):
+    """The reference's single-threaded compute_all_attention restated in C++
+    (hash sets), timed on a bounded sample of clusters per level and scaled."""
+    if rank != 0:
+        return
+    import fluxion_b200 as fx
+    from oracle import oracle as orc
+    syn = fx.synth_plain(args.seed, args.gates, args.nets, args.die)
+    c = syn.circuit
+    ap, ai = orc.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    t = orc.build_hierarchy(c.num_gates, ap, ai, c.chip_width, c.chip_height)
+    lv = fx.hierarchy_levels(t["leaf_ptr"], t["leaf_gate"], t["leaf_depth"])
+    levels = [(d, cp, cg) for d, (cp, cg) in enumerate(lv) if len(cp) - 1 >= 2]
+    per = []
+    for i in range(args.warmup + args.steps):
+        sec, k = attention_cpu_sample(c, levels, k_max=8)
+        if i >= args.warmup:
+            per.append(sec)
+    sec = float(np.mean(per))
+    out = {"metric": ATTN_METRIC, "value": 1.0 / sec, "unit": "passes/s", "impl": "reference",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+           "data": "synthetic",
+           "config": {"workload": f"attention: {args.gates} gates, {args.nets} nets, "
+                                  f"{len(levels)} levels, top {ATTN_TOP_K}", "seed": args.seed},
+           "cpu_baseline": {"value": 1.0 / sec, "unit": "passes/s", "cores": 1, "kind": "port",
+                            "sample": f"{k} sampled clusters per pass (the oracle's hierarchy), "
+                                      "each phase scaled to the whole level"},
+           "e2e": {"value": 1.0 / sec, "unit": "passes/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
 def run_leaves_reference(args, rank, world):
     """place_gates_in_leaf (placer.rs:210-287, the oracle's restatement) over
     the same clusters on all host threads, on a bounded sample of clusters."""
@@ -1053,6 +1189,14 @@ def main():
             run_leaves_reference(args, rank, world)
             return
         run_leaves(args, rank, world, local_rank)
+        return
+    if args.workload == "attention":
+        args.steps = max(1, min(args.steps, 50))
+        if args.impl == "reference":
+            args.steps, args.warmup = min(args.steps, 3), min(args.warmup, 1)
+            run_attention_reference(args, rank, world)
+            return
+        run_attention(args, rank, world, local_rank)
         return
     if args.workload == "serve":
         if args.impl == "reference":

@@ -79,7 +79,8 @@ int fx_ctx_synchronize(fx_ctx *ctx);
 #define FX_STAGE_CONGESTION        6 /* rows D+F: bbox, counting, HPWL        */
 #define FX_STAGE_LEAF              7 /* row H: batched leaf placer            */
 #define FX_STAGE_FIEDLER           8 /* row G: power iteration                */
-#define FX_STAGE_COUNT             9
+#define FX_STAGE_ATTENTION         9 /* (f.4) attention scores of a level     */
+#define FX_STAGE_COUNT             10
 
 /* ---- designs (device-resident netlists) -------------------------------- */
 /* Uploads a netlist and builds every device structure the hot path needs
@@ -192,6 +193,18 @@ int fx_part_cfg_default(fx_part_cfg *cfg);
 int fx_partition(fx_ctx *ctx, fx_design *design, const fx_part_cfg *cfg,
                  int32_t leaf_capacity, int32_t *out_leaf_ptr, int32_t *out_leaf_gate,
                  float *out_region, int32_t *out_leaf_depth, fx_part_stats *out_stats);
+
+/* ---- (f.4) attention scores between the clusters of one level ------------ */
+/* Mirrors compute_level_attention (H/src/algorithm/attention.rs:50-88) for
+ * the clusters of one hierarchy level, given as a CSR over gates (disjoint;
+ * gates in no cluster are ignored): score(A -> B) = |nets touching A and B| /
+ * |nets touching A| in f32, and per cluster the top_k clusters by score
+ * (descending, ties by smaller index, zero scores dropped; unused slots -1).
+ * out_topk[n * top_k] and the dense out_scores[n * n] (row A, column B) are
+ * host buffers and may be NULL. At most 65535 clusters. */
+int fx_attention(fx_ctx *ctx, fx_design *design, int32_t n_clusters,
+                 const int32_t *cluster_ptr, const int32_t *cluster_gate, int32_t top_k,
+                 int32_t *out_topk, float *out_scores);
 
 /* ---- rows A..F: the plain composite force iteration -------------------- */
 typedef struct fx_iter_cfg {

@@ -25,7 +25,7 @@ FX_DCT_BF16 = 2
 FX_DCT_SIMT = 3
 
 STAGES = ["attract_integrate", "bh_keys", "bh_sort", "bh_tree", "bh_walk",
-          "density", "congestion", "leaf", "fiedler"]
+          "density", "congestion", "leaf", "fiedler", "attention"]
 
 _CODES = {FX_EINVAL: "FX_EINVAL", FX_ENOMEM: "FX_ENOMEM", FX_ECUDA: "FX_ECUDA",
           FX_ETIMEOUT: "FX_ETIMEOUT", FX_EADMIT: "FX_EADMIT",
@@ -177,6 +177,7 @@ SIGNATURES = {
     "fx_fiedler": (C.c_int, [P, P, I32, PI32, PI32, I32, C.c_double, PF32, PI32, PF64]),
     "fx_refine_cfg_default": (C.c_int, [C.POINTER(RefineCfg)]),
     "fx_part_cfg_default": (C.c_int, [C.POINTER(PartCfg)]),
+    "fx_attention": (C.c_int, [P, P, I32, PI32, PI32, I32, PI32, PF32]),
     "fx_blif_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, I32]),
     "fx_def_write": (C.c_int, [C.c_char_p, C.c_char_p, I32, PF32, PF32, F32, F32, C.c_char_p]),
     "fx_serve_cfg_default": (C.c_int, [C.POINTER(ServeCfg)]),

@@ -375,6 +375,36 @@ class Design:
                     leaf_depth=ld[:L], num_nodes=st.n_nodes, max_depth=st.max_depth,
                     levels=st.levels, power_iterations=st.power_iterations)
 
+    # -- (f.4) attention scores between the clusters of one level ----------------
+    def attention_level(self, cluster_ptr, cluster_gate, top_k: int = 10,
+                        scores: bool = False):
+        """compute_level_attention (attention.rs:50-88) for one level's clusters
+        (CSR over gates). Returns (top[n, top_k] int32, -1 padded; scores[n, n]
+        f32 or None)."""
+        cp = np.ascontiguousarray(cluster_ptr, np.int32)
+        cg = np.ascontiguousarray(cluster_gate, np.int32)
+        n = len(cp) - 1
+        top = np.full((n, top_k), -1, np.int32)
+        sc = np.zeros((n, n), np.float32) if scores else None
+        check(self.lib.fx_attention(self.ctx.handle, self.handle, n, ptr(cp, C.c_int32),
+                                    ptr(cg, C.c_int32), top_k, ptr(top, C.c_int32),
+                                    ptr(sc, C.c_float)), "fx_attention")
+        return top, sc
+
+    def attention(self, tree: dict, top_k: int = 10, scores: bool = False) -> list:
+        """compute_all_attention (attention.rs:33-48) over a hierarchy from
+        partition(): one dict(level_index, top_k, scores) per depth with at
+        least two clusters; top_k is a list of lists as in AttentionLevel."""
+        out = []
+        for depth, (cp, cg) in enumerate(hierarchy_levels(tree["leaf_ptr"], tree["leaf_gate"],
+                                                          tree["leaf_depth"])):
+            if len(cp) - 1 < 2:
+                continue
+            top, sc = self.attention_level(cp, cg, top_k, scores)
+            out.append(dict(level_index=depth, top_k=[[int(j) for j in r if j >= 0] for r in top],
+                            scores=sc))
+        return out
+
     # -- congestion refinement ----------------------------------------------------
     def refine(self, cfg=None, x=None, y=None, counts: bool = False):
         """refiner.rs:34-126 refine_placement. With x/y (host arrays, updated
@@ -406,6 +436,52 @@ class Design:
         if y is not None and ya is not y:
             y[...] = ya
         return st
+
+
+def hierarchy_levels(leaf_ptr, leaf_gate, leaf_depth) -> list:
+    """HierarchyTree::clusters_at_depth (hierarchy.rs:134-159) for every depth
+    0..max_depth of a hierarchy given by its leaves in DFS order and their
+    depths (recursive_bisect makes two children per internal node,
+    partitioner.rs:85-99, so the depths fix the tree): a list over depth of
+    (cluster_ptr, cluster_gate), the clusters in DFS order, each cluster's
+    gates those of its leaves in order."""
+    lp = np.asarray(leaf_ptr, np.int64)
+    lg = np.asarray(leaf_gate, np.int32)
+    d = [int(v) for v in leaf_depth]
+    L = len(d)
+    if L == 0:
+        return []
+    # path of each leaf as a binary code of d[i] bits (0 = first child)
+    code = [0] * L
+    for i in range(1, L):
+        c = code[i - 1] + 1
+        if d[i] >= d[i - 1]:
+            c <<= d[i] - d[i - 1]
+        else:
+            k = d[i - 1] - d[i]
+            if c & ((1 << k) - 1):
+                raise ValueError("leaf depths do not form a full binary tree")
+            c >>= k
+        code[i] = c
+    if code[-1] + 1 != 1 << d[-1] or code[0] != 0:
+        raise ValueError("leaf depths do not form a full binary tree")
+    wide = max(d) > 62
+    dd = np.asarray(d, np.int64)
+    cc = np.asarray(code, object if wide else np.int64)
+    size = np.diff(lp)
+    levels = []
+    for t in range(max(d) + 1):
+        idx = np.nonzero(dd >= t)[0]
+        pre = cc[idx] >> (dd[idx] - t).astype(cc.dtype)
+        first = np.ones(len(idx), bool)
+        first[1:] = pre[1:] != pre[:-1]
+        run = np.cumsum(first) - 1
+        csize = np.bincount(run, weights=size[idx], minlength=int(first.sum())).astype(np.int64)
+        cp = np.zeros(len(csize) + 1, np.int32)
+        cp[1:] = np.cumsum(csize)
+        cg = np.concatenate([lg[lp[i]:lp[i + 1]] for i in idx]) if len(idx) else lg[:0]
+        levels.append((cp, cg.astype(np.int32)))
+    return levels
 
 
 def leaf_cfg(**overrides) -> "_lib.LeafCfg":

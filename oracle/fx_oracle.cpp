@@ -12,7 +12,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <chrono>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include <thread>
@@ -955,6 +957,73 @@ void or_repulsion_exact(int32_t n, const float *x, const float *y, double k,
     fx[i] = ax;
     fy[i] = ay;
   }
+}
+
+// compute_level_attention (H/src/algorithm/attention.rs:50-88) with its hash
+// sets, for k sampled clusters of one level (all of them when k = n): the
+// nets of each sampled cluster by nets_touching_gates (:90-99, a scan of every
+// net), the k x k scores among them (HashSet intersection iterates the smaller
+// set), and one top-k sort of an n-entry row per sample (:74-84, stable,
+// descending). out_scores[k * k] (may be NULL) gets scores[rows[a]][rows[b]];
+// t_out[3] the seconds of the three phases, for scaling to the whole level.
+void or_attention_sample(int32_t m, const int32_t *net_ptr, const int32_t *net_gate,
+                         int32_t n, const int32_t *cluster_ptr, const int32_t *cluster_gate,
+                         int32_t k, const int32_t *rows, int32_t top_k, float *out_scores,
+                         int32_t *out_topk, double *t_out) {
+  using clk = std::chrono::steady_clock;
+  auto secs = [](clk::time_point a, clk::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+  };
+  const auto t0 = clk::now();
+  std::vector<std::unordered_set<int64_t>> nets(k);
+  for (int32_t a = 0; a < k; ++a) {
+    const int32_t c = rows[a];
+    std::unordered_set<int64_t> gates(cluster_gate + cluster_ptr[c],
+                                      cluster_gate + cluster_ptr[c + 1]);
+    for (int32_t e = 0; e < m; ++e)
+      for (int32_t q = net_ptr[e]; q < net_ptr[e + 1]; ++q)
+        if (gates.count(net_gate[q])) {
+          nets[a].insert(e);
+          break;
+        }
+  }
+  const auto t1 = clk::now();
+  std::vector<float> sc((size_t)k * k, 0.0f);
+  for (int32_t a = 0; a < k; ++a) {
+    const size_t total = nets[a].size();
+    if (total == 0) continue;
+    for (int32_t b = 0; b < k; ++b) {
+      if (a == b) continue;
+      const auto &x = nets[a].size() <= nets[b].size() ? nets[a] : nets[b];
+      const auto &y = nets[a].size() <= nets[b].size() ? nets[b] : nets[a];
+      size_t shared = 0;
+      for (int64_t e : x) shared += y.count(e);
+      sc[(size_t)a * k + b] = (float)shared / (float)total;
+    }
+  }
+  const auto t2 = clk::now();
+  // row a of the level: the sampled columns carry their scores, the rest 0
+  std::vector<std::pair<int32_t, float>> row;
+  for (int32_t a = 0; a < k; ++a) {
+    std::vector<float> full((size_t)n, 0.0f);
+    for (int32_t b = 0; b < k; ++b) full[rows[b]] = sc[(size_t)a * k + b];
+    row.clear();
+    for (int32_t j = 0; j < n; ++j)
+      if (j != rows[a]) row.emplace_back(j, full[j]);
+    std::stable_sort(row.begin(), row.end(),
+                     [](const std::pair<int32_t, float> &u,
+                        const std::pair<int32_t, float> &v) { return u.second > v.second; });
+    int32_t w = 0;
+    for (int32_t r = 0; r < top_k && r < (int32_t)row.size(); ++r)
+      if (row[r].second > 0.0f && out_topk) out_topk[(size_t)a * top_k + w++] = row[r].first;
+    if (out_topk)
+      for (; w < top_k; ++w) out_topk[(size_t)a * top_k + w] = -1;
+  }
+  const auto t3 = clk::now();
+  if (out_scores) std::copy(sc.begin(), sc.end(), out_scores);
+  t_out[0] = secs(t0, t1);
+  t_out[1] = secs(t1, t2);
+  t_out[2] = secs(t2, t3);
 }
 
 }  // extern "C"

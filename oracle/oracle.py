@@ -97,6 +97,8 @@ def lib() -> C.CDLL:
                                    C.c_int32, F32P, F32P]
         L.or_repulsion_exact.argtypes = [C.c_int32, F32P, F32P, C.c_double, C.c_double,
                                          F64P, F64P]
+        L.or_attention_sample.argtypes = [C.c_int32, I32P, I32P, C.c_int32, I32P, I32P,
+                                          C.c_int32, I32P, C.c_int32, F32P, I32P, F64P]
         _lib = L
     return _lib
 
@@ -414,3 +416,139 @@ def density_forces(x, y, area, die_w, die_h, G, target=0.7, weight=1.0):
     fy = q * ey[row, col] * weight
     energy = float(np.sum(0.5 * q * phi[row, col]) * weight)
     return dict(fx=fx, fy=fy, rho=charge, phi=phi, ex=ex, ey=ey, energy=energy)
+
+
+# ---- attention scores (attention.rs, hierarchy.rs) -------------------------
+def hierarchy_nodes(leaf_ptr, leaf_gate, leaf_depth):
+    """The explicit binary tree of a hierarchy from its leaves in DFS order and
+    their depths (every internal node of recursive_bisect has two children,
+    partitioner.rs:85-99): a list of (depth, gates) for every node, in DFS
+    preorder. Internal nodes hold the union of their leaves' gates."""
+    leaf_ptr, leaf_gate, leaf_depth = list(leaf_ptr), list(leaf_gate), list(leaf_depth)
+    nodes = []
+    pos = [0]
+
+    def parse(depth):
+        i = pos[0]
+        if i >= len(leaf_depth):
+            raise ValueError("leaf depths do not form a full binary tree")
+        slot = len(nodes)
+        nodes.append(None)
+        if leaf_depth[i] == depth:
+            pos[0] += 1
+            gates = leaf_gate[leaf_ptr[i]:leaf_ptr[i + 1]]
+        elif leaf_depth[i] > depth:
+            gates = parse(depth + 1) + parse(depth + 1)
+        else:
+            raise ValueError("leaf depths do not form a full binary tree")
+        nodes[slot] = (depth, gates)
+        return gates
+
+    if leaf_depth:
+        parse(0)
+        if pos[0] != len(leaf_depth):
+            raise ValueError("leaf depths do not form a full binary tree")
+    return nodes
+
+
+def clusters_at_depth(nodes, depth):
+    """HierarchyTree::clusters_at_depth (hierarchy.rs:134-159): the nodes at
+    `depth` in DFS order (preorder lists them in that order)."""
+    return [g for d, g in nodes if d == depth]
+
+
+def attention_level(net_ptr, net_gate, clusters, top_k=10):
+    """compute_level_attention (attention.rs:50-88) literally, with
+    nets_touching_gates (:90-99) as Python sets: scores[n][n] f32 and the
+    top_k lists. For small cases."""
+    net_ptr, net_gate = list(net_ptr), list(net_gate)
+    m = len(net_ptr) - 1
+    n = len(clusters)
+    nets = []
+    for gates in clusters:
+        gs = set(int(g) for g in gates)
+        nets.append({e for e in range(m)
+                     if any(g in gs for g in net_gate[net_ptr[e]:net_ptr[e + 1]])})
+    scores = np.zeros((n, n), np.float32)
+    for i in range(n):
+        total = len(nets[i])
+        if total == 0:
+            continue
+        for j in range(n):
+            if i != j:
+                scores[i, j] = np.float32(len(nets[i] & nets[j])) / np.float32(total)
+    tops = []
+    for i in range(n):
+        idx = sorted((j for j in range(n) if j != i), key=lambda j: -scores[i, j])
+        tops.append([j for j in idx[:top_k] if scores[i, j] > 0])
+    return scores, tops
+
+
+def attention_all(net_ptr, net_gate, leaf_ptr, leaf_gate, leaf_depth, top_k=10):
+    """compute_all_attention (attention.rs:33-48): one (depth, scores, top_k)
+    per depth with at least two clusters."""
+    nodes = hierarchy_nodes(leaf_ptr, leaf_gate, leaf_depth)
+    out = []
+    for depth in range(max((d for d, _ in nodes), default=-1) + 1):
+        cl = clusters_at_depth(nodes, depth)
+        if len(cl) >= 2:
+            s, t = attention_level(net_ptr, net_gate, cl, top_k)
+            out.append((depth, s, t))
+    return out
+
+
+def attention_level_sparse(net_ptr, net_gate, n_gates, cluster_ptr, cluster_gate, top_k=10):
+    """The same level as attention_level, vectorised for large cases with a
+    sparse cluster-by-net incidence matrix B (scipy.sparse): shared = B B^T,
+    totals = row sums of B. Returns the nonzero off-diagonal scores as
+    (rows, cols, f32 scores) sorted by (row, col) and the top_k lists padded
+    with -1 to [n, top_k]."""
+    import scipy.sparse as sp
+
+    net_ptr, net_gate = np.asarray(net_ptr, np.int64), np.asarray(net_gate, np.int64)
+    cluster_ptr = np.asarray(cluster_ptr, np.int64)
+    n = len(cluster_ptr) - 1
+    m = len(net_ptr) - 1
+    cl = np.full(n_gates, -1, np.int64)
+    cl[np.asarray(cluster_gate, np.int64)] = np.repeat(np.arange(n), np.diff(cluster_ptr))
+    pin_net = np.repeat(np.arange(m), np.diff(net_ptr))
+    pin_cl = cl[net_gate]
+    keep = pin_cl >= 0
+    B = sp.csr_matrix((np.ones(int(keep.sum()), np.int64), (pin_cl[keep], pin_net[keep])),
+                      shape=(n, m))
+    B.sum_duplicates()
+    B.data[:] = 1  # a net touching a cluster through several pins counts once
+    total = np.asarray(B.sum(axis=1)).ravel()
+    S = (B @ B.T).tocoo()
+    off = S.row != S.col
+    r, c, v = S.row[off].astype(np.int64), S.col[off].astype(np.int64), S.data[off]
+    o = np.lexsort((c, r))
+    r, c, v = r[o], c[o], v[o]
+    sc = v.astype(np.float32) / total[r].astype(np.float32)
+    tk = np.full((n, max(top_k, 0)), -1, np.int32)
+    if top_k > 0 and len(r):
+        o = np.lexsort((c, -sc.astype(np.float64), r))
+        rr, cc = r[o], c[o]
+        start = np.searchsorted(rr, np.arange(n))
+        rank = np.arange(len(rr)) - start[rr]
+        sel = rank < top_k
+        tk[rr[sel], rank[sel]] = cc[sel]
+    return r, c, sc, tk
+
+
+def attention_sample(net_ptr, net_gate, cluster_ptr, cluster_gate, rows, top_k=10):
+    """The C++ restatement of compute_level_attention on the sampled clusters
+    `rows` of one level (all of them for the whole level): (scores among the
+    samples [k, k], top_k lists [k, top_k] -1 padded, seconds of the net-set,
+    intersection and top-k phases)."""
+    net_ptr, net_gate = _i32(net_ptr), _i32(net_gate)
+    cp, cg, rows = _i32(cluster_ptr), _i32(cluster_gate), _i32(rows)
+    k = len(rows)
+    sc = np.zeros((k, k), np.float32)
+    tk = np.full((k, max(top_k, 1)), -1, np.int32)
+    t = np.zeros(3, np.float64)
+    lib().or_attention_sample(len(net_ptr) - 1, _p(net_ptr, C.c_int32), _p(net_gate, C.c_int32),
+                              len(cp) - 1, _p(cp, C.c_int32), _p(cg, C.c_int32), k,
+                              _p(rows, C.c_int32), top_k, _p(sc, C.c_float),
+                              _p(tk, C.c_int32), _p(t, C.c_double))
+    return sc, tk[:, :top_k], t
