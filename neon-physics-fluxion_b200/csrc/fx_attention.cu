@@ -6,15 +6,15 @@
 // as the stable sort_by of :81-82; zero scores dropped).
 //
 // The reference forms the dense n x n matrix from per-cluster net sets
-// (nets_touching_gates, :90-99). Here the pins, tagged with their gate's
-// cluster, are radix sorted by (net, cluster); the distinct records are the
-// (net, cluster) incidences. Every net emits each ordered pair of its distinct
-// clusters once, and a radix sort + run-length count of the pair keys gives
-// the shared-net counts of the pairs that have any: the work follows the pins
-// and the pairs, not n^2, and a high-fanout net costs no more than its
-// pairs. Scans are three-phase tile scans of 1024 elements. All counts are integers, so the f32
-// scores are those of the reference formula (shared as f32 / total as f32,
-// rounded to nearest).
+// (nets_touching_gates, :90-99). Here every net finds its distinct clusters
+// (a warp per net with __match_any_sync up to 32 pins; a block per larger net
+// over a shared-memory bitmap of the level's clusters), emits each ordered
+// pair of them once, and a radix sort + run-length count of the pair keys
+// gives the shared-net counts of the pairs that have any: the work follows
+// the pins and the pairs, not n^2, and a high-fanout net costs no more than
+// its pairs. Scans are three-phase tile scans of 1024 elements. All counts
+// are integers, so the f32 scores are those of the reference formula (shared
+// as f32 / total as f32, rounded to nearest).
 #include <algorithm>
 #include <vector>
 
@@ -41,77 +41,6 @@ __global__ void attn_map_kernel(int n, int G, int n_gates, const int32_t *__rest
     return;
   }
   if (atomicCAS(cl + g, -1, lo) != -1) atomicOr(bad, 2);
-}
-
-// One record per pin: its gate's cluster (kNoCluster when the gate is in no
-// cluster of the level) and its net.
-constexpr uint32_t kNoCluster = 0xFFFFu;  // cluster ids are < 65535
-
-__global__ void attn_pin_kernel(int m, const int32_t *__restrict__ net_ptr,
-                                const int32_t *__restrict__ net_gate,
-                                const int32_t *__restrict__ cl, uint32_t *__restrict__ pc,
-                                int32_t *__restrict__ pn) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m) return;
-  for (int q = net_ptr[e]; q < net_ptr[e + 1]; ++q) {
-    const int a = cl[net_gate[q]];
-    pc[q] = a >= 0 ? (uint32_t)a : kNoCluster;
-    pn[q] = e;
-  }
-}
-
-// Records sorted by (net, cluster): head[i] = 1 where a distinct (net,
-// cluster) pair with a real cluster starts; head[p] = 0.
-__global__ void attn_rec_head_kernel(const int32_t *__restrict__ rn,
-                                     const int32_t *__restrict__ rc, int p,
-                                     uint32_t *__restrict__ head) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > p) return;
-  head[i] = (i < p && (uint32_t)rc[i] != kNoCluster &&
-             (i == 0 || rn[i] != rn[i - 1] || rc[i] != rc[i - 1])) ? 1u : 0u;
-}
-
-// Distinct records in order (dn = net, dc = cluster); each is one net
-// touching one cluster, so touch[a] = |nets touching a|.
-__global__ void attn_rec_compact_kernel(const int32_t *__restrict__ rn,
-                                        const int32_t *__restrict__ rc, int p,
-                                        const uint32_t *__restrict__ idx,
-                                        int32_t *__restrict__ dn, int32_t *__restrict__ dc,
-                                        int32_t *__restrict__ touch) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p || idx[i + 1] == idx[i]) return;
-  dn[idx[i]] = rn[i];
-  dc[idx[i]] = rc[i];
-  atomicAdd(touch + rc[i], 1);
-}
-
-// Sorting by net keeps every net's pins at [net_ptr[e], net_ptr[e+1]), so
-// its distinct clusters are [idx[net_ptr[e]], idx[net_ptr[e+1]]): c of them,
-// c (c - 1) ordered pairs.
-__global__ void attn_net_pairs_kernel(int m, const int32_t *__restrict__ net_ptr,
-                                      const uint32_t *__restrict__ idx,
-                                      unsigned long long *__restrict__ npairs) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m) return;
-  const unsigned long long c = idx[net_ptr[e + 1]] - idx[net_ptr[e]];
-  npairs[e] = c * (c > 0 ? c - 1 : 0);
-}
-
-// Distinct record j of net e emits (a_j, a_k) for every other distinct
-// cluster k of e, as keys a_j * n + a_k, at off[e] + (j - s) (c - 1).
-__global__ void attn_emit_kernel(int D, int n, const int32_t *__restrict__ net_ptr,
-                                 const uint32_t *__restrict__ idx,
-                                 const int32_t *__restrict__ dn, const int32_t *__restrict__ dc,
-                                 const unsigned long long *__restrict__ off,
-                                 uint32_t *__restrict__ keys) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= D) return;
-  const int e = dn[j];
-  const int s = (int)idx[net_ptr[e]], t = (int)idx[net_ptr[e + 1]];
-  unsigned long long o = off[e] + (unsigned long long)(j - s) * (unsigned long long)(t - s - 1);
-  const uint32_t row = (uint32_t)dc[j] * (uint32_t)n;
-  for (int k = s; k < t; ++k)
-    if (k != j) keys[o++] = row + (uint32_t)dc[k];
 }
 
 // ---- exclusive scan in place: tile sums, scan of the sums, tile scans ------
@@ -194,6 +123,195 @@ int exclusive_scan(T *a, long long n, T *tsum, cudaStream_t s) {
   return FX_OK;
 }
 
+// ---- distinct clusters of every net ---------------------------------------
+// For net e with pins [b, t): its c distinct clusters go to dc[b .. b+c) in
+// first-pin order, dn[b + k] = e for k < c and -1 beyond, cnt[e] = c,
+// npairs[e] = c (c - 1), and touch[a] += 1 for each (|nets touching a|).
+constexpr int kSmallNet = 32;
+constexpr int kMaxClusters = 65535;
+constexpr int kBitmapWords = (kMaxClusters + 31) / 32;
+constexpr int kBigThreads = 256;
+
+// The distinct clusters of net e by one warp (at most 32 pins).
+__device__ __forceinline__ void dedupe_warp_net(int e, int lane,
+                                                const int32_t *__restrict__ net_ptr,
+                                                const int32_t *__restrict__ net_gate,
+                                                const int32_t *__restrict__ cl,
+                                                int32_t *__restrict__ dc,
+                                                int32_t *__restrict__ dn,
+                                                int32_t *__restrict__ cnt,
+                                                unsigned long long *__restrict__ npairs,
+                                                int32_t *__restrict__ touch) {
+  const int b = net_ptr[e], deg = net_ptr[e + 1] - b;
+  // lanes past the net's pins get distinct negative tags, pins of no cluster -1
+  const int c = lane < deg ? cl[net_gate[b + lane]] : -2 - lane;
+  const unsigned same = __match_any_sync(0xffffffffu, c);
+  const bool first = c >= 0 && (__ffs(same) - 1) == lane;
+  const unsigned firsts = __ballot_sync(0xffffffffu, first);
+  const int k = __popc(firsts);
+  if (first) {
+    const int pos = __popc(firsts & ((1u << lane) - 1u));
+    dc[b + pos] = c;
+    atomicAdd(touch + c, 1);
+  }
+  if (lane < deg) dn[b + lane] = lane < k ? e : -1;
+  if (lane == 0) {
+    cnt[e] = k;
+    npairs[e] = (unsigned long long)k * (unsigned long long)(k > 0 ? k - 1 : 0);
+  }
+}
+
+constexpr int kThreadNet = 16;
+
+// Appends e to list[] for every lane with `take`, one atomic per warp.
+__device__ __forceinline__ void warp_push(bool take, int e, int32_t *__restrict__ list,
+                                          int32_t *__restrict__ count) {
+  const unsigned mask = __ballot_sync(0xffffffffu, take);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (take) list[base + __popc(mask & ((1u << lane) - 1u))] = e;
+}
+
+// One thread per net of at most 16 pins, deduplicated in registers; nets of
+// 17..32 pins are listed in mid[], larger ones in big[]. The touches of a
+// warp's nets are added once per distinct cluster and pin slot
+// (__match_any_sync), which keeps the few counters of shallow levels from
+// serialising the kernel.
+__global__ void __launch_bounds__(256)
+attn_dedupe_thread_kernel(int m, const int32_t *__restrict__ net_ptr,
+                          const int32_t *__restrict__ net_gate, const int32_t *__restrict__ cl,
+                          int32_t *__restrict__ dc, int32_t *__restrict__ dn,
+                          int32_t *__restrict__ cnt, unsigned long long *__restrict__ npairs,
+                          int32_t *__restrict__ touch, int32_t *__restrict__ mid,
+                          int32_t *__restrict__ n_mid, int32_t *__restrict__ big,
+                          int32_t *__restrict__ n_big) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool active = e < m;  // no early return: the warp votes below
+  int b = 0, deg = 0;
+  if (active) {
+    b = net_ptr[e];
+    deg = net_ptr[e + 1] - b;
+  }
+  const bool small = active && deg <= kThreadNet;
+  warp_push(active && deg > kThreadNet && deg <= kSmallNet, e, mid, n_mid);
+  warp_push(active && deg > kSmallNet, e, big, n_big);
+  int cc[kThreadNet];
+#pragma unroll
+  for (int i = 0; i < kThreadNet; ++i) cc[i] = (small && i < deg) ? cl[net_gate[b + i]] : -1;
+  unsigned firsts = 0;
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < kThreadNet; ++i) {
+    bool f = cc[i] >= 0;
+#pragma unroll
+    for (int j = 0; j < i; ++j) f = f && cc[j] != cc[i];
+    if (f) {
+      dc[b + k] = cc[i];
+      ++k;
+      firsts |= 1u << i;
+    }
+  }
+  if (small) {
+    for (int q = 0; q < deg; ++q) dn[b + q] = q < k ? e : -1;
+    cnt[e] = k;
+    npairs[e] = (unsigned long long)k * (unsigned long long)(k > 0 ? k - 1 : 0);
+  }
+  const int maxdeg = __reduce_max_sync(0xffffffffu, small ? deg : 0);
+#pragma unroll
+  for (int i = 0; i < kThreadNet; ++i) {
+    if (i >= maxdeg) break;  // uniform across the warp
+    const int c = (firsts >> i) & 1u ? cc[i] : -1;
+    const unsigned same = __match_any_sync(0xffffffffu, c);
+    if (c >= 0 && (__ffs(same) - 1) == lane) atomicAdd(touch + c, __popc(same));
+  }
+}
+
+// One warp per listed net of 17..32 pins (grid-stride over *n_mid).
+__global__ void attn_dedupe_warp_kernel(const int32_t *__restrict__ mid,
+                                        const int32_t *__restrict__ n_mid,
+                                        const int32_t *__restrict__ net_ptr,
+                                        const int32_t *__restrict__ net_gate,
+                                        const int32_t *__restrict__ cl,
+                                        int32_t *__restrict__ dc, int32_t *__restrict__ dn,
+                                        int32_t *__restrict__ cnt,
+                                        unsigned long long *__restrict__ npairs,
+                                        int32_t *__restrict__ touch) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int nm = *n_mid;
+  for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < nm; i += warps)
+    dedupe_warp_net(mid[i], lane, net_ptr, net_gate, cl, dc, dn, cnt, npairs, touch);
+}
+// One block per listed net (grid-stride over *n_big); the bitmap holds the
+// clusters seen so far in the net and is cleared pin by pin afterwards.
+__global__ void __launch_bounds__(kBigThreads)
+attn_dedupe_big_kernel(const int32_t *__restrict__ big, const int32_t *__restrict__ n_big,
+                       const int32_t *__restrict__ net_ptr,
+                       const int32_t *__restrict__ net_gate, const int32_t *__restrict__ cl,
+                       int n, int32_t *__restrict__ dc, int32_t *__restrict__ dn,
+                       int32_t *__restrict__ cnt, unsigned long long *__restrict__ npairs,
+                       int32_t *__restrict__ touch) {
+  __shared__ uint32_t seen[kBitmapWords];
+  const int words = (n + 31) >> 5;
+  for (int w = threadIdx.x; w < words; w += blockDim.x) seen[w] = 0u;
+  __syncthreads();
+  const int nb = *n_big;
+  for (int i = blockIdx.x; i < nb; i += gridDim.x) {
+    const int e = big[i];
+    const int b = net_ptr[e], t = net_ptr[e + 1];
+    int base = 0;
+    for (int q0 = b; q0 < t; q0 += blockDim.x) {  // uniform trip count
+      const int q = q0 + threadIdx.x;
+      const int c = q < t ? cl[net_gate[q]] : -1;
+      int first = 0;
+      if (c >= 0) {
+        const uint32_t bit = 1u << (c & 31);
+        first = (atomicOr(seen + (c >> 5), bit) & bit) == 0u;
+      }
+      int total;
+      const int pos = base + block_exclusive(first, &total);
+      if (first) {
+        dc[b + pos] = c;
+        atomicAdd(touch + c, 1);
+      }
+      base += total;
+    }
+    for (int q = b + threadIdx.x; q < t; q += blockDim.x) dn[q] = q - b < base ? e : -1;
+    if (threadIdx.x == 0) {
+      cnt[e] = base;
+      npairs[e] = (unsigned long long)base * (unsigned long long)(base > 0 ? base - 1 : 0);
+    }
+    __syncthreads();  // every bit of this net is set before any is cleared
+    for (int q = b + threadIdx.x; q < t; q += blockDim.x) {
+      const int c = cl[net_gate[q]];
+      if (c >= 0) seen[c >> 5] = 0u;
+    }
+    __syncthreads();
+  }
+}
+
+// Record slot q of net e (dn[q] = e) emits (a, a_k) for every other distinct
+// cluster k of e, as keys a * n + a_k, at off[e] + j (c - 1), j = q - b.
+__global__ void attn_emit_kernel(int pins, int n, const int32_t *__restrict__ net_ptr,
+                                 const int32_t *__restrict__ dn, const int32_t *__restrict__ dc,
+                                 const int32_t *__restrict__ cnt,
+                                 const unsigned long long *__restrict__ off,
+                                 uint32_t *__restrict__ keys) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= pins) return;
+  const int e = dn[q];
+  if (e < 0) return;
+  const int b = net_ptr[e], c = cnt[e], j = q - b;
+  unsigned long long o = off[e] + (unsigned long long)j * (unsigned long long)(c - 1);
+  const uint32_t row = (uint32_t)dc[q] * (uint32_t)n;
+  for (int k = 0; k < c; ++k)
+    if (k != j) keys[o++] = row + (uint32_t)dc[b + k];
+}
+
 // ---- run-length count of the sorted pair keys ------------------------------
 // head[i] = 1 where a run of equal keys starts; head[p] = 0 (after the scan
 // it holds the number of runs).
@@ -233,42 +351,50 @@ __global__ void attn_score_kernel(int p, int n, const uint32_t *__restrict__ nu,
   if (dense) dense[(size_t)a * n + b] = s;
 }
 
-// Per cluster: its pairs are a contiguous run of the sorted keys (ascending
-// b); keep the top_k by score, ties by smaller b (stable descending sort).
-__global__ void attn_topk_kernel(int n, const uint32_t *__restrict__ nu, int top_k,
-                                 const uint32_t *__restrict__ ukey,
-                                 const float *__restrict__ score, int32_t *__restrict__ best_b,
-                                 float *__restrict__ best_s, int32_t *__restrict__ out) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
-  const int u = nu ? (int)*nu : 0;
-  // first key >= a * n
-  const uint32_t lo_key = (uint32_t)a * (uint32_t)n;
+// One warp per cluster a: its pairs are the run of sorted keys in
+// [a n, (a + 1) n), by ascending b. Round r picks the best entry below the
+// previous pick in the order (score descending, b ascending) -- the stable
+// descending sort of the reference -- as the warp maximum of the 64-bit key
+// (score bits, ~b); positive f32 scores order like their bit patterns.
+__device__ __forceinline__ int lower_bound_u32(const uint32_t *__restrict__ a, int u,
+                                               uint32_t v) {
   int lo = 0, hi = u;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
-    if (ukey[mid] < lo_key) lo = mid + 1; else hi = mid;
+    if (a[mid] < v) lo = mid + 1; else hi = mid;
   }
-  int32_t *bb = best_b + (size_t)a * top_k;
-  float *bs = best_s + (size_t)a * top_k;
-  int have = 0;
-  for (int i = lo; i < u && ukey[i] / (uint32_t)n == (uint32_t)a; ++i) {
-    const float s = score[i];
-    const int32_t b = (int32_t)(ukey[i] % (uint32_t)n);
-    // entries come by ascending b, so an equal score never displaces one
-    int pos = have;
-    while (pos > 0 && bs[pos - 1] < s) --pos;
-    if (pos >= top_k) continue;
-    const int last = have < top_k ? have : top_k - 1;
-    for (int r = last; r > pos; --r) {
-      bs[r] = bs[r - 1];
-      bb[r] = bb[r - 1];
+  return lo;
+}
+
+__global__ void attn_topk_kernel(int n, const uint32_t *__restrict__ nu, int top_k,
+                                 const uint32_t *__restrict__ ukey,
+                                 const float *__restrict__ score, int32_t *__restrict__ out) {
+  const int a = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (a >= n) return;  // uniform per warp
+  const int u = nu ? (int)*nu : 0;
+  const uint32_t row = (uint32_t)a * (uint32_t)n;
+  const int lo = lower_bound_u32(ukey, u, row);
+  const int hi = lower_bound_u32(ukey, u, row + (uint32_t)n);  // (n - 1) n + n < 2^32
+  int32_t *o = out + (size_t)a * top_k;
+  unsigned long long last = ~0ull;
+  int r = 0;
+  for (; r < top_k; ++r) {
+    unsigned long long best = 0;
+    for (int i = lo + lane; i < hi; i += 32) {
+      const unsigned long long key =
+          ((unsigned long long)__float_as_uint(score[i]) << 32) | (0xFFFFFFFFu - (ukey[i] - row));
+      if (key < last && key > best) best = key;
     }
-    bs[pos] = s;
-    bb[pos] = b;
-    if (have < top_k) ++have;
+    for (int off = 16; off > 0; off >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
+      best = other > best ? other : best;
+    }
+    if (best == 0) break;  // the row has no entry left
+    if (lane == 0) o[r] = (int32_t)(0xFFFFFFFFu - (uint32_t)best);
+    last = best;
   }
-  for (int r = 0; r < top_k; ++r) out[(size_t)a * top_k + r] = r < have ? bb[r] : -1;
+  for (int rr = r + lane; rr < top_k; rr += 32) o[rr] = -1;
 }
 
 }  // namespace
@@ -314,43 +440,32 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   }
   const int pins = m > 0 ? (int)d->p : 0;
   const size_t nk = top_k > 0 ? (size_t)n * top_k : 1;
-  const int mb = (m + 255) / 256;
   int launches = 0;
-  DevBuf<int32_t> d_cl, touch, bb, out, dn, dc;
+  const size_t pp = (size_t)pins + 1, mm = (size_t)m + 1;
+  DevBuf<int32_t> d_cl, d_cptr, d_cgate, d_bad, touch, dc, dn, cnt, mid, big, out;
   DevBuf<unsigned long long> npairs, psum;
-  DevBuf<uint32_t> rc[2], idx, isum;
-  DevBuf<int32_t> rn[2];
-  DevBuf<float> bs, score, dense;
-  const size_t pp = (size_t)pins + 1;
-  DevBuf<int32_t> d_cptr, d_cgate, d_bad;
+  DevBuf<float> score, dense;
   FX_TRY(d_cl.alloc(d->n));
   FX_TRY(d_cptr.alloc((size_t)n + 1));
   FX_TRY(d_cgate.alloc(G > 0 ? (size_t)G : 1));
-  FX_TRY(d_bad.alloc(1));
+  FX_TRY(d_bad.alloc(3));  // [0] error flags, [1] nets of > 32 pins, [2] of 17..32
   FX_TRY(touch.alloc(n));
-  FX_TRY(npairs.alloc((size_t)m + 1));
-  FX_TRY(psum.alloc(scan_tiles((long long)m + 1)));
-  FX_TRY(rc[0].alloc(pp));
-  FX_TRY(rc[1].alloc(pp));
-  FX_TRY(rn[0].alloc(pp));
-  FX_TRY(rn[1].alloc(pp));
-  FX_TRY(idx.alloc(pp));
-  FX_TRY(isum.alloc(scan_tiles((long long)pp)));
-  FX_TRY(dn.alloc(pp));
   FX_TRY(dc.alloc(pp));
-  DevBuf<uint32_t> th, ts, dt;
-  FX_TRY(th.alloc((size_t)256 * radix_sort_tiles(pins > 0 ? pins : 1)));
-  FX_TRY(ts.alloc((size_t)256 * radix_sort_tiles(pins > 0 ? pins : 1)));
-  FX_TRY(dt.alloc(256));
+  FX_TRY(dn.alloc(pp));
+  FX_TRY(cnt.alloc(mm));
+  FX_TRY(mid.alloc(mm));
+  FX_TRY(big.alloc(mm));
+  FX_TRY(npairs.alloc(mm));
+  FX_TRY(psum.alloc(scan_tiles((long long)mm)));
   FX_CHECK_CUDA(cudaMemcpyAsync(d_cptr.p, cluster_ptr, ((size_t)n + 1) * 4,
                                 cudaMemcpyHostToDevice, s));
   if (G > 0)
     FX_CHECK_CUDA(cudaMemcpyAsync(d_cgate.p, cluster_gate, (size_t)G * 4,
                                   cudaMemcpyHostToDevice, s));
   FX_CHECK_CUDA(cudaMemsetAsync(d_cl.p, 0xFF, (size_t)d->n * 4, s));
-  FX_CHECK_CUDA(cudaMemsetAsync(d_bad.p, 0, 4, s));
+  FX_CHECK_CUDA(cudaMemsetAsync(d_bad.p, 0, 12, s));
   FX_CHECK_CUDA(cudaMemsetAsync(touch.p, 0, (size_t)n * 4, s));
-  FX_CHECK_CUDA(cudaMemsetAsync(npairs.p, 0, ((size_t)m + 1) * 8, s));
+  FX_CHECK_CUDA(cudaMemsetAsync(npairs.p + m, 0, 8, s));  // the total's slot
   cudaEvent_t t0;  // device time of the level, both halves around the host read
   timer_begin(ctx, FX_STAGE_ATTENTION, s, &t0);
   if (G > 0) {
@@ -359,43 +474,26 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     FX_CHECK_LAUNCH();
     ++launches;
   }
-  if (pins > 0) {
-    attn_pin_kernel<<<mb, 256, 0, s>>>(m, d->net_ptr.p, d->net_gate.p, d_cl.p, rc[0].p,
-                                       rn[0].p);
+  if (m > 0) {
+    attn_dedupe_thread_kernel<<<(m + 255) / 256, 256, 0, s>>>(
+        m, d->net_ptr.p, d->net_gate.p, d_cl.p, dc.p, dn.p, cnt.p, npairs.p, touch.p, mid.p,
+        d_bad.p + 2, big.p, d_bad.p + 1);
+    attn_dedupe_warp_kernel<<<4 * ctx->num_sms, 256, 0, s>>>(
+        mid.p, d_bad.p + 2, d->net_ptr.p, d->net_gate.p, d_cl.p, dc.p, dn.p, cnt.p, npairs.p,
+        touch.p);
+    attn_dedupe_big_kernel<<<4 * ctx->num_sms, kBigThreads, 0, s>>>(
+        big.p, d_bad.p + 1, d->net_ptr.p, d->net_gate.p, d_cl.p, n, dc.p, dn.p, cnt.p,
+        npairs.p, touch.p);
     FX_CHECK_LAUNCH();
-    // (net, cluster) order: stable by cluster (16 bits), then stable by net
-    uint32_t *k1[2] = {rc[0].p, rc[1].p};
-    int32_t *v1[2] = {rn[0].p, rn[1].p};
-    FX_TRY(radix_sort_pairs(k1, v1, pins, 2, th.p, ts.p, dt.p, s));  // result in buffer 0
-    int net_passes = 0;
-    while (net_passes < 4 && ((uint32_t)(m - 1) >> (8 * net_passes)) != 0) ++net_passes;
-    uint32_t *k2[2] = {reinterpret_cast<uint32_t *>(rn[0].p),
-                       reinterpret_cast<uint32_t *>(rn[1].p)};
-    int32_t *v2[2] = {reinterpret_cast<int32_t *>(rc[0].p),
-                      reinterpret_cast<int32_t *>(rc[1].p)};
-    FX_TRY(radix_sort_pairs(k2, v2, pins, net_passes, th.p, ts.p, dt.p, s));
-    const int rb = net_passes & 1;  // buffer holding the sorted records
-    const int32_t *rnet = rn[rb].p;
-    const int32_t *rcl = reinterpret_cast<const int32_t *>(rc[rb].p);
-    attn_rec_head_kernel<<<(pins + 256) / 256, 256, 0, s>>>(rnet, rcl, pins, idx.p);
-    FX_CHECK_LAUNCH();
-    FX_TRY(exclusive_scan(idx.p, (long long)pp, isum.p, s));
-    attn_rec_compact_kernel<<<(pins + 255) / 256, 256, 0, s>>>(rnet, rcl, pins, idx.p, dn.p,
-                                                               dc.p, touch.p);
-    attn_net_pairs_kernel<<<mb, 256, 0, s>>>(m, d->net_ptr.p, idx.p, npairs.p);
-    FX_CHECK_LAUNCH();
-    launches += 1 + 3 * 2 + 3 * net_passes + 1 + 3 + 2;
+    launches += 3;
   }
   // exclusive offsets of the pairs; the extra (zero) slot becomes the total
-  FX_TRY(exclusive_scan(npairs.p, (long long)m + 1, psum.p, s));
-  if (m > 0) launches += 3;
+  FX_TRY(exclusive_scan(npairs.p, (long long)mm, psum.p, s));
+  launches += 3;
   timer_end(ctx, FX_STAGE_ATTENTION, s, t0);
   unsigned long long total = 0;
-  uint32_t distinct = 0;
-  FX_CHECK_CUDA(cudaMemcpyAsync(&total, npairs.p + m, 8, cudaMemcpyDeviceToHost, s));
   int32_t bad = 0;
-  if (pins > 0)
-    FX_CHECK_CUDA(cudaMemcpyAsync(&distinct, idx.p + pins, 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(&total, npairs.p + m, 8, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaMemcpyAsync(&bad, d_bad.p, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
   if (bad) {
@@ -407,7 +505,7 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     set_error("fx_attention: %llu cluster pairs exceed the buffer limit", total);
     return FX_EINVAL;
   }
-  const int P = (int)total, D = (int)distinct;
+  const int P = (int)total;
   const size_t pc = (size_t)P + 1;
   DevBuf<uint32_t> keys[2], head, hsum;
   DevBuf<int32_t> vals[2];
@@ -418,12 +516,11 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   FX_TRY(head.alloc(pc));
   FX_TRY(hsum.alloc(scan_tiles((long long)pc)));
   FX_TRY(score.alloc(pc));
-  FX_TRY(bb.alloc(nk));
-  FX_TRY(bs.alloc(nk));
   FX_TRY(out.alloc(nk));
-  DevBuf<uint32_t> kh, ks;
+  DevBuf<uint32_t> kh, ks, dt;
   FX_TRY(kh.alloc((size_t)256 * radix_sort_tiles(P > 0 ? P : 1)));
   FX_TRY(ks.alloc((size_t)256 * radix_sort_tiles(P > 0 ? P : 1)));
+  FX_TRY(dt.alloc(256));
   if (out_scores) {
     FX_TRY(dense.alloc((size_t)n * n));
     FX_CHECK_CUDA(cudaMemsetAsync(dense.p, 0, (size_t)n * n * 4, s));
@@ -431,8 +528,8 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   cudaEvent_t t1;
   timer_begin(ctx, FX_STAGE_ATTENTION, s, &t1);
   if (P > 0) {
-    attn_emit_kernel<<<(D + 255) / 256, 256, 0, s>>>(D, n, d->net_ptr.p, idx.p, dn.p, dc.p,
-                                                     npairs.p, keys[0].p);
+    attn_emit_kernel<<<(pins + 255) / 256, 256, 0, s>>>(pins, n, d->net_ptr.p, dn.p, dc.p,
+                                                        cnt.p, npairs.p, keys[0].p);
     FX_CHECK_LAUNCH();
     // keys < n^2: as many 8-bit passes as n^2 - 1 has bytes
     const uint32_t kmax = (uint32_t)n * (uint32_t)n - 1u;
@@ -454,14 +551,14 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     FX_CHECK_LAUNCH();
     launches += 1 + 3 * kp + 1 + 3 + 2;
     if (top_k > 0) {
-      attn_topk_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, head.p + P, top_k, ukey, score.p,
-                                                       bb.p, bs.p, out.p);
+      attn_topk_kernel<<<(n + 7) / 8, 256, 0, s>>>(n, head.p + P, top_k, ukey, score.p,
+                                                   out.p);
       FX_CHECK_LAUNCH();
       ++launches;
     }
   } else if (top_k > 0) {
-    attn_topk_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, nullptr, top_k, keys[0].p, score.p,
-                                                     bb.p, bs.p, out.p);
+    attn_topk_kernel<<<(n + 7) / 8, 256, 0, s>>>(n, nullptr, top_k, keys[0].p, score.p,
+                                                 out.p);
     FX_CHECK_LAUNCH();
     ++launches;
   }

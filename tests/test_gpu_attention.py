@@ -96,3 +96,48 @@ def test_edge_cases(fx, ctx, oracle):
             d.attention_level([0, 2, 1], [0, 1], 3)  # decreasing cluster_ptr
     finally:
         d.close()
+
+
+def test_high_fanout_nets(fx, ctx, oracle):
+    """Nets beyond one warp's 32 pins take the block path (a bitmap of the
+    level's clusters): degrees 33..600, repeated gates, pins outside every
+    cluster, and one net over almost all gates."""
+    rng = np.random.default_rng(17)
+    n_gates, n_clusters = 700, 61
+    degs = np.concatenate([rng.integers(2, 9, 150), [33, 40, 64, 65, 127, 300, 600, 690]])
+    rng.shuffle(degs)
+    net_ptr = np.concatenate([[0], np.cumsum(degs)]).astype(np.int32)
+    net_gate = rng.integers(0, n_gates, int(degs.sum())).astype(np.int32)
+    gates = rng.permutation(n_gates)[:650].astype(np.int32)
+    cuts = np.sort(rng.choice(np.arange(1, 650), n_clusters - 1, replace=False))
+    cp = np.concatenate([[0], cuts, [650]]).astype(np.int32)
+    d = _design(fx, ctx, n_gates, net_ptr, net_gate)
+    try:
+        top, sc = d.attention_level(cp, gates, 12, scores=True)
+        top2, sc2 = d.attention_level(cp, gates, 12, scores=True)
+    finally:
+        d.close()
+    clusters = [gates[cp[i]:cp[i + 1]].tolist() for i in range(n_clusters)]
+    s, want = oracle.attention_level(net_ptr, net_gate, clusters, 12)
+    assert np.array_equal(sc.view(np.uint32), s.view(np.uint32))
+    assert [[j for j in r if j >= 0] for r in top.tolist()] == want
+    assert np.array_equal(top, top2) and np.array_equal(sc, sc2)
+
+
+def test_many_clusters_with_big_nets(fx, ctx, oracle):
+    rng = np.random.default_rng(23)
+    n_gates, n_clusters = 120_000, 20_000
+    degs = np.where(rng.random(90_000) < 0.01, rng.integers(33, 200, 90_000),
+                    rng.integers(2, 8, 90_000))
+    net_ptr = np.concatenate([[0], np.cumsum(degs)]).astype(np.int32)
+    net_gate = rng.integers(0, n_gates, int(degs.sum())).astype(np.int32)
+    gates = rng.permutation(n_gates).astype(np.int32)
+    cuts = np.sort(rng.choice(np.arange(1, n_gates), n_clusters - 1, replace=False))
+    cp = np.concatenate([[0], cuts, [n_gates]]).astype(np.int32)
+    d = _design(fx, ctx, n_gates, net_ptr, net_gate)
+    try:
+        top, _ = d.attention_level(cp, gates, 10)
+    finally:
+        d.close()
+    _, _, _, want = oracle.attention_level_sparse(net_ptr, net_gate, n_gates, cp, gates, 10)
+    assert np.array_equal(top, want)
