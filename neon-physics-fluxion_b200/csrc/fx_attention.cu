@@ -176,57 +176,74 @@ __device__ __forceinline__ void warp_push(bool take, int e, int32_t *__restrict_
 }
 
 // One thread per net of at most 16 pins, deduplicated in registers; nets of
-// 17..32 pins are listed in mid[], larger ones in big[]. The touches of a
-// warp's nets are added once per distinct cluster and pin slot
-// (__match_any_sync), which keeps the few counters of shallow levels from
-// serialising the kernel.
+// 17..32 pins are listed in mid[], larger ones in big[]. Grid-stride over the
+// nets. The touches of a warp's nets are added once per distinct cluster and
+// pin slot (__match_any_sync), into a per-block shared histogram when the
+// level has at most kHist clusters (flushed at the end): the few counters of
+// shallow levels would otherwise serialise the kernel.
+constexpr int kHist = 4096;
+
 __global__ void __launch_bounds__(256)
-attn_dedupe_thread_kernel(int m, const int32_t *__restrict__ net_ptr,
+attn_dedupe_thread_kernel(int m, int n, const int32_t *__restrict__ net_ptr,
                           const int32_t *__restrict__ net_gate, const int32_t *__restrict__ cl,
                           int32_t *__restrict__ dc, int32_t *__restrict__ dn,
                           int32_t *__restrict__ cnt, unsigned long long *__restrict__ npairs,
                           int32_t *__restrict__ touch, int32_t *__restrict__ mid,
                           int32_t *__restrict__ n_mid, int32_t *__restrict__ big,
                           int32_t *__restrict__ n_big) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const bool active = e < m;  // no early return: the warp votes below
-  int b = 0, deg = 0;
-  if (active) {
-    b = net_ptr[e];
-    deg = net_ptr[e + 1] - b;
+  __shared__ int32_t hist[kHist];
+  const bool shared_hist = n <= kHist;
+  if (shared_hist) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
   }
-  const bool small = active && deg <= kThreadNet;
-  warp_push(active && deg > kThreadNet && deg <= kSmallNet, e, mid, n_mid);
-  warp_push(active && deg > kSmallNet, e, big, n_big);
-  int cc[kThreadNet];
+  int32_t *tgt = shared_hist ? hist : touch;
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < m; base += gridDim.x * blockDim.x) {
+    const int e = base + threadIdx.x;
+    const bool active = e < m;  // no early exit: the warp votes below
+    int b = 0, deg = 0;
+    if (active) {
+      b = net_ptr[e];
+      deg = net_ptr[e + 1] - b;
+    }
+    const bool small = active && deg <= kThreadNet;
+    warp_push(active && deg > kThreadNet && deg <= kSmallNet, e, mid, n_mid);
+    warp_push(active && deg > kSmallNet, e, big, n_big);
+    int cc[kThreadNet];
 #pragma unroll
-  for (int i = 0; i < kThreadNet; ++i) cc[i] = (small && i < deg) ? cl[net_gate[b + i]] : -1;
-  unsigned firsts = 0;
-  int k = 0;
+    for (int i = 0; i < kThreadNet; ++i) cc[i] = (small && i < deg) ? cl[net_gate[b + i]] : -1;
+    unsigned firsts = 0;
+    int k = 0;
 #pragma unroll
-  for (int i = 0; i < kThreadNet; ++i) {
-    bool f = cc[i] >= 0;
+    for (int i = 0; i < kThreadNet; ++i) {
+      bool f = cc[i] >= 0;
 #pragma unroll
-    for (int j = 0; j < i; ++j) f = f && cc[j] != cc[i];
-    if (f) {
-      dc[b + k] = cc[i];
-      ++k;
-      firsts |= 1u << i;
+      for (int j = 0; j < i; ++j) f = f && cc[j] != cc[i];
+      if (f) {
+        dc[b + k] = cc[i];
+        ++k;
+        firsts |= 1u << i;
+      }
+    }
+    if (small) {
+      for (int q = 0; q < deg; ++q) dn[b + q] = q < k ? e : -1;
+      cnt[e] = k;
+      npairs[e] = (unsigned long long)k * (unsigned long long)(k > 0 ? k - 1 : 0);
+    }
+    const int maxdeg = __reduce_max_sync(0xffffffffu, small ? deg : 0);
+#pragma unroll
+    for (int i = 0; i < kThreadNet; ++i) {
+      if (i >= maxdeg) break;  // uniform across the warp
+      const int c = (firsts >> i) & 1u ? cc[i] : -1;
+      const unsigned same = __match_any_sync(0xffffffffu, c);
+      if (c >= 0 && (__ffs(same) - 1) == lane) atomicAdd(tgt + c, __popc(same));
     }
   }
-  if (small) {
-    for (int q = 0; q < deg; ++q) dn[b + q] = q < k ? e : -1;
-    cnt[e] = k;
-    npairs[e] = (unsigned long long)k * (unsigned long long)(k > 0 ? k - 1 : 0);
-  }
-  const int maxdeg = __reduce_max_sync(0xffffffffu, small ? deg : 0);
-#pragma unroll
-  for (int i = 0; i < kThreadNet; ++i) {
-    if (i >= maxdeg) break;  // uniform across the warp
-    const int c = (firsts >> i) & 1u ? cc[i] : -1;
-    const unsigned same = __match_any_sync(0xffffffffu, c);
-    if (c >= 0 && (__ffs(same) - 1) == lane) atomicAdd(touch + c, __popc(same));
+  if (shared_hist) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      if (hist[i]) atomicAdd(touch + i, hist[i]);
   }
 }
 
@@ -294,88 +311,303 @@ attn_dedupe_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
   }
 }
 
-// Record slot q of net e (dn[q] = e) emits (a, a_k) for every other distinct
-// cluster k of e, as keys a * n + a_k, at off[e] + j (c - 1), j = q - b.
-__global__ void attn_emit_kernel(int pins, int n, const int32_t *__restrict__ net_ptr,
-                                 const int32_t *__restrict__ dn, const int32_t *__restrict__ dc,
-                                 const int32_t *__restrict__ cnt,
-                                 const unsigned long long *__restrict__ off,
-                                 uint32_t *__restrict__ keys) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= pins) return;
-  const int e = dn[q];
-  if (e < 0) return;
-  const int b = net_ptr[e], c = cnt[e], j = q - b;
-  unsigned long long o = off[e] + (unsigned long long)j * (unsigned long long)(c - 1);
-  const uint32_t row = (uint32_t)dc[q] * (uint32_t)n;
-  for (int k = 0; k < c; ++k)
-    if (k != j) keys[o++] = row + (uint32_t)dc[b + k];
-}
+// ---- shared-net counts, n <= kDenseMax: an n x n matrix per block ---------
+// Each block adds the pairs of its nets into a shared n x n count matrix
+// (a thread per net of <= 16 pins, a warp per listed larger net) and flushes
+// it into the global matrix gm.
+constexpr int kDenseMax = 128;
 
-// ---- run-length count of the sorted pair keys ------------------------------
-// head[i] = 1 where a run of equal keys starts; head[p] = 0 (after the scan
-// it holds the number of runs).
-__global__ void attn_head_kernel(const uint32_t *__restrict__ key, int p,
-                                 uint32_t *__restrict__ head) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > p) return;
-  head[i] = (i < p && (i == 0 || key[i] != key[i - 1])) ? 1u : 0u;
-}
-
-// The first key of every run and where the run starts, at the run's index.
-__global__ void attn_compact_kernel(const uint32_t *__restrict__ key, int p,
-                                    const uint32_t *__restrict__ idx,
-                                    uint32_t *__restrict__ ukey, int32_t *__restrict__ ustart) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p) return;
-  if (idx[i + 1] != idx[i]) {  // a run starts at i
-    ukey[idx[i]] = key[i];
-    ustart[idx[i]] = i;
+__global__ void __launch_bounds__(256)
+attn_dense_count_kernel(int m, int n, const int32_t *__restrict__ net_ptr,
+                        const int32_t *__restrict__ dc, const int32_t *__restrict__ cnt,
+                        const int32_t *__restrict__ mid, const int32_t *__restrict__ n_mid,
+                        const int32_t *__restrict__ big, const int32_t *__restrict__ n_big,
+                        int32_t *__restrict__ gm) {
+  extern __shared__ int32_t sm[];
+  const int nn = n * n;
+  for (int i = threadIdx.x; i < nn; i += blockDim.x) sm[i] = 0;
+  __syncthreads();
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
+    const int b = net_ptr[e], deg = net_ptr[e + 1] - b;
+    if (deg > kThreadNet) continue;  // listed: a warp takes it below
+    const int c = cnt[e];
+    int cc[kThreadNet];
+#pragma unroll
+    for (int i = 0; i < kThreadNet; ++i) cc[i] = i < c ? dc[b + i] : 0;
+#pragma unroll
+    for (int i = 0; i < kThreadNet; ++i) {
+      if (i >= c) break;
+#pragma unroll
+      for (int j = 0; j < kThreadNet; ++j) {
+        if (j >= c) break;
+        if (j != i) atomicAdd(sm + cc[i] * n + cc[j], 1);
+      }
+    }
   }
-}
-
-// Scores of the pairs with shared nets (count = length of the key's run),
-// and the dense matrix when asked. *nu = number of runs.
-__global__ void attn_score_kernel(int p, int n, const uint32_t *__restrict__ nu,
-                                  const uint32_t *__restrict__ ukey,
-                                  const int32_t *__restrict__ ustart,
-                                  const int32_t *__restrict__ touch,
-                                  float *__restrict__ score, float *__restrict__ dense) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int u = (int)*nu;
-  if (i >= u) return;
-  const int cnt = (i + 1 < u ? ustart[i + 1] : p) - ustart[i];
-  const uint32_t a = ukey[i] / (uint32_t)n, b = ukey[i] % (uint32_t)n;
-  const float s = __fdiv_rn((float)cnt, (float)touch[a]);
-  score[i] = s;
-  if (dense) dense[(size_t)a * n + b] = s;
-}
-
-// One warp per cluster a: its pairs are the run of sorted keys in
-// [a n, (a + 1) n), by ascending b. Round r picks the best entry below the
-// previous pick in the order (score descending, b ascending) -- the stable
-// descending sort of the reference -- as the warp maximum of the 64-bit key
-// (score bits, ~b); positive f32 scores order like their bit patterns.
-__device__ __forceinline__ int lower_bound_u32(const uint32_t *__restrict__ a, int u,
-                                               uint32_t v) {
-  int lo = 0, hi = u;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (a[mid] < v) lo = mid + 1; else hi = mid;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = stride >> 5;
+  const int nm = *n_mid, nb = *n_big;
+  for (int i = warp; i < nm + nb; i += warps) {
+    const int e = i < nm ? mid[i] : big[i - nm];
+    const int b = net_ptr[e], c = cnt[e];
+    for (int t = lane; t < c * c; t += 32) {
+      const int u = t / c, v = t - u * c;
+      if (u != v) atomicAdd(sm + dc[b + u] * n + dc[b + v], 1);
+    }
   }
-  return lo;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nn; i += blockDim.x)
+    if (sm[i]) atomicAdd(gm + i, sm[i]);
 }
 
-__global__ void attn_topk_kernel(int n, const uint32_t *__restrict__ nu, int top_k,
-                                 const uint32_t *__restrict__ ukey,
-                                 const float *__restrict__ score, int32_t *__restrict__ out) {
+// One warp per row a of the n x n counts: scores, dense row, top-k rounds.
+__device__ __forceinline__ unsigned long long rank_key(float score, int b) {
+  return ((unsigned long long)__float_as_uint(score) << 32) | (0xFFFFFFFFu - (uint32_t)b);
+}
+
+__global__ void attn_dense_rows_kernel(int n, int top_k, const int32_t *__restrict__ gm,
+                                       const int32_t *__restrict__ touch,
+                                       float *__restrict__ dense, int32_t *__restrict__ out) {
   const int a = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (a >= n) return;  // uniform per warp
-  const int u = nu ? (int)*nu : 0;
-  const uint32_t row = (uint32_t)a * (uint32_t)n;
-  const int lo = lower_bound_u32(ukey, u, row);
-  const int hi = lower_bound_u32(ukey, u, row + (uint32_t)n);  // (n - 1) n + n < 2^32
+  const int32_t *row = gm + (size_t)a * n;
+  const float tot = (float)touch[a];
+  if (dense)
+    for (int b = lane; b < n; b += 32)
+      dense[(size_t)a * n + b] = row[b] ? __fdiv_rn((float)row[b], tot) : 0.0f;
+  int32_t *o = out + (size_t)a * top_k;
+  unsigned long long last = ~0ull;
+  int r = 0;
+  for (; r < top_k; ++r) {
+    unsigned long long best = 0;
+    for (int b = lane; b < n; b += 32) {
+      if (!row[b]) continue;
+      const unsigned long long key = rank_key(__fdiv_rn((float)row[b], tot), b);
+      if (key < last && key > best) best = key;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
+      best = other > best ? other : best;
+    }
+    if (best == 0) break;
+    if (lane == 0) o[r] = (int32_t)(0xFFFFFFFFu - (uint32_t)best);
+    last = best;
+  }
+  for (int rr = r + lane; rr < top_k; rr += 32) o[rr] = -1;
+}
+
+// ---- shared-net counts, n <= kRowMax: one block per row -------------------
+// The distinct (net, cluster) records are bucketed by cluster (rnet, by
+// rp); the block of row a walks the nets touching a and counts the clusters
+// of each in shared memory, listing each cluster on its first count.
+constexpr int kRowMax = 16384;
+constexpr int kRowThreads = 256;
+constexpr int kKeyRegs = 4;
+
+// Counting sort of the record slots by cluster, one contiguous chunk of
+// slots per block: a shared histogram, one global reservation per (block,
+// cluster), then the scatter through shared cursors.
+constexpr int kBucketThreads = 512;
+
+__global__ void __launch_bounds__(kBucketThreads)
+attn_bucket_kernel(int pins, int n, const int32_t *__restrict__ dn,
+                   const int32_t *__restrict__ dc, int32_t *__restrict__ cursor,
+                   int32_t *__restrict__ rnet) {
+  extern __shared__ int32_t sm[];
+  int32_t *hist = sm, *base = sm + n;
+  const int chunk = (pins + gridDim.x - 1) / gridDim.x;
+  const int q0 = blockIdx.x * chunk, q1 = min(pins, q0 + chunk);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x)
+    if (dn[q] >= 0) atomicAdd(hist + dc[q], 1);
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (hist[i]) base[i] = atomicAdd(cursor + i, hist[i]);
+    hist[i] = 0;
+  }
+  __syncthreads();
+  for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+    const int e = dn[q];
+    if (e < 0) continue;
+    const int a = dc[q];
+    rnet[base[a] + atomicAdd(hist + a, 1)] = e;
+  }
+}
+
+__global__ void __launch_bounds__(kRowThreads)
+attn_rows_kernel(int n, int top_k, const int32_t *__restrict__ rp,
+                 const int32_t *__restrict__ rnet, const int32_t *__restrict__ net_ptr,
+                 const int32_t *__restrict__ dc, const int32_t *__restrict__ cnt,
+                 const int32_t *__restrict__ touch, float *__restrict__ dense,
+                 int32_t *__restrict__ out) {
+  extern __shared__ int32_t sm[];
+  int32_t *count = sm;                                        // [n]
+  uint16_t *list = reinterpret_cast<uint16_t *>(sm + n);      // [n]
+  __shared__ int list_n;
+  __shared__ unsigned long long wbest[2 * (kRowThreads / 32)];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < n; i += blockDim.x) count[i] = 0;
+  for (int a = blockIdx.x; a < n; a += gridDim.x) {
+    if (tid == 0) list_n = 0;
+    __syncthreads();
+    const int lo = rp[a], hi = rp[a + 1];
+    for (int r = lo + tid; r < hi; r += blockDim.x) {  // a record per thread
+      const int e = rnet[r];
+      const int b0 = net_ptr[e], c = cnt[e];
+      for (int k = 0; k < c; ++k) {
+        const int b = dc[b0 + k];
+        if (b != a && atomicAdd(count + b, 1) == 0) list[atomicAdd(&list_n, 1)] = (uint16_t)b;
+      }
+    }
+    __syncthreads();
+    const int L = list_n;
+    const float tot = (float)touch[a];
+    if (dense)
+      for (int i = tid; i < L; i += blockDim.x) {
+        const int b = list[i];
+        dense[(size_t)a * n + b] = __fdiv_rn((float)count[b], tot);
+      }
+    // rank keys held in registers when the row has at most kKeyRegs * threads
+    // entries, else recomputed every round
+    unsigned long long kr[kKeyRegs];
+    const bool in_regs = L <= kKeyRegs * kRowThreads;
+#pragma unroll
+    for (int j = 0; j < kKeyRegs; ++j) {
+      const int i = tid + j * kRowThreads;
+      kr[j] = 0;
+      if (in_regs && i < L) kr[j] = rank_key(__fdiv_rn((float)count[list[i]], tot), list[i]);
+    }
+    unsigned long long last = ~0ull;
+    int r = 0;
+    for (; r < top_k; ++r) {
+      unsigned long long best = 0;
+      if (in_regs) {
+#pragma unroll
+        for (int j = 0; j < kKeyRegs; ++j)
+          if (kr[j] < last && kr[j] > best) best = kr[j];
+      } else {
+        for (int i = tid; i < L; i += blockDim.x) {
+          const int b = list[i];
+          const unsigned long long key = rank_key(__fdiv_rn((float)count[b], tot), b);
+          if (key < last && key > best) best = key;
+        }
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
+        best = other > best ? other : best;
+      }
+      // double-buffered: round r + 1 writes the other half, and round r + 2
+      // comes after the barrier of round r + 1
+      unsigned long long *wb = wbest + (r & 1) * (kRowThreads / 32);
+      if (lane == 0) wb[warp] = best;
+      __syncthreads();
+      best = 0;
+      for (int w = 0; w < kRowThreads / 32; ++w) best = wb[w] > best ? wb[w] : best;
+      if (best == 0) break;  // the same for every thread
+      if (tid == 0) out[(size_t)a * top_k + r] = (int32_t)(0xFFFFFFFFu - (uint32_t)best);
+      last = best;
+    }
+    for (int rr = r + tid; rr < top_k; rr += blockDim.x) out[(size_t)a * top_k + rr] = -1;
+    for (int i = tid; i < L; i += blockDim.x) count[list[i]] = 0;
+    __syncthreads();
+  }
+}
+
+// ---- shared-net counts in a hash table of the pair keys -------------------
+// Open addressing with linear probing over T = 2^log_t >= 2 P slots (key
+// kEmpty = free); counts are added to the key's slot. The table's order is
+// irrelevant: rows are bucketed afterwards and the top-k order is total.
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;  // a * n + b < n^2 <= 65535^2 < kEmpty
+
+__device__ __forceinline__ uint32_t pair_slot(uint32_t key, int log_t) {
+  return (uint32_t)(((unsigned long long)key * 0x9E3779B97F4A7C15ull) >> (64 - log_t));
+}
+
+// Record slot q of net e (dn[q] = e, j = q - net_ptr[e]) adds the pairs
+// (a_j, a_k), k != j, of the net's c distinct clusters. Lanes with the same
+// key in one round add once (__match_any_sync). bad[0] |= 4 if a probe ever
+// went round the whole table (it cannot at load factor <= 1/2).
+__global__ void __launch_bounds__(256)
+attn_pairs_kernel(int pins, int n, const int32_t *__restrict__ net_ptr,
+                  const int32_t *__restrict__ dn, const int32_t *__restrict__ dc,
+                  const int32_t *__restrict__ cnt, int log_t, uint32_t *__restrict__ tkey,
+                  uint32_t *__restrict__ tcnt, int32_t *__restrict__ bad) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int e = -1, b = 0, c = 0, j = 0;
+  if (q < pins) e = dn[q];
+  if (e >= 0) {
+    b = net_ptr[e];
+    c = cnt[e];
+    j = q - b;
+  }
+  const uint32_t row = e >= 0 ? (uint32_t)dc[q] * (uint32_t)n : 0u;
+  const uint32_t mask = (1u << log_t) - 1u;
+  const int rounds = __reduce_max_sync(0xffffffffu, c);
+  for (int t = 0; t < rounds; ++t) {
+    const uint32_t key = (t < c && t != j) ? row + (uint32_t)dc[b + t] : kEmpty;
+    const unsigned same = __match_any_sync(0xffffffffu, key);
+    if (key == kEmpty || (__ffs(same) - 1) != lane) continue;
+    uint32_t h = pair_slot(key, log_t);
+    bool done = false;
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const uint32_t prev = atomicCAS(tkey + h, kEmpty, key);
+      if (prev == kEmpty || prev == key) {
+        atomicAdd(tcnt + h, (uint32_t)__popc(same));
+        done = true;
+        break;
+      }
+      h = (h + 1u) & mask;
+    }
+    if (!done) atomicOr(bad, 4);
+  }
+}
+
+// Entries per row (cluster a), counted over the table.
+__global__ void attn_row_count_kernel(uint32_t T, int n, const uint32_t *__restrict__ tkey,
+                                      int32_t *__restrict__ rowcnt) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t key = i < T ? tkey[i] : kEmpty;
+  const int a = key != kEmpty ? (int)(key / (uint32_t)n) : -1;
+  const unsigned same = __match_any_sync(0xffffffffu, a);
+  if (a >= 0 && (__ffs(same) - 1) == (int)(threadIdx.x & 31))
+    atomicAdd(rowcnt + a, __popc(same));
+}
+
+// Each entry to its row's bucket (rowcur starts at the row offsets) with its
+// score shared / |nets touching a| in f32, and to the dense matrix if asked.
+__global__ void attn_row_fill_kernel(uint32_t T, int n, const uint32_t *__restrict__ tkey,
+                                     const uint32_t *__restrict__ tcnt,
+                                     const int32_t *__restrict__ touch,
+                                     int32_t *__restrict__ rowcur, int32_t *__restrict__ rb,
+                                     float *__restrict__ rs, float *__restrict__ dense) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  const uint32_t key = tkey[i];
+  if (key == kEmpty) return;
+  const uint32_t a = key / (uint32_t)n, b = key % (uint32_t)n;
+  const float sc = __fdiv_rn((float)tcnt[i], (float)touch[a]);
+  const int pos = atomicAdd(rowcur + a, 1);
+  rb[pos] = (int32_t)b;
+  rs[pos] = sc;
+  if (dense) dense[(size_t)a * n + b] = sc;
+}
+
+// One warp per cluster a over its bucket [rowptr[a], rowptr[a+1]) (any
+// order). Round r picks the best entry below the previous pick in the order
+// (score descending, b ascending) -- the stable descending sort of the
+// reference -- as the warp maximum of the 64-bit key (score bits, ~b);
+// positive f32 scores order like their bit patterns.
+__global__ void attn_topk_kernel(int n, int top_k, const int32_t *__restrict__ rowptr,
+                                 const int32_t *__restrict__ rb, const float *__restrict__ rs,
+                                 int32_t *__restrict__ out) {
+  const int a = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (a >= n) return;  // uniform per warp
+  const int lo = rowptr[a], hi = rowptr[a + 1];
   int32_t *o = out + (size_t)a * top_k;
   unsigned long long last = ~0ull;
   int r = 0;
@@ -383,7 +615,7 @@ __global__ void attn_topk_kernel(int n, const uint32_t *__restrict__ nu, int top
     unsigned long long best = 0;
     for (int i = lo + lane; i < hi; i += 32) {
       const unsigned long long key =
-          ((unsigned long long)__float_as_uint(score[i]) << 32) | (0xFFFFFFFFu - (ukey[i] - row));
+          ((unsigned long long)__float_as_uint(rs[i]) << 32) | (0xFFFFFFFFu - (uint32_t)rb[i]);
       if (key < last && key > best) best = key;
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -444,7 +676,7 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   const size_t pp = (size_t)pins + 1, mm = (size_t)m + 1;
   DevBuf<int32_t> d_cl, d_cptr, d_cgate, d_bad, touch, dc, dn, cnt, mid, big, out;
   DevBuf<unsigned long long> npairs, psum;
-  DevBuf<float> score, dense;
+  DevBuf<float> dense;
   FX_TRY(d_cl.alloc(d->n));
   FX_TRY(d_cptr.alloc((size_t)n + 1));
   FX_TRY(d_cgate.alloc(G > 0 ? (size_t)G : 1));
@@ -475,9 +707,10 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     ++launches;
   }
   if (m > 0) {
-    attn_dedupe_thread_kernel<<<(m + 255) / 256, 256, 0, s>>>(
-        m, d->net_ptr.p, d->net_gate.p, d_cl.p, dc.p, dn.p, cnt.p, npairs.p, touch.p, mid.p,
-        d_bad.p + 2, big.p, d_bad.p + 1);
+    const int tb = std::min((m + 255) / 256, 4 * ctx->num_sms);
+    attn_dedupe_thread_kernel<<<tb, 256, 0, s>>>(m, n, d->net_ptr.p, d->net_gate.p, d_cl.p,
+                                                 dc.p, dn.p, cnt.p, npairs.p, touch.p, mid.p,
+                                                 d_bad.p + 2, big.p, d_bad.p + 1);
     attn_dedupe_warp_kernel<<<4 * ctx->num_sms, 256, 0, s>>>(
         mid.p, d_bad.p + 2, d->net_ptr.p, d->net_gate.p, d_cl.p, dc.p, dn.p, cnt.p, npairs.p,
         touch.p);
@@ -487,6 +720,86 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     FX_CHECK_LAUNCH();
     launches += 3;
   }
+  if (n <= kRowMax) {  // shared-memory counts, no pair list
+    FX_TRY(out.alloc(nk));
+    if (out_scores) {
+      FX_TRY(dense.alloc((size_t)n * n));
+      FX_CHECK_CUDA(cudaMemsetAsync(dense.p, 0, (size_t)n * n * 4, s));
+    }
+    DevBuf<int32_t> gm, rp, rcur, rsum, rnet;
+    if (n <= kDenseMax) {
+      // the whole level's counts as an n x n matrix
+      FX_TRY(gm.alloc((size_t)n * n));
+      FX_CHECK_CUDA(cudaMemsetAsync(gm.p, 0, (size_t)n * n * 4, s));
+      const int smem = n * n * 4;
+      FX_CHECK_CUDA(cudaFuncSetAttribute(attn_dense_count_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      if (m > 0) {
+        attn_dense_count_kernel<<<ctx->num_sms, 256, smem, s>>>(
+            m, n, d->net_ptr.p, dc.p, cnt.p, mid.p, d_bad.p + 2, big.p, d_bad.p + 1, gm.p);
+        FX_CHECK_LAUNCH();
+        ++launches;
+      }
+      if (top_k > 0 || out_scores) {
+        attn_dense_rows_kernel<<<(n + 7) / 8, 256, 0, s>>>(n, top_k, gm.p, touch.p,
+                                                           out_scores ? dense.p : nullptr,
+                                                           out.p);
+        FX_CHECK_LAUNCH();
+        ++launches;
+      }
+    } else {
+      // records bucketed by cluster, then one block per row
+      FX_TRY(rp.alloc((size_t)n + 1));
+      FX_TRY(rcur.alloc((size_t)n + 1));
+      FX_TRY(rsum.alloc(scan_tiles((long long)n + 1)));
+      FX_TRY(rnet.alloc(pp));
+      FX_CHECK_CUDA(cudaMemcpyAsync(rp.p, touch.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+      FX_CHECK_CUDA(cudaMemsetAsync(rp.p + n, 0, 4, s));
+      FX_TRY(exclusive_scan(rp.p, (long long)n + 1, rsum.p, s));
+      FX_CHECK_CUDA(cudaMemcpyAsync(rcur.p, rp.p, ((size_t)n + 1) * 4,
+                                    cudaMemcpyDeviceToDevice, s));
+      launches += 3;
+      if (pins > 0) {
+        const int bsm = 2 * n * 4;
+        FX_CHECK_CUDA(cudaFuncSetAttribute(attn_bucket_kernel,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
+        attn_bucket_kernel<<<ctx->num_sms, kBucketThreads, bsm, s>>>(pins, n, dn.p, dc.p,
+                                                                     rcur.p, rnet.p);
+        FX_CHECK_LAUNCH();
+        ++launches;
+      }
+      const int smem = n * 4 + ((n * 2 + 15) & ~15);
+      FX_CHECK_CUDA(cudaFuncSetAttribute(attn_rows_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      int per_sm = 1;
+      FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, attn_rows_kernel,
+                                                                  kRowThreads, smem));
+      attn_rows_kernel<<<std::min(n, std::max(1, per_sm) * ctx->num_sms), kRowThreads, smem,
+                         s>>>(
+          n, top_k, rp.p, rnet.p, d->net_ptr.p, dc.p, cnt.p, touch.p,
+          out_scores ? dense.p : nullptr, out.p);
+      FX_CHECK_LAUNCH();
+      ++launches;
+    }
+    timer_end(ctx, FX_STAGE_ATTENTION, s, t0);
+    int32_t bad = 0;
+    FX_CHECK_CUDA(cudaMemcpyAsync(&bad, d_bad.p, 4, cudaMemcpyDeviceToHost, s));
+    FX_CHECK_CUDA(cudaStreamSynchronize(s));
+    if (bad) {
+      set_error("fx_attention: %s", (bad & 1) ? "a cluster gate is out of range"
+                                              : "a gate is listed in two clusters");
+      return FX_EINVAL;
+    }
+    if (top_k > 0 && out_topk)
+      FX_CHECK_CUDA(cudaMemcpyAsync(out_topk, out.p, nk * 4, cudaMemcpyDeviceToHost, s));
+    if (out_scores)
+      FX_CHECK_CUDA(cudaMemcpyAsync(out_scores, dense.p, (size_t)n * n * 4,
+                                    cudaMemcpyDeviceToHost, s));
+    FX_CHECK_CUDA(cudaStreamSynchronize(s));
+    ctx->launches += launches;
+    return FX_OK;
+  }
+  // n > kRowMax: pair keys counted in a hash table
   // exclusive offsets of the pairs; the extra (zero) slot becomes the total
   FX_TRY(exclusive_scan(npairs.p, (long long)mm, psum.p, s));
   launches += 3;
@@ -506,63 +819,53 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     return FX_EINVAL;
   }
   const int P = (int)total;
-  const size_t pc = (size_t)P + 1;
-  DevBuf<uint32_t> keys[2], head, hsum;
-  DevBuf<int32_t> vals[2];
-  FX_TRY(keys[0].alloc(pc));
-  FX_TRY(keys[1].alloc(pc));
-  FX_TRY(vals[0].alloc(pc));
-  FX_TRY(vals[1].alloc(pc));
-  FX_TRY(head.alloc(pc));
-  FX_TRY(hsum.alloc(scan_tiles((long long)pc)));
-  FX_TRY(score.alloc(pc));
+  int log_t = 10;
+  while (log_t < 31 && (1ull << log_t) < 2ull * (unsigned long long)P) ++log_t;
+  const uint32_t T = 1u << log_t;
+  DevBuf<uint32_t> tkey, tcnt;
+  DevBuf<int32_t> rowptr, rowcur, rb, rsum;
+  DevBuf<float> rs;
+  FX_TRY(tkey.alloc(T));
+  FX_TRY(tcnt.alloc(T));
+  FX_TRY(rowptr.alloc((size_t)n + 1));
+  FX_TRY(rowcur.alloc((size_t)n + 1));
+  FX_TRY(rsum.alloc(scan_tiles((long long)n + 1)));
+  FX_TRY(rb.alloc((size_t)P + 1));
+  FX_TRY(rs.alloc((size_t)P + 1));
   FX_TRY(out.alloc(nk));
-  DevBuf<uint32_t> kh, ks, dt;
-  FX_TRY(kh.alloc((size_t)256 * radix_sort_tiles(P > 0 ? P : 1)));
-  FX_TRY(ks.alloc((size_t)256 * radix_sort_tiles(P > 0 ? P : 1)));
-  FX_TRY(dt.alloc(256));
   if (out_scores) {
     FX_TRY(dense.alloc((size_t)n * n));
     FX_CHECK_CUDA(cudaMemsetAsync(dense.p, 0, (size_t)n * n * 4, s));
   }
+  FX_CHECK_CUDA(cudaMemsetAsync(rowptr.p, 0, ((size_t)n + 1) * 4, s));
+  if (P > 0) {
+    FX_CHECK_CUDA(cudaMemsetAsync(tkey.p, 0xFF, (size_t)T * 4, s));
+    FX_CHECK_CUDA(cudaMemsetAsync(tcnt.p, 0, (size_t)T * 4, s));
+  }
   cudaEvent_t t1;
   timer_begin(ctx, FX_STAGE_ATTENTION, s, &t1);
   if (P > 0) {
-    attn_emit_kernel<<<(pins + 255) / 256, 256, 0, s>>>(pins, n, d->net_ptr.p, dn.p, dc.p,
-                                                        cnt.p, npairs.p, keys[0].p);
+    attn_pairs_kernel<<<(pins + 255) / 256, 256, 0, s>>>(pins, n, d->net_ptr.p, dn.p, dc.p,
+                                                         cnt.p, log_t, tkey.p, tcnt.p, d_bad.p);
+    attn_row_count_kernel<<<(T + 255) / 256, 256, 0, s>>>(T, n, tkey.p, rowptr.p);
     FX_CHECK_LAUNCH();
-    // keys < n^2: as many 8-bit passes as n^2 - 1 has bytes
-    const uint32_t kmax = (uint32_t)n * (uint32_t)n - 1u;
-    int kp = 0;
-    while (kp < 4 && (kmax >> (8 * kp)) != 0) ++kp;
-    uint32_t *kk[2] = {keys[0].p, keys[1].p};
-    int32_t *vv[2] = {vals[0].p, vals[1].p};
-    FX_TRY(radix_sort_pairs(kk, vv, P, kp, kh.p, ks.p, dt.p, s));
-    const uint32_t *skey = keys[kp & 1].p;
-    uint32_t *ukey = keys[(kp & 1) ^ 1].p;
-    // runs of equal keys: run index by a scan of the run heads
-    attn_head_kernel<<<(P + 256) / 256, 256, 0, s>>>(skey, P, head.p);
+    FX_TRY(exclusive_scan(rowptr.p, (long long)n + 1, rsum.p, s));
+    FX_CHECK_CUDA(cudaMemcpyAsync(rowcur.p, rowptr.p, ((size_t)n + 1) * 4,
+                                  cudaMemcpyDeviceToDevice, s));
+    attn_row_fill_kernel<<<(T + 255) / 256, 256, 0, s>>>(T, n, tkey.p, tcnt.p, touch.p,
+                                                         rowcur.p, rb.p, rs.p,
+                                                         out_scores ? dense.p : nullptr);
     FX_CHECK_LAUNCH();
-    FX_TRY(exclusive_scan(head.p, (long long)P + 1, hsum.p, s));
-    attn_compact_kernel<<<(P + 255) / 256, 256, 0, s>>>(skey, P, head.p, ukey, vals[0].p);
-    attn_score_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, n, head.p + P, ukey, vals[0].p,
-                                                      touch.p, score.p,
-                                                      out_scores ? dense.p : nullptr);
-    FX_CHECK_LAUNCH();
-    launches += 1 + 3 * kp + 1 + 3 + 2;
-    if (top_k > 0) {
-      attn_topk_kernel<<<(n + 7) / 8, 256, 0, s>>>(n, head.p + P, top_k, ukey, score.p,
-                                                   out.p);
-      FX_CHECK_LAUNCH();
-      ++launches;
-    }
-  } else if (top_k > 0) {
-    attn_topk_kernel<<<(n + 7) / 8, 256, 0, s>>>(n, nullptr, top_k, keys[0].p, score.p,
-                                                 out.p);
+    launches += 2 + 3 + 1;
+  }
+  if (top_k > 0) {
+    attn_topk_kernel<<<(n + 7) / 8, 256, 0, s>>>(n, top_k, rowptr.p, rb.p, rs.p, out.p);
     FX_CHECK_LAUNCH();
     ++launches;
   }
   timer_end(ctx, FX_STAGE_ATTENTION, s, t1);
+  int32_t bad2 = 0;
+  FX_CHECK_CUDA(cudaMemcpyAsync(&bad2, d_bad.p, 4, cudaMemcpyDeviceToHost, s));
   if (top_k > 0 && out_topk)
     FX_CHECK_CUDA(cudaMemcpyAsync(out_topk, out.p, nk * 4, cudaMemcpyDeviceToHost, s));
   if (out_scores)
@@ -570,5 +873,9 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
                                   cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
   ctx->launches += launches;
+  if (bad2 & 4) {
+    set_error("fx_attention: the pair table overflowed");
+    return FX_ECUDA;
+  }
   return FX_OK;
 }

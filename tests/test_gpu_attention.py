@@ -124,9 +124,12 @@ def test_high_fanout_nets(fx, ctx, oracle):
     assert np.array_equal(top, top2) and np.array_equal(sc, sc2)
 
 
-def test_many_clusters_with_big_nets(fx, ctx, oracle):
+@pytest.mark.parametrize("n_clusters", [100, 5000, 20_000])
+def test_many_clusters_with_big_nets(fx, ctx, oracle, n_clusters):
+    """The three count paths: an n x n matrix per block (n <= 128), a block
+    per row (n <= 16384) and the pair hash table beyond."""
     rng = np.random.default_rng(23)
-    n_gates, n_clusters = 120_000, 20_000
+    n_gates = 120_000
     degs = np.where(rng.random(90_000) < 0.01, rng.integers(33, 200, 90_000),
                     rng.integers(2, 8, 90_000))
     net_ptr = np.concatenate([[0], np.cumsum(degs)]).astype(np.int32)
