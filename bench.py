@@ -1056,9 +1056,14 @@ def run_attention(args, rank, world, local_rank):
     n_cl = [len(cp) - 1 for _, cp, _ in levels]
     d.close()
     ctx.close()
-    # algorithmic bytes of one pass: per level the netlist's pin lists and each
-    # pin's cluster (net_ptr, net_gate, cluster id), each ordered pair key
-    # once, the unique pairs' keys and scores once, and the top-k lists
+    # algorithmic bytes of one pass: per level, the pin lists read once
+    # (net_ptr, net_gate), each pin's cluster (one 4-byte gather), the level's
+    # cluster lists and the top-k lists written
+    p = int(c.net_ptr[-1])
+    alg = sum(4 * (c.num_nets + 1) + 8 * p + 4 * (len(cp) + len(cg)) + 4 * (len(cp) - 1)
+              * ATTN_TOP_K for _, cp, cg in levels)
+    hbm, _, peak_src = peaks()
+    achieved = alg / (dev_ms * 1e-3) / 1e9
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         sec, k = attention_cpu_sample(c, levels)
@@ -1077,6 +1082,12 @@ def run_attention(args, rank, world, local_rank):
                                   f"{ATTN_TOP_K}", "seed": args.seed,
                       "l2": "inputs (pins, pair keys) larger than L2 at the deep levels"},
            "levels": n_cl, "same_result_every_step": bool(same), "cpu_baseline": cpu,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                        "frac": achieved / hbm, "traffic": None,
+                        "kernel": "all kernels of a pass (stage events)",
+                        "algorithmic_bytes_per_pass": alg, "peak_source": peak_src,
+                        "limiter": "shared-memory atomics and dependent loads of the "
+                                   "per-row counting (attn_rows_kernel), not bandwidth"},
            "e2e": {"value": world * args.steps / wall, "unit": "passes/s",
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                    "call": "fx_attention per level with host cluster lists"},
