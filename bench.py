@@ -450,14 +450,14 @@ def run_fluxion(args, rank, world, local_rank):
     dens_roof = None
     if "density" in per_iter:
         fl = f_alg["density"] * 6 / 4  # six GEMMs per step (no potential)
-        a = fl / (per_iter["density"] * 1e-3) / 1e12
+        d_tf = fl / (per_iter["density"] * 1e-3) / 1e12
         if PREC[args.precision] == 3:
             pk, ps = 148 * 128 * 2 * 1.965e9 / 1e12, "nominal FP32 CUDA cores 148 x 128 x 2 x 1.965 GHz"
         else:
             pk = bf16 if args.precision == "bf16" else bf16 / 2
             ps = f"{src} bf16 dense" + ("" if args.precision == "bf16" else " / 2 (tf32)")
         dens_roof = {"bound": "fp32-pipe" if PREC[args.precision] == 3 else "tensor",
-                     "achieved": a, "peak": pk, "unit": "TFLOP/s", "frac": a / pk,
+                     "achieved": d_tf, "peak": pk, "unit": "TFLOP/s", "frac": d_tf / pk,
                      "peak_source": ps, "note": "side stream, overlapped with Barnes-Hut: "
                                                 "its span includes time it yields"}
     B_iter = sum(b_alg.values())
