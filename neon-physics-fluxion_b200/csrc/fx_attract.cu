@@ -374,6 +374,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     ctx->launches += 1;
     timer_end(ctx, FX_STAGE_ATTRACT_INTEGRATE, s, ev);
     d->cur = nxt;
+    d->pos_in_box = true;  // the step clamps every position to the die
     if (use_cong)
       FX_TRY(congestion_run(ctx, d, d->x[d->cur].p, d->y[d->cur].p, c.cong_cols,
                             c.cong_rows, s));

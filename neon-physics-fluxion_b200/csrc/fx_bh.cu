@@ -21,6 +21,15 @@
 // the same level) are always opened. Points that share all 30 key bits form
 // a bucket (a cell of level 15): it is accepted as a whole by the same rule,
 // otherwise each of its points interacts directly.
+// Deep keys: the distance in the opening rule is clamped to min_dist, so a
+// cell smaller than theta * min_dist is accepted by every point. When a
+// level-15 cell is not (size^2 >= theta^2 min_dist^2, decided on the device
+// from the root square), each point also gets the 24-bit key of its sub-cell
+// within its level-15 cell (12 more levels, computed in f64), the points are
+// sorted by (key, sub-key, index), and the tree has 27 levels: its buckets
+// are then accepted whole by every point, and a crowded cell costs log k per
+// point instead of k. The host skips these kernels when the positions lie in
+// the die and (die + 2) / 2^15 < theta * min_dist.
 //
 // Every value is fixed by the sorted keys alone: node mass sums are added in
 // tree order (left + right, FP64) by a bottom-up sweep, decisions and forces
@@ -40,7 +49,10 @@ constexpr int kSortThreads = 256;
 constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys
 constexpr int kWalkWarps = 8;
-constexpr int kStack = 64;
+constexpr int kStack = 64;       // walk stack of a 15-level tree (<= 3 * 15 + 4)
+constexpr int kStackDeep = 96;   // of a 27-level tree (<= 3 * 27 + 4)
+constexpr int kDeepLevels = 12;  // levels below 15 in deep mode
+constexpr int kKeyBits = 30, kDeepBits = kKeyBits + 2 * kDeepLevels;
 
 // ---- bounding box and root square ----------------------------------------
 __global__ void bh_bbox_kernel(const float *__restrict__ x,
@@ -88,7 +100,7 @@ __global__ void bh_bbox_kernel(const float *__restrict__ x,
 // Root square from the box (BarnesHutTree.cpp:24-46, in f32 without
 // contraction), then re-arms the box for the next accumulation.
 __global__ void bh_root_kernel(unsigned int *__restrict__ bbox,
-                               float *__restrict__ root) {
+                               float *__restrict__ root, float th2, float md2) {
   float mnx = ord2f(bbox[0]), mny = ord2f(bbox[1]);
   float mxx = ord2f(bbox[2]), mxy = ord2f(bbox[3]);
   mnx = __fsub_rn(mnx, 1.0f);
@@ -102,6 +114,9 @@ __global__ void bh_root_kernel(unsigned int *__restrict__ bbox,
   root[0] = __fsub_rn(cx, half);
   root[1] = __fsub_rn(cy, half);
   root[2] = size;
+  // deep keys when a level-15 cell is not always accepted
+  const float s15 = ldexpf(size, -15);
+  root[3] = __fmul_rn(s15, s15) >= __fmul_rn(th2, md2) ? 1.0f : 0.0f;
   bbox[0] = 0xffffffffu;
   bbox[1] = 0xffffffffu;
   bbox[2] = 0u;
@@ -125,11 +140,27 @@ __device__ __forceinline__ uint32_t spread15(uint32_t v) {
   return v;
 }
 
+// Sub-cell (0..4095) of p within its level-15 cell c15, in f64 without
+// contraction; a point the f32 quantisation put in c15 but that lies just
+// outside it is clamped to the edge sub-cell, so cells nest.
+__device__ __forceinline__ uint32_t quantize_sub(float p, float o, float size, uint32_t c15) {
+  const double w = __ddiv_rn((double)size, 32768.0);
+  const double o15 = __dadd_rn((double)o, __dmul_rn((double)c15, w));
+  const double t = __dmul_rn(__ddiv_rn(__dsub_rn((double)p, o15), w), 4096.0);
+  if (!(t > 0.0)) return 0u;
+  const double c = ceil(t);
+  if (c >= 4096.0) return 4095u;
+  return (uint32_t)c - 1u;
+}
+
+// Keys (and identity indices); with klo, also the 24-bit sub-cell keys and
+// the deep sort's inputs.
 __global__ void bh_keys_kernel(const float *__restrict__ x,
                                const float *__restrict__ y, int n,
                                const float *__restrict__ root,
                                uint32_t *__restrict__ keys,
-                               int32_t *__restrict__ idx) {
+                               int32_t *__restrict__ idx, uint32_t *__restrict__ klo,
+                               uint32_t *__restrict__ kl0, int32_t *__restrict__ il0) {
   const float ox = root[0], oy = root[1], size = root[2];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
@@ -137,13 +168,58 @@ __global__ void bh_keys_kernel(const float *__restrict__ x,
     const uint32_t qy = quantize15(y[i], oy, size);
     keys[i] = (spread15(qx) << 1) | spread15(qy);
     idx[i] = i;
+    if (klo) {
+      const uint32_t lo = (spread15(quantize_sub(x[i], ox, size, qx)) << 1) |
+                          spread15(quantize_sub(y[i], oy, size, qy));
+      klo[i] = lo;
+      kl0[i] = lo;
+      il0[i] = i;
+    }
   }
+}
+
+// Deep mode only (root[3] set): the primary keys and indices in the order of
+// the sub-key sort (gather into buffer 1, then copy back to buffer 0), and
+// the sub-keys in the final sorted order.
+__global__ void bh_deep_gather_kernel(const float *__restrict__ root, int n,
+                                      const uint32_t *__restrict__ keys0,
+                                      const int32_t *__restrict__ il1,
+                                      uint32_t *__restrict__ keys1,
+                                      int32_t *__restrict__ idx1) {
+  if (!(root[3] > 0.f)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int g = il1[i];
+    keys1[i] = keys0[g];
+    idx1[i] = g;
+  }
+}
+
+__global__ void bh_deep_copy_kernel(const float *__restrict__ root, int n,
+                                    const uint32_t *__restrict__ keys1,
+                                    const int32_t *__restrict__ idx1,
+                                    uint32_t *__restrict__ keys0, int32_t *__restrict__ idx0) {
+  if (!(root[3] > 0.f)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    keys0[i] = keys1[i];
+    idx0[i] = idx1[i];
+  }
+}
+
+__global__ void bh_deep_slo_kernel(const float *__restrict__ root, int n,
+                                   const uint32_t *__restrict__ klo,
+                                   const int32_t *__restrict__ idx0,
+                                   uint32_t *__restrict__ slo) {
+  if (!(root[3] > 0.f)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    slo[i] = klo[idx0[i]];
 }
 
 // ---- stable LSD radix sort (8-bit digits) ------------------------------------
 __global__ void __launch_bounds__(kSortThreads)
 radix_hist_kernel(const uint32_t *__restrict__ keys, int n, int shift,
-                  uint32_t *__restrict__ tile_hist, int T) {
+                  uint32_t *__restrict__ tile_hist, int T,
+                  const float *__restrict__ gate = nullptr) {
+  if (gate && !(gate[3] > 0.f)) return;  // a deep-key pass outside deep mode
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
@@ -161,7 +237,9 @@ radix_hist_kernel(const uint32_t *__restrict__ keys, int n, int shift,
 // the T tile counts of digit d and records the digit's total.
 __global__ void __launch_bounds__(256)
 radix_scan_kernel(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-                  uint32_t *__restrict__ digit_total, int T) {
+                  uint32_t *__restrict__ digit_total, int T,
+                  const float *__restrict__ gate = nullptr) {
+  if (gate && !(gate[3] > 0.f)) return;
   __shared__ uint32_t ws[8];
   const int d = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
   const uint32_t *row = in + (size_t)d * T;
@@ -197,7 +275,9 @@ radix_scatter_kernel(const uint32_t *__restrict__ kin,
                      const int32_t *__restrict__ iin,
                      uint32_t *__restrict__ kout, int32_t *__restrict__ iout,
                      int n, int shift, const uint32_t *__restrict__ tile_scan,
-                     const uint32_t *__restrict__ digit_total, int T) {
+                     const uint32_t *__restrict__ digit_total, int T,
+                     const float *__restrict__ gate = nullptr) {
+  if (gate && !(gate[3] > 0.f)) return;
   constexpr int kWarps = kSortThreads / 32;
   __shared__ uint32_t cnt[kWarps][256];
   __shared__ uint32_t doff[256];
@@ -327,35 +407,46 @@ __global__ void bh_gather_kernel(const float *__restrict__ x,
 }
 
 // ---- radix tree (Karras 2012) -----------------------------------------------
+// Common prefix length of the keys at sorted positions i and j: 30-bit key,
+// then (deep mode, lo != null) the 24-bit sub-key, then the index.
 __device__ __forceinline__ int bh_delta(const uint32_t *__restrict__ keys,
+                                        const uint32_t *__restrict__ lo,
                                         int n, int i, int j) {
   if (j < 0 || j >= n) return -1;
   const uint32_t a = keys[i], b = keys[j];
   if (a != b) return __clz(a ^ b) - 2;
-  return 30 + __clz((uint32_t)(i ^ j));
+  if (lo) {
+    const uint32_t la = lo[i], lb = lo[j];
+    if (la != lb) return kKeyBits + __clz(la ^ lb) - 8;
+    return kDeepBits + __clz((uint32_t)(i ^ j));
+  }
+  return kKeyBits + __clz((uint32_t)(i ^ j));
 }
 
-__global__ void bh_tree_kernel(const uint32_t *__restrict__ keys, int n,
+__global__ void bh_tree_kernel(const uint32_t *__restrict__ keys,
+                               const uint32_t *__restrict__ slo,
+                               const float *__restrict__ root, int n,
                                int32_t *__restrict__ child,
                                int32_t *__restrict__ range,
                                int32_t *__restrict__ dnode,
                                int32_t *__restrict__ dparent) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
-  const int dr = bh_delta(keys, n, i, i + 1), dl = bh_delta(keys, n, i, i - 1);
+  const uint32_t *sub = (slo && root[3] > 0.f) ? slo : nullptr;
+  const int dr = bh_delta(keys, sub, n, i, i + 1), dl = bh_delta(keys, sub, n, i, i - 1);
   const int d = (dr - dl) >= 0 ? 1 : -1;
-  const int dmin = bh_delta(keys, n, i, i - d);
+  const int dmin = bh_delta(keys, sub, n, i, i - d);
   int lmax = 2;
-  while (bh_delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+  while (bh_delta(keys, sub, n, i, i + lmax * d) > dmin) lmax *= 2;
   int l = 0;
   for (int t = lmax / 2; t >= 1; t /= 2)
-    if (bh_delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    if (bh_delta(keys, sub, n, i, i + (l + t) * d) > dmin) l += t;
   const int j = i + l * d;
-  const int dn = bh_delta(keys, n, i, j);
+  const int dn = bh_delta(keys, sub, n, i, j);
   int s = 0;
   for (int div = 2;; div *= 2) {
     const int t = (l + div - 1) / div;
-    if (bh_delta(keys, n, i, i + (s + t) * d) > dn) s += t;
+    if (bh_delta(keys, sub, n, i, i + (s + t) * d) > dn) s += t;
     if (t == 1) break;
   }
   const int gamma = i + s * d + min(d, 0);
@@ -525,10 +616,12 @@ __global__ void bh_node_kernel(int n, const int32_t *__restrict__ range,
                                const int32_t *__restrict__ dnode,
                                const int32_t *__restrict__ dparent,
                                const ulonglong4 *__restrict__ prefix,
-                               const float *__restrict__ root,
+                               const float *__restrict__ root, int deep_ok,
                                float4 *__restrict__ node) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
+  const bool deep = deep_ok && root[3] > 0.f;
+  const int kb = deep ? kDeepBits : kKeyBits;  // prefix length of a bucket
   const int f = range[2 * i], l = range[2 * i + 1];
   const int cnt = l - f + 1;
   const ulonglong4 pl = prefix[l];
@@ -546,8 +639,8 @@ __global__ void bh_node_kernel(int n, const int32_t *__restrict__ range,
   const int dn = dnode[i], dp = dparent[i];
   const float rs = root[2];
   float c, s2;
-  if (dn >= 30) {
-    const float sz = ldexpf(rs, -15);
+  if (dn >= kb) {
+    const float sz = ldexpf(rs, -(kb >> 1));
     c = -(float)cnt;
     s2 = __fmul_rn(sz, sz);
   } else {
@@ -570,16 +663,18 @@ constexpr int kNone = INT_MIN;
 
 __global__ void bh_qchild_kernel(int n, const int32_t *__restrict__ child,
                                  const int32_t *__restrict__ dnode,
+                                 const float *__restrict__ root, int deep_ok,
                                  int4 *__restrict__ qchild) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
+  const int kb = (deep_ok && root[3] > 0.f) ? kDeepBits : kKeyBits;
   int out[4] = {kNone, kNone, kNone, kNone};
   int k = 0;
   const int lv = dnode[i] >> 1;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int c = child[2 * i + h];
-    if (c >= 0 && dnode[c] < 30 && (dnode[c] >> 1) == lv) {
+    if (c >= 0 && dnode[c] < kb && (dnode[c] >> 1) == lv) {
       out[k++] = child[2 * c];
       out[k++] = child[2 * c + 1];
     } else {
@@ -675,6 +770,7 @@ __device__ __forceinline__ unsigned bh_eval(int c, bool in, bool cell, int s,
 constexpr int kWalkGroup = 8;                    // lanes per group
 constexpr int kWalkGroups = 32 / kWalkGroup;     // groups per warp
 
+template <int Stack>
 __global__ void __launch_bounds__(kWalkWarps * 32)
 bh_walk_kernel(int n, const float2 *__restrict__ spos,
                const int32_t *__restrict__ perm,
@@ -683,8 +779,8 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
                float2 *__restrict__ force, unsigned int *__restrict__ err) {
   // one stack per group; the odd stride puts the groups' tops (often at the
   // same depth) in different banks
-  __shared__ int32_t st_node[kWalkWarps][kWalkGroups][kStack + 1];
-  __shared__ unsigned st_mask[kWalkWarps][kWalkGroups][kStack + 1];
+  __shared__ int32_t st_node[kWalkWarps][kWalkGroups][Stack + 1];
+  __shared__ unsigned st_mask[kWalkWarps][kWalkGroups][Stack + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int g = lane / kWalkGroup;
   const bool leader = (lane % kWalkGroup) == 0;
@@ -729,7 +825,7 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
               gmask;
     }
     const int np = (om[0] != 0u) + (om[1] != 0u) + (om[2] != 0u) + (om[3] != 0u);
-    if (sp + np > kStack) {
+    if (sp + np > Stack) {
       if (leader) atomicOr(err, 1u);
     } else {
       // push the opened children in reverse so the first one is popped first
@@ -778,6 +874,29 @@ static int bh_alloc(fx_design *d) {
   return FX_OK;
 }
 
+static int bh_alloc_deep(fx_design *d) {
+  BHWork &b = d->bh;
+  const size_t n = (size_t)d->n;
+  if (b.klo.p && b.klo.n >= n) return FX_OK;
+  FX_TRY(b.klo.alloc(n));
+  FX_TRY(b.kl[0].alloc(n));
+  FX_TRY(b.kl[1].alloc(n));
+  FX_TRY(b.il[0].alloc(n));
+  FX_TRY(b.il[1].alloc(n));
+  FX_TRY(b.slo.alloc(n));
+  return FX_OK;
+}
+
+// Whether the deep-key kernels can be needed: unless the positions are known
+// to lie in the die and a level-15 cell of the largest possible root square,
+// (die + 2) / 2^15, is accepted by every point (margins cover f32 rounding).
+static bool bh_maybe_deep(const fx_design *d, float th2, float md2) {
+  if (!d->pos_in_box) return true;
+  const double rb = ((double)std::max(d->chip_w, d->chip_h) + 2.0) * (1.0 + 1e-6);
+  const double s15 = rb / 32768.0;
+  return s15 * s15 >= (double)th2 * (double)md2 * (1.0 - 1e-6);
+}
+
 // Bounding box of the given positions into bh.bbox (re-armed first).
 int bh_bbox(fx_ctx *ctx, fx_design *d, const float *x, const float *y,
             cudaStream_t s) {
@@ -802,15 +921,43 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
   const float *x = d->x[d->cur].p, *y = d->y[d->cur].p;
   const int T = (n + kSortTile - 1) / kSortTile;
   unsigned int *err = b.bbox.p + 4;
+  const float th2 = theta * theta, md2 = min_dist * min_dist;
+  const bool deep = bh_maybe_deep(d, th2, md2);  // launch the deep-key kernels
+  if (deep) FX_TRY(bh_alloc_deep(d));
   cudaEvent_t ev;
   const int gb = (n + 255) / 256;
+  int launches = 0;
   timer_begin(ctx, FX_STAGE_BH_KEYS, s, &ev);
-  bh_root_kernel<<<1, 1, 0, s>>>(b.bbox.p, b.root.p);
+  bh_root_kernel<<<1, 1, 0, s>>>(b.bbox.p, b.root.p, th2, md2);
   FX_CHECK_LAUNCH();
-  bh_keys_kernel<<<gb, 256, 0, s>>>(x, y, n, b.root.p, b.keys[0].p, b.idx[0].p);
+  bh_keys_kernel<<<gb, 256, 0, s>>>(x, y, n, b.root.p, b.keys[0].p, b.idx[0].p,
+                                    deep ? b.klo.p : nullptr, deep ? b.kl[0].p : nullptr,
+                                    deep ? b.il[0].p : nullptr);
   FX_CHECK_LAUNCH();
+  launches += 2;
   timer_end(ctx, FX_STAGE_BH_KEYS, s, ev);
   timer_begin(ctx, FX_STAGE_BH_SORT, s, &ev);
+  const float *gate = b.root.p;
+  if (deep) {
+    // stable sort by the 24-bit sub-key (3 passes; no-ops unless root[3]),
+    // then the primary keys and indices in that order into buffer 0
+    for (int pass = 0; pass < 3; ++pass) {
+      const int src = pass & 1, dst = src ^ 1;
+      radix_hist_kernel<<<T, kSortThreads, 0, s>>>(b.kl[src].p, n, 8 * pass, b.tile_hist.p, T,
+                                                   gate);
+      radix_scan_kernel<<<256, 256, 0, s>>>(b.tile_hist.p, b.tile_scan.p, b.digit_total.p, T,
+                                            gate);
+      radix_scatter_kernel<<<T, kSortThreads, 0, s>>>(
+          b.kl[src].p, b.il[src].p, b.kl[dst].p, b.il[dst].p, n, 8 * pass, b.tile_scan.p,
+          b.digit_total.p, T, gate);
+    }
+    bh_deep_gather_kernel<<<gb, 256, 0, s>>>(gate, n, b.keys[0].p, b.il[1].p, b.keys[1].p,
+                                             b.idx[1].p);
+    bh_deep_copy_kernel<<<gb, 256, 0, s>>>(gate, n, b.keys[1].p, b.idx[1].p, b.keys[0].p,
+                                           b.idx[0].p);
+    FX_CHECK_LAUNCH();
+    launches += 9 + 2;
+  }
   for (int pass = 0; pass < 4; ++pass) {
     const int src = pass & 1, dst = src ^ 1;
     radix_hist_kernel<<<T, kSortThreads, 0, s>>>(b.keys[src].p, n, 8 * pass,
@@ -821,35 +968,45 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
         b.keys[src].p, b.idx[src].p, b.keys[dst].p, b.idx[dst].p, n, 8 * pass,
         b.tile_scan.p, b.digit_total.p, T);
   }
+  launches += 12;
+  if (deep) {
+    bh_deep_slo_kernel<<<gb, 256, 0, s>>>(gate, n, b.klo.p, b.idx[0].p, b.slo.p);
+    ++launches;
+  }
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_SORT, s, ev);
   timer_begin(ctx, FX_STAGE_BH_TREE, s, &ev);
   bh_gather_kernel<<<gb, 256, 0, s>>>(x, y, b.idx[0].p, n, b.spos.p);
-  int launches = 1;
+  ++launches;
   if (n >= 2) {
     const int tb = (n - 1 + 255) / 256;
-    bh_tree_kernel<<<tb, 256, 0, s>>>(b.keys[0].p, n, b.child.p, b.range.p,
-                                      b.dnode.p, b.dparent.p);
+    bh_tree_kernel<<<tb, 256, 0, s>>>(b.keys[0].p, deep ? b.slo.p : nullptr, b.root.p, n,
+                                      b.child.p, b.range.p, b.dnode.p, b.dparent.p);
     // exact prefix sums: tile sums, tile offsets, point prefixes
     const int tiles = (n + kFixTile - 1) / kFixTile;
     fix_tile_kernel<<<tiles, kFixThreads, 0, s>>>(b.spos.p, n, b.tile_fix.p);
     fix_top_kernel<<<1, kFixThreads, 0, s>>>(b.tile_fix.p, tiles);
     fix_prefix_kernel<<<tiles, kFixThreads, 0, s>>>(b.spos.p, n, b.tile_fix.p, b.prefix.p);
     bh_node_kernel<<<tb, 256, 0, s>>>(n, b.range.p, b.dnode.p, b.dparent.p,
-                                      b.prefix.p, b.root.p, b.node.p);
-    bh_qchild_kernel<<<tb, 256, 0, s>>>(n, b.child.p, b.dnode.p, b.qchild.p);
+                                      b.prefix.p, b.root.p, deep ? 1 : 0, b.node.p);
+    bh_qchild_kernel<<<tb, 256, 0, s>>>(n, b.child.p, b.dnode.p, b.root.p, deep ? 1 : 0,
+                                        b.qchild.p);
     launches += 6;
   }
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_TREE, s, ev);
   timer_begin(ctx, FX_STAGE_BH_WALK, s, &ev);
   const int wb = (n + kWalkWarps * 32 - 1) / (kWalkWarps * 32);
-  bh_walk_kernel<<<wb, kWalkWarps * 32, 0, s>>>(
-      n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, theta * theta,
-      min_dist * min_dist, b.force.p, err);
+  if (deep)
+    bh_walk_kernel<kStackDeep><<<wb, kWalkWarps * 32, 0, s>>>(
+        n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err);
+  else
+    bh_walk_kernel<kStack><<<wb, kWalkWarps * 32, 0, s>>>(
+        n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err);
   FX_CHECK_LAUNCH();
+  ++launches;
   timer_end(ctx, FX_STAGE_BH_WALK, s, ev);
-  ctx->launches += 2 + 12 + launches + 1;
+  ctx->launches += launches;
   return FX_OK;
 }
 

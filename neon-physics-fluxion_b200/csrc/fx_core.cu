@@ -387,7 +387,7 @@ extern "C" int fx_design_load(fx_ctx *ctx, int32_t n_gates, int32_t n_nets,
       (rc = d->area.alloc(N)) || (rc = d->x[0].alloc(N)) ||
       (rc = d->y[0].alloc(N)) || (rc = d->x[1].alloc(N)) ||
       (rc = d->y[1].alloc(N)) || (rc = d->vx.alloc(N)) ||
-      (rc = d->vy.alloc(N)) || (rc = d->fattr.alloc(N)))
+      (rc = d->vy.alloc(N)) || (rc = d->fattr.alloc(N)) || (rc = d->box_flag.alloc(1)))
     return fail(rc);
   cudaStream_t s = ctx->stream;
   if (cudaMemcpyAsync(d->net_ptr.p, net_ptr, ((size_t)n_nets + 1) * 4,
@@ -431,6 +431,8 @@ extern "C" int fx_design_free(fx_design *d) {
   d->vx.release();
   d->vy.release();
   d->fattr.release();
+  d->box_flag.release();
+  for (auto &b : d->saved) b.release();
   auto rel = [](auto &buf) { buf.release(); };
   d->bh.for_each(rel);
   d->dens.for_each(rel);
@@ -461,6 +463,15 @@ extern "C" int fx_design_adjacency(const fx_design *d, int32_t *out_adj_ptr,
   return FX_OK;
 }
 
+// Clears *flag when a position lies outside [0, w] x [0, h] or is NaN.
+__global__ void box_check_kernel(const float *__restrict__ x, const float *__restrict__ y,
+                                 int n, float w, float h, unsigned int *__restrict__ flag) {
+  bool out = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out |= !(x[i] >= 0.f && x[i] <= w && y[i] >= 0.f && y[i] <= h);
+  if (__any_sync(0xffffffffu, out) && (threadIdx.x & 31) == 0) *flag = 0u;
+}
+
 extern "C" int fx_design_set_positions(fx_design *d, const float *x,
                                        const float *y) {
   if (!d || !x || !y) return FX_EINVAL;
@@ -472,7 +483,20 @@ extern "C" int fx_design_set_positions(fx_design *d, const float *x,
   FX_CHECK_CUDA(cudaMemcpyAsync(d->y[0].p, y, b, cudaMemcpyHostToDevice, s));
   FX_CHECK_CUDA(cudaMemsetAsync(d->vx.p, 0, b, s));
   FX_CHECK_CUDA(cudaMemsetAsync(d->vy.p, 0, b, s));
+  // whether the positions lie in the die (it lets Barnes-Hut skip its deep
+  // key kernels when the die is small enough), read with the sync below
+  unsigned int in_box = 0;
+  FX_CHECK_CUDA(cudaMemsetAsync(d->box_flag.p, 0xFF, 4, s));
+  if (d->n > 0) {
+    const int nb = std::min((d->n + 255) / 256, 4 * d->ctx->num_sms);
+    box_check_kernel<<<nb, 256, 0, s>>>(d->x[0].p, d->y[0].p, d->n, d->chip_w, d->chip_h,
+                                        d->box_flag.p);
+    FX_CHECK_CUDA(cudaGetLastError());
+    d->ctx->launches += 1;
+  }
+  FX_CHECK_CUDA(cudaMemcpyAsync(&in_box, d->box_flag.p, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  d->pos_in_box = in_box != 0u;
   return FX_OK;
 }
 
@@ -499,6 +523,7 @@ extern "C" int fx_design_save_state(fx_design *d) {
     if (!d->saved[i].p) FX_TRY(d->saved[i].alloc(d->n));
     FX_CHECK_CUDA(cudaMemcpyAsync(d->saved[i].p, src[i], b, cudaMemcpyDeviceToDevice, s));
   }
+  d->saved_in_box = d->pos_in_box;
   return FX_OK;
 }
 
@@ -514,6 +539,7 @@ extern "C" int fx_design_restore_state(fx_design *d) {
   float *dst[4] = {d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p};
   for (int i = 0; i < 4; ++i)
     FX_CHECK_CUDA(cudaMemcpyAsync(dst[i], d->saved[i].p, b, cudaMemcpyDeviceToDevice, s));
+  d->pos_in_box = d->saved_in_box;
   return FX_OK;
 }
 

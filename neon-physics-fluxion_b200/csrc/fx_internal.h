@@ -138,7 +138,12 @@ struct BHWork {
   DevBuf<ulonglong4> tile_fix;  // per-tile exact (x, y) sums, then offsets
   DevBuf<ulonglong4> prefix;    // inclusive exact prefix sums of spos (2 x int128)
   DevBuf<float4> node;          // internal nodes: 2 x float4 walk records
-  DevBuf<float> root;           // {x_min, y_min, size}
+  DevBuf<float> root;           // {x_min, y_min, size, deep (1) or not (0)}
+  // deep keys (levels 16..27) when a level-15 cell could be opened:
+  DevBuf<uint32_t> klo;         // 24-bit sub-cell key per gate (gate order)
+  DevBuf<uint32_t> kl[2];       // its radix sort ping-pong
+  DevBuf<int32_t> il[2];        // gate index payload of that sort
+  DevBuf<uint32_t> slo;         // sub-cell key in sorted order
   DevBuf<unsigned int> bbox;    // [0..3] ordered-int box, [4] error flag
   DevBuf<float2> force;         // per gate (original order)
   template <class F>
@@ -146,7 +151,7 @@ struct BHWork {
     for (auto &b : keys) f(b);
     for (auto &b : idx) f(b);
     f(tile_hist); f(tile_scan); f(digit_total); f(spos); f(child); f(range);
-    f(dnode); f(dparent); f(qchild);
+    f(dnode); f(dparent); f(qchild); f(klo); f(kl[0]); f(kl[1]); f(il[0]); f(il[1]); f(slo);
     f(tile_fix); f(prefix); f(node); f(root); f(bbox); f(force);
   }
 };
@@ -246,6 +251,11 @@ struct fx_design {
   int cur = 0;
   fx::DevBuf<float> vx, vy;
   fx::DevBuf<float> saved[4];    // checkpoint: x, y, vx, vy
+  // The positions are known to lie in [0, chip_w] x [0, chip_h] (set by the
+  // box check of fx_design_set_positions and by every integration step, which
+  // clamps to the die); with the saved copy's flag.
+  bool pos_in_box = false, saved_in_box = false;
+  fx::DevBuf<unsigned int> box_flag;
   fx::DevBuf<float2> fattr;      // attraction-only force output (stage API)
   // workspaces
   fx::BHWork bh;

@@ -131,6 +131,7 @@ extern "C" int fx_refine(fx_ctx *ctx, fx_design *d, const fx_refine_cfg *cfg,
   const float cw = d->chip_w / (float)cols, ch = d->chip_h / (float)rows;
   const float cap = (cw + ch) * 0.5f;
   float *px = d->x[d->cur].p, *py = d->y[d->cur].p;
+  d->pos_in_box = false;  // moved positions are not re-checked against the die
   DevBuf<float> tot;
   DevBuf<unsigned int> moved;
   FX_TRY(tot.alloc(2));

@@ -88,7 +88,7 @@ int64_t estimate_place(int64_t n, int64_t m, int64_t p, int64_t a, const fx_refi
 int64_t estimate_eco(int64_t n, const fx_iter_cfg &it, int64_t moves) {
   const int64_t G = it.density_bins;
   const int64_t cells = (int64_t)(it.cong_cols + 1) * (it.cong_rows + 1);
-  return 200 * n                      // Barnes-Hut work (keys, sort, tree, nodes, forces)
+  return 224 * n                      // Barnes-Hut work (keys, sub-keys, sort, tree, forces)
          + 120 * G * G                // density grids, operators, split copies
          + 8 * cells + 4 * 65536 + 16 * n  // congestion, step partials
          + 12 * moves + ((int64_t)4 << 20);

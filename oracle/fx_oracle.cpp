@@ -654,6 +654,19 @@ static uint32_t q15(float p, float o, float size) {
   return (uint32_t)c - 1u;
 }
 
+// The sub-cell (0..4095) of p within its level-15 cell c15, in f64: the
+// deep keys of levels 16..27, used when a level-15 cell is not accepted by
+// every point (device: quantize_sub).
+static uint32_t q_sub(float p, float o, float size, uint32_t c15) {
+  const double w = (double)size / 32768.0;
+  const double o15 = (double)o + (double)c15 * w;
+  const double t = (((double)p - o15) / w) * 4096.0;
+  if (!(t > 0.0)) return 0u;
+  const double c = std::ceil(t);
+  if (c >= 4096.0) return 4095u;
+  return (uint32_t)c - 1u;
+}
+
 static uint32_t interleave15(uint32_t qx, uint32_t qy) {
   uint32_t k = 0;
   for (int b = 14; b >= 0; --b) {
@@ -722,7 +735,10 @@ static double fixed_to_double(__int128 v) {
 // internal node ids or ~leaf (sorted position), as on the device.
 struct BHTree {
   int32_t n;
+  bool deep = false;              // 24-bit sub-keys below the 30-bit keys
+  int kb = 30;                    // prefix length of a bucket (30 or 54)
   std::vector<uint32_t> key;      // sorted keys
+  std::vector<uint32_t> lo;       // sorted sub-keys (deep)
   std::vector<int32_t> perm;      // sorted -> original
   std::vector<float> sx, sy;      // sorted positions
   std::vector<__int128> px, py;   // exact fixed-point prefix sums
@@ -737,6 +753,10 @@ struct BHTree {
   int delta(int32_t i, int32_t j) const {
     if (j < 0 || j >= n) return -1;
     if (key[i] != key[j]) return __builtin_clz(key[i] ^ key[j]) - 2;
+    if (deep) {
+      if (lo[i] != lo[j]) return 30 + __builtin_clz(lo[i] ^ lo[j]) - 8;
+      return 54 + __builtin_clz((uint32_t)(i ^ j));
+    }
     return 30 + __builtin_clz((uint32_t)(i ^ j));
   }
   int32_t split(int32_t f, int32_t l) const {
@@ -774,8 +794,8 @@ struct BHTree {
     nd.hy = (float)nd.cyd;
     nd.lx = (float)(nd.cxd - (double)nd.hx);
     nd.ly = (float)(nd.cyd - (double)nd.hy);
-    nd.bucket = dn >= 30;
-    const int lmax = nd.bucket ? 15 : dn >> 1;
+    nd.bucket = dn >= kb;
+    const int lmax = nd.bucket ? kb >> 1 : dn >> 1;
     const float sz = std::ldexp(rsize, -lmax);
     nd.s2 = (!nd.bucket && dp >= 0 && (dp >> 1) == lmax) ? -1.0f : sz * sz;
     return id;
@@ -786,7 +806,7 @@ struct BHTree {
     int k = 0;
     const Node &nd = nodes[c];
     for (int32_t h : {nd.left, nd.right}) {
-      if (h >= 0 && nodes[h].dn < 30 && (nodes[h].dn >> 1) == (nd.dn >> 1)) {
+      if (h >= 0 && nodes[h].dn < kb && (nodes[h].dn >> 1) == (nd.dn >> 1)) {
         out[k++] = nodes[h].left;
         out[k++] = nodes[h].right;
       } else {
@@ -899,12 +919,28 @@ void or_bh_forces(int32_t n, const float *x, const float *y, double k,
   BHTree t;
   t.n = n;
   t.rsize = root[2];
-  std::vector<uint32_t> keys((size_t)n);
+  const float mdf = (float)min_dist;
+  const float th2 = theta * theta, md2 = mdf * mdf, kf = (float)k;
+  // deep keys when a level-15 cell is not accepted by every point
+  const float s15 = std::ldexp(root[2], -15);
+  t.deep = s15 * s15 >= th2 * md2;
+  t.kb = t.deep ? 54 : 30;
+  std::vector<uint32_t> keys((size_t)n), sub(t.deep ? (size_t)n : 0);
   or_bh_keys(n, x, y, root, keys.data());
+  if (t.deep)
+    for (int32_t i = 0; i < n; ++i)
+      sub[i] = interleave15(q_sub(x[i], root[0], root[2], q15(x[i], root[0], root[2])),
+                            q_sub(y[i], root[1], root[2], q15(y[i], root[1], root[2])));
   t.perm.resize((size_t)n);
   for (int32_t i = 0; i < n; ++i) t.perm[i] = i;
-  std::stable_sort(t.perm.begin(), t.perm.end(),
-                   [&](int32_t a, int32_t b) { return keys[a] < keys[b]; });
+  std::stable_sort(t.perm.begin(), t.perm.end(), [&](int32_t a, int32_t b) {
+    if (keys[a] != keys[b]) return keys[a] < keys[b];
+    return t.deep && sub[a] < sub[b];
+  });
+  if (t.deep) {
+    t.lo.resize((size_t)n);
+    for (int32_t s = 0; s < n; ++s) t.lo[s] = sub[t.perm[s]];
+  }
   t.key.resize((size_t)n);
   t.sx.resize((size_t)n);
   t.sy.resize((size_t)n);
@@ -923,8 +959,6 @@ void or_bh_forces(int32_t n, const float *x, const float *y, double k,
   }
   t.nodes.reserve(n > 1 ? (size_t)n - 1 : 1);
   if (n >= 2) t.build(0, n - 1, -1);
-  const float mdf = (float)min_dist;
-  const float th2 = theta * theta, md2 = mdf * mdf, kf = (float)k;
   par_for(n, threads, [&](int32_t s) {
     Walker w{t, k, min_dist, kf, th2, md2, s, t.sx[s], t.sy[s]};
     if (n >= 2 && w.eval(0)) w.open(0);
