@@ -828,9 +828,11 @@ def run_leaves(args, rank, world, local_rank):
 
 
 PREC_METRIC = "density solve precision sweep (field/force rel. L2 vs FP64, tensor TFLOP/s)"
-# plain iterations behind the HPWL delta: few enough that the placement has
-# not contracted (a contracted placement crowds the Barnes-Hut buckets)
-HPWL_ITERS = 3
+# plain iterations after which the HPWL delta is reported, in one run: the
+# reference's plain iteration contracts the netlist within ~100 iterations and
+# amplifies small differences on the way, so early counts show the solve's
+# precision and later ones the divergence of the trajectories
+HPWL_ITERS = (3, 10, 50)
 
 
 def run_precision(args, rank, world, local_rank):
@@ -839,9 +841,9 @@ def run_precision(args, rank, world, local_rank):
     (BF16, TF32, 3xTF32, SIMT FP32; FP32 accumulation throughout), the
     field / force / potential relative L2 error against the FP64 FFT oracle
     (scipy dctn/idctn of force_electrostatic.py), the density stage's device
-    time and GEMM throughput, and the HPWL after HPWL_ITERS plain iterations
-    against the SIMT FP32 run. HPWL and energy are FP64 reductions on the
-    device."""
+    time and GEMM throughput, and the HPWL of a plain run against the SIMT
+    FP32 run after each count of HPWL_ITERS. HPWL and energy are FP64
+    reductions on the device."""
     if rank != 0:
         return
     import fluxion_b200 as fx
@@ -889,8 +891,13 @@ def run_precision(args, rank, world, local_rank):
             cfg = fx.iter_cfg(density_bins=G, dct_precision=code, density_weight=1e-4,
                               cong_cols=512, cong_rows=512)
             x0, y0 = p.gate_x.copy(), p.gate_y.copy()
-            st = d.force_iterate(cfg, HPWL_ITERS, x0, y0)
-            hp[name] = st.hpwl
+            hpwl_at, done = {}, 0
+            for it in HPWL_ITERS:  # one run, continued on the device
+                st = (d.force_iterate(cfg, it, x0, y0) if done == 0
+                      else d.force_iterate(cfg, it - done))
+                done = it
+                hpwl_at[it] = st.hpwl
+            hp[name] = hpwl_at
             print(f"precision sweep: G={G} {name}: {time.perf_counter() - t_phase:.1f} s",
                   file=sys.stderr, flush=True)
             peak = bf16_peak if code == fx.FX_DCT_BF16 else bf16_peak / 2
@@ -902,11 +909,12 @@ def run_precision(args, rank, world, local_rank):
                                                     if code != fx.FX_DCT_SIMT else None),
                          "tensor_frac_of_measured": (flops / (ms * 1e-3) / 1e12 / peak
                                                      if code != fx.FX_DCT_SIMT else None),
-                         "hpwl_after_iters": st.hpwl})
+                         "hpwl_after_iters": {str(k): v for k, v in hpwl_at.items()}})
         for r in rows:
             if r["G"] == G:
-                r["hpwl_delta_vs_fp32"] = ((r["hpwl_after_iters"] - hp["fp32_simt"]) /
-                                           hp["fp32_simt"])
+                r["hpwl_delta_vs_fp32"] = {
+                    str(it): (hp[r["precision"]][it] - hp["fp32_simt"][it]) / hp["fp32_simt"][it]
+                    for it in HPWL_ITERS}
     d.close()
     ctx.close()
     best = max((r for r in rows if r["G"] == 4096 and r["tensor_tflops_executed"]),
