@@ -31,6 +31,21 @@ def test_blif_reader_follows_the_reference_rules(fx):
     assert _nets(c) == [[0, 1, 4], [1, 2], [2, 3, 4], [0, 5], [1, 5]]
 
 
+REF_SMALL_BLIF = Path("/root/reference/HAPR_fluxion_v4/tests/fixtures/small.blif")
+
+
+@pytest.mark.skipif(not REF_SMALL_BLIF.exists(), reason="the reference's fixture is not here")
+def test_blif_reader_on_the_reference_fixture(fx):
+    """The reference's end-to-end fixture (tests/test_integration.py:10-38
+    places it), read where it lies: four .gate lines (AND2 a b -> n1, OR2 c d
+    -> n2, XOR2 n1 n2 -> y, INV n2 -> z). By blif.rs:88-116 the driven nets
+    n1 = {g0, g2} and n2 = {g1, g2, g3} remain; y, z and the primary inputs
+    touch one gate each and are dropped."""
+    c = fx.read_blif(REF_SMALL_BLIF)
+    assert c.num_gates == 4 and c.name == "small"
+    assert _nets(c) == [[0, 2], [1, 2, 3]]
+
+
 def test_blif_reader_rejects_missing_file(fx):
     with pytest.raises(fx.FluxionError, match="open BLIF"):
         fx.read_blif("/nonexistent/x.blif")
