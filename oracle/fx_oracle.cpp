@@ -110,6 +110,45 @@ void or_congestion(int32_t m, const int32_t *net_ptr, const int32_t *net_gate,
   }
 }
 
+// The counts of compute_congestion_cpu (h == v) for large netlists: the same
+// bounding boxes and cell_at, with each covered rectangle added through a
+// 2-D difference array and prefix sums (O(nets + cells) instead of
+// O(sum of rectangle areas)); checked against or_congestion by the tests.
+void or_congestion_counts(int32_t m, const int32_t *net_ptr, const int32_t *net_gate,
+                          const float *x, const float *y, float chip_w, float chip_h,
+                          int64_t cols, int64_t rows, uint32_t *counts) {
+  float cw, ch, cap;
+  or_grid_geometry(chip_w, chip_h, cols, rows, &cw, &ch, &cap);
+  const int64_t ld = cols + 1;
+  std::vector<int64_t> diff((size_t)(ld * (rows + 1)), 0);
+  for (int32_t e = 0; e < m; ++e) {
+    const int32_t b = net_ptr[e], t = net_ptr[e + 1];
+    if (t - b < 2) continue;
+    float min_x = 3.40282347e+38f, max_x = -3.40282347e+38f;
+    float min_y = 3.40282347e+38f, max_y = -3.40282347e+38f;
+    for (int32_t q = b; q < t; ++q) {
+      const float px = x[net_gate[q]], py = y[net_gate[q]];
+      min_x = std::fmin(min_x, px);
+      max_x = std::fmax(max_x, px);
+      min_y = std::fmin(min_y, py);
+      max_y = std::fmax(max_y, py);
+    }
+    const int64_t c0 = or_cell_at(min_x, cw, cols), r0 = or_cell_at(min_y, ch, rows);
+    const int64_t c1 = or_cell_at(max_x, cw, cols), r1 = or_cell_at(max_y, ch, rows);
+    if (c0 > c1 || r0 > r1) continue;
+    diff[(size_t)(r0 * ld + c0)] += 1;
+    diff[(size_t)(r0 * ld + c1 + 1)] -= 1;
+    diff[(size_t)((r1 + 1) * ld + c0)] -= 1;
+    diff[(size_t)((r1 + 1) * ld + c1 + 1)] += 1;
+  }
+  for (int64_t r = 0; r <= rows; ++r)
+    for (int64_t c = 1; c <= cols; ++c) diff[(size_t)(r * ld + c)] += diff[(size_t)(r * ld + c - 1)];
+  for (int64_t r = 1; r <= rows; ++r)
+    for (int64_t c = 0; c <= cols; ++c) diff[(size_t)(r * ld + c)] += diff[(size_t)((r - 1) * ld + c)];
+  for (int64_t r = 0; r < rows; ++r)
+    for (int64_t c = 0; c < cols; ++c) counts[(size_t)(r * cols + c)] = (uint32_t)diff[(size_t)(r * ld + c)];
+}
+
 // compute_congestion_cpu restricted to nets e with e % stride == 0 (the grids
 // are cleared first). Used to time a bounded sample of the reference's
 // congestion loop; the full call is stride 1.

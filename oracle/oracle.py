@@ -99,6 +99,8 @@ def lib() -> C.CDLL:
                                          F64P, F64P]
         L.or_attention_sample.argtypes = [C.c_int32, I32P, I32P, C.c_int32, I32P, I32P,
                                           C.c_int32, I32P, C.c_int32, F32P, I32P, F64P]
+        L.or_congestion_counts.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
+                                           C.c_float, C.c_int64, C.c_int64, U32P]
         _lib = L
     return _lib
 
@@ -149,6 +151,17 @@ def congestion(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows):
                         _p(x, C.c_float), _p(y, C.c_float), chip_w, chip_h, cols, rows,
                         _p(h, C.c_float), _p(v, C.c_float))
     return h, v
+
+
+def congestion_counts(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows):
+    """The counts of compute_congestion_cpu (h == v) through a difference array:
+    O(nets + cells), for full-size netlists."""
+    net_ptr, net_gate, x, y = _i32(net_ptr), _i32(net_gate), _f32(x), _f32(y)
+    out = np.empty(cols * rows, np.uint32)
+    lib().or_congestion_counts(len(net_ptr) - 1, _p(net_ptr, C.c_int32),
+                               _p(net_gate, C.c_int32), _p(x, C.c_float), _p(y, C.c_float),
+                               chip_w, chip_h, cols, rows, _p(out, C.c_uint32))
+    return out
 
 
 def congestion_sample(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows, stride):

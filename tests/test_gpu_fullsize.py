@@ -1,0 +1,111 @@
+"""Parity at the full plain-1M size (1,000,000 gates, 1,200,000 nets, die
+1200 x 1200, 512 x 512 congestion, DCT 1024 x 1024): every stage against the
+oracle on the whole netlist. The literal congestion loop is O(sum of bounding
+box areas), so the counts are checked against the oracle's difference-array
+restatement of it (tested against the literal loop on the CPU); Barnes-Hut
+runs the oracle's walk on all host threads."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+F32_01 = float(np.float32(0.1))
+
+
+@pytest.fixture(scope="module")
+def full(fx):
+    return fx.synth_plain(42, 1_000_000, 1_200_000, 1200.0)
+
+
+@pytest.fixture(scope="module")
+def full_design(fx, ctx, full):
+    d = fx.Design(ctx, full.circuit)
+    yield d
+    d.close()
+
+
+def _rel(ax, ay, bx, by):
+    num = np.sqrt(((np.asarray(ax, np.float64) - bx) ** 2 + (np.asarray(ay, np.float64) - by) ** 2).sum())
+    return num / np.sqrt((np.asarray(bx, np.float64) ** 2 + np.asarray(by, np.float64) ** 2).sum())
+
+
+def test_congestion_and_hpwl(full_design, full, oracle):
+    c, p = full.circuit, full.placement
+    counts, hpwl, tot, mx = full_design.congestion(512, 512, p.gate_x, p.gate_y)
+    want = oracle.congestion_counts(c.net_ptr, c.net_gate, p.gate_x, p.gate_y,
+                                    c.chip_width, c.chip_height, 512, 512)
+    assert np.array_equal(counts, want)
+    ref = oracle.hpwl_f64(c.net_ptr, c.net_gate, p.gate_x, p.gate_y)
+    assert abs(hpwl - ref) <= 1e-12 * ref
+    _, _, cap = oracle.grid_geometry(c.chip_width, c.chip_height, 512, 512)
+    h = want.astype(np.float32)
+    rt, rm = oracle.overflow(h, h, 512, 512, cap)
+    assert mx == rm and abs(tot - rt) <= 5e-3 * max(rt, 1.0)
+
+
+def test_adjacency_and_attraction(full_design, full, oracle):
+    c, p = full.circuit, full.placement
+    ap, ai = full_design.adjacency()
+    rp, ri = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    assert np.array_equal(ap, rp) and np.array_equal(ai, ri)
+    full_design.set_positions(p.gate_x, p.gate_y)
+    fx_, fy_ = full_design.attraction(1.0)
+    ox, oy = oracle.attraction_f32(rp, ri, p.gate_x, p.gate_y, 1.0)
+    assert np.array_equal(fx_, ox) and np.array_equal(fy_, oy)
+    dx, dy = oracle.attraction_f64(rp, ri, p.gate_x, p.gate_y, 1.0)
+    assert _rel(fx_, fy_, dx, dy) < 1e-5
+
+
+def test_barnes_hut_and_one_plain_iteration(fx, full_design, full, oracle):
+    """Keys, sort order and forces of all 1M points bit-exact; then one plain
+    iteration (attraction + Barnes-Hut + damped step, density off) ends on the
+    oracle's positions, and the congestion of those positions matches."""
+    c, p = full.circuit, full.placement
+    d = full_design
+    d.set_positions(p.gate_x, p.gate_y)
+    bx, by, keys, perm, root = d.barnes_hut(0.5, 0.5, 0.1)
+    o = oracle.bh_forces(p.gate_x, p.gate_y, 0.5, 0.5, F32_01, threads=os.cpu_count() or 1)
+    assert np.array_equal(root, o["root"])
+    assert np.array_equal(keys, o["keys"]) and np.array_equal(perm, o["perm"])
+    assert np.array_equal(bx, o["fx32"]) and np.array_equal(by, o["fy32"])
+    assert _rel(bx, by, o["fx"], o["fy"]) < 1e-5
+    cfg = fx.iter_cfg(density_bins=0, cong_cols=512, cong_rows=512)
+    x, y = p.gate_x.copy(), p.gate_y.copy()
+    st = d.force_iterate(cfg, 1, x, y)
+    rp, ri = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    ax, ay = oracle.attraction_f32(rp, ri, p.gate_x, p.gate_y, 1.0)
+    ox, oy = p.gate_x.copy(), p.gate_y.copy()
+    vx, vy = np.zeros_like(ox), np.zeros_like(oy)
+    oracle.integrate(ox, oy, vx, vy, ax + o["fx32"], ay + o["fy32"], 0.1, 0.9,
+                     (0.0, 0.0, c.chip_width, c.chip_height))
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
+    want = oracle.congestion_counts(c.net_ptr, c.net_gate, ox, oy, c.chip_width,
+                                    c.chip_height, 512, 512)
+    counts, hpwl, _, _ = d.congestion(512, 512)
+    assert np.array_equal(counts, want)
+    assert hpwl == st.hpwl
+    assert abs(hpwl - oracle.hpwl_f64(c.net_ptr, c.net_gate, ox, oy)) <= 1e-12 * hpwl
+
+
+def test_density_field_and_forces(fx, full_design, full, oracle):
+    c, p = full.circuit, full.placement
+    full_design.set_positions(p.gate_x, p.gate_y)
+    out = full_design.density(1024, 0.7, 1.0, fx.FX_DCT_SIMT, grids=True)
+    area = (c.gate_widths * c.gate_heights).astype(np.float64)
+    ref = oracle.density_forces(p.gate_x, p.gate_y, area, c.chip_width, c.chip_height, 1024,
+                                0.7, 1.0)
+    assert _rel(out["ex"], out["ey"], ref["ex"], ref["ey"]) < 1e-4
+    assert _rel(out["fx"], out["fy"], ref["fx"], ref["fy"]) < 1e-4
+
+
+def test_hierarchy(fx, full_design, full, oracle):
+    c = full.circuit
+    tree = full_design.partition(fx.part_cfg())
+    ap, ai = full_design.adjacency()
+    ot = oracle.build_hierarchy(c.num_gates, ap, ai, c.chip_width, c.chip_height)
+    assert np.array_equal(tree["leaf_ptr"], ot["leaf_ptr"])
+    assert np.array_equal(tree["leaf_gate"], ot["leaf_gate"])
+    assert np.array_equal(tree["leaf_depth"], ot["leaf_depth"])
+    assert tree["num_nodes"] == ot["num_nodes"]

@@ -115,3 +115,23 @@ def test_leaf_init_ignores_positions(oracle):
     ap = np.zeros(6, np.int32)
     x, y = oracle.place_leaf(gates, ap, np.zeros(0, np.int32), (5.0, 5.0, 10.0, 10.0), 0)
     assert np.allclose(x, [0, 2, 4, 6, 8]) and np.allclose(y, [0, 4, 8, 2, 6])
+
+
+def test_difference_array_congestion_matches_the_literal_loop(oracle):
+    """oracle.congestion_counts (difference array, for full-size checks) gives
+    the literal compute_congestion_cpu counts, edge cases included: pins
+    outside the die, on its edges, negative, NaN, repeated, one-pin nets."""
+    rng = np.random.default_rng(0)
+    n, m = 3000, 2500
+    x = rng.uniform(-5, 105, n).astype(np.float32)
+    y = rng.uniform(-5, 85, n).astype(np.float32)
+    x[:4] = [0.0, 100.0, np.nan, -0.0]
+    y[:4] = [80.0, 0.0, 3.0, np.nan]
+    deg = rng.integers(1, 9, m)
+    ptr = np.concatenate([[0], np.cumsum(deg)]).astype(np.int32)
+    gate = rng.integers(0, n, int(deg.sum())).astype(np.int32)
+    gate[:8] = [0, 1, 2, 2, 3, 0, 1, 3]
+    for cols, rows in [(64, 64), (37, 23), (1, 1)]:
+        h, v = oracle.congestion(ptr, gate, x, y, 100.0, 80.0, cols, rows)
+        c = oracle.congestion_counts(ptr, gate, x, y, 100.0, 80.0, cols, rows)
+        assert np.array_equal(c.astype(np.float32), h) and np.array_equal(h, v)
