@@ -109,3 +109,30 @@ def test_hierarchy(fx, full_design, full, oracle):
     assert np.array_equal(tree["leaf_gate"], ot["leaf_gate"])
     assert np.array_equal(tree["leaf_depth"], ot["leaf_depth"])
     assert tree["num_nodes"] == ot["num_nodes"]
+
+
+def test_leaf_batch_full_size(fx, ctx, oracle):
+    """The batched-leaf workload in full: 16,384 clusters of 16-128 gates, 300
+    iterations, autotuned schedule; every gate bit-identical to the oracle's
+    place_gates_in_leaf, run leaf by leaf on all host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+    s = fx.synth_leaves(42, 16_384, 16, 128, 1.5)
+    c = s.circuit
+    gates = np.arange(c.num_gates, dtype=np.int32)
+    d = fx.Design(ctx, c)
+    try:
+        x, y, _ = d.place_leaves(s.leaf_ptr, gates, s.region, fx.leaf_cfg(force_iterations=300))
+    finally:
+        d.close()
+    ap, ai = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    ox = np.zeros(c.num_gates, np.float32)
+    oy = np.zeros(c.num_gates, np.float32)
+    lp, reg = s.leaf_ptr, s.region.reshape(-1, 4)
+
+    def one(l):  # ctypes releases the GIL during the call
+        oracle.place_leaf(gates[lp[l]:lp[l + 1]], ap, ai, reg[l], 300, 1.0, 0.5, 0.9, 0.1,
+                          ox, oy)
+
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        list(ex.map(one, range(len(lp) - 1)))
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
