@@ -320,6 +320,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     FX_TRY(density_scatter(ctx, d, d->x[d->cur].p, d->y[d->cur].p, G,
                            c.dct_precision, s));
   const int nb = (d->n + kGates - 1) / kGates;
+  bool copied_out = false;  // positions already on their way to x, y
   // One iteration; `last` adds the potential (energy statistic).
   auto step = [&](bool last) -> int {
     if (use_dens) {
@@ -375,6 +376,16 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     timer_end(ctx, FX_STAGE_ATTRACT_INTEGRATE, s, ev);
     d->cur = nxt;
     d->pos_in_box = true;  // the step clamps every position to the die
+    if (last && x) {
+      // the final positions go to the caller's buffers on the second stream
+      // while the congestion of the same positions runs on the first
+      const size_t bytes = (size_t)d->n * 4;
+      FX_CHECK_CUDA(cudaEventRecord(ctx->fork, s));
+      FX_CHECK_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
+      FX_CHECK_CUDA(cudaMemcpyAsync(x, d->x[d->cur].p, bytes, cudaMemcpyDeviceToHost, s2));
+      FX_CHECK_CUDA(cudaMemcpyAsync(y, d->y[d->cur].p, bytes, cudaMemcpyDeviceToHost, s2));
+      copied_out = true;
+    }
     if (use_cong)
       FX_TRY(congestion_run(ctx, d, d->x[d->cur].p, d->y[d->cur].p, c.cong_cols,
                             c.cong_rows, s));
@@ -430,6 +441,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   if (use_bh && iters > 0)
     FX_CHECK_CUDA(cudaMemcpyAsync(&err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (copied_out) FX_CHECK_CUDA(cudaStreamSynchronize(s2));
   if (err) {
     set_error("Barnes-Hut walk stack overflow");
     return FX_EINVAL;
@@ -445,7 +457,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   st.hpwl = res[0];
   st.total_overflow = res[1];
   st.bh_nodes = use_bh ? d->n - 1 : 0;
-  if (x) FX_TRY(fx_design_get_positions(d, x, y));
+  if (x && !copied_out) FX_TRY(fx_design_get_positions(d, x, y));
   if (stats) *stats = st;
   return FX_OK;
 }
