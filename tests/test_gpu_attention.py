@@ -124,10 +124,11 @@ def test_high_fanout_nets(fx, ctx, oracle):
     assert np.array_equal(top, top2) and np.array_equal(sc, sc2)
 
 
-@pytest.mark.parametrize("n_clusters", [100, 5000, 20_000])
-def test_many_clusters_with_big_nets(fx, ctx, oracle, n_clusters):
+@pytest.mark.parametrize("n_clusters,top_k", [(100, 10), (5000, 10), (5000, 40), (20_000, 10)])
+def test_many_clusters_with_big_nets(fx, ctx, oracle, n_clusters, top_k):
     """The three count paths: an n x n matrix per block (n <= 128), a block
-    per row (n <= 16384) and the pair hash table beyond."""
+    per row (n <= 16384) and the pair hash table beyond; top_k 40 takes more
+    selection rounds than the row's keys held per thread."""
     rng = np.random.default_rng(23)
     n_gates = 120_000
     degs = np.where(rng.random(90_000) < 0.01, rng.integers(33, 200, 90_000),
@@ -139,8 +140,8 @@ def test_many_clusters_with_big_nets(fx, ctx, oracle, n_clusters):
     cp = np.concatenate([[0], cuts, [n_gates]]).astype(np.int32)
     d = _design(fx, ctx, n_gates, net_ptr, net_gate)
     try:
-        top, _ = d.attention_level(cp, gates, 10)
+        top, _ = d.attention_level(cp, gates, top_k)
     finally:
         d.close()
-    _, _, _, want = oracle.attention_level_sparse(net_ptr, net_gate, n_gates, cp, gates, 10)
+    _, _, _, want = oracle.attention_level_sparse(net_ptr, net_gate, n_gates, cp, gates, top_k)
     assert np.array_equal(top, want)
