@@ -456,10 +456,16 @@ def run_fluxion(args, rank, world, local_rank):
         else:
             pk = bf16 if args.precision == "bf16" else bf16 / 2
             ps = f"{src} bf16 dense" + ("" if args.precision == "bf16" else " / 2 (tf32)")
+        halves = PREC[args.precision] == 3 and args.bins % 256 == 0
         dens_roof = {"bound": "fp32-pipe" if PREC[args.precision] == 3 else "tensor",
                      "achieved": d_tf, "peak": pk, "unit": "TFLOP/s", "frac": d_tf / pk,
-                     "peak_source": ps, "note": "side stream, overlapped with Barnes-Hut: "
-                                                "its span includes time it yields"}
+                     "peak_source": ps,
+                     "flops": "algorithmic: the dense GEMM form, 6 x 2 G^3 per step",
+                     "executed_tflops": d_tf / 2 if halves else d_tf,
+                     "note": ("the CUDA-core path splits each GEMM in two half-size ones by the "
+                              "DCT's even/odd symmetry (half the executed flops); " if halves
+                              else "") + "side stream, overlapped with Barnes-Hut: its span "
+                                         "includes time it yields"}
     B_iter = sum(b_alg.values())
     it_ms = ms_max / args.steps
 

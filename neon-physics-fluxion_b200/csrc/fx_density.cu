@@ -17,6 +17,7 @@
 // previous GEMM (see density_run).
 // Bin areas are accumulated as 64-bit fixed point so the density is exact
 // and independent of the scatter order.
+#include <algorithm>
 #include <cmath>
 
 #include "fx_internal.h"
@@ -65,6 +66,33 @@ __global__ void dens_charge_kernel(unsigned long long *__restrict__ acc,
     const float v = (float)(a - (double)target);
     acc[i] = 0ull;
     store_operand(v, i, rho, rho_lo, rho_bf);
+  }
+}
+
+// Even/odd halves of a data operand B (G x G, row-major), each G x (G/2):
+// fold (for products with C, whose columns mirror as C[i][G-1-k] =
+// (-1)^i C[i][k]): B[j][k] + B[j][G-1-k] and B[j][k] - B[j][G-1-k];
+// split (for C^T-type operators, whose rows mirror): B[j][2m] and B[j][2m+1].
+__global__ void dct_fold_kernel(const float *__restrict__ B, int G, float *__restrict__ out) {
+  const int h = G >> 1;
+  const size_t half = (size_t)G * h;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t j = i / (size_t)h, k = i - j * (size_t)h;
+    const float a = B[j * G + k], b = B[j * G + (G - 1 - k)];
+    out[i] = a + b;
+    out[half + i] = a - b;
+  }
+}
+
+__global__ void dct_split_kernel(const float *__restrict__ B, int G, float *__restrict__ out) {
+  const int h = G >> 1;
+  const size_t half = (size_t)G * h;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float2 v = reinterpret_cast<const float2 *>(B)[i];  // B[j][2m], B[j][2m+1]
+    out[i] = v.x;
+    out[half + i] = v.y;
   }
 }
 
@@ -143,9 +171,20 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   FX_TRY(w.ey.alloc(cells));
   FX_TRY(w.energy.alloc(4096 + 8));
   FX_TRY(w.force.alloc((size_t)d->n));
+  // The CUDA-core path halves its GEMMs by the DCT's even/odd symmetry when
+  // G is a multiple of 256 (tiles of 128 on each half).
+  w.halves = precision == FX_DCT_SIMT && G % 256 == 0;
   if (precision == FX_DCT_SIMT) {
-    const int sp = sgemm_splits(G, d->ctx->num_sms);
-    if (sp > 1) FX_TRY(w.split_ws.alloc((size_t)sp * cells));
+    int sp = sgemm_splits(G, d->ctx->num_sms);
+    if (w.halves) sp = std::max(sp, half_splits(G, d->ctx->num_sms));
+    if (sp > 1 || w.halves) FX_TRY(w.split_ws.alloc((size_t)sp * cells));
+  }
+  if (w.halves) {
+    FX_TRY(w.c_h.alloc(cells / 2));
+    FX_TRY(w.ct_h.alloc(cells / 2));
+    FX_TRY(w.dx_h.alloc(cells / 2));
+    FX_TRY(w.dy_h.alloc(cells / 2));
+    for (int i = 0; i < 3; ++i) FX_TRY(w.hw[i].alloc(cells));
   }
   const bool split = precision == FX_DCT_FP32, half = precision == FX_DCT_BF16;
   if (split) {
@@ -210,6 +249,29 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
                         half ? w.dxct_bf.p : nullptr, s));
   FX_TRY(upload_operand(dy, precision, w.dyct.p, split ? w.dyct_lo.p : nullptr,
                         half ? w.dyct_bf.p : nullptr, s));
+  if (w.halves) {
+    // [rows 2r | rows 2r+1] of C, first G/2 columns (C's columns mirror);
+    // [columns 2m | columns 2m+1] of C^T, Dx C^T, Dy C^T, first G/2 rows
+    // (their rows mirror): exact slices of the FP64 operators
+    const int h = G / 2;
+    const size_t hh = (size_t)h * h;
+    std::vector<double> chh(2 * hh), cth(2 * hh), dxh(2 * hh), dyh(2 * hh);
+    for (int r = 0; r < h; ++r)
+      for (int k = 0; k < h; ++k) {
+        chh[(size_t)r * h + k] = c[(size_t)(2 * r) * G + k];
+        chh[hh + (size_t)r * h + k] = c[(size_t)(2 * r + 1) * G + k];
+        cth[(size_t)r * h + k] = ct[(size_t)r * G + 2 * k];
+        cth[hh + (size_t)r * h + k] = ct[(size_t)r * G + 2 * k + 1];
+        dxh[(size_t)r * h + k] = dx[(size_t)r * G + 2 * k];
+        dxh[hh + (size_t)r * h + k] = dx[(size_t)r * G + 2 * k + 1];
+        dyh[(size_t)r * h + k] = dy[(size_t)r * G + 2 * k];
+        dyh[hh + (size_t)r * h + k] = dy[(size_t)r * G + 2 * k + 1];
+      }
+    FX_TRY(upload_operand(chh, precision, w.c_h.p, nullptr, nullptr, s));
+    FX_TRY(upload_operand(cth, precision, w.ct_h.p, nullptr, nullptr, s));
+    FX_TRY(upload_operand(dxh, precision, w.dx_h.p, nullptr, nullptr, s));
+    FX_TRY(upload_operand(dyh, precision, w.dy_h.p, nullptr, nullptr, s));
+  }
   FX_CHECK_CUDA(cudaMemsetAsync(w.area_fx.p, 0, cells * 8, s));
   FX_CHECK_CUDA(cudaMemsetAsync(w.energy.p, 0, (4096 + 8) * 8, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
@@ -264,6 +326,36 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   float *WS = precision == FX_DCT_SIMT ? w.split_ws.p : nullptr;
+  if (w.halves) {
+    // each product as two half-size GEMMs on the folded or split operand
+    auto fold = [&](const float *B, float *out) {
+      dct_fold_kernel<<<eb, 256, 0, s>>>(B, G, out);
+      ctx->launches += 1;
+    };
+    auto split = [&](const float *B, float *out) {
+      dct_split_kernel<<<eb, 256, 0, s>>>(B, G, out);
+      ctx->launches += 1;
+    };
+    float *rho = w.buf[0].p, *t1 = w.buf[1].p, *phat = w.buf[2].p, *t3 = w.buf[1].p;
+    float *t4 = w.buf[4].p, *phi = w.buf[3].p;
+    float *h0 = w.hw[0].p, *h1 = w.hw[1].p, *h2 = w.hw[2].p;
+    fold(rho, h0);
+    FX_TRY(gemm_half(ctx, G, w.c_h.p, h0, kHalfRows, 1.f, nullptr, t1, WS, s));
+    fold(t1, h0);
+    FX_TRY(gemm_half(ctx, G, w.c_h.p, h0, kHalfRows, 1.f, w.inv_eig.p, phat, WS, s));
+    split(phat, h1);
+    FX_TRY(gemm_half(ctx, G, w.ct_h.p, h1, kHalfPair, 1.f, nullptr, t3, WS, s));
+    split(t3, h2);
+    FX_TRY(gemm_half(ctx, G, w.dy_h.p, h2, kHalfPair, -1.f, nullptr, w.ey.p, WS, s));
+    if (need_phi)
+      FX_TRY(gemm_half(ctx, G, w.ct_h.p, h2, kHalfPair, 1.f, nullptr, phi, WS, s));
+    FX_TRY(gemm_half(ctx, G, w.dx_h.p, h1, kHalfPair, -1.f, nullptr, t4, WS, s));
+    split(t4, h0);
+    FX_TRY(gemm_half(ctx, G, w.ct_h.p, h0, kHalfPair, 1.f, nullptr, w.ex.p, WS, s));
+    FX_CHECK_LAUNCH();
+    timer_end(ctx, FX_STAGE_DENSITY, s, ev);
+    return FX_OK;
+  }
   const GemmOperands C = K(w.cmat.p, w.cmat_lo.p, w.cmat_bf.p);
   const GemmOperands Ct = K(w.cmat_t.p, w.cmat_t_lo.p, w.cmat_t_bf.p);
   const GemmOperands DxCt = K(w.dxct.p, w.dxct_lo.p, w.dxct_bf.p);
