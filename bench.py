@@ -1012,7 +1012,7 @@ def attention_setup(args, rank):
 def attention_levels(fx, d):
     tree = d.partition(fx.part_cfg())
     lv = fx.hierarchy_levels(tree["leaf_ptr"], tree["leaf_gate"], tree["leaf_depth"])
-    return [(t, cp, cg) for t, (cp, cg) in enumerate(lv) if len(cp) - 1 >= 2]
+    return tree, [(t, cp, cg) for t, (cp, cg) in enumerate(lv) if len(cp) - 1 >= 2]
 
 
 def attention_cpu_sample(c, levels, k_max=16):
@@ -1038,19 +1038,18 @@ def attention_cpu_sample(c, levels, k_max=16):
 def run_attention(args, rank, world, local_rank):
     """(f.4) attention scores, compute_all_attention (attention.rs:33-48),
     over every level of the plain netlist's hierarchy: one step = one
-    fx_attention call per level with host cluster lists in and top-10 lists
-    out. `value` from the device time of the calls (stage events), `e2e` from
-    the calls' wall time; the dense n x n score matrices are not requested
-    (fx_attention returns them on request)."""
+    fx_attention_tree call with the host leaf lists in and every level's
+    top-10 lists out. `value` from the device time of the levels (stage
+    events), `e2e` from the call's wall time; the dense n x n score matrices
+    are not requested (fx_attention returns them per level on request)."""
     syn, fx = attention_setup(args, rank)
     c = syn.circuit
     ctx = fx.Context(local_rank)
     d = fx.Design(ctx, c)
-    levels = attention_levels(fx, d)
-    first = [d.attention_level(cp, cg, ATTN_TOP_K)[0] for _, cp, cg in levels]
+    tree, levels = attention_levels(fx, d)
+    first = d.attention(tree, ATTN_TOP_K)
     for _ in range(max(0, args.warmup - 1)):
-        for _, cp, cg in levels:
-            d.attention_level(cp, cg, ATTN_TOP_K)
+        d.attention(tree, ATTN_TOP_K)
     ctx.synchronize()
     ctx.reset_stage_times()
     ctx.set_profiling(True)
@@ -1059,9 +1058,8 @@ def run_attention(args, rank, world, local_rank):
     t0 = time.perf_counter()
     same = True
     for _ in range(args.steps):
-        for (_, cp, cg), f in zip(levels, first):
-            top, _ = d.attention_level(cp, cg, ATTN_TOP_K)
-            same = same and np.array_equal(top, f)
+        got = d.attention(tree, ATTN_TOP_K)
+        same = same and all(np.array_equal(a["top_k"], b["top_k"]) for a, b in zip(got, first))
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     ctx.set_profiling(False)
@@ -1085,7 +1083,8 @@ def run_attention(args, rank, world, local_rank):
                "sample": f"{k} sampled clusters over {len(levels)} levels through the C++ "
                          "hash-set restatement of compute_level_attention, each phase scaled "
                          "to the whole level"}
-    h2d = sum(4 * (len(cp) + len(cg)) for _, cp, cg in levels)
+    L = len(tree["leaf_ptr"]) - 1
+    h2d = 4 * (2 * L + 1 + len(tree["leaf_gate"])) + 4 * L * len(levels)
     d2h = sum(4 * n * ATTN_TOP_K for n in n_cl)
     out = {"metric": ATTN_METRIC, "value": world * 1e3 / dev_ms, "unit": "passes/s",
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
@@ -1104,7 +1103,7 @@ def run_attention(args, rank, world, local_rank):
                                    "per-row counting (attn_rows_kernel), not bandwidth"},
            "e2e": {"value": world * args.steps / wall, "unit": "passes/s",
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                   "call": "fx_attention per level with host cluster lists"},
+                   "call": "fx_attention_tree with the host leaf lists (one call per pass)"},
            "gpu_launches": launches, "clocks": clk}
     if rank == 0:
         print(json.dumps(out), flush=True)

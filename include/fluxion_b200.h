@@ -205,6 +205,20 @@ int fx_partition(fx_ctx *ctx, fx_design *design, const fx_part_cfg *cfg,
 int fx_attention(fx_ctx *ctx, fx_design *design, int32_t n_clusters,
                  const int32_t *cluster_ptr, const int32_t *cluster_gate, int32_t top_k,
                  int32_t *out_topk, float *out_scores);
+/* Mirrors compute_all_attention (H/src/algorithm/attention.rs:33-48) for a
+ * hierarchy given as its leaves in DFS order (leaf_ptr[L+1] over leaf_gate,
+ * leaf_depth[L], depths <= 62; every internal node has two children, as
+ * build_hierarchy makes them): every depth with at least two clusters
+ * (clusters_at_depth, hierarchy.rs:134-159), in depth order. Per level:
+ * out_level_depth[v], out_level_clusters[v] (n_v, <= 65535) and n_v * top_k
+ * top-k entries appended to out_topk (-1 padded; NULL to size the call).
+ * FX_EINVAL when max_levels or topk_capacity is too small (the error text
+ * gives the sizes); sum n_v <= 2 L. */
+int fx_attention_tree(fx_ctx *ctx, fx_design *design, int32_t n_leaves,
+                      const int32_t *leaf_ptr, const int32_t *leaf_gate,
+                      const int32_t *leaf_depth, int32_t top_k, int32_t max_levels,
+                      int32_t *out_n_levels, int32_t *out_level_depth,
+                      int32_t *out_level_clusters, int64_t topk_capacity, int32_t *out_topk);
 
 /* ---- rows A..F: the plain composite force iteration -------------------- */
 typedef struct fx_iter_cfg {

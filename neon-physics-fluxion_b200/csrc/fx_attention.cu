@@ -16,6 +16,7 @@
 // are integers, so the f32 scores are those of the reference formula (shared
 // as f32 / total as f32, rounded to nearest).
 #include <algorithm>
+#include <functional>
 #include <vector>
 
 #include "fx_internal.h"
@@ -41,6 +42,18 @@ __global__ void attn_map_kernel(int n, int G, int n_gates, const int32_t *__rest
     return;
   }
   if (atomicCAS(cl + g, -1, lo) != -1) atomicOr(bad, 2);
+}
+
+// A level's gate -> cluster map from the gate -> leaf map and the level's
+// leaf -> cluster index (-1: a leaf above the level).
+__global__ void attn_level_map_kernel(int n_gates, const int32_t *__restrict__ gate_leaf,
+                                      const int32_t *__restrict__ leaf_cluster,
+                                      int32_t *__restrict__ cl) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n_gates;
+       g += gridDim.x * blockDim.x) {
+    const int l = gate_leaf[g];
+    cl[g] = l >= 0 ? leaf_cluster[l] : -1;
+  }
 }
 
 // ---- exclusive scan in place: tile sums, scan of the sums, tile scans ------
@@ -634,34 +647,13 @@ __global__ void attn_topk_kernel(int n, int top_k, const int32_t *__restrict__ r
 
 using namespace fx;
 
-extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
-                            const int32_t *cluster_ptr, const int32_t *cluster_gate,
-                            int32_t top_k, int32_t *out_topk, float *out_scores) {
-  if (!ctx || !d || n_clusters < 0 || top_k < 0 || top_k > 1024 ||
-      (n_clusters > 0 && !cluster_ptr)) {
-    set_error("fx_attention: invalid arguments");
-    return FX_EINVAL;
-  }
-  if (n_clusters > 65535) {
-    set_error("fx_attention: %d clusters; at most 65535 per level", n_clusters);
-    return FX_EINVAL;
-  }
-  const int n = n_clusters;
-  if (n == 0) return FX_OK;
-  if (cluster_ptr[0] != 0) {
-    set_error("fx_attention: cluster_ptr[0] must be 0");
-    return FX_EINVAL;
-  }
-  for (int c = 0; c < n; ++c)
-    if (cluster_ptr[c + 1] < cluster_ptr[c]) {
-      set_error("fx_attention: cluster_ptr decreases at %d", c);
-      return FX_EINVAL;
-    }
-  const int G = cluster_ptr[n];
-  if (G > 0 && !cluster_gate) {
-    set_error("fx_attention: cluster_gate is NULL");
-    return FX_EINVAL;
-  }
+// One level's scores and top-k. build_map enqueues on ctx->stream the
+// kernels that fill the gate -> cluster map d_cl (preset to -1) and may set
+// bad[0] (1: a gate out of range, 2: a gate in two clusters).
+using MapBuilder = std::function<int(int32_t *d_cl, int32_t *bad, int *launches)>;
+
+static int level_attention(fx_ctx *ctx, fx_design *d, int n, const MapBuilder &build_map,
+                           int top_k, int32_t *out_topk, float *out_scores) {
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
   AllocScope alloc_scope(ctx->stream);
   cudaStream_t s = ctx->stream;
@@ -674,12 +666,10 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   const size_t nk = top_k > 0 ? (size_t)n * top_k : 1;
   int launches = 0;
   const size_t pp = (size_t)pins + 1, mm = (size_t)m + 1;
-  DevBuf<int32_t> d_cl, d_cptr, d_cgate, d_bad, touch, dc, dn, cnt, mid, big, out;
+  DevBuf<int32_t> d_cl, d_bad, touch, dc, dn, cnt, mid, big, out;
   DevBuf<unsigned long long> npairs, psum;
   DevBuf<float> dense;
   FX_TRY(d_cl.alloc(d->n));
-  FX_TRY(d_cptr.alloc((size_t)n + 1));
-  FX_TRY(d_cgate.alloc(G > 0 ? (size_t)G : 1));
   FX_TRY(d_bad.alloc(3));  // [0] error flags, [1] nets of > 32 pins, [2] of 17..32
   FX_TRY(touch.alloc(n));
   FX_TRY(dc.alloc(pp));
@@ -689,23 +679,13 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   FX_TRY(big.alloc(mm));
   FX_TRY(npairs.alloc(mm));
   FX_TRY(psum.alloc(scan_tiles((long long)mm)));
-  FX_CHECK_CUDA(cudaMemcpyAsync(d_cptr.p, cluster_ptr, ((size_t)n + 1) * 4,
-                                cudaMemcpyHostToDevice, s));
-  if (G > 0)
-    FX_CHECK_CUDA(cudaMemcpyAsync(d_cgate.p, cluster_gate, (size_t)G * 4,
-                                  cudaMemcpyHostToDevice, s));
   FX_CHECK_CUDA(cudaMemsetAsync(d_cl.p, 0xFF, (size_t)d->n * 4, s));
   FX_CHECK_CUDA(cudaMemsetAsync(d_bad.p, 0, 12, s));
   FX_CHECK_CUDA(cudaMemsetAsync(touch.p, 0, (size_t)n * 4, s));
   FX_CHECK_CUDA(cudaMemsetAsync(npairs.p + m, 0, 8, s));  // the total's slot
   cudaEvent_t t0;  // device time of the level, both halves around the host read
   timer_begin(ctx, FX_STAGE_ATTENTION, s, &t0);
-  if (G > 0) {
-    attn_map_kernel<<<(G + 255) / 256, 256, 0, s>>>(n, G, d->n, d_cptr.p, d_cgate.p, d_cl.p,
-                                                    d_bad.p);
-    FX_CHECK_LAUNCH();
-    ++launches;
-  }
+  FX_TRY(build_map(d_cl.p, d_bad.p, &launches));
   if (m > 0) {
     const int tb = std::min((m + 255) / 256, 4 * ctx->num_sms);
     attn_dedupe_thread_kernel<<<tb, 256, 0, s>>>(m, n, d->net_ptr.p, d->net_gate.p, d_cl.p,
@@ -877,5 +857,197 @@ extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     set_error("fx_attention: the pair table overflowed");
     return FX_ECUDA;
   }
+  return FX_OK;
+}
+
+extern "C" int fx_attention(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
+                            const int32_t *cluster_ptr, const int32_t *cluster_gate,
+                            int32_t top_k, int32_t *out_topk, float *out_scores) {
+  if (!ctx || !d || n_clusters < 0 || top_k < 0 || top_k > 1024 ||
+      (n_clusters > 0 && !cluster_ptr)) {
+    set_error("fx_attention: invalid arguments");
+    return FX_EINVAL;
+  }
+  if (n_clusters > 65535) {
+    set_error("fx_attention: %d clusters; at most 65535 per level", n_clusters);
+    return FX_EINVAL;
+  }
+  const int n = n_clusters;
+  if (n == 0) return FX_OK;
+  if (cluster_ptr[0] != 0) {
+    set_error("fx_attention: cluster_ptr[0] must be 0");
+    return FX_EINVAL;
+  }
+  for (int c = 0; c < n; ++c)
+    if (cluster_ptr[c + 1] < cluster_ptr[c]) {
+      set_error("fx_attention: cluster_ptr decreases at %d", c);
+      return FX_EINVAL;
+    }
+  const int G = cluster_ptr[n];
+  if (G > 0 && !cluster_gate) {
+    set_error("fx_attention: cluster_gate is NULL");
+    return FX_EINVAL;
+  }
+  return level_attention(
+      ctx, d, n,
+      [&](int32_t *d_cl, int32_t *bad, int *launches) -> int {
+        cudaStream_t s = ctx->stream;
+        DevBuf<int32_t> d_cptr, d_cgate;  // freed in stream order after the map
+        FX_TRY(d_cptr.alloc((size_t)n + 1));
+        FX_TRY(d_cgate.alloc(G > 0 ? (size_t)G : 1));
+        FX_CHECK_CUDA(cudaMemcpyAsync(d_cptr.p, cluster_ptr, ((size_t)n + 1) * 4,
+                                      cudaMemcpyHostToDevice, s));
+        if (G > 0) {
+          FX_CHECK_CUDA(cudaMemcpyAsync(d_cgate.p, cluster_gate, (size_t)G * 4,
+                                        cudaMemcpyHostToDevice, s));
+          attn_map_kernel<<<(G + 255) / 256, 256, 0, s>>>(n, G, d->n, d_cptr.p, d_cgate.p,
+                                                          d_cl, bad);
+          FX_CHECK_LAUNCH();
+          ++*launches;
+        }
+        return FX_OK;
+      },
+      top_k, out_topk, out_scores);
+}
+
+// All levels of a hierarchy given by its leaves in DFS order and their depths
+// (every internal node has two children, so the depths fix the tree):
+// compute_all_attention (H/src/algorithm/attention.rs:33-48), the levels with
+// at least two clusters in depth order. The leaf lists go up once; each level
+// then needs only its leaf -> cluster index.
+extern "C" int fx_attention_tree(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
+                                 const int32_t *leaf_ptr, const int32_t *leaf_gate,
+                                 const int32_t *leaf_depth, int32_t top_k, int32_t max_levels,
+                                 int32_t *out_n_levels, int32_t *out_level_depth,
+                                 int32_t *out_level_clusters, int64_t topk_capacity,
+                                 int32_t *out_topk) {
+  if (!ctx || !d || n_leaves < 0 || top_k < 0 || top_k > 1024 || max_levels < 0 ||
+      !out_n_levels || (n_leaves > 0 && (!leaf_ptr || !leaf_depth)) ||
+      (max_levels > 0 && (!out_level_depth || !out_level_clusters))) {
+    set_error("fx_attention_tree: invalid arguments");
+    return FX_EINVAL;
+  }
+  *out_n_levels = 0;
+  const int L = n_leaves;
+  if (L == 0) return FX_OK;
+  if (leaf_ptr[0] != 0) {
+    set_error("fx_attention_tree: leaf_ptr[0] must be 0");
+    return FX_EINVAL;
+  }
+  int dmax = 0;
+  for (int l = 0; l < L; ++l) {
+    if (leaf_ptr[l + 1] < leaf_ptr[l] || leaf_depth[l] < 0 || leaf_depth[l] > 62) {
+      set_error("fx_attention_tree: leaf %d: bad range or depth (0..62)", l);
+      return FX_EINVAL;
+    }
+    dmax = std::max(dmax, (int)leaf_depth[l]);
+  }
+  const int G = leaf_ptr[L];
+  if (G > 0 && !leaf_gate) {
+    set_error("fx_attention_tree: leaf_gate is NULL");
+    return FX_EINVAL;
+  }
+  // path of each leaf as a dmax-free binary code (0 = first child); the
+  // depths form a full binary tree iff the codes count up to 2^d - 1
+  std::vector<uint64_t> code((size_t)L, 0);
+  for (int l = 1; l < L; ++l) {
+    uint64_t c = code[l - 1] + 1;
+    const int dp = leaf_depth[l - 1], dl = leaf_depth[l];
+    if (dl >= dp) {
+      c <<= (dl - dp);
+    } else {
+      const int k = dp - dl;
+      if (c & ((1ull << k) - 1ull)) {
+        set_error("fx_attention_tree: leaf depths do not form a full binary tree");
+        return FX_EINVAL;
+      }
+      c >>= k;
+    }
+    code[l] = c;
+  }
+  if (code[L - 1] + 1 != (1ull << leaf_depth[L - 1])) {
+    set_error("fx_attention_tree: leaf depths do not form a full binary tree");
+    return FX_EINVAL;
+  }
+  // per depth: the leaf -> cluster index and the cluster count
+  std::vector<std::vector<int32_t>> lc;
+  std::vector<int32_t> depth, count;
+  int64_t need = 0;
+  for (int t = 0; t <= dmax; ++t) {
+    std::vector<int32_t> m((size_t)L, -1);
+    int nt = 0;
+    uint64_t prev = 0;
+    bool any = false;
+    for (int l = 0; l < L; ++l) {
+      if (leaf_depth[l] < t) continue;
+      const uint64_t pre = code[l] >> (leaf_depth[l] - t);
+      if (!any || pre != prev) ++nt;
+      any = true;
+      prev = pre;
+      m[l] = nt - 1;
+    }
+    if (nt < 2) continue;
+    if (nt > 65535) {
+      set_error("fx_attention_tree: %d clusters at depth %d; at most 65535", nt, t);
+      return FX_EINVAL;
+    }
+    lc.push_back(std::move(m));
+    depth.push_back(t);
+    count.push_back(nt);
+    need += (int64_t)nt * top_k;
+  }
+  const int nl = (int)depth.size();
+  if (nl > max_levels || (out_topk && need > topk_capacity)) {
+    set_error("fx_attention_tree: needs %d levels and %lld top-k slots", nl, (long long)need);
+    return FX_EINVAL;
+  }
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  AllocScope alloc_scope(ctx->stream);
+  cudaStream_t s = ctx->stream;
+  // gate -> leaf, once (the same checks as a level's clusters)
+  DevBuf<int32_t> gate_leaf, d_lp, d_lg, d_err, d_lc;
+  FX_TRY(gate_leaf.alloc(d->n));
+  FX_TRY(d_lp.alloc((size_t)L + 1));
+  FX_TRY(d_lg.alloc(G > 0 ? (size_t)G : 1));
+  FX_TRY(d_err.alloc(1));
+  FX_TRY(d_lc.alloc((size_t)L));
+  FX_CHECK_CUDA(cudaMemsetAsync(gate_leaf.p, 0xFF, (size_t)d->n * 4, s));
+  FX_CHECK_CUDA(cudaMemsetAsync(d_err.p, 0, 4, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(d_lp.p, leaf_ptr, ((size_t)L + 1) * 4, cudaMemcpyHostToDevice, s));
+  if (G > 0) {
+    FX_CHECK_CUDA(cudaMemcpyAsync(d_lg.p, leaf_gate, (size_t)G * 4, cudaMemcpyHostToDevice, s));
+    attn_map_kernel<<<(G + 255) / 256, 256, 0, s>>>(L, G, d->n, d_lp.p, d_lg.p, gate_leaf.p,
+                                                    d_err.p);
+    FX_CHECK_LAUNCH();
+    ctx->launches += 1;
+  }
+  int32_t err = 0;
+  FX_CHECK_CUDA(cudaMemcpyAsync(&err, d_err.p, 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (err) {
+    set_error("fx_attention_tree: %s", (err & 1) ? "a leaf gate is out of range"
+                                                 : "a gate is listed in two leaves");
+    return FX_EINVAL;
+  }
+  int64_t off = 0;
+  for (int v = 0; v < nl; ++v) {
+    const std::vector<int32_t> &m = lc[v];
+    FX_TRY(level_attention(
+        ctx, d, count[v],
+        [&](int32_t *d_cl, int32_t *, int *launches) -> int {
+          FX_CHECK_CUDA(cudaMemcpyAsync(d_lc.p, m.data(), (size_t)L * 4,
+                                        cudaMemcpyHostToDevice, s));
+          attn_level_map_kernel<<<std::min((d->n + 255) / 256, 8 * ctx->num_sms), 256, 0, s>>>(
+              d->n, gate_leaf.p, d_lc.p, d_cl);
+          FX_CHECK_LAUNCH();
+          ++*launches;
+          return FX_OK;
+        },
+        top_k, out_topk ? out_topk + off : nullptr, nullptr));
+    out_level_depth[v] = depth[v];
+    out_level_clusters[v] = count[v];
+    off += (int64_t)count[v] * top_k;
+  }
+  *out_n_levels = nl;
   return FX_OK;
 }

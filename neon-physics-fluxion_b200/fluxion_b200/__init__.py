@@ -10,7 +10,7 @@ from ._lib import (FX_DCT_BF16, FX_DCT_FP32, FX_DCT_SIMT, FX_DCT_TF32, FX_LEAF_A
                    IterStats, LeafCfg, PartCfg, load)
 from .api import (Circuit, Context, Design, Placement, RoutingGrid, Server, Synth,
                   build_adjacency, build_and_compute, compute_congestion, compute_hpwl, default_context,
-                  hierarchy_levels, iter_cfg, leaf_cfg, part_cfg, read_blif, refine_cfg, serve_estimate,
+                  hierarchy_levels, iter_cfg, top_k_lists, leaf_cfg, part_cfg, read_blif, refine_cfg, serve_estimate,
                   synth_leaves, synth_plain, write_def)
 from . import engine
 from .engine import FluxionEngine
@@ -23,5 +23,5 @@ __all__ = [
     "LeafCfg", "FX_LEAF_AUTO", "FX_LEAF_WARP", "FX_LEAF_CTA64", "FX_LEAF_CTA128",
     "FX_LEAF_CTA256", "FX_LEAF_PER_CLUSTER", "refine_cfg", "part_cfg", "PartCfg",
     "FX_PART_EXACT", "FX_PART_FP64", "Server", "serve_estimate", "read_blif", "write_def",
-    "FluxionEngine", "hierarchy_levels",
+    "FluxionEngine", "hierarchy_levels", "top_k_lists",
 ]

@@ -178,6 +178,8 @@ SIGNATURES = {
     "fx_refine_cfg_default": (C.c_int, [C.POINTER(RefineCfg)]),
     "fx_part_cfg_default": (C.c_int, [C.POINTER(PartCfg)]),
     "fx_attention": (C.c_int, [P, P, I32, PI32, PI32, I32, PI32, PF32]),
+    "fx_attention_tree": (C.c_int, [P, P, I32, PI32, PI32, PI32, I32, I32, PI32, PI32, PI32,
+                                    C.c_int64, PI32]),
     "fx_blif_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, I32]),
     "fx_def_write": (C.c_int, [C.c_char_p, C.c_char_p, I32, PF32, PF32, F32, F32, C.c_char_p]),
     "fx_serve_cfg_default": (C.c_int, [C.POINTER(ServeCfg)]),

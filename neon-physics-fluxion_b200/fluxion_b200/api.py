@@ -394,15 +394,42 @@ class Design:
     def attention(self, tree: dict, top_k: int = 10, scores: bool = False) -> list:
         """compute_all_attention (attention.rs:33-48) over a hierarchy from
         partition(): one dict(level_index, top_k, scores) per depth with at
-        least two clusters; top_k is a list of lists as in AttentionLevel."""
+        least two clusters. top_k is an (n, top_k) int32 array, each row the
+        AttentionLevel.top_k list padded with -1 (top_k_lists() gives the
+        lists). Without scores the whole hierarchy goes to fx_attention_tree
+        in one call; with them each level is an fx_attention call (dense
+        n x n)."""
+        if not scores:
+            lp = np.ascontiguousarray(tree["leaf_ptr"], np.int32)
+            lg = np.ascontiguousarray(tree["leaf_gate"], np.int32)
+            ld = np.ascontiguousarray(tree["leaf_depth"], np.int32)
+            L = len(lp) - 1
+            cap = 64
+            depth = np.zeros(cap, np.int32)
+            count = np.zeros(cap, np.int32)
+            top = np.full(max(1, 2 * L * top_k), -1, np.int32)
+            nl = C.c_int32()
+            check(self.lib.fx_attention_tree(self.ctx.handle, self.handle, L,
+                                             ptr(lp, C.c_int32), ptr(lg, C.c_int32),
+                                             ptr(ld, C.c_int32), top_k, cap, C.byref(nl),
+                                             ptr(depth, C.c_int32), ptr(count, C.c_int32),
+                                             len(top), ptr(top, C.c_int32)),
+                  "fx_attention_tree")
+            out, off = [], 0
+            for v in range(nl.value):
+                n = int(count[v])
+                rows = top[off:off + n * top_k].reshape(n, top_k) if top_k else \
+                    np.zeros((n, 0), np.int32)
+                out.append(dict(level_index=int(depth[v]), top_k=rows, scores=None))
+                off += n * top_k
+            return out
         out = []
         for depth, (cp, cg) in enumerate(hierarchy_levels(tree["leaf_ptr"], tree["leaf_gate"],
                                                           tree["leaf_depth"])):
             if len(cp) - 1 < 2:
                 continue
             top, sc = self.attention_level(cp, cg, top_k, scores)
-            out.append(dict(level_index=depth, top_k=[[int(j) for j in r if j >= 0] for r in top],
-                            scores=sc))
+            out.append(dict(level_index=depth, top_k=top, scores=sc))
         return out
 
     # -- congestion refinement ----------------------------------------------------
@@ -436,6 +463,11 @@ class Design:
         if y is not None and ya is not y:
             y[...] = ya
         return st
+
+
+def top_k_lists(top) -> list:
+    """AttentionLevel.top_k (attention.rs:15) from a -1 padded top-k array."""
+    return [[int(j) for j in r if j >= 0] for r in np.asarray(top)]
 
 
 def hierarchy_levels(leaf_ptr, leaf_gate, leaf_depth) -> list:

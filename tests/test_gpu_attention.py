@@ -69,7 +69,7 @@ def test_all_levels_of_a_device_hierarchy(fx, ctx, oracle, plain_small):
         dense = np.zeros_like(lv["scores"])
         dense[r, col] = v
         assert np.array_equal(lv["scores"].view(np.uint32), dense.view(np.uint32))
-        assert lv["top_k"] == [[j for j in row if j >= 0] for row in tk.tolist()]
+        assert fx.top_k_lists(lv["top_k"]) == fx.top_k_lists(tk)
 
 
 def test_edge_cases(fx, ctx, oracle):
@@ -145,3 +145,29 @@ def test_many_clusters_with_big_nets(fx, ctx, oracle, n_clusters, top_k):
         d.close()
     _, _, _, want = oracle.attention_level_sparse(net_ptr, net_gate, n_gates, cp, gates, top_k)
     assert np.array_equal(top, want)
+
+
+def test_whole_hierarchy_call_matches_the_levels(fx, ctx, oracle, plain_small):
+    """fx_attention_tree (one call over the hierarchy) gives the same levels
+    and top-k lists as one fx_attention call per level, and as the oracle."""
+    c = plain_small.circuit
+    d = fx.Design(ctx, c)
+    try:
+        tree = d.partition(fx.part_cfg())
+        whole = d.attention(tree, top_k=10)
+        per_level = d.attention(tree, top_k=10, scores=True)
+        one = d.attention(tree, top_k=1)
+        # malformed trees are refused
+        with pytest.raises(fx.FluxionError):
+            d.attention(dict(tree, leaf_depth=np.ones_like(tree["leaf_depth"])), top_k=10)
+    finally:
+        d.close()
+    assert [lv["level_index"] for lv in whole] == [lv["level_index"] for lv in per_level]
+    assert all(np.array_equal(a["top_k"], b["top_k"]) for a, b in zip(whole, per_level))
+    assert all(np.array_equal(a["top_k"], b["top_k"][:, :1]) for a, b in zip(one, whole))
+    levels = fx.hierarchy_levels(tree["leaf_ptr"], tree["leaf_gate"], tree["leaf_depth"])
+    for lv in whole:
+        cp, cg = levels[lv["level_index"]]
+        _, _, _, tk = oracle.attention_level_sparse(c.net_ptr, c.net_gate, c.num_gates, cp, cg,
+                                                    10)
+        assert fx.top_k_lists(lv["top_k"]) == fx.top_k_lists(tk)
