@@ -127,8 +127,8 @@ def test_high_fanout_nets(fx, ctx, oracle):
 @pytest.mark.parametrize("n_clusters,top_k", [(100, 10), (5000, 10), (5000, 40), (20_000, 10)])
 def test_many_clusters_with_big_nets(fx, ctx, oracle, n_clusters, top_k):
     """The three count paths: an n x n matrix per block (n <= 128), a block
-    per row (n <= 16384) and the pair hash table beyond; top_k 40 takes more
-    selection rounds than the row's keys held per thread."""
+    per row (n <= 16384) and the pair hash table beyond; top-10 and, through
+    the block-per-row path, top-40 lists."""
     rng = np.random.default_rng(23)
     n_gates = 120_000
     degs = np.where(rng.random(90_000) < 0.01, rng.integers(33, 200, 90_000),
