@@ -887,7 +887,10 @@ def run_precision(args, rank, world, local_rank):
                 d.density(G, 0.7, 1.0, code)
             ctx.set_profiling(False)
             ms = ctx.stage_times()["density"][0] / reps
-            flops = 6 * 2.0 * G ** 3 * (3 if code == fx.FX_DCT_FP32 else 1)
+            # executed: the even/odd half GEMMs (G a multiple of 256, not
+            # 3xTF32) do G^3 each instead of 2 G^3; 3xTF32 runs three MMAs
+            halves = G % 256 == 0 and code != fx.FX_DCT_FP32
+            flops = 6 * (1.0 if halves else 2.0) * G ** 3 * (3 if code == fx.FX_DCT_FP32 else 1)
             fld = float(np.sqrt((np.linalg.norm(out["ex"] - ref["ex"]) ** 2 +
                                  np.linalg.norm(out["ey"] - ref["ey"]) ** 2) /
                                 (np.linalg.norm(ref["ex"]) ** 2 + np.linalg.norm(ref["ey"]) ** 2)))

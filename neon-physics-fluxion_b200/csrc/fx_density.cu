@@ -73,26 +73,30 @@ __global__ void dens_charge_kernel(unsigned long long *__restrict__ acc,
 // fold (for products with C, whose columns mirror as C[i][G-1-k] =
 // (-1)^i C[i][k]): B[j][k] + B[j][G-1-k] and B[j][k] - B[j][G-1-k];
 // split (for C^T-type operators, whose rows mirror): B[j][2m] and B[j][2m+1].
-__global__ void dct_fold_kernel(const float *__restrict__ B, int G, float *__restrict__ out) {
+// Outputs go out in the operand formats of the GEMM path (f32 or TF32 head,
+// 3xTF32 residual, bf16), as store_operand writes them.
+__global__ void dct_fold_kernel(const float *__restrict__ B, int G, float *__restrict__ out,
+                                float *__restrict__ out_lo, uint16_t *__restrict__ out_bf) {
   const int h = G >> 1;
   const size_t half = (size_t)G * h;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
        i += (size_t)gridDim.x * blockDim.x) {
     const size_t j = i / (size_t)h, k = i - j * (size_t)h;
     const float a = B[j * G + k], b = B[j * G + (G - 1 - k)];
-    out[i] = a + b;
-    out[half + i] = a - b;
+    store_operand(a + b, i, out, out_lo, out_bf);
+    store_operand(a - b, half + i, out, out_lo, out_bf);
   }
 }
 
-__global__ void dct_split_kernel(const float *__restrict__ B, int G, float *__restrict__ out) {
+__global__ void dct_split_kernel(const float *__restrict__ B, int G, float *__restrict__ out,
+                                 float *__restrict__ out_lo, uint16_t *__restrict__ out_bf) {
   const int h = G >> 1;
   const size_t half = (size_t)G * h;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
        i += (size_t)gridDim.x * blockDim.x) {
     const float2 v = reinterpret_cast<const float2 *>(B)[i];  // B[j][2m], B[j][2m+1]
-    out[i] = v.x;
-    out[half + i] = v.y;
+    store_operand(v.x, i, out, out_lo, out_bf);
+    store_operand(v.y, half + i, out, out_lo, out_bf);
   }
 }
 
@@ -171,20 +175,37 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   FX_TRY(w.ey.alloc(cells));
   FX_TRY(w.energy.alloc(4096 + 8));
   FX_TRY(w.force.alloc((size_t)d->n));
-  // The CUDA-core path halves its GEMMs by the DCT's even/odd symmetry when
-  // G is a multiple of 256 (tiles of 128 on each half).
-  w.halves = precision == FX_DCT_SIMT && G % 256 == 0;
-  if (precision == FX_DCT_SIMT) {
-    int sp = sgemm_splits(G, d->ctx->num_sms);
-    if (w.halves) sp = std::max(sp, half_splits(G, d->ctx->num_sms));
+  // The GEMMs are halved by the DCT's even/odd symmetry when G is a multiple
+  // of 256 (tiles of 128 on each half). Not for 3xTF32: rows G-1-i come out
+  // as E - O, and that difference magnifies the tensor cores' accumulation
+  // error (2.1e-4 instead of 5e-5 at G = 256).
+  w.halves = G % 256 == 0 && precision != FX_DCT_FP32;
+  {
+    int sp = precision == FX_DCT_SIMT ? sgemm_splits(G, d->ctx->num_sms) : 1;
+    if (w.halves && precision == FX_DCT_SIMT) sp = std::max(sp, half_splits(G, d->ctx->num_sms));
     if (sp > 1 || w.halves) FX_TRY(w.split_ws.alloc((size_t)sp * cells));
   }
+  const bool split_fmt = precision == FX_DCT_FP32, bf_fmt = precision == FX_DCT_BF16;
   if (w.halves) {
     FX_TRY(w.c_h.alloc(cells / 2));
     FX_TRY(w.ct_h.alloc(cells / 2));
     FX_TRY(w.dx_h.alloc(cells / 2));
     FX_TRY(w.dy_h.alloc(cells / 2));
     for (int i = 0; i < 3; ++i) FX_TRY(w.hw[i].alloc(cells));
+    if (split_fmt) {
+      FX_TRY(w.c_h_lo.alloc(cells / 2));
+      FX_TRY(w.ct_h_lo.alloc(cells / 2));
+      FX_TRY(w.dx_h_lo.alloc(cells / 2));
+      FX_TRY(w.dy_h_lo.alloc(cells / 2));
+      for (int i = 0; i < 3; ++i) FX_TRY(w.hw_lo[i].alloc(cells));
+    }
+    if (bf_fmt) {
+      FX_TRY(w.c_h_bf.alloc(cells / 2));
+      FX_TRY(w.ct_h_bf.alloc(cells / 2));
+      FX_TRY(w.dx_h_bf.alloc(cells / 2));
+      FX_TRY(w.dy_h_bf.alloc(cells / 2));
+      for (int i = 0; i < 3; ++i) FX_TRY(w.hw_bf[i].alloc(cells));
+    }
   }
   const bool split = precision == FX_DCT_FP32, half = precision == FX_DCT_BF16;
   if (split) {
@@ -267,10 +288,14 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
         dyh[(size_t)r * h + k] = dy[(size_t)r * G + 2 * k];
         dyh[hh + (size_t)r * h + k] = dy[(size_t)r * G + 2 * k + 1];
       }
-    FX_TRY(upload_operand(chh, precision, w.c_h.p, nullptr, nullptr, s));
-    FX_TRY(upload_operand(cth, precision, w.ct_h.p, nullptr, nullptr, s));
-    FX_TRY(upload_operand(dxh, precision, w.dx_h.p, nullptr, nullptr, s));
-    FX_TRY(upload_operand(dyh, precision, w.dy_h.p, nullptr, nullptr, s));
+    FX_TRY(upload_operand(chh, precision, w.c_h.p, split_fmt ? w.c_h_lo.p : nullptr,
+                          bf_fmt ? w.c_h_bf.p : nullptr, s));
+    FX_TRY(upload_operand(cth, precision, w.ct_h.p, split_fmt ? w.ct_h_lo.p : nullptr,
+                          bf_fmt ? w.ct_h_bf.p : nullptr, s));
+    FX_TRY(upload_operand(dxh, precision, w.dx_h.p, split_fmt ? w.dx_h_lo.p : nullptr,
+                          bf_fmt ? w.dx_h_bf.p : nullptr, s));
+    FX_TRY(upload_operand(dyh, precision, w.dy_h.p, split_fmt ? w.dy_h_lo.p : nullptr,
+                          bf_fmt ? w.dy_h_bf.p : nullptr, s));
   }
   FX_CHECK_CUDA(cudaMemsetAsync(w.area_fx.p, 0, cells * 8, s));
   FX_CHECK_CUDA(cudaMemsetAsync(w.energy.p, 0, (4096 + 8) * 8, s));
@@ -327,31 +352,40 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
   ctx->launches += 1;
   float *WS = precision == FX_DCT_SIMT ? w.split_ws.p : nullptr;
   if (w.halves) {
-    // each product as two half-size GEMMs on the folded or split operand
-    auto fold = [&](const float *B, float *out) {
-      dct_fold_kernel<<<eb, 256, 0, s>>>(B, G, out);
+    // each product as two half-size GEMMs on the folded or split operand;
+    // products come back as f32 and the folds write the GEMM formats
+    auto H = [&](int i) {
+      return GemmOperands{w.hw[i].p, split ? w.hw_lo[i].p : nullptr,
+                          half ? w.hw_bf[i].p : nullptr};
+    };
+    auto fold = [&](const float *B, const GemmOperands &o) {
+      dct_fold_kernel<<<eb, 256, 0, s>>>(B, G, o.f32, o.lo, o.bf);
       ctx->launches += 1;
     };
-    auto split = [&](const float *B, float *out) {
-      dct_split_kernel<<<eb, 256, 0, s>>>(B, G, out);
+    auto split_k = [&](const float *B, const GemmOperands &o) {
+      dct_split_kernel<<<eb, 256, 0, s>>>(B, G, o.f32, o.lo, o.bf);
       ctx->launches += 1;
     };
+    const GemmOperands Ch = K(w.c_h.p, w.c_h_lo.p, w.c_h_bf.p);
+    const GemmOperands Cth = K(w.ct_h.p, w.ct_h_lo.p, w.ct_h_bf.p);
+    const GemmOperands Dxh = K(w.dx_h.p, w.dx_h_lo.p, w.dx_h_bf.p);
+    const GemmOperands Dyh = K(w.dy_h.p, w.dy_h_lo.p, w.dy_h_bf.p);
     float *rho = w.buf[0].p, *t1 = w.buf[1].p, *phat = w.buf[2].p, *t3 = w.buf[1].p;
     float *t4 = w.buf[4].p, *phi = w.buf[3].p;
-    float *h0 = w.hw[0].p, *h1 = w.hw[1].p, *h2 = w.hw[2].p;
-    fold(rho, h0);
-    FX_TRY(gemm_half(ctx, G, w.c_h.p, h0, kHalfRows, 1.f, nullptr, t1, WS, s));
-    fold(t1, h0);
-    FX_TRY(gemm_half(ctx, G, w.c_h.p, h0, kHalfRows, 1.f, w.inv_eig.p, phat, WS, s));
-    split(phat, h1);
-    FX_TRY(gemm_half(ctx, G, w.ct_h.p, h1, kHalfPair, 1.f, nullptr, t3, WS, s));
-    split(t3, h2);
-    FX_TRY(gemm_half(ctx, G, w.dy_h.p, h2, kHalfPair, -1.f, nullptr, w.ey.p, WS, s));
+    float *P = w.split_ws.p;
+    fold(rho, H(0));
+    FX_TRY(gemm_half(ctx, precision, G, Ch, H(0), kHalfRows, 1.f, nullptr, t1, P, s));
+    fold(t1, H(0));
+    FX_TRY(gemm_half(ctx, precision, G, Ch, H(0), kHalfRows, 1.f, w.inv_eig.p, phat, P, s));
+    split_k(phat, H(1));
+    FX_TRY(gemm_half(ctx, precision, G, Cth, H(1), kHalfPair, 1.f, nullptr, t3, P, s));
+    split_k(t3, H(2));
+    FX_TRY(gemm_half(ctx, precision, G, Dyh, H(2), kHalfPair, -1.f, nullptr, w.ey.p, P, s));
     if (need_phi)
-      FX_TRY(gemm_half(ctx, G, w.ct_h.p, h2, kHalfPair, 1.f, nullptr, phi, WS, s));
-    FX_TRY(gemm_half(ctx, G, w.dx_h.p, h1, kHalfPair, -1.f, nullptr, t4, WS, s));
-    split(t4, h0);
-    FX_TRY(gemm_half(ctx, G, w.ct_h.p, h0, kHalfPair, 1.f, nullptr, w.ex.p, WS, s));
+      FX_TRY(gemm_half(ctx, precision, G, Cth, H(2), kHalfPair, 1.f, nullptr, phi, P, s));
+    FX_TRY(gemm_half(ctx, precision, G, Dxh, H(1), kHalfPair, -1.f, nullptr, t4, P, s));
+    split_k(t4, H(0));
+    FX_TRY(gemm_half(ctx, precision, G, Cth, H(0), kHalfPair, 1.f, nullptr, w.ex.p, P, s));
     FX_CHECK_LAUNCH();
     timer_end(ctx, FX_STAGE_DENSITY, s, ev);
     return FX_OK;

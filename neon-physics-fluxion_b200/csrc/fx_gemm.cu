@@ -8,6 +8,8 @@ namespace fx {
 int gemm_nt_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
                const GemmOperands &B, const float *S, const GemmOperands &D,
                cudaStream_t s);
+int gemm_half_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
+                 const GemmOperands &Bh, float *part, cudaStream_t s);
 
 constexpr int kBM = 128, kBN = 128, kBK = 16;
 
@@ -229,19 +231,26 @@ int half_splits(int G, int num_sms) {
   return s;
 }
 
-int gemm_half(fx_ctx *ctx, int G, const float *Ah, const float *Bh, int mode, float sign,
-              const float *S, float *D, float *part, cudaStream_t s) {
+int gemm_half(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
+              const GemmOperands &Bh, int mode, float sign, const float *S, float *D,
+              float *part, cudaStream_t s) {
   if (G % 256 != 0) {
     set_error("gemm_half: G=%d is not a multiple of 256", G);
     return FX_EINVAL;
   }
-  const int splits = half_splits(G, ctx->num_sms);
-  dim3 grid(G / kBN, (G / 2) / kBM, 2 * splits);
-  sgemm_half_kernel<<<grid, 256, 0, s>>>(Ah, Bh, G, splits, part);
+  int splits = 1;
+  if (precision == FX_DCT_SIMT) {
+    splits = half_splits(G, ctx->num_sms);
+    dim3 grid(G / kBN, (G / 2) / kBM, 2 * splits);
+    sgemm_half_kernel<<<grid, 256, 0, s>>>(Ah.f32, Bh.f32, G, splits, part);
+    ctx->launches += 1;
+  } else {
+    FX_TRY(gemm_half_tc(ctx, precision, G, Ah, Bh, part, s));
+  }
   sgemm_half_reduce_kernel<<<ctx->num_sms * 8, 256, 0, s>>>(part, splits, G, mode, sign, S, D,
                                                             nullptr, nullptr);
   FX_CHECK_LAUNCH();
-  ctx->launches += 2;
+  ctx->launches += 1;
   return FX_OK;
 }
 

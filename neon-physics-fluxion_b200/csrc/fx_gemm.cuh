@@ -68,14 +68,17 @@ int gemm_nt(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
             cudaStream_t s, float *split_ws = nullptr);
 int sgemm_splits(int G, int num_sms);
 
-// Even/odd halves of a DCT-stage GEMM on the CUDA cores (G a multiple of 256):
-// Ah holds two (G/2) x (G/2) operator halves, Bh the two G x (G/2) halves of
-// the folded or split data operand; kHalfRows interleaves the results as
-// even/odd rows, kHalfPair writes rows r and G-1-r as E + O and sign (E - O).
-// part: half_splits(G, sms) * G * G floats of split-K partials.
+// Even/odd halves of a DCT-stage GEMM (G a multiple of 256), on the CUDA
+// cores (FX_DCT_SIMT) or the tensor cores: Ah holds two (G/2) x (G/2)
+// operator halves, Bh the two G x (G/2) halves of the folded or split data
+// operand, each in the formats of `precision`; kHalfRows interleaves the
+// results as even/odd rows, kHalfPair writes rows r and G-1-r as E + O and
+// sign (E - O); D gets f32 values. part: half_splits(G, sms) * G * G floats
+// (SIMT split-K partials) or G * G (tensor cores).
 constexpr int kHalfRows = 0, kHalfPair = 1;
 int half_splits(int G, int num_sms);
-int gemm_half(fx_ctx *ctx, int G, const float *Ah, const float *Bh, int mode, float sign,
-              const float *S, float *D, float *part, cudaStream_t s);
+int gemm_half(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
+              const GemmOperands &Bh, int mode, float sign, const float *S, float *D,
+              float *part, cudaStream_t s);
 
 }  // namespace fx

@@ -141,10 +141,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
                const __grid_constant__ CUtensorMap tAlo,
                const __grid_constant__ CUtensorMap tB,
-               const __grid_constant__ CUtensorMap tBlo, int G,
-               const float *__restrict__ S, float *__restrict__ D,
+               const __grid_constant__ CUtensorMap tBlo, int G, int K, int a_batch_rows,
+               int b_batch_rows, const float *__restrict__ S, float *__restrict__ D,
                float *__restrict__ Dlo, uint16_t *__restrict__ Dbf,
-               unsigned int *__restrict__ err) {
+               float *__restrict__ part, unsigned int *__restrict__ err) {
   using Cfg = TcCfg<PREC>;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -162,7 +162,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int bm = blockIdx.y * kTcBM, bn = blockIdx.x * kTcBN;
-  const int KB = G / Cfg::kKBlock;
+  // batch z (half GEMMs): operand rows offset by z * a_batch_rows / b_batch_rows
+  const int am = bm + (int)blockIdx.z * a_batch_rows, bnz = bn + (int)blockIdx.z * b_batch_rows;
+  const int KB = K / Cfg::kKBlock;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::kStages; ++s) {
@@ -200,11 +202,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
       const uint32_t st = base + s * Cfg::kStageBytes;
       mbar_expect_tx(full_bar(s), Cfg::kStageBytes);
       const int x = kb * Cfg::kKBlock;
-      tma_load_2d(st, &tA, full_bar(s), x, bm);
-      tma_load_2d(st + kTileBytes, &tB, full_bar(s), x, bn);
+      tma_load_2d(st, &tA, full_bar(s), x, am);
+      tma_load_2d(st + kTileBytes, &tB, full_bar(s), x, bnz);
       if (PREC == 0) {
-        tma_load_2d(st + 2 * kTileBytes, &tAlo, full_bar(s), x, bm);
-        tma_load_2d(st + 3 * kTileBytes, &tBlo, full_bar(s), x, bn);
+        tma_load_2d(st + 2 * kTileBytes, &tAlo, full_bar(s), x, am);
+        tma_load_2d(st + 3 * kTileBytes, &tBlo, full_bar(s), x, bnz);
       }
       issued = kb + 1;
     }
@@ -265,6 +267,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
       uint32_t v[32];
       tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
       const size_t o = (size_t)r * G + bn + c0;
+      if (part) {  // raw partial of batch z: rows gridDim.y * 128, stride G
+        float *pz = part + (size_t)blockIdx.z * gridDim.y * kTcBM * G;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) pz[o + j] = __uint_as_float(v[j]);
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         float x = __uint_as_float(v[j]);
@@ -304,8 +312,9 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// A G x G row-major operand as a 2-D tensor map with 128 x 128-byte boxes.
-static int make_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
+// A rows x cols row-major operand as a 2-D tensor map with 128 x 128-byte
+// boxes.
+static int make_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap *out) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled is unavailable");
@@ -316,8 +325,8 @@ static int make_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
     return FX_EINVAL;
   }
   const int esz = bf16 ? 2 : 4;
-  const cuuint64_t dims[2] = {(cuuint64_t)G, (cuuint64_t)G};
-  const cuuint64_t strides[1] = {(cuuint64_t)G * esz};
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * esz};
   const cuuint32_t box[2] = {(cuuint32_t)(128 / esz), 128u};
   const cuuint32_t estr[2] = {1u, 1u};
   const CUresult r =
@@ -334,27 +343,30 @@ static int make_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
 
 struct MapKey {
   const void *p;
-  int G;
+  int cols, rows;
   bool bf;
-  bool operator==(const MapKey &o) const { return p == o.p && G == o.G && bf == o.bf; }
+  bool operator==(const MapKey &o) const {
+    return p == o.p && cols == o.cols && rows == o.rows && bf == o.bf;
+  }
 };
 struct MapKeyHash {
   size_t operator()(const MapKey &k) const {
-    return std::hash<const void *>()(k.p) ^ ((size_t)k.G << 1) ^ (size_t)k.bf;
+    return std::hash<const void *>()(k.p) ^ ((size_t)k.cols << 1) ^ ((size_t)k.rows << 21) ^
+           (size_t)k.bf;
   }
 };
 
-static int get_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
+static int get_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap *out) {
   static std::mutex mu;
   static std::unordered_map<MapKey, CUtensorMap, MapKeyHash> cache;
   std::lock_guard<std::mutex> g(mu);
-  const MapKey k{ptr, G, bf16};
+  const MapKey k{ptr, cols, rows, bf16};
   auto it = cache.find(k);
   if (it != cache.end()) {
     *out = it->second;
     return FX_OK;
   }
-  FX_TRY(make_map(ptr, G, bf16, out));
+  FX_TRY(make_map(ptr, cols, rows, bf16, out));
   if (cache.size() >= 4096) cache.clear();  // bounded: designs come and go
   cache.emplace(k, *out);
   return FX_OK;
@@ -362,9 +374,13 @@ static int get_map(const void *ptr, int G, bool bf16, CUtensorMap *out) {
 
 static DevBuf<unsigned int> g_tc_err;
 
+// half == false: D = A B^T on G x G operands (epilogue: S, formats).
+// half == true: the two (G/2) x G x (G/2) products of the even/odd halves
+// (A: 2 x (G/2) x (G/2), B: 2 x G x (G/2)) as raw partials in `part`.
 template <int PREC>
 static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands &B,
-                  const float *S, const GemmOperands &D, cudaStream_t s) {
+                  const float *S, const GemmOperands &D, cudaStream_t s, bool half = false,
+                  float *part = nullptr) {
   using Cfg = TcCfg<PREC>;
   const bool bf = PREC == 2;
   CUtensorMap ta, talo, tb, tblo;
@@ -374,11 +390,13 @@ static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands 
     set_error("gemm_nt: operand format missing for precision %d", PREC);
     return FX_EINVAL;
   }
-  FX_TRY(get_map(pa, G, bf, &ta));
-  FX_TRY(get_map(pb, G, bf, &tb));
+  const int h = G / 2;
+  const int kc = half ? h : G, ar = half ? 2 * h : G, br = half ? 2 * G : G;
+  FX_TRY(get_map(pa, kc, ar, bf, &ta));
+  FX_TRY(get_map(pb, kc, br, bf, &tb));
   if (PREC == 0) {
-    FX_TRY(get_map(A.lo, G, false, &talo));
-    FX_TRY(get_map(B.lo, G, false, &tblo));
+    FX_TRY(get_map(A.lo, kc, ar, false, &talo));
+    FX_TRY(get_map(B.lo, kc, br, false, &tblo));
   } else {
     talo = ta;
     tblo = tb;
@@ -400,9 +418,15 @@ static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands 
       FX_CHECK_CUDA(cudaMemset(g_tc_err.p, 0, 4));
     }
   }
-  dim3 grid(G / kTcBN, G / kTcBM);
-  tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(ta, talo, tb, tblo, G, S, D.f32,
-                                                            D.lo, D.bf, g_tc_err.p);
+  if (half) {
+    dim3 grid(G / kTcBN, h / kTcBM, 2);
+    tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(
+        ta, talo, tb, tblo, G, h, h, G, nullptr, nullptr, nullptr, nullptr, part, g_tc_err.p);
+  } else {
+    dim3 grid(G / kTcBN, G / kTcBM);
+    tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(
+        ta, talo, tb, tblo, G, G, 0, 0, S, D.f32, D.lo, D.bf, nullptr, g_tc_err.p);
+  }
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   return FX_OK;
@@ -417,6 +441,18 @@ int gemm_nt_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
     case FX_DCT_BF16: return launch<2>(ctx, G, A, B, S, D, s);
   }
   set_error("gemm_nt: unknown precision %d", precision);
+  return FX_EINVAL;
+}
+
+int gemm_half_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
+                 const GemmOperands &Bh, float *part, cudaStream_t s) {
+  const GemmOperands none{nullptr, nullptr, nullptr};
+  switch (precision) {
+    case FX_DCT_FP32: return launch<0>(ctx, G, Ah, Bh, nullptr, none, s, true, part);
+    case FX_DCT_TF32: return launch<1>(ctx, G, Ah, Bh, nullptr, none, s, true, part);
+    case FX_DCT_BF16: return launch<2>(ctx, G, Ah, Bh, nullptr, none, s, true, part);
+  }
+  set_error("gemm_half: unknown precision %d", precision);
   return FX_EINVAL;
 }
 

@@ -177,13 +177,16 @@ struct DensityWork {
   DevBuf<double> energy;               // FP64 partials
   DevBuf<float2> force;                // per gate
   DevBuf<float> split_ws;              // SIMT split-K partial tiles
-  // SIMT even/odd path (G a multiple of 256): the half operators
+  // even/odd path (G a multiple of 256): the half operators
   // [C even rows | C odd rows], [C^T even cols | odd cols], Dx C^T, Dy C^T
   // likewise, each (G/2) x (G/2) pair in one buffer of G*G/2; and three
   // folded or split data operands of G*G each
   bool halves = false;
   DevBuf<float> c_h, ct_h, dx_h, dy_h;
-  DevBuf<float> hw[3];
+  DevBuf<float> c_h_lo, ct_h_lo, dx_h_lo, dy_h_lo;      // 3xTF32 residuals
+  DevBuf<uint16_t> c_h_bf, ct_h_bf, dx_h_bf, dy_h_bf;   // bf16 copies
+  DevBuf<float> hw[3], hw_lo[3];
+  DevBuf<uint16_t> hw_bf[3];
   template <class F>
   void for_each(F &&f) {
     f(area_fx); f(cmat); f(cmat_t); f(cmat_lo); f(cmat_t_lo); f(cmat_bf);
@@ -194,7 +197,11 @@ struct DensityWork {
     for (auto &b : bf) f(b);
     f(ex); f(ey); f(energy); f(force); f(split_ws);
     f(c_h); f(ct_h); f(dx_h); f(dy_h);
+    f(c_h_lo); f(ct_h_lo); f(dx_h_lo); f(dy_h_lo);
+    f(c_h_bf); f(ct_h_bf); f(dx_h_bf); f(dy_h_bf);
     for (auto &b : hw) f(b);
+    for (auto &b : hw_lo) f(b);
+    for (auto &b : hw_bf) f(b);
   }
 };
 
