@@ -224,10 +224,13 @@ __global__ void sgemm_half_reduce_kernel(const float *__restrict__ part, int spl
   }
 }
 
+// Split-K of the half GEMMs: the largest power of two (<= 8) that keeps the
+// launch to one 256-thread CTA per SM. A CTA holds half an SM's registers, so
+// the Barnes-Hut kernels that run beside the density stage still find room.
 int half_splits(int G, int num_sms) {
   const int h = G / 2, tiles = 2 * (h / kBM) * (G / kBN);
   int s = 1;
-  while (tiles * 2 * s <= 2 * num_sms && s < 8 && (h / (2 * s)) % kBK == 0) s *= 2;
+  while (tiles * 2 * s <= num_sms && s < 8 && (h / (2 * s)) % kBK == 0) s *= 2;
   return s;
 }
 
