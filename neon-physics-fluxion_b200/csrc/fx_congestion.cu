@@ -183,6 +183,10 @@ cong_scan_cols_kernel(int32_t *__restrict__ diff, uint32_t *__restrict__ counts,
 int congestion_run(fx_ctx *ctx, fx_design *d, const float *dx,
                    const float *dy, int cols, int rows, cudaStream_t s) {
   CongWork &w = d->cong;
+  if ((int64_t)(cols + 1) * (rows + 1) > (int64_t)INT32_MAX) {  // corner indexes are 31-bit
+    set_error("congestion grid %d x %d too large", cols, rows);
+    return FX_EINVAL;
+  }
   if (w.cols != cols || w.rows != rows || !w.diff.p) {
     const size_t cells1 = (size_t)(cols + 1) * (rows + 1);
     FX_TRY(w.diff.alloc(cells1));

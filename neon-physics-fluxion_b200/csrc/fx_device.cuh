@@ -117,7 +117,8 @@ __device__ __forceinline__ void agg_add_u64(unsigned long long *base, long long 
 // Adds the same constant `v` from every lane naming idx (>= 0).
 __device__ __forceinline__ void agg_add_const_i32(int *base, long long idx, int v) {
   const unsigned lane = threadIdx.x & 31u;
-  const unsigned peers = __match_any_sync(0xffffffffu, idx);
+  // indexes fit 31 bits: a 32-bit match is the cheaper instruction
+  const unsigned peers = __match_any_sync(0xffffffffu, (int)idx);
   if (idx >= 0 && lane == (unsigned)(__ffs(peers) - 1))
     atomicAdd(base + idx, v * __popc(peers));
 }
