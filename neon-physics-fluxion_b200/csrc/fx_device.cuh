@@ -99,7 +99,8 @@ __device__ __forceinline__ void last_block_sum(double block_value,
 __device__ __forceinline__ void agg_add_u64(unsigned long long *base, long long idx,
                                             unsigned long long v) {
   const unsigned lane = threadIdx.x & 31u;
-  const unsigned peers = __match_any_sync(0xffffffffu, idx);
+  // indexes fit 31 bits (density bins: G^2 <= 8192^2): a 32-bit match
+  const unsigned peers = __match_any_sync(0xffffffffu, (int)idx);
   const bool alone = __all_sync(0xffffffffu, peers == (1u << lane));
   if (alone) {
     if (idx >= 0) atomicAdd(base + idx, v);
