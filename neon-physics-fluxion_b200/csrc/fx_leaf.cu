@@ -31,6 +31,7 @@ namespace fx {
 
 constexpr int kLeafMax = 512;  // gates per leaf held in shared memory
 constexpr int kLeafArrays = 6;  // x, y, vx, vy, fx, fy
+constexpr int kPairUnroll = 4;  // partners whose repulsion terms are in flight at once
 
 struct LeafBatch {
   const int32_t *gptr;     // [L+1] offsets into the gate list (leaf order)
@@ -95,7 +96,28 @@ __device__ void place_leaf(const LeafBatch &b, int leaf, int tid, float *sm, int
         ax = __fadd_rn(ax, __fmul_rn(b.k, __fsub_rn(sx[j], xi)));
         ay = __fadd_rn(ay, __fmul_rn(b.k, __fsub_rn(sy[j], yi)));
       }
-      for (int m = 0; m < n; ++m) {
+      // partners in order m = 0..n-1; four partners' terms are computed
+      // independently (their sqrt and divisions overlap), then added in order
+      int m = 0;
+      for (; m + kPairUnroll <= n; m += kPairUnroll) {
+        float tx[kPairUnroll], ty[kPairUnroll];
+#pragma unroll
+        for (int u = 0; u < kPairUnroll; ++u) {
+          const float dx = __fsub_rn(xi, sx[m + u]), dy = __fsub_rn(yi, sy[m + u]);
+          const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+          const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
+          const float force = __fdiv_rn(b.repel, __fmul_rn(dist, dist));
+          tx[u] = __fdiv_rn(__fmul_rn(force, dx), dist);
+          ty[u] = __fdiv_rn(__fmul_rn(force, dy), dist);
+        }
+#pragma unroll
+        for (int u = 0; u < kPairUnroll; ++u)
+          if (m + u != i) {
+            ax = __fadd_rn(ax, tx[u]);
+            ay = __fadd_rn(ay, ty[u]);
+          }
+      }
+      for (; m < n; ++m) {
         if (m == i) continue;
         const float dx = __fsub_rn(xi, sx[m]), dy = __fsub_rn(yi, sy[m]);
         const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
