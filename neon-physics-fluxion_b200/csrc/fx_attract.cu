@@ -425,7 +425,14 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     }
     if (graph) cudaGraphDestroy(graph);
   }
-  for (; it < iters; ++it) FX_TRY(step(it == iters - 1));
+  for (; it < iters; ++it) {
+    const int rc = step(it == iters - 1);
+    if (rc != FX_OK) {
+      // never return while a copy into the caller's buffers is in flight
+      if (copied_out) cudaStreamSynchronize(s2);
+      return rc;
+    }
+  }
   fx_iter_stats st{};
   st.iterations = iters;
   double res[2] = {0, 0};
