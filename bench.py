@@ -818,7 +818,9 @@ def run_leaves(args, rank, world, local_rank):
                       "schedule": int(sched), "seed": args.seed},
            "roofline": {"bound": "fp32-pipe", "achieved": achieved, "peak": lane_peak,
                         "unit": "Tops/s", "frac": achieved / lane_peak, "traffic": None,
-                        "kernel": "leaf_batch_kernel",
+                        "kernel": ("leaf_pairs_kernel" if sched in (
+                            fx.FX_LEAF_PAIR64, fx.FX_LEAF_PAIR128, fx.FX_LEAF_PAIR256)
+                            else "leaf_batch_kernel"),
                         "peak_source": "nominal 148 SMs x 128 FP32 lanes x 1.965 GHz, 17 ops "
                                        "per unordered pair"},
            "per_cluster_launches_ms": pc_ms, "speedup_vs_per_cluster": pc_ms / kms,

@@ -308,6 +308,9 @@ typedef struct fx_leaf_cfg {
 #define FX_LEAF_CTA128      3 /* 128 threads per leaf                         */
 #define FX_LEAF_CTA256      4 /* one 256-thread block per leaf                */
 #define FX_LEAF_PER_CLUSTER 5 /* baseline: one kernel launch per leaf         */
+#define FX_LEAF_PAIR64      6 /* pair-triangle, 64 threads per leaf (<= 128 gates) */
+#define FX_LEAF_PAIR128     7 /* pair-triangle, 128 threads per leaf (<= 128 gates) */
+#define FX_LEAF_PAIR256     8 /* pair-triangle, 256 threads per leaf (<= 128 gates) */
 
 int fx_leaf_cfg_default(fx_leaf_cfg *cfg);
 

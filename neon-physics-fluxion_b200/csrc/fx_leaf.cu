@@ -175,6 +175,258 @@ leaf_batch_kernel(LeafBatch b, int per_cluster_leaf) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Pair-triangle schedules (leaves of at most kPairMax gates). The reference's
+// pair loop computes each pair's force once and applies it to both gates; so
+// do these. Phase 1 spreads the n(n-1)/2 pair terms t(r, c) = force *
+// (p_r - p_c) / dist (r < c) over every thread of the group; phase 2 has each
+// gate add its terms in partner order m = 0..n-1: -t(m, j) for m < j (the
+// reference's "-= f"), t(j, m) for m > j. The per-gate sums are unchanged, so
+// the results are those of the other schedules bit for bit.
+//
+// The triangle is folded into a rectangle of U = n/2 rows of stride s:
+// triangle row r < U sits at rect row r, columns c - r - 1; row r >= U at
+// rect row n - 2 - r, column c (rows r and n-2-r together hold n entries).
+// Phase 1 walks the rectangle in order (contiguous stores). In phase 2 the
+// lanes of a warp read either one triangle row (contiguous) or one column
+// (step s - 1 or -s): s is the least value >= n with s = 2 (mod 4), which
+// keeps those reads to at most two wavefronts per half-warp.
+constexpr int kPairMax = 128;
+constexpr int kMidUnroll = 8;  // mixed-segment partners loaded ahead of their adds
+
+__host__ __device__ __forceinline__ int pair_rows(int n) { return n >> 1; }
+__host__ __device__ __forceinline__ int pair_stride(int n) { return ((n + 1) | 3) - 1; }
+
+inline size_t pair_smem_bytes(int nmax) {
+  return (size_t)pair_rows(nmax) * pair_stride(nmax) * sizeof(float2) +
+         (size_t)kLeafArrays * nmax * sizeof(float);
+}
+
+// One leaf on a T-thread block. tri: the folded triangle; pos: x0, y0, x1,
+// y1, vx, vy (nmax each; positions double-buffered across iterations).
+template <int T>
+__device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 *tri,
+                                 float *pos) {
+  const int tid = threadIdx.x;
+  const int g0 = b.gptr[leaf];
+  const int n = b.gptr[leaf + 1] - g0;
+  if (n <= 0) return;
+  // buffer p holds x at pos + 2p nmax and y at pos + (2p + 1) nmax
+  float *svx = pos + 4 * nmax, *svy = pos + 5 * nmax;
+  const float4 r4 = b.region[leaf];
+  const float half_w = r4.z / 2.0f, half_h = r4.w / 2.0f;
+  const float min_x = __fsub_rn(r4.x, half_w), min_y = __fsub_rn(r4.y, half_h);
+  const float max_x = __fadd_rn(min_x, r4.z), max_y = __fadd_rn(min_y, r4.w);
+  const float nf = (float)n;
+  for (int i = tid; i < n; i += T) {
+    pos[i] = __fadd_rn(min_x, __fmul_rn(__fdiv_rn((float)i, nf), r4.z));
+    pos[nmax + i] = __fadd_rn(min_y, __fmul_rn(__fdiv_rn((float)((i * 7) % n), nf), r4.w));
+    svx[i] = 0.f;
+    svy[i] = 0.f;
+  }
+  const int U = pair_rows(n), s = pair_stride(n);
+  const int npairs = n * (n - 1) / 2;
+  const int qd = T / n, qm = T % n;    // rect (row, col) advance per stride of T
+  const int dat = qd * s + qm;         // rect address advance (before a row wrap)
+  const int u0 = tid / n, c0 = tid % n;
+  __syncthreads();
+  for (int it = 0; it < b.iters; ++it) {
+    const float *sx = pos + (it & 1) * 2 * nmax, *sy = sx + nmax;
+    float *nx = pos + ((it & 1) ^ 1) * 2 * nmax, *ny = nx + nmax;
+    // attraction of the gates this thread owns (it reads only this
+    // iteration's positions, so its load chain runs while every warp is busy
+    // with phase 1); phase 2 continues these sums with the pair terms
+    constexpr int kOwn = (kPairMax + T - 1) / T;
+    float atx[kOwn], aty[kOwn];
+#pragma unroll
+    for (int g = 0; g < kOwn; ++g) {
+      const int j = tid + g * T;
+      float ax = 0.f, ay = 0.f;
+      if (j < n) {
+        const float xj = sx[j], yj = sy[j];
+        const int a0 = b.aptr[g0 + j], a1 = b.aptr[g0 + j + 1];
+        for (int e = a0; e < a1; ++e) {
+          const int o = b.aidx[e];
+          ax = __fadd_rn(ax, __fmul_rn(b.k, __fsub_rn(sx[o], xj)));
+          ay = __fadd_rn(ay, __fmul_rn(b.k, __fsub_rn(sy[o], yj)));
+        }
+      }
+      atx[g] = ax;
+      aty[g] = ay;
+    }
+    // phase 1: pair terms, kPairUnroll rect entries per thread in flight.
+    // Entry q = (u, col) = (q / n, q % n): c1 = u + 1 + col < n puts it in the
+    // first segment (r = u, c = c1), else the second (r = n-2-u, c = col).
+    // The n(n-1)/2 valid entries are exactly q < npairs (for even n the
+    // unused half of the last rect row comes last).
+    int u = u0, col = c0, nu = n - 2 - u0, at = u0 * s + c0;
+    for (int q = tid; q < npairs; q += kPairUnroll * T) {
+      float2 t[kPairUnroll];
+      int at_k[kPairUnroll];
+      bool ok[kPairUnroll];
+#pragma unroll
+      for (int k = 0; k < kPairUnroll; ++k) {
+        const int c1 = u + 1 + col;
+        const bool first = c1 < n;
+        ok[k] = q + k * T < npairs;
+        at_k[k] = at;
+        const int rr = ok[k] ? (first ? u : nu) : 0, cc = ok[k] ? (first ? c1 : col) : 0;
+        const float dx = __fsub_rn(sx[rr], sx[cc]), dy = __fsub_rn(sy[rr], sy[cc]);
+        const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
+        const float force = __fdiv_rn(b.repel, __fmul_rn(dist, dist));
+        t[k] = make_float2(__fdiv_rn(__fmul_rn(force, dx), dist),
+                           __fdiv_rn(__fmul_rn(force, dy), dist));
+        col += qm;
+        u += qd;
+        nu -= qd;
+        at += dat;
+        if (col >= n) {
+          col -= n;
+          ++u;
+          --nu;
+          at += s - n;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kPairUnroll; ++k)
+        if (ok[k]) tri[at_k[k]] = t[k];
+    }
+    __syncthreads();
+    // phase 2: the pair terms in partner order after the attraction; damped step
+#pragma unroll
+    for (int g = 0; g < kOwn; ++g) {
+      const int j = tid + g * T;
+      if (j >= n) break;
+      const float xj = sx[j], yj = sy[j];
+      float ax = atx[g], ay = aty[g];
+      // Partner m < j adds -t(m, j) (row m), m > j adds t(j, m) (row j);
+      // a + (-t) is a - t. The warp's gates are w..w+31, so partners below w
+      // are column reads for every lane (A: rows < U, address step s - 1;
+      // B: rows >= U, step -s), partners from w + 32 on are row reads (D,
+      // step 1), and only the 32 partners in between (C) need per-lane code.
+      const int w = j - (tid & 31);
+      const int eA = min(w, U);
+      {
+        const float2 *p = tri + (j - 1);
+        const int st = s - 1;
+        int m = 0;
+#pragma unroll 8
+        for (; m < eA; ++m, p += st) {
+          const float2 v = *p;
+          ax = __fsub_rn(ax, v.x);
+          ay = __fsub_rn(ay, v.y);
+        }
+      }
+      {
+        const float2 *p = tri + ((n - 2 - U) * s + j);
+#pragma unroll 8
+        for (int m = U; m < w; ++m, p -= s) {
+          const float2 v = *p;
+          ax = __fsub_rn(ax, v.x);
+          ay = __fsub_rn(ay, v.y);
+        }
+      }
+      const int rowbase = j < U ? j * s - j - 1 : (n - 2 - j) * s;
+      const int eC = min(w + 32, n);
+      for (int m = w; m < eC; m += kMidUnroll) {  // loads ahead, exact sign flips
+        float2 v[kMidUnroll];
+        unsigned int neg[kMidUnroll];
+        bool use[kMidUnroll];
+#pragma unroll
+        for (int k = 0; k < kMidUnroll; ++k) {
+          const int mm = m + k;
+          use[k] = mm < eC && mm != j;
+          const int ca = mm < U ? mm * (s - 1) + j - 1 : (n - 2 - mm) * s + j;
+          neg[k] = mm < j ? 0x80000000u : 0u;
+          v[k] = tri[use[k] ? (mm < j ? ca : rowbase + mm) : 0];
+        }
+#pragma unroll
+        for (int k = 0; k < kMidUnroll; ++k)
+          if (use[k]) {
+            ax = __fadd_rn(ax, __uint_as_float(__float_as_uint(v[k].x) ^ neg[k]));
+            ay = __fadd_rn(ay, __uint_as_float(__float_as_uint(v[k].y) ^ neg[k]));
+          }
+      }
+      {
+        const float2 *p = tri + rowbase;
+#pragma unroll 8
+        for (int m = eC; m < n; ++m) {
+          const float2 v = p[m];
+          ax = __fadd_rn(ax, v.x);
+          ay = __fadd_rn(ay, v.y);
+        }
+      }
+      const float vx = __fmul_rn(__fadd_rn(svx[j], __fmul_rn(ax, b.dt)), b.damping);
+      const float vy = __fmul_rn(__fadd_rn(svy[j], __fmul_rn(ay, b.dt)), b.damping);
+      svx[j] = vx;
+      svy[j] = vy;
+      nx[j] = rclamp(__fadd_rn(xj, __fmul_rn(vx, b.dt)), min_x, max_x);
+      ny[j] = rclamp(__fadd_rn(yj, __fmul_rn(vy, b.dt)), min_y, max_y);
+    }
+    __syncthreads();
+  }
+  const float *fx_ = pos + (b.iters & 1) * 2 * nmax, *fy_ = fx_ + nmax;
+  for (int i = tid; i < n; i += T) {
+    const int g = b.gate[g0 + i];
+    b.out_x[g] = fx_[i];
+    b.out_y[g] = fy_[i];
+  }
+}
+
+// One T-thread block per leaf at a time, pulling leaves from the counter.
+template <int T>
+__global__ void __launch_bounds__(T, 3) leaf_pairs_kernel(LeafBatch b, int nmax) {
+  extern __shared__ float4 lpair[];
+  float2 *tri = reinterpret_cast<float2 *>(lpair);
+  float *pos = reinterpret_cast<float *>(tri + (size_t)pair_rows(nmax) * pair_stride(nmax));
+  __shared__ int next;
+  while (true) {
+    if (threadIdx.x == 0) {
+      const unsigned int w = atomicAdd(b.counter, 1u);
+      next = w < (unsigned)b.n_leaves ? b.order[w] : -1;
+    }
+    __syncthreads();
+    const int leaf = next;
+    __syncthreads();
+    if (leaf < 0) break;
+    place_leaf_pairs<T>(b, leaf, nmax, tri, pos);
+  }
+}
+
+template <int T>
+static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, int nmax, cudaStream_t s) {
+  if (nmax > kPairMax) {
+    set_error("pair schedules take leaves of at most %d gates (largest: %d)", kPairMax, nmax);
+    return FX_EINVAL;
+  }
+  if (nmax < 1) nmax = 1;
+  const size_t smem = pair_smem_bytes(nmax);
+  {
+    static std::mutex mu;
+    static bool attr = false;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!attr) {
+      FX_CHECK_CUDA(cudaFuncSetAttribute(leaf_pairs_kernel<T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pair_smem_bytes(kPairMax)));
+      attr = true;
+    }
+  }
+  int per_sm = 0;
+  FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_pairs_kernel<T>,
+                                                               T, smem));
+  if (per_sm < 1) per_sm = 1;
+  int grid = ctx->num_sms * per_sm;
+  if (grid > b.n_leaves) grid = b.n_leaves;
+  if (grid < 1) grid = 1;
+  FX_CHECK_CUDA(cudaMemsetAsync(b.counter, 0, 4, s));
+  leaf_pairs_kernel<T><<<grid, T, smem, s>>>(b, nmax);
+  FX_CHECK_LAUNCH();
+  ctx->launches += 1;
+  return FX_OK;
+}
+
 // Host-side leaf structures: in-leaf adjacency in the reference's order and
 // a largest-first processing order.
 struct LeafHost {
@@ -259,9 +511,12 @@ static int launch_leaf(fx_ctx *ctx, const LeafBatch &b, bool per_cluster,
   return FX_OK;
 }
 
-static int run_schedule(fx_ctx *ctx, const LeafBatch &b, int schedule,
+static int run_schedule(fx_ctx *ctx, const LeafBatch &b, int schedule, int nmax,
                         cudaStream_t s) {
   switch (schedule) {
+    case FX_LEAF_PAIR64: return launch_pairs<64>(ctx, b, nmax, s);
+    case FX_LEAF_PAIR128: return launch_pairs<128>(ctx, b, nmax, s);
+    case FX_LEAF_PAIR256: return launch_pairs<256>(ctx, b, nmax, s);
     case FX_LEAF_WARP: return launch_leaf<32>(ctx, b, false, s);
     case FX_LEAF_CTA64: return launch_leaf<64>(ctx, b, false, s);
     case FX_LEAF_CTA128: return launch_leaf<128>(ctx, b, false, s);
@@ -314,6 +569,8 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
   LeafHost h;
   FX_TRY(build_leaf_host(d, n_leaves, leaf_ptr, leaf_gate, h));
   const int32_t G = leaf_ptr[n_leaves];
+  int nmax = 0;
+  for (int l = 0; l < n_leaves; ++l) nmax = std::max(nmax, leaf_ptr[l + 1] - leaf_ptr[l]);
   DevBuf<int32_t> gptr, gate, aptr, order;
   DevBuf<int16_t> aidx;
   DevBuf<float4> reg;
@@ -367,9 +624,11 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
     cudaEvent_t e0, e1;
     FX_CHECK_CUDA(cudaEventCreate(&e0));
     FX_CHECK_CUDA(cudaEventCreate(&e1));
-    for (int sc : {FX_LEAF_WARP, FX_LEAF_CTA64, FX_LEAF_CTA128, FX_LEAF_CTA256}) {
+    for (int sc : {FX_LEAF_WARP, FX_LEAF_CTA64, FX_LEAF_CTA128, FX_LEAF_CTA256,
+                   FX_LEAF_PAIR64, FX_LEAF_PAIR128, FX_LEAF_PAIR256}) {
+      if (sc >= FX_LEAF_PAIR64 && nmax > kPairMax) continue;
       FX_CHECK_CUDA(cudaEventRecord(e0, s));
-      int rc = run_schedule(ctx, b, sc, s);
+      int rc = run_schedule(ctx, b, sc, nmax, s);
       if (rc != FX_OK) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -394,7 +653,7 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
   if (!done) {
     cudaEvent_t ev;
     timer_begin(ctx, FX_STAGE_LEAF, s, &ev);
-    FX_TRY(run_schedule(ctx, b, schedule, s));
+    FX_TRY(run_schedule(ctx, b, schedule, nmax, s));
     timer_end(ctx, FX_STAGE_LEAF, s, ev);
   }
   FX_CHECK_CUDA(cudaMemcpyAsync(out_x, ox.p, (size_t)d->n * 4, cudaMemcpyDeviceToHost, s));

@@ -5,7 +5,8 @@ of include/fluxion_b200.h); this package is the host-side mirror of the
 reference's data types and entry points.
 """
 from ._lib import (FX_DCT_BF16, FX_DCT_FP32, FX_DCT_SIMT, FX_DCT_TF32, FX_LEAF_AUTO,
-                   FX_LEAF_CTA64, FX_LEAF_CTA128, FX_LEAF_CTA256, FX_LEAF_PER_CLUSTER,
+                   FX_LEAF_CTA64, FX_LEAF_CTA128, FX_LEAF_CTA256, FX_LEAF_PAIR64,
+                   FX_LEAF_PAIR128, FX_LEAF_PAIR256, FX_LEAF_PER_CLUSTER,
                    FX_LEAF_WARP, FX_PART_EXACT, FX_PART_FP64, FluxionError, IterCfg,
                    IterStats, LeafCfg, PartCfg, load)
 from .api import (Circuit, Context, Design, Placement, RoutingGrid, Server, Synth,
@@ -21,7 +22,8 @@ __all__ = [
     "iter_cfg", "synth_leaves", "synth_plain", "FluxionError", "IterCfg", "IterStats",
     "load", "FX_DCT_FP32", "FX_DCT_TF32", "FX_DCT_BF16", "FX_DCT_SIMT", "leaf_cfg",
     "LeafCfg", "FX_LEAF_AUTO", "FX_LEAF_WARP", "FX_LEAF_CTA64", "FX_LEAF_CTA128",
-    "FX_LEAF_CTA256", "FX_LEAF_PER_CLUSTER", "refine_cfg", "part_cfg", "PartCfg",
+    "FX_LEAF_CTA256", "FX_LEAF_PAIR64", "FX_LEAF_PAIR128", "FX_LEAF_PAIR256",
+    "FX_LEAF_PER_CLUSTER", "refine_cfg", "part_cfg", "PartCfg",
     "FX_PART_EXACT", "FX_PART_FP64", "Server", "serve_estimate", "read_blif", "write_def",
     "FluxionEngine", "hierarchy_levels", "top_k_lists",
 ]

@@ -69,6 +69,9 @@ FX_LEAF_CTA64 = 2
 FX_LEAF_CTA128 = 3
 FX_LEAF_CTA256 = 4
 FX_LEAF_PER_CLUSTER = 5
+FX_LEAF_PAIR64 = 6
+FX_LEAF_PAIR128 = 7
+FX_LEAF_PAIR256 = 8
 
 
 class RefineCfg(C.Structure):

@@ -24,10 +24,20 @@ def batch(fx):
     return fx.synth_leaves(7, 192, 16, 128, 1.5)
 
 
-@pytest.mark.parametrize("schedule", ["warp", "cta64", "cta128", "cta256", "per_cluster"])
+SCHEDULES = ["warp", "cta64", "cta128", "cta256", "pair64", "pair128", "pair256",
+             "per_cluster"]
+
+
+def _code(fx, schedule):
+    return {"warp": fx.FX_LEAF_WARP, "cta64": fx.FX_LEAF_CTA64, "cta128": fx.FX_LEAF_CTA128,
+            "cta256": fx.FX_LEAF_CTA256, "pair64": fx.FX_LEAF_PAIR64,
+            "pair128": fx.FX_LEAF_PAIR128, "pair256": fx.FX_LEAF_PAIR256,
+            "per_cluster": fx.FX_LEAF_PER_CLUSTER}[schedule]
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
 def test_leaf_schedules_bit_exact(fx, ctx, oracle, batch, schedule):
-    code = {"warp": fx.FX_LEAF_WARP, "cta64": fx.FX_LEAF_CTA64, "cta128": fx.FX_LEAF_CTA128,
-            "cta256": fx.FX_LEAF_CTA256, "per_cluster": fx.FX_LEAF_PER_CLUSTER}[schedule]
+    code = _code(fx, schedule)
     d = fx.Design(ctx, batch.circuit)
     try:
         cfg = fx.leaf_cfg(force_iterations=60, schedule=code)
@@ -51,7 +61,8 @@ def test_leaf_autotune_and_full_run(fx, ctx, oracle):
                                     fx.leaf_cfg(force_iterations=300))
     finally:
         d.close()
-    assert used in (fx.FX_LEAF_WARP, fx.FX_LEAF_CTA64, fx.FX_LEAF_CTA128, fx.FX_LEAF_CTA256)
+    assert used in (fx.FX_LEAF_WARP, fx.FX_LEAF_CTA64, fx.FX_LEAF_CTA128, fx.FX_LEAF_CTA256,
+                    fx.FX_LEAF_PAIR64, fx.FX_LEAF_PAIR128, fx.FX_LEAF_PAIR256)
     ox, oy = _oracle_leaves(oracle, s, 300)
     assert np.array_equal(x, ox) and np.array_equal(y, oy)
 
@@ -94,3 +105,69 @@ def test_leaf_too_large_is_rejected(fx, ctx):
             d.place_leaves([0, 600], np.arange(600), [20, 20, 40, 40])
     finally:
         d.close()
+
+
+def _every_size_batch(fx, sizes, seed):
+    """One leaf of each listed size, gates numbered leaf by leaf, nets of 2-4
+    pins inside each leaf, every leaf on its own unit box."""
+    rng = np.random.default_rng(seed)
+    nets, base = [], 0
+    for n in sizes:
+        for _ in range(int(1.5 * n) if n > 1 else 0):
+            k = min(n, int(rng.integers(2, 5)))
+            nets.append(list(base + rng.choice(n, size=k, replace=False)))
+        base += n
+    if not nets:
+        nets = [[0, 0]]
+    circ = fx.Circuit.from_nets(nets, base, float(len(sizes)), 1.0)
+    lp = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    reg = np.array([[l + 0.5, 0.5, 1.0, 1.0] for l in range(len(sizes))], np.float32)
+    return circ, lp, reg
+
+
+@pytest.mark.parametrize("schedule", ["pair64", "pair128", "pair256", "cta64"])
+def test_leaf_every_size_up_to_128(fx, ctx, oracle, schedule):
+    """Leaves of 1..128 gates (both parities of n, a leaf of one gate, the
+    128-gate maximum of the pair schedules), shuffled: every schedule lands on
+    the reference's positions bit for bit."""
+    sizes = np.random.default_rng(3).permutation(np.arange(1, 129))
+    circ, lp, reg = _every_size_batch(fx, sizes, 5)
+    gates = np.arange(circ.num_gates, dtype=np.int32)
+    d = fx.Design(ctx, circ)
+    try:
+        x, y, used = d.place_leaves(lp, gates, reg.ravel(),
+                                    fx.leaf_cfg(force_iterations=25, schedule=_code(fx, schedule)))
+    finally:
+        d.close()
+    assert used == _code(fx, schedule)
+    ap, ai = oracle.build_adjacency(circ.num_gates, circ.net_ptr, circ.net_gate)
+    ox = np.zeros(circ.num_gates, np.float32)
+    oy = np.zeros(circ.num_gates, np.float32)
+    for l in range(len(sizes)):
+        oracle.place_leaf(gates[lp[l]:lp[l + 1]], ap, ai, reg[l], 25, 1.0, 0.5, 0.9, 0.1,
+                          ox, oy)
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
+
+
+def test_leaf_pair_schedules_take_at_most_128_gates(fx, ctx, oracle):
+    """A batch with a 129-gate leaf: the pair schedules refuse it, and the
+    autotuner picks among the others (the result still matches)."""
+    sizes = np.array([129, 40, 7])
+    circ, lp, reg = _every_size_batch(fx, sizes, 9)
+    gates = np.arange(circ.num_gates, dtype=np.int32)
+    d = fx.Design(ctx, circ)
+    try:
+        with pytest.raises(fx.FluxionError):
+            d.place_leaves(lp, gates, reg.ravel(),
+                           fx.leaf_cfg(force_iterations=5, schedule=fx.FX_LEAF_PAIR128))
+        x, y, used = d.place_leaves(lp, gates, reg.ravel(), fx.leaf_cfg(force_iterations=5))
+    finally:
+        d.close()
+    assert used in (fx.FX_LEAF_WARP, fx.FX_LEAF_CTA64, fx.FX_LEAF_CTA128, fx.FX_LEAF_CTA256)
+    ap, ai = oracle.build_adjacency(circ.num_gates, circ.net_ptr, circ.net_gate)
+    ox = np.zeros(circ.num_gates, np.float32)
+    oy = np.zeros(circ.num_gates, np.float32)
+    for l in range(len(sizes)):
+        oracle.place_leaf(gates[lp[l]:lp[l + 1]], ap, ai, reg[l], 5, 1.0, 0.5, 0.9, 0.1,
+                          ox, oy)
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
