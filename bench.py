@@ -73,6 +73,10 @@ def parse():
                          "attention: every level of the 1M-gate hierarchy")
     ap.add_argument("--clusters", type=int, default=16_384, help="leaves: clusters")
     ap.add_argument("--leaf-iters", type=int, default=300, help="leaves: force iterations")
+    ap.add_argument("--leaf-schedule", type=int, default=0,
+                    help="leaves: FX_LEAF_* schedule (0 = autotune)")
+    ap.add_argument("--no-per-cluster", action="store_true",
+                    help="leaves: skip the one-launch-per-cluster comparison run")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent jobs")
@@ -760,8 +764,8 @@ def run_leaves(args, rank, world, local_rank):
     pairs = int((sizes * (sizes - 1) // 2).sum())
     ctx = fx.Context(local_rank)
     d = fx.Design(ctx, c)
-    cfg = fx.leaf_cfg(force_iterations=args.leaf_iters)
-    x, y, sched = d.place_leaves(lp, lg, region, cfg)  # tunes the schedule
+    cfg = fx.leaf_cfg(force_iterations=args.leaf_iters, schedule=args.leaf_schedule)
+    x, y, sched = d.place_leaves(lp, lg, region, cfg)  # tunes the schedule unless given
     cfg.schedule = sched
     for _ in range(max(0, args.warmup - 1)):
         d.place_leaves(lp, lg, region, cfg)
@@ -780,13 +784,15 @@ def run_leaves(args, rank, world, local_rank):
     kms = ctx.stage_times()["leaf"][0] / args.steps
     assert np.array_equal(x, x2) and np.array_equal(y, y2)
     # per-cluster launches (one launch per leaf), once
-    pc = fx.leaf_cfg(force_iterations=args.leaf_iters, schedule=fx.FX_LEAF_PER_CLUSTER)
-    ctx.reset_stage_times()
-    ctx.set_profiling(True)
-    xp, yp, _ = d.place_leaves(lp, lg, region, pc)
-    ctx.set_profiling(False)
-    pc_ms = ctx.stage_times()["leaf"][0]
-    same = bool(np.array_equal(xp, x) and np.array_equal(yp, y))
+    pc_ms, same = None, None
+    if not args.no_per_cluster:
+        pc = fx.leaf_cfg(force_iterations=args.leaf_iters, schedule=fx.FX_LEAF_PER_CLUSTER)
+        ctx.reset_stage_times()
+        ctx.set_profiling(True)
+        xp, yp, _ = d.place_leaves(lp, lg, region, pc)
+        ctx.set_profiling(False)
+        pc_ms = ctx.stage_times()["leaf"][0]
+        same = bool(np.array_equal(xp, x) and np.array_equal(yp, y))
     d.close()
     ctx.close()
     units = args.clusters * args.leaf_iters
@@ -823,7 +829,8 @@ def run_leaves(args, rank, world, local_rank):
                             else "leaf_batch_kernel"),
                         "peak_source": "nominal 148 SMs x 128 FP32 lanes x 1.965 GHz, 17 ops "
                                        "per unordered pair"},
-           "per_cluster_launches_ms": pc_ms, "speedup_vs_per_cluster": pc_ms / kms,
+           "per_cluster_launches_ms": pc_ms,
+           "speedup_vs_per_cluster": None if pc_ms is None else pc_ms / kms,
            "same_result_as_per_cluster": same, "cpu_baseline": cpu,
            "e2e": {"value": world * units * args.steps / wall, "unit": "cluster-iterations/s",
                    "h2d_bytes_per_step": 4 * (len(lp) + c.num_gates) + 16 * args.clusters
