@@ -197,17 +197,29 @@ constexpr int kMidUnroll = 8;  // mixed-segment partners loaded ahead of their a
 __host__ __device__ __forceinline__ int pair_rows(int n) { return n >> 1; }
 __host__ __device__ __forceinline__ int pair_stride(int n) { return ((n + 1) | 3) - 1; }
 
-inline size_t pair_smem_bytes(int nmax) {
-  return (size_t)pair_rows(nmax) * pair_stride(nmax) * sizeof(float2) +
-         (size_t)kLeafArrays * nmax * sizeof(float);
+__host__ __device__ __forceinline__ size_t pair_smem_bytes(int nmax) {
+  const size_t b = (size_t)pair_rows(nmax) * pair_stride(nmax) * sizeof(float2) +
+                   (size_t)kLeafArrays * nmax * sizeof(float);
+  return (b + 15) & ~(size_t)15;
 }
 
-// One leaf on a T-thread block. tri: the folded triangle; pos: x0, y0, x1,
-// y1, vx, vy (nmax each; positions double-buffered across iterations).
-template <int T>
+// Barrier of a G-thread group: the whole block, or named barrier id (1, 2)
+// of one half.
+template <int G, int kBar>
+__device__ __forceinline__ void pair_sync() {
+  if (kBar == 0)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, %1;" ::"n"(kBar), "n"(G) : "memory");
+}
+
+// One leaf on a group of T threads (tid in [0, T); the block with kBar = 0,
+// or one half of it with named barrier kBar). tri: the folded triangle; pos:
+// x0, y0, x1, y1, vx, vy (nmax each; positions double-buffered across
+// iterations).
+template <int T, int kBar>
 __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 *tri,
-                                 float *pos) {
-  const int tid = threadIdx.x;
+                                 float *pos, int tid) {
   const int g0 = b.gptr[leaf];
   const int n = b.gptr[leaf + 1] - g0;
   if (n <= 0) return;
@@ -229,7 +241,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
   const int qd = T / n, qm = T % n;    // rect (row, col) advance per stride of T
   const int dat = qd * s + qm;         // rect address advance (before a row wrap)
   const int u0 = tid / n, c0 = tid % n;
-  __syncthreads();
+  pair_sync<T, kBar>();
   for (int it = 0; it < b.iters; ++it) {
     const float *sx = pos + (it & 1) * 2 * nmax, *sy = sx + nmax;
     float *nx = pos + ((it & 1) ^ 1) * 2 * nmax, *ny = nx + nmax;
@@ -292,7 +304,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
       for (int k = 0; k < kPairUnroll; ++k)
         if (ok[k]) tri[at_k[k]] = t[k];
     }
-    __syncthreads();
+    pair_sync<T, kBar>();
     // phase 2: the pair terms in partner order after the attraction; damped step
 #pragma unroll
     for (int g = 0; g < kOwn; ++g) {
@@ -364,7 +376,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
       nx[j] = rclamp(__fadd_rn(xj, __fmul_rn(vx, b.dt)), min_x, max_x);
       ny[j] = rclamp(__fadd_rn(yj, __fmul_rn(vy, b.dt)), min_y, max_y);
     }
-    __syncthreads();
+    pair_sync<T, kBar>();
   }
   const float *fx_ = pos + (b.iters & 1) * 2 * nmax, *fy_ = fx_ + nmax;
   for (int i = tid; i < n; i += T) {
@@ -374,34 +386,89 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
   }
 }
 
-// One T-thread block per leaf at a time, pulling leaves from the counter.
-template <int T>
-__global__ void __launch_bounds__(T, 3) leaf_pairs_kernel(LeafBatch b, int nmax) {
-  extern __shared__ float4 lpair[];
-  float2 *tri = reinterpret_cast<float2 *>(lpair);
-  float *pos = reinterpret_cast<float *>(tri + (size_t)pair_rows(nmax) * pair_stride(nmax));
-  __shared__ int next;
+// One half of a block: leaves order[split..) from counter[1], named barrier kBar.
+template <int H, int kBar>
+__device__ __forceinline__ void half_loop(const LeafBatch &b, int split, int nhalf, float2 *tri,
+                                          float *pos, int ht, int *next) {
   while (true) {
-    if (threadIdx.x == 0) {
-      const unsigned int w = atomicAdd(b.counter, 1u);
-      next = w < (unsigned)b.n_leaves ? b.order[w] : -1;
+    if (ht == 0) {
+      const unsigned int w = atomicAdd(&b.counter[1], 1u);
+      *next = (unsigned)split + w < (unsigned)b.n_leaves ? b.order[split + w] : -1;
     }
-    __syncthreads();
-    const int leaf = next;
-    __syncthreads();
+    pair_sync<H, kBar>();
+    const int leaf = *next;
+    pair_sync<H, kBar>();
     if (leaf < 0) break;
-    place_leaf_pairs<T>(b, leaf, nmax, tri, pos);
+    place_leaf_pairs<H, kBar>(b, leaf, nhalf, tri, pos, ht);
   }
 }
 
+// T-thread blocks pull leaves largest-first from counter[0] while they are
+// larger than nhalf; then each half of the block (T/2 threads, its own named
+// barrier and half of the shared memory) pulls the remaining leaves from
+// counter[1]. Two leaves of at most nhalf gates fit where one of nmax does,
+// so the smaller leaves run twice as many to an SM.
 template <int T>
-static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, int nmax, cudaStream_t s) {
-  if (nmax > kPairMax) {
-    set_error("pair schedules take leaves of at most %d gates (largest: %d)", kPairMax, nmax);
+__global__ void __launch_bounds__(T, 3)
+leaf_pairs_kernel(LeafBatch b, int nmax, int split, int nhalf) {
+  extern __shared__ float4 lpair[];
+  __shared__ int next[2];
+  {
+    float2 *tri = reinterpret_cast<float2 *>(lpair);
+    float *pos = reinterpret_cast<float *>(tri + (size_t)pair_rows(nmax) * pair_stride(nmax));
+    while (true) {
+      if (threadIdx.x == 0) {
+        const unsigned int w = atomicAdd(&b.counter[0], 1u);
+        next[0] = w < (unsigned)split ? b.order[w] : -1;
+      }
+      __syncthreads();
+      const int leaf = next[0];
+      __syncthreads();
+      if (leaf < 0) break;
+      place_leaf_pairs<T, 0>(b, leaf, nmax, tri, pos, threadIdx.x);
+    }
+  }
+  if (split >= b.n_leaves) return;
+  constexpr int H = T / 2;
+  const int h = threadIdx.x / H, ht = threadIdx.x % H;
+  float2 *tri = reinterpret_cast<float2 *>(reinterpret_cast<char *>(lpair) +
+                                           h * pair_smem_bytes(nhalf));
+  float *pos = reinterpret_cast<float *>(tri + (size_t)pair_rows(nhalf) * pair_stride(nhalf));
+  if (h == 0)
+    half_loop<H, 1>(b, split, nhalf, tri, pos, ht, next);
+  else
+    half_loop<H, 2>(b, split, nhalf, tri, pos, ht, next + 1);
+}
+
+// The batch's split for leaf_pairs_kernel: the largest nhalf whose two slots
+// fit in one nmax slot, and the number of leaves (largest first) above it.
+struct PairPlan {
+  int nmax, nhalf, split;
+};
+
+static PairPlan pair_plan(int n_leaves, const int32_t *leaf_ptr, const std::vector<int32_t> &order) {
+  PairPlan p;
+  p.nmax = 1;
+  for (int l = 0; l < n_leaves; ++l) p.nmax = std::max(p.nmax, leaf_ptr[l + 1] - leaf_ptr[l]);
+  const size_t whole = pair_smem_bytes(p.nmax);
+  p.nhalf = p.nmax;
+  while (p.nhalf > 0 && 2 * pair_smem_bytes(p.nhalf) > whole) --p.nhalf;
+  p.split = 0;
+  while (p.split < n_leaves &&
+         leaf_ptr[order[p.split] + 1] - leaf_ptr[order[p.split]] > p.nhalf)
+    ++p.split;
+  if (p.nhalf < 1) p.split = n_leaves;
+  return p;
+}
+
+template <int T>
+static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, const PairPlan &plan, cudaStream_t s) {
+  if (plan.nmax > kPairMax) {
+    set_error("pair schedules take leaves of at most %d gates (largest: %d)", kPairMax,
+              plan.nmax);
     return FX_EINVAL;
   }
-  if (nmax < 1) nmax = 1;
-  const size_t smem = pair_smem_bytes(nmax);
+  const size_t smem = pair_smem_bytes(plan.nmax);
   {
     static std::mutex mu;
     static bool attr = false;
@@ -420,8 +487,8 @@ static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, int nmax, cudaStream_t 
   int grid = ctx->num_sms * per_sm;
   if (grid > b.n_leaves) grid = b.n_leaves;
   if (grid < 1) grid = 1;
-  FX_CHECK_CUDA(cudaMemsetAsync(b.counter, 0, 4, s));
-  leaf_pairs_kernel<T><<<grid, T, smem, s>>>(b, nmax);
+  FX_CHECK_CUDA(cudaMemsetAsync(b.counter, 0, 8, s));
+  leaf_pairs_kernel<T><<<grid, T, smem, s>>>(b, plan.nmax, plan.split, plan.nhalf);
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   return FX_OK;
@@ -511,12 +578,12 @@ static int launch_leaf(fx_ctx *ctx, const LeafBatch &b, bool per_cluster,
   return FX_OK;
 }
 
-static int run_schedule(fx_ctx *ctx, const LeafBatch &b, int schedule, int nmax,
+static int run_schedule(fx_ctx *ctx, const LeafBatch &b, int schedule, const PairPlan &plan,
                         cudaStream_t s) {
   switch (schedule) {
-    case FX_LEAF_PAIR64: return launch_pairs<64>(ctx, b, nmax, s);
-    case FX_LEAF_PAIR128: return launch_pairs<128>(ctx, b, nmax, s);
-    case FX_LEAF_PAIR256: return launch_pairs<256>(ctx, b, nmax, s);
+    case FX_LEAF_PAIR64: return launch_pairs<64>(ctx, b, plan, s);
+    case FX_LEAF_PAIR128: return launch_pairs<128>(ctx, b, plan, s);
+    case FX_LEAF_PAIR256: return launch_pairs<256>(ctx, b, plan, s);
     case FX_LEAF_WARP: return launch_leaf<32>(ctx, b, false, s);
     case FX_LEAF_CTA64: return launch_leaf<64>(ctx, b, false, s);
     case FX_LEAF_CTA128: return launch_leaf<128>(ctx, b, false, s);
@@ -569,8 +636,7 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
   LeafHost h;
   FX_TRY(build_leaf_host(d, n_leaves, leaf_ptr, leaf_gate, h));
   const int32_t G = leaf_ptr[n_leaves];
-  int nmax = 0;
-  for (int l = 0; l < n_leaves; ++l) nmax = std::max(nmax, leaf_ptr[l + 1] - leaf_ptr[l]);
+  const PairPlan plan = pair_plan(n_leaves, leaf_ptr, h.order);
   DevBuf<int32_t> gptr, gate, aptr, order;
   DevBuf<int16_t> aidx;
   DevBuf<float4> reg;
@@ -626,9 +692,9 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
     FX_CHECK_CUDA(cudaEventCreate(&e1));
     for (int sc : {FX_LEAF_WARP, FX_LEAF_CTA64, FX_LEAF_CTA128, FX_LEAF_CTA256,
                    FX_LEAF_PAIR64, FX_LEAF_PAIR128, FX_LEAF_PAIR256}) {
-      if (sc >= FX_LEAF_PAIR64 && nmax > kPairMax) continue;
+      if (sc >= FX_LEAF_PAIR64 && plan.nmax > kPairMax) continue;
       FX_CHECK_CUDA(cudaEventRecord(e0, s));
-      int rc = run_schedule(ctx, b, sc, nmax, s);
+      int rc = run_schedule(ctx, b, sc, plan, s);
       if (rc != FX_OK) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -653,7 +719,7 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
   if (!done) {
     cudaEvent_t ev;
     timer_begin(ctx, FX_STAGE_LEAF, s, &ev);
-    FX_TRY(run_schedule(ctx, b, schedule, nmax, s));
+    FX_TRY(run_schedule(ctx, b, schedule, plan, s));
     timer_end(ctx, FX_STAGE_LEAF, s, ev);
   }
   FX_CHECK_CUDA(cudaMemcpyAsync(out_x, ox.p, (size_t)d->n * 4, cudaMemcpyDeviceToHost, s));
