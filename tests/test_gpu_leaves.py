@@ -171,3 +171,33 @@ def test_leaf_pair_schedules_take_at_most_128_gates(fx, ctx, oracle):
         oracle.place_leaf(gates[lp[l]:lp[l + 1]], ap, ai, reg[l], 5, 1.0, 0.5, 0.9, 0.1,
                           ox, oy)
     assert np.array_equal(x, ox) and np.array_equal(y, oy)
+
+
+@pytest.mark.parametrize("sizes,iters", [
+    ([90, 64, 63, 62, 40, 17, 2, 1], 30),   # largest 90: halves take leaves <= 62
+    ([2, 1, 2, 1, 1], 12),                  # largest 2: one-gate leaves run two to a block
+    ([128, 91, 90, 3], 0),                  # no iterations: the initial layout
+    ([128, 91, 90, 3], 1),
+])
+@pytest.mark.parametrize("schedule", ["pair64", "pair128", "pair256"])
+def test_leaf_pair_split_points(fx, ctx, oracle, schedule, sizes, iters):
+    """The pair schedules hand the largest leaves to whole blocks and the rest
+    to half blocks, by a split the host derives from the largest leaf: batches
+    whose largest leaf sits at, above and below the split, leaves of one and
+    two gates, and zero or one iteration, against the reference loop."""
+    sizes = np.array(sizes)
+    circ, lp, reg = _every_size_batch(fx, sizes, 13)
+    gates = np.arange(circ.num_gates, dtype=np.int32)
+    d = fx.Design(ctx, circ)
+    try:
+        x, y, _ = d.place_leaves(lp, gates, reg.ravel(),
+                                 fx.leaf_cfg(force_iterations=iters, schedule=_code(fx, schedule)))
+    finally:
+        d.close()
+    ap, ai = oracle.build_adjacency(circ.num_gates, circ.net_ptr, circ.net_gate)
+    ox = np.zeros(circ.num_gates, np.float32)
+    oy = np.zeros(circ.num_gates, np.float32)
+    for l in range(len(sizes)):
+        oracle.place_leaf(gates[lp[l]:lp[l + 1]], ap, ai, reg[l], iters, 1.0, 0.5, 0.9, 0.1,
+                          ox, oy)
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
