@@ -213,28 +213,37 @@ __device__ __forceinline__ void pair_sync() {
     asm volatile("bar.sync %0, %1;" ::"n"(kBar), "n"(G) : "memory");
 }
 
+// Repulsion term of the pair (r, c), r < c, from their positions:
+// force * (p_r - p_c) / dist with the reference's rounding steps.
+__device__ __forceinline__ float2 pair_term(float2 pr, float2 pc, float repel) {
+  const float dx = __fsub_rn(pr.x, pc.x), dy = __fsub_rn(pr.y, pc.y);
+  const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
+  const float force = __fdiv_rn(repel, __fmul_rn(dist, dist));
+  return make_float2(__fdiv_rn(__fmul_rn(force, dx), dist), __fdiv_rn(__fmul_rn(force, dy), dist));
+}
+
 // One leaf on a group of T threads (tid in [0, T); the block with kBar = 0,
 // or one half of it with named barrier kBar). tri: the folded triangle; pos:
-// x0, y0, x1, y1, vx, vy (nmax each; positions double-buffered across
-// iterations).
+// positions (x, y) in two buffers of nmax float2 (double-buffered across
+// iterations), then velocities (nmax float2).
 template <int T, int kBar>
 __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 *tri,
                                  float *pos, int tid) {
   const int g0 = b.gptr[leaf];
   const int n = b.gptr[leaf + 1] - g0;
   if (n <= 0) return;
-  // buffer p holds x at pos + 2p nmax and y at pos + (2p + 1) nmax
-  float *svx = pos + 4 * nmax, *svy = pos + 5 * nmax;
+  float2 *xy = reinterpret_cast<float2 *>(pos);  // buffer p at xy + p nmax
+  float2 *sv = xy + 2 * nmax;
   const float4 r4 = b.region[leaf];
   const float half_w = r4.z / 2.0f, half_h = r4.w / 2.0f;
   const float min_x = __fsub_rn(r4.x, half_w), min_y = __fsub_rn(r4.y, half_h);
   const float max_x = __fadd_rn(min_x, r4.z), max_y = __fadd_rn(min_y, r4.w);
   const float nf = (float)n;
   for (int i = tid; i < n; i += T) {
-    pos[i] = __fadd_rn(min_x, __fmul_rn(__fdiv_rn((float)i, nf), r4.z));
-    pos[nmax + i] = __fadd_rn(min_y, __fmul_rn(__fdiv_rn((float)((i * 7) % n), nf), r4.w));
-    svx[i] = 0.f;
-    svy[i] = 0.f;
+    xy[i] = make_float2(__fadd_rn(min_x, __fmul_rn(__fdiv_rn((float)i, nf), r4.z)),
+                        __fadd_rn(min_y, __fmul_rn(__fdiv_rn((float)((i * 7) % n), nf), r4.w)));
+    sv[i] = make_float2(0.f, 0.f);
   }
   const int U = pair_rows(n), s = pair_stride(n);
   const int npairs = n * (n - 1) / 2;
@@ -243,8 +252,8 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
   const int u0 = tid / n, c0 = tid % n;
   pair_sync<T, kBar>();
   for (int it = 0; it < b.iters; ++it) {
-    const float *sx = pos + (it & 1) * 2 * nmax, *sy = sx + nmax;
-    float *nx = pos + ((it & 1) ^ 1) * 2 * nmax, *ny = nx + nmax;
+    const float2 *sxy = xy + (it & 1) * nmax;
+    float2 *nxy = xy + ((it & 1) ^ 1) * nmax;
     // attraction of the gates this thread owns (it reads only this
     // iteration's positions, so its load chain runs while every warp is busy
     // with phase 1); phase 2 continues these sums with the pair terms
@@ -255,12 +264,12 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
       const int j = tid + g * T;
       float ax = 0.f, ay = 0.f;
       if (j < n) {
-        const float xj = sx[j], yj = sy[j];
+        const float2 pj = sxy[j];
         const int a0 = b.aptr[g0 + j], a1 = b.aptr[g0 + j + 1];
         for (int e = a0; e < a1; ++e) {
-          const int o = b.aidx[e];
-          ax = __fadd_rn(ax, __fmul_rn(b.k, __fsub_rn(sx[o], xj)));
-          ay = __fadd_rn(ay, __fmul_rn(b.k, __fsub_rn(sy[o], yj)));
+          const float2 po = sxy[b.aidx[e]];
+          ax = __fadd_rn(ax, __fmul_rn(b.k, __fsub_rn(po.x, pj.x)));
+          ay = __fadd_rn(ay, __fmul_rn(b.k, __fsub_rn(po.y, pj.y)));
         }
       }
       atx[g] = ax;
@@ -270,39 +279,39 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
     // Entry q = (u, col) = (q / n, q % n): c1 = u + 1 + col < n puts it in the
     // first segment (r = u, c = c1), else the second (r = n-2-u, c = col).
     // The n(n-1)/2 valid entries are exactly q < npairs (for even n the
-    // unused half of the last rect row comes last).
-    int u = u0, col = c0, nu = n - 2 - u0, at = u0 * s + c0;
-    for (int q = tid; q < npairs; q += kPairUnroll * T) {
+    // unused half of the last rect row comes last). Whole batches of
+    // kPairUnroll entries need no bounds test; the last partial one does.
+    int u = u0, col = c0, at = u0 * s + c0;
+    auto advance = [&]() {
+      col += qm;
+      u += qd;
+      at += dat;
+      if (col >= n) {
+        col -= n;
+        ++u;
+        at += s - n;
+      }
+    };
+    int q = tid;
+    for (; q + (kPairUnroll - 1) * T < npairs; q += kPairUnroll * T) {
       float2 t[kPairUnroll];
       int at_k[kPairUnroll];
-      bool ok[kPairUnroll];
 #pragma unroll
       for (int k = 0; k < kPairUnroll; ++k) {
         const int c1 = u + 1 + col;
         const bool first = c1 < n;
-        ok[k] = q + k * T < npairs;
         at_k[k] = at;
-        const int rr = ok[k] ? (first ? u : nu) : 0, cc = ok[k] ? (first ? c1 : col) : 0;
-        const float dx = __fsub_rn(sx[rr], sx[cc]), dy = __fsub_rn(sy[rr], sy[cc]);
-        const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-        const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
-        const float force = __fdiv_rn(b.repel, __fmul_rn(dist, dist));
-        t[k] = make_float2(__fdiv_rn(__fmul_rn(force, dx), dist),
-                           __fdiv_rn(__fmul_rn(force, dy), dist));
-        col += qm;
-        u += qd;
-        nu -= qd;
-        at += dat;
-        if (col >= n) {
-          col -= n;
-          ++u;
-          --nu;
-          at += s - n;
-        }
+        t[k] = pair_term(sxy[first ? u : n - 2 - u], sxy[first ? c1 : col], b.repel);
+        advance();
       }
 #pragma unroll
-      for (int k = 0; k < kPairUnroll; ++k)
-        if (ok[k]) tri[at_k[k]] = t[k];
+      for (int k = 0; k < kPairUnroll; ++k) tri[at_k[k]] = t[k];
+    }
+    for (; q < npairs; q += T) {
+      const int c1 = u + 1 + col;
+      const bool first = c1 < n;
+      tri[at] = pair_term(sxy[first ? u : n - 2 - u], sxy[first ? c1 : col], b.repel);
+      advance();
     }
     pair_sync<T, kBar>();
     // phase 2: the pair terms in partner order after the attraction; damped step
@@ -310,7 +319,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
     for (int g = 0; g < kOwn; ++g) {
       const int j = tid + g * T;
       if (j >= n) break;
-      const float xj = sx[j], yj = sy[j];
+      const float2 pj = sxy[j];
       float ax = atx[g], ay = aty[g];
       // Partner m < j adds -t(m, j) (row m), m > j adds t(j, m) (row j);
       // a + (-t) is a - t. The warp's gates are w..w+31, so partners below w
@@ -369,20 +378,21 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
           ay = __fadd_rn(ay, v.y);
         }
       }
-      const float vx = __fmul_rn(__fadd_rn(svx[j], __fmul_rn(ax, b.dt)), b.damping);
-      const float vy = __fmul_rn(__fadd_rn(svy[j], __fmul_rn(ay, b.dt)), b.damping);
-      svx[j] = vx;
-      svy[j] = vy;
-      nx[j] = rclamp(__fadd_rn(xj, __fmul_rn(vx, b.dt)), min_x, max_x);
-      ny[j] = rclamp(__fadd_rn(yj, __fmul_rn(vy, b.dt)), min_y, max_y);
+      const float2 v0 = sv[j];
+      const float vx = __fmul_rn(__fadd_rn(v0.x, __fmul_rn(ax, b.dt)), b.damping);
+      const float vy = __fmul_rn(__fadd_rn(v0.y, __fmul_rn(ay, b.dt)), b.damping);
+      sv[j] = make_float2(vx, vy);
+      nxy[j] = make_float2(rclamp(__fadd_rn(pj.x, __fmul_rn(vx, b.dt)), min_x, max_x),
+                           rclamp(__fadd_rn(pj.y, __fmul_rn(vy, b.dt)), min_y, max_y));
     }
     pair_sync<T, kBar>();
   }
-  const float *fx_ = pos + (b.iters & 1) * 2 * nmax, *fy_ = fx_ + nmax;
+  const float2 *fxy = xy + (b.iters & 1) * nmax;
   for (int i = tid; i < n; i += T) {
     const int g = b.gate[g0 + i];
-    b.out_x[g] = fx_[i];
-    b.out_y[g] = fy_[i];
+    const float2 f = fxy[i];
+    b.out_x[g] = f.x;
+    b.out_y[g] = f.y;
   }
 }
 
