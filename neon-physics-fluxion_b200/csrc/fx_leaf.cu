@@ -17,8 +17,10 @@
 // Schedules: a group of T threads (T = 32, 64, 128 or 256) owns one leaf at a
 // time, looping over gates when n > T; groups pull leaves (largest first)
 // from an atomic work counter until the batch is done, running all
-// iterations of a leaf in shared memory. Every schedule gives identical
-// results, so the autotuner is free to pick the fastest.
+// iterations of a leaf in shared memory. The pair-triangle schedules (leaves
+// of at most 128 gates, below) compute each pair's term once instead of once
+// per gate. Every schedule gives identical results, so the autotuner is free
+// to pick the fastest.
 #include <algorithm>
 #include <numeric>
 #include <unordered_map>
