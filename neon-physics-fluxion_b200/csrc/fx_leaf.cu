@@ -26,6 +26,8 @@
 #include <unordered_map>
 
 #include <mutex>
+#include <system_error>
+#include <thread>
 
 #include "fx_internal.h"
 
@@ -514,35 +516,81 @@ struct LeafHost {
   std::vector<int32_t> order;
 };
 
-static int build_leaf_host(const fx_design *d, int L, const int32_t *leaf_ptr,
-                           const int32_t *leaf_gate, LeafHost &h) {
-  const int32_t G = leaf_ptr[L];
-  h.aptr.assign((size_t)G + 1, 0);
-  h.aidx.clear();
-  std::vector<int32_t> local((size_t)d->n, -1);
-  for (int l = 0; l < L; ++l) {
+// In-leaf adjacency of leaves [l0, l1) into aptr (counts relative to the
+// range's first entry) and out; local: a -1-filled gate map of d->n entries,
+// left -1-filled.
+static void leaf_adjacency(const fx_design *d, int l0, int l1, const int32_t *leaf_ptr,
+                           const int32_t *leaf_gate, std::vector<int32_t> &local,
+                           int32_t *aptr, std::vector<int16_t> &out) {
+  for (int l = l0; l < l1; ++l) {
     const int32_t b = leaf_ptr[l], e = leaf_ptr[l + 1];
-    if (e - b > kLeafMax) {
-      set_error("leaf %d has %d gates (limit %d)", l, e - b, kLeafMax);
-      return FX_EINVAL;
-    }
-    for (int32_t i = b; i < e; ++i) {
-      const int32_t g = leaf_gate[i];
-      if (g < 0 || g >= d->n) {
-        set_error("leaf gate %d out of range", g);
-        return FX_EINVAL;
-      }
-      local[g] = i - b;  // HashMap insert: a repeated gate keeps the last slot
-    }
+    for (int32_t i = b; i < e; ++i)
+      local[leaf_gate[i]] = i - b;  // HashMap insert: a repeated gate keeps the last slot
     for (int32_t i = b; i < e; ++i) {
       const int32_t g = leaf_gate[i];
       for (int32_t q = d->h_adj_ptr[g]; q < d->h_adj_ptr[g + 1]; ++q) {
         const int32_t j = d->h_adj_idx[q];
-        if (local[j] >= 0) h.aidx.push_back((int16_t)local[j]);
+        if (local[j] >= 0) out.push_back((int16_t)local[j]);
       }
-      h.aptr[(size_t)i + 1] = (int32_t)h.aidx.size();
+      aptr[(size_t)i + 1] = (int32_t)out.size();
     }
     for (int32_t i = b; i < e; ++i) local[leaf_gate[i]] = -1;
+  }
+}
+
+static int build_leaf_host(const fx_design *d, int L, const int32_t *leaf_ptr,
+                           const int32_t *leaf_gate, LeafHost &h) {
+  const int32_t G = leaf_ptr[L];
+  for (int l = 0; l < L; ++l)
+    if (leaf_ptr[l + 1] - leaf_ptr[l] > kLeafMax) {
+      set_error("leaf %d has %d gates (limit %d)", l, leaf_ptr[l + 1] - leaf_ptr[l], kLeafMax);
+      return FX_EINVAL;
+    }
+  for (int32_t i = 0; i < G; ++i)
+    if (leaf_gate[i] < 0 || leaf_gate[i] >= d->n) {
+      set_error("leaf gate %d out of range", leaf_gate[i]);
+      return FX_EINVAL;
+    }
+  h.aptr.assign((size_t)G + 1, 0);
+  h.aidx.clear();
+  // Leaves are independent: large batches split them over host threads in
+  // ranges of about equal gate counts, then join the ranges in leaf order.
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = G >= 65536 ? (int)std::min<unsigned>(std::min(hw, 16u), (unsigned)L) : 1;
+  if (nt <= 1) {
+    std::vector<int32_t> local((size_t)d->n, -1);
+    leaf_adjacency(d, 0, L, leaf_ptr, leaf_gate, local, h.aptr.data(), h.aidx);
+  } else {
+    std::vector<int> cut(nt + 1, L);
+    cut[0] = 0;
+    for (int t = 1, l = 0; t < nt; ++t) {
+      const int64_t target = (int64_t)G * t / nt;
+      while (l < L && leaf_ptr[l] < target) ++l;
+      cut[t] = l;
+    }
+    std::vector<std::vector<int16_t>> part(nt);
+    auto range = [&](int t) {
+      std::vector<int32_t> local((size_t)d->n, -1);
+      leaf_adjacency(d, cut[t], cut[t + 1], leaf_ptr, leaf_gate, local, h.aptr.data(), part[t]);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) {
+      try {
+        pool.emplace_back(range, t);
+      } catch (const std::system_error &) {
+        range(t);  // no thread to be had: do this range here
+      }
+    }
+    range(0);
+    for (auto &th : pool) th.join();
+    size_t off = 0;
+    for (int t = 0; t < nt; ++t) {
+      for (int32_t i = leaf_ptr[cut[t]]; i < leaf_ptr[cut[t + 1]]; ++i)
+        h.aptr[(size_t)i + 1] += (int32_t)off;
+      off += part[t].size();
+    }
+    h.aidx.reserve(off);
+    for (auto &p : part) h.aidx.insert(h.aidx.end(), p.begin(), p.end());
   }
   h.order.resize(L);
   std::iota(h.order.begin(), h.order.end(), 0);
