@@ -762,6 +762,15 @@ def run_leaves(args, rank, world, local_rank):
     lg = np.arange(c.num_gates, dtype=np.int32)
     sizes = np.diff(lp).astype(np.int64)
     pairs = int((sizes * (sizes - 1) // 2).sum())
+    # the call uploads the caller's lists and positions plus what it derives:
+    # the in-leaf adjacency (row offsets, int16 neighbour slots) and the order
+    ap_all, ai_all = fx.build_adjacency(c)
+    leaf_of = np.empty(c.num_gates, np.int64)
+    leaf_of[lg] = np.repeat(np.arange(len(sizes)), sizes)
+    in_leaf = int((leaf_of[np.repeat(np.arange(c.num_gates), np.diff(ap_all))]
+                   == leaf_of[ai_all]).sum())
+    h2d_bytes = (4 * (len(lp) + c.num_gates) + 16 * args.clusters + 8 * c.num_gates
+                 + 4 * (c.num_gates + 1) + 2 * in_leaf + 4 * args.clusters)
     ctx = fx.Context(local_rank)
     d = fx.Design(ctx, c)
     cfg = fx.leaf_cfg(force_iterations=args.leaf_iters, schedule=args.leaf_schedule)
@@ -833,10 +842,10 @@ def run_leaves(args, rank, world, local_rank):
            "speedup_vs_per_cluster": None if pc_ms is None else pc_ms / kms,
            "same_result_as_per_cluster": same, "cpu_baseline": cpu,
            "e2e": {"value": world * units * args.steps / wall, "unit": "cluster-iterations/s",
-                   "h2d_bytes_per_step": 4 * (len(lp) + c.num_gates) + 16 * args.clusters
-                   + 8 * c.num_gates,
+                   "h2d_bytes_per_step": h2d_bytes,
                    "d2h_bytes_per_step": 8 * c.num_gates,
-                   "call": "fx_hapr_place_leaves with host leaf lists and regions"},
+                   "call": "fx_hapr_place_leaves with host leaf lists and regions (the "
+                           "in-leaf adjacency it derives on the host is uploaded too)"},
            "gpu_launches": launches, "clocks": clk}
     if rank == 0:
         print(json.dumps(out), flush=True)
