@@ -6,7 +6,9 @@
 //   * init (placer.rs:226-227): x_i = min_x + (i/n) w,
 //     y_i = min_y + ((7i mod n)/n) h, velocities 0;
 //   * attraction (:243-255): for each neighbour of gate i in adjacency order
-//     that lies in the leaf, F_i += k (p_j - p_i);
+//     that lies in the leaf, F_i += k (p_j - p_i); a gate listed more than
+//     once gets all its listings' springs on its last slot (the HashMap
+//     index), and the positions go out slot by slot, so the last slot wins;
 //   * repulsion (:258-272): the reference walks pairs i < j and adds the pair
 //     force to i and subtracts it from j, so gate j receives its terms in
 //     partner order m = 0..n-1. Each thread owns one gate and adds, in that
@@ -39,7 +41,8 @@ constexpr int kPairUnroll = 4;  // partners whose repulsion terms are in flight 
 
 struct LeafBatch {
   const int32_t *gptr;     // [L+1] offsets into the gate list (leaf order)
-  const int32_t *gate;     // [G] global gate ids
+  const int32_t *gate;     // [G] global gate ids; ~gate for a slot whose gate a
+                           // later slot of the batch writes again
   const int32_t *aptr;     // [G+1] in-leaf adjacency row offsets
   const int16_t *aidx;     // in-leaf neighbour local indices (reference order)
   const float4 *region;    // [L] (cx, cy, w, h)
@@ -145,9 +148,11 @@ __device__ void place_leaf(const LeafBatch &b, int leaf, int tid, float *sm, int
     group_sync<T>(sid);
   }
   for (int i = tid; i < n; i += T) {
-    const int g = b.gate[g0 + i];
-    b.out_x[g] = sx[i];
-    b.out_y[g] = sy[i];
+    const int g = b.gate[g0 + i];  // ~gate: a later slot of the batch writes this gate
+    if (g >= 0) {
+      b.out_x[g] = sx[i];
+      b.out_y[g] = sy[i];
+    }
   }
   group_sync<T>(sid);
 }
@@ -393,10 +398,12 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
   }
   const float2 *fxy = xy + (b.iters & 1) * nmax;
   for (int i = tid; i < n; i += T) {
-    const int g = b.gate[g0 + i];
-    const float2 f = fxy[i];
-    b.out_x[g] = f.x;
-    b.out_y[g] = f.y;
+    const int g = b.gate[g0 + i];  // ~gate: a later slot of the batch writes this gate
+    if (g >= 0) {
+      const float2 f = fxy[i];
+      b.out_x[g] = f.x;
+      b.out_y[g] = f.y;
+    }
   }
 }
 
@@ -524,14 +531,28 @@ static void leaf_adjacency(const fx_design *d, int l0, int l1, const int32_t *le
                            int32_t *aptr, std::vector<int16_t> &out) {
   for (int l = l0; l < l1; ++l) {
     const int32_t b = leaf_ptr[l], e = leaf_ptr[l + 1];
-    for (int32_t i = b; i < e; ++i)
-      local[leaf_gate[i]] = i - b;  // HashMap insert: a repeated gate keeps the last slot
+    bool repeats = false;
     for (int32_t i = b; i < e; ++i) {
       const int32_t g = leaf_gate[i];
-      for (int32_t q = d->h_adj_ptr[g]; q < d->h_adj_ptr[g + 1]; ++q) {
-        const int32_t j = d->h_adj_idx[q];
-        if (local[j] >= 0) out.push_back((int16_t)local[j]);
+      repeats |= local[g] >= 0;
+      local[g] = i - b;  // HashMap insert: a repeated gate keeps the last slot
+    }
+    for (int32_t i = b; i < e; ++i) {
+      const int32_t g = leaf_gate[i];
+      // The reference adds every listing's springs to the gate's mapped
+      // (last) slot, in slot order: that slot's row is the neighbour list
+      // once per listing, the gate's other slots have none.
+      int32_t reps = 1;
+      if (repeats) {
+        reps = 0;
+        if (local[g] == i - b)
+          for (int32_t k = b; k <= i; ++k) reps += leaf_gate[k] == g;
       }
+      for (int32_t r = 0; r < reps; ++r)
+        for (int32_t q = d->h_adj_ptr[g]; q < d->h_adj_ptr[g + 1]; ++q) {
+          const int32_t j = d->h_adj_idx[q];
+          if (local[j] >= 0) out.push_back((int16_t)local[j]);
+        }
       aptr[(size_t)i + 1] = (int32_t)out.size();
     }
     for (int32_t i = b; i < e; ++i) local[leaf_gate[i]] = -1;
@@ -715,7 +736,23 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
     return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s) : cudaSuccess;
   };
   FX_CHECK_CUDA(up(gptr.p, leaf_ptr, ((size_t)n_leaves + 1) * 4));
-  FX_CHECK_CUDA(up(gate.p, leaf_gate, (size_t)G * 4));
+  // The reference writes the positions slot by slot, leaf by leaf, so a gate
+  // listed more than once keeps its last slot's position. The kernels write
+  // concurrently: every slot but a gate's last goes up as ~gate and skips
+  // the write. Batches without repeats go up unchanged.
+  std::vector<int32_t> gate_last;
+  {
+    std::vector<uint8_t> seen((size_t)d->n, 0);
+    for (int32_t i = G - 1; i >= 0; --i) {
+      const int32_t g = leaf_gate[i];
+      if (seen[g]) {
+        if (gate_last.empty()) gate_last.assign(leaf_gate, leaf_gate + G);
+        gate_last[i] = ~g;
+      }
+      seen[g] = 1;
+    }
+  }
+  FX_CHECK_CUDA(up(gate.p, gate_last.empty() ? leaf_gate : gate_last.data(), (size_t)G * 4));
   FX_CHECK_CUDA(up(aptr.p, h.aptr.data(), h.aptr.size() * 4));
   FX_CHECK_CUDA(up(aidx.p, h.aidx.data(), h.aidx.size() * 2));
   FX_CHECK_CUDA(up(order.p, h.order.data(), h.order.size() * 4));

@@ -201,3 +201,30 @@ def test_leaf_pair_split_points(fx, ctx, oracle, schedule, sizes, iters):
         oracle.place_leaf(gates[lp[l]:lp[l + 1]], ap, ai, reg[l], iters, 1.0, 0.5, 0.9, 0.1,
                           ox, oy)
     assert np.array_equal(x, ox) and np.array_equal(y, oy)
+
+
+@pytest.mark.parametrize("schedule", ["warp", "cta64", "pair128", "pair256", "per_cluster"])
+def test_leaf_repeated_gates_keep_the_last_slot(fx, ctx, oracle, schedule):
+    """A gate listed twice in one leaf, and a gate listed in two leaves: the
+    reference writes positions slot by slot, leaf by leaf, so the last listing
+    wins; a gate that lost its only slot to a repeat keeps its input position."""
+    sizes = np.array([20, 30, 25, 40])
+    circ, lp, reg = _every_size_batch(fx, sizes, 21)
+    lg = np.arange(circ.num_gates, dtype=np.int32)
+    lg[5] = lg[2]                 # within leaf 0
+    lg[lp[2]] = lg[lp[1] + 7]     # leaf 2 repeats a gate of leaf 1
+    lg[lp[3] + 39] = lg[lp[3]]    # within leaf 3, the last slot repeats the first
+    x0 = np.full(circ.num_gates, 3.25, np.float32)
+    d = fx.Design(ctx, circ)
+    try:
+        x, y, _ = d.place_leaves(lp, lg, reg.ravel(),
+                                 fx.leaf_cfg(force_iterations=20, schedule=_code(fx, schedule)),
+                                 x0, x0.copy())
+    finally:
+        d.close()
+    ap, ai = oracle.build_adjacency(circ.num_gates, circ.net_ptr, circ.net_gate)
+    ox, oy = x0.copy(), x0.copy()
+    for l in range(len(sizes)):
+        oracle.place_leaf(lg[lp[l]:lp[l + 1]], ap, ai, reg[l], 20, 1.0, 0.5, 0.9, 0.1, ox, oy)
+    assert np.array_equal(x, ox) and np.array_equal(y, oy)
+    assert x[5] == 3.25 and x[lp[2]] == 3.25  # their slots went to repeats
