@@ -383,7 +383,8 @@ int fx_refine(fx_ctx *ctx, fx_design *design, const fx_refine_cfg *cfg,
  *                 netlist: fx_partition -> fx_hapr_place_leaves -> fx_refine;
  *                 the placed design can stay resident for later ECO jobs;
  *   FX_JOB_ECO    on a resident design: move the given gates (clamped to the
- *                 die), then `iterations` plain iterations (fx_force_iterate).
+ *                 die; each gate listed at most once, else the job fails with
+ *                 FX_EINVAL), then `iterations` plain iterations (fx_force_iterate).
  * Up to `slots` jobs run at once, each on its own worker thread and context
  * (own streams), so their kernels overlap on the device. A queued job is
  * admitted when a slot is free and its estimated device footprint fits in

@@ -197,11 +197,20 @@ int run_eco(fx_ctx *ctx, Job &j, fx_design *d) {
   cudaStream_t s = ctx->stream;
   const int32_t nm = j.desc.n_moves;
   if (nm > 0) {
-    for (int32_t i = 0; i < nm; ++i)
-      if (j.move_gate[i] < 0 || j.move_gate[i] >= d->n) {
-        set_error("ECO move of gate %d outside the design", j.move_gate[i]);
+    // the moves apply in parallel, so each gate may be listed once
+    std::vector<uint8_t> listed((size_t)d->n, 0);
+    for (int32_t i = 0; i < nm; ++i) {
+      const int32_t g = j.move_gate[i];
+      if (g < 0 || g >= d->n) {
+        set_error("ECO move of gate %d outside the design", g);
         return FX_EINVAL;
       }
+      if (listed[g]) {
+        set_error("ECO moves list gate %d twice", g);
+        return FX_EINVAL;
+      }
+      listed[g] = 1;
+    }
     AllocScope as(s);
     DevBuf<int32_t> g;
     DevBuf<float> dx, dy;

@@ -139,5 +139,8 @@ def test_eco_on_unknown_or_released_design(fx):
         sv.submit_eco(bad, np.array([c.num_gates + 5], np.int32), np.zeros(1), np.zeros(1))
         r = sv.poll(-1)
         assert r["status"] == -1 and "outside" in r["error"]
+        sv.submit_eco(bad, np.array([3, 9, 3], np.int32), np.ones(3), np.ones(3))
+        r = sv.poll(-1)
+        assert r["status"] == -1 and "twice" in r["error"]
     finally:
         sv.close()
