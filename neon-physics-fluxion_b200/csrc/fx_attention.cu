@@ -712,8 +712,7 @@ static int level_attention(fx_ctx *ctx, fx_design *d, int n, const MapBuilder &b
       FX_TRY(gm.alloc((size_t)n * n));
       FX_CHECK_CUDA(cudaMemsetAsync(gm.p, 0, (size_t)n * n * 4, s));
       const int smem = n * n * 4;
-      FX_CHECK_CUDA(cudaFuncSetAttribute(attn_dense_count_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(attn_dense_count_kernel), smem));
       if (m > 0) {
         attn_dense_count_kernel<<<ctx->num_sms, 256, smem, s>>>(
             m, n, d->net_ptr.p, dc.p, cnt.p, mid.p, d_bad.p + 2, big.p, d_bad.p + 1, gm.p);
@@ -741,16 +740,14 @@ static int level_attention(fx_ctx *ctx, fx_design *d, int n, const MapBuilder &b
       launches += 3;
       if (pins > 0) {
         const int bsm = 2 * n * 4;
-        FX_CHECK_CUDA(cudaFuncSetAttribute(attn_bucket_kernel,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
+        FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(attn_bucket_kernel), bsm));
         attn_bucket_kernel<<<ctx->num_sms, kBucketThreads, bsm, s>>>(pins, n, dn.p, dc.p,
                                                                      rcur.p, rnet.p);
         FX_CHECK_LAUNCH();
         ++launches;
       }
       const int smem = n * 4 + ((n * 2 + 15) & ~15);
-      FX_CHECK_CUDA(cudaFuncSetAttribute(attn_rows_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(attn_rows_kernel), smem));
       int per_sm = 1;
       FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, attn_rows_kernel,
                                                                   kRowThreads, smem));

@@ -5,7 +5,10 @@
 #include <new>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <thread>
+#include <utility>
 
 #include "fx_internal.h"
 
@@ -67,6 +70,19 @@ void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a) {
   cudaEventRecord(b, s);
   ctx->timer.pending.push_back({stage, a, b});
   if (ctx->timer.pending.size() > 4096) ctx->timer.resolve();
+}
+
+int raise_smem_limit(const void *func, int bytes) {
+  int dev = 0;
+  FX_CHECK_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> limit;  // (kernel, device)
+  std::lock_guard<std::mutex> lock(mu);
+  int &cur = limit[{func, dev}];
+  if (bytes <= cur) return FX_OK;
+  FX_CHECK_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  cur = bytes;
+  return FX_OK;
 }
 
 // Deduplicated clique-expansion adjacency (H/src/data/circuit.rs:154-171),

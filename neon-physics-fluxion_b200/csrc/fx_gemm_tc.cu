@@ -372,7 +372,27 @@ static int get_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap *
   return FX_OK;
 }
 
-static DevBuf<unsigned int> g_tc_err;
+// Error word of the tensor-core GEMMs, one per device (a library global).
+constexpr int kMaxDevices = 64;
+static DevBuf<unsigned int> g_tc_err[kMaxDevices];
+static std::mutex g_tc_mu;
+
+static int tc_err_word(unsigned int **out) {
+  int dev = 0;
+  FX_CHECK_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("tensor-core GEMM: device %d beyond the supported %d", dev, kMaxDevices);
+    return FX_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(g_tc_mu);
+  if (!g_tc_err[dev].p) {
+    AllocScope global_alloc(nullptr);  // a library global: plain cudaMalloc
+    FX_TRY(g_tc_err[dev].alloc(1));
+    FX_CHECK_CUDA(cudaMemset(g_tc_err[dev].p, 0, 4));
+  }
+  *out = g_tc_err[dev].p;
+  return FX_OK;
+}
 
 // half == false: D = A B^T on G x G operands (epilogue: S, formats).
 // half == true: the two (G/2) x G x (G/2) products of the even/odd halves
@@ -401,31 +421,17 @@ static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands 
     talo = ta;
     tblo = tb;
   }
-  {
-    // one-time set-up, shared by all contexts and host threads
-    static std::mutex mu;
-    static bool attr_set = false;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!attr_set) {
-      FX_CHECK_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<PREC>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Cfg::kSmem));
-      attr_set = true;
-    }
-    if (!g_tc_err.p) {
-      AllocScope global_alloc(nullptr);  // a library global: plain cudaMalloc
-      FX_TRY(g_tc_err.alloc(1));
-      FX_CHECK_CUDA(cudaMemset(g_tc_err.p, 0, 4));
-    }
-  }
+  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(tc_gemm_kernel<PREC>), Cfg::kSmem));
+  unsigned int *err = nullptr;
+  FX_TRY(tc_err_word(&err));
   if (half) {
     dim3 grid(G / kTcBN, h / kTcBM, 2);
     tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(
-        ta, talo, tb, tblo, G, h, h, G, nullptr, nullptr, nullptr, nullptr, part, g_tc_err.p);
+        ta, talo, tb, tblo, G, h, h, G, nullptr, nullptr, nullptr, nullptr, part, err);
   } else {
     dim3 grid(G / kTcBN, G / kTcBM);
     tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(
-        ta, talo, tb, tblo, G, G, 0, 0, S, D.f32, D.lo, D.bf, nullptr, g_tc_err.p);
+        ta, talo, tb, tblo, G, G, 0, 0, S, D.f32, D.lo, D.bf, nullptr, err);
   }
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
@@ -459,8 +465,15 @@ int gemm_half_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
 // Error word of the tensor-core GEMMs (bit 1: a bounded wait expired).
 int gemm_tc_error(unsigned int *out, cudaStream_t s) {
   *out = 0;
-  if (!g_tc_err.p) return FX_OK;
-  FX_CHECK_CUDA(cudaMemcpyAsync(out, g_tc_err.p, 4, cudaMemcpyDeviceToHost, s));
+  int dev = 0;
+  FX_CHECK_CUDA(cudaGetDevice(&dev));
+  const unsigned int *word = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_tc_mu);
+    if (dev >= 0 && dev < kMaxDevices) word = g_tc_err[dev].p;
+  }
+  if (!word) return FX_OK;
+  FX_CHECK_CUDA(cudaMemcpyAsync(out, word, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
   return FX_OK;
 }

@@ -298,4 +298,8 @@ int radix_sort_pairs(uint32_t *k[2], int32_t *v[2], int n, int passes,
 int radix_sort_tiles(int n);
 void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a);
 void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a);
+// Raises kernel `func`'s dynamic shared-memory limit on the current device to
+// at least `bytes`. Under a lock and never downwards, so host threads that
+// launch the kernel with different sizes cannot undo each other's setting.
+int raise_smem_limit(const void *func, int bytes);
 }  // namespace fx

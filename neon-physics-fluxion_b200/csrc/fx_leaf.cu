@@ -490,17 +490,7 @@ static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, const PairPlan &plan, c
     return FX_EINVAL;
   }
   const size_t smem = pair_smem_bytes(plan.nmax);
-  {
-    static std::mutex mu;
-    static bool attr = false;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!attr) {
-      FX_CHECK_CUDA(cudaFuncSetAttribute(leaf_pairs_kernel<T>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)pair_smem_bytes(kPairMax)));
-      attr = true;
-    }
-  }
+  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(leaf_pairs_kernel<T>), (int)smem));
   int per_sm = 0;
   FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_pairs_kernel<T>,
                                                                T, smem));
@@ -626,17 +616,7 @@ static int launch_leaf(fx_ctx *ctx, const LeafBatch &b, bool per_cluster,
                        cudaStream_t s) {
   constexpr int kGroups = 256 / T;
   const size_t smem = (size_t)kGroups * kLeafArrays * kLeafMax * sizeof(float);
-  {
-    static std::mutex mu;  // concurrent host threads (serving workers)
-    static bool attr = false;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!attr) {
-      FX_CHECK_CUDA(cudaFuncSetAttribute(leaf_batch_kernel<T>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-      attr = true;
-    }
-  }
+  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(leaf_batch_kernel<T>), (int)smem));
   if (per_cluster) {
     for (int l = 0; l < b.n_leaves; ++l)
       leaf_batch_kernel<T><<<1, 256, smem, s>>>(b, l);
