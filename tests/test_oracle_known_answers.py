@@ -135,3 +135,69 @@ def test_difference_array_congestion_matches_the_literal_loop(oracle):
         h, v = oracle.congestion(ptr, gate, x, y, 100.0, 80.0, cols, rows)
         c = oracle.congestion_counts(ptr, gate, x, y, 100.0, 80.0, cols, rows)
         assert np.array_equal(c.astype(np.float32), h) and np.array_equal(h, v)
+
+
+def _place_gates_in_leaf_literal(gates, adjacency, region, iters, attract=1.0, repel=0.5,
+                                 damping=0.9, dt=0.1):
+    """placer.rs:210-287 line by line in numpy float32 scalars (every operation
+    rounds to f32, as in Rust): the gate-to-slot map keeps a repeated gate's
+    last slot (:232-235), springs go to the mapped slot (:243-255), and the
+    final positions are written slot by slot (:283-286)."""
+    f = np.float32
+    cx, cy, w, h = (f(v) for v in region)
+    n = len(gates)
+    min_x, min_y = cx - w / f(2.0), cy - h / f(2.0)
+    px = [min_x + (f(i) / f(n)) * w for i in range(n)]
+    py = [min_y + (f(i * 7 % n) / f(n)) * h for i in range(n)]
+    vx, vy = [f(0)] * n, [f(0)] * n
+    g2l = {}
+    for i, g in enumerate(gates):
+        g2l[g] = i
+    for _ in range(iters):
+        fx, fy = [f(0)] * n, [f(0)] * n
+        for g in gates:
+            li = g2l[g]
+            for nb in adjacency[g]:
+                if nb in g2l:
+                    lj = g2l[nb]
+                    fx[li] = fx[li] + f(attract) * (px[lj] - px[li])
+                    fy[li] = fy[li] + f(attract) * (py[lj] - py[li])
+        for i in range(n):
+            for j in range(i + 1, n):
+                dx, dy = px[i] - px[j], py[i] - py[j]
+                dist = max(np.sqrt(dx * dx + dy * dy), f(0.1))
+                force = f(repel) / (dist * dist)
+                fxij, fyij = force * dx / dist, force * dy / dist
+                fx[i], fy[i] = fx[i] + fxij, fy[i] + fyij
+                fx[j], fy[j] = fx[j] - fxij, fy[j] - fyij
+        for i in range(n):
+            vx[i] = (vx[i] + fx[i] * f(dt)) * f(damping)
+            vy[i] = (vy[i] + fy[i] * f(dt)) * f(damping)
+            px[i] = min(max(px[i] + vx[i] * f(dt), min_x), min_x + w)
+            py[i] = min(max(py[i] + vy[i] * f(dt), min_y), min_y + h)
+    out = {}
+    for i, g in enumerate(gates):
+        out[g] = (px[i], py[i])
+    return out
+
+
+def test_leaf_with_repeated_gates_matches_the_literal_loop(oracle):
+    """A leaf listing gates 3 and 1 twice: the oracle's place_leaf gives the
+    literal loop's positions bit for bit (springs on the last slot, last slot
+    written)."""
+    adjacency = {0: [1], 1: [0, 2, 3], 2: [1, 3], 3: [1, 2, 4], 4: [3]}
+    ap = np.zeros(6, np.int32)
+    ai = []
+    for g in range(5):
+        ai += adjacency[g]
+        ap[g + 1] = len(ai)
+    gates = [3, 1, 3, 2, 1, 4]
+    region = (2.0, 3.0, 4.0, 2.0)
+    want = _place_gates_in_leaf_literal(gates, adjacency, region, 12)
+    x = np.full(5, 9.0, np.float32)
+    y = np.full(5, 9.0, np.float32)
+    oracle.place_leaf(np.array(gates), ap, np.array(ai, np.int32), region, 12, 1.0, 0.5, 0.9,
+                      0.1, x, y)
+    for g, (wx, wy) in want.items():
+        assert x[g] == wx and y[g] == wy, g
+    assert x[0] == 9.0 and y[0] == 9.0  # not in the leaf
