@@ -201,3 +201,174 @@ def test_leaf_with_repeated_gates_matches_the_literal_loop(oracle):
     for g, (wx, wy) in want.items():
         assert x[g] == wx and y[g] == wy, g
     assert x[0] == 9.0 and y[0] == 9.0  # not in the leaf
+
+
+def _sinf():
+    """The platform C library's sinf, which Rust's f32::sin calls on Linux."""
+    import ctypes
+    import ctypes.util
+    libm = ctypes.CDLL(ctypes.util.find_library("m"))
+    libm.sinf.restype = ctypes.c_float
+    libm.sinf.argtypes = [ctypes.c_float]
+    return lambda v: np.float32(libm.sinf(float(v)))
+
+
+def _fiedler_literal(gates, adjacency, iters):
+    """partitioner.rs:106-185 compute_fiedler_vector line by line in float32."""
+    f = np.float32
+    sinf = _sinf()
+    n = len(gates)
+    if n <= 1:
+        return [f(0)] * n
+    g2l = {}
+    for i, g in enumerate(gates):
+        g2l[g] = i
+    degree = [f(0)] * n
+    pairs = []
+    for g in gates:
+        for nb in adjacency[g]:
+            if nb in g2l:
+                lg = g2l[g]
+                pairs.append((lg, g2l[nb]))
+                degree[lg] = degree[lg] + f(1.0)
+    v = [sinf(f(i) * f(2.71828)) for i in range(n)]
+    norm = f(0)
+    for t in v:
+        norm = norm + t * t
+    norm = np.sqrt(norm)
+    if norm > f(1e-10):
+        v = [t / norm for t in v]
+    for _ in range(iters):
+        lv = [degree[i] * v[i] for i in range(n)]
+        for i, j in pairs:
+            lv[i] = lv[i] - v[j]
+        s = f(0)
+        for t in lv:
+            s = s + t
+        mean = s / f(n)
+        lv = [t - mean for t in lv]
+        norm = f(0)
+        for t in lv:
+            norm = norm + t * t
+        norm = np.sqrt(norm)
+        if norm > f(1e-10):
+            lv = [t / norm for t in lv]
+        v = lv
+    return v
+
+
+def test_fiedler_matches_the_literal_loop(oracle):
+    """The oracle's compute_fiedler_vector against a literal float32
+    transcription on a 40-gate subset of a random netlist (subset listed out
+    of order), 30 iterations: every component bit for bit."""
+    rng = np.random.default_rng(4)
+    n = 60
+    nets = [list(rng.choice(n, size=rng.integers(2, 5), replace=False)) for _ in range(90)]
+    ptr = np.zeros(len(nets) + 1, np.int32)
+    for e, net in enumerate(nets):
+        ptr[e + 1] = ptr[e] + len(net)
+    ap, ai = oracle.build_adjacency(n, ptr, np.concatenate(nets).astype(np.int32))
+    adjacency = {g: list(ai[ap[g]:ap[g + 1]]) for g in range(n)}
+    gates = [int(g) for g in rng.permutation(n)[:40]]
+    want = _fiedler_literal(gates, adjacency, 30)
+    got = oracle.fiedler_vector(ap, ai, np.array(gates), 30)
+    assert np.array_equal(got, np.array(want, np.float32))
+
+
+def _refine_literal(net_ptr, net_gate, x, y, chip_w, chip_h, max_iters, max_move, threshold,
+                    cols, rows):
+    """refiner.rs:34-126 with grid.rs and congestion.rs:11-93, line by line in
+    float32; returns the positions and the number of iterations that moved
+    gates."""
+    f = np.float32
+    x, y = [f(v) for v in x], [f(v) for v in y]
+    cw, ch = f(chip_w) / f(cols), f(chip_h) / f(rows)
+    cap = (cw + ch) * f(0.5)
+
+    def cell_at(px, py):
+        def cast(v):  # Rust's saturating `as usize`
+            return 0 if not v > 0 else int(min(float(v), 2.0 ** 64 - 1))
+        return min(cast(px / cw), cols - 1), min(cast(py / ch), rows - 1)
+
+    def congestion():
+        h = [f(0)] * (cols * rows)
+        for e in range(len(net_ptr) - 1):
+            gs = net_gate[net_ptr[e]:net_ptr[e + 1]]
+            if len(gs) < 2:
+                continue
+            mnx, mxx = f(np.finfo(np.float32).max), f(np.finfo(np.float32).min)
+            mny, mxy = mnx, mxx
+            for g in gs:
+                mnx, mxx = min(mnx, x[g]), max(mxx, x[g])
+                mny, mxy = min(mny, y[g]), max(mxy, y[g])
+            c0, r0 = cell_at(mnx, mny)
+            c1, r1 = cell_at(mxx, mxy)
+            for r in range(r0, r1 + 1):
+                for c in range(c0, c1 + 1):
+                    h[r * cols + c] = h[r * cols + c] + f(1.0)
+        return h  # v equals h cell for cell
+
+    def overflow(h, c, r):
+        t = h[r * cols + c] + h[r * cols + c]
+        return max(t - cap, f(0.0))
+
+    prev, stall, moved_iters = f(np.finfo(np.float32).max), 0, 0
+    for _ in range(max_iters):
+        h = congestion()
+        total = f(0)
+        for r in range(rows):
+            for c in range(cols):
+                total = total + overflow(h, c, r)
+        if total <= f(threshold):
+            break
+        if abs(prev - total) < f(0.01) * max(prev, f(1.0)):
+            stall += 1
+            if stall >= 10:
+                break
+        else:
+            stall = 0
+        prev = total
+        hot = {(c, r) for r in range(rows) for c in range(cols)
+               if overflow(h, c, r) > f(threshold)}
+        for g in [g for g in range(len(x)) if cell_at(x[g], y[g]) in hot]:
+            gx, gy = x[g], y[g]
+            col, row = cell_at(gx, gy)
+            best = None
+            for dr in range(-3, 4):
+                for dc in range(-3, 4):
+                    if dr == 0 and dc == 0:
+                        continue
+                    nc, nr = col + dc, row + dr
+                    if 0 <= nc < cols and 0 <= nr < rows:
+                        t = h[nr * cols + nc] + h[nr * cols + nc]
+                        if best is None or t < best[0]:
+                            best = (t, nc, nr)
+            if best is None:
+                continue
+            tx, ty = (f(best[1]) + f(0.5)) * cw, (f(best[2]) + f(0.5)) * ch
+            dx = min(max(tx - gx, f(-max_move)), f(max_move))
+            dy = min(max(ty - gy, f(-max_move)), f(max_move))
+            x[g] = min(max(gx + dx, f(0.0)), f(chip_w))
+            y[g] = min(max(gy + dy, f(0.0)), f(chip_h))
+        moved_iters += 1
+    return np.array(x, np.float32), np.array(y, np.float32), moved_iters
+
+
+def test_refine_matches_the_literal_loop(oracle):
+    """The oracle's refine_placement against a literal float32 transcription:
+    80 gates crowded into one corner of a 40 x 40 die, 8 x 8 grid, up to 25
+    iterations; positions bit for bit and the same number of moving iterations."""
+    rng = np.random.default_rng(8)
+    n = 80
+    nets = [list(rng.choice(n, size=rng.integers(2, 4), replace=False)) for _ in range(120)]
+    ptr = np.zeros(len(nets) + 1, np.int32)
+    for e, net in enumerate(nets):
+        ptr[e + 1] = ptr[e] + len(net)
+    gate = np.concatenate(nets).astype(np.int32)
+    x0 = rng.uniform(0, 12, n).astype(np.float32)
+    y0 = rng.uniform(0, 12, n).astype(np.float32)
+    wx, wy, wit = _refine_literal(ptr, gate, x0, y0, 40.0, 40.0, 25, 5.0, 1.0, 8, 8)
+    gx, gy, git, _ = oracle.refine(ptr, gate, x0, y0, 40.0, 40.0, max_iters=25,
+                                   move_distance=5.0, threshold=1.0, cols=8, rows=8)
+    assert wit > 0
+    assert np.array_equal(gx, wx) and np.array_equal(gy, wy) and git == wit
