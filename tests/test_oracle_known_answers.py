@@ -372,3 +372,44 @@ def test_refine_matches_the_literal_loop(oracle):
                                    move_distance=5.0, threshold=1.0, cols=8, rows=8)
     assert wit > 0
     assert np.array_equal(gx, wx) and np.array_equal(gy, wy) and git == wit
+
+
+def test_attraction_and_damped_step_match_the_literal_loops(oracle):
+    """The plain iteration's spring forces (placer.rs:243-255 over every gate:
+    F_g += k (p_nb - p_g) in adjacency order) and damped step
+    (placer.rs:275-280 with Rust's clamp to the die) against literal float32
+    loops, bit for bit."""
+    f = np.float32
+    rng = np.random.default_rng(6)
+    n = 50
+    nets = [list(rng.choice(n, size=rng.integers(2, 6), replace=False)) for _ in range(70)]
+    ptr = np.zeros(len(nets) + 1, np.int32)
+    for e, net in enumerate(nets):
+        ptr[e + 1] = ptr[e] + len(net)
+    ap, ai = oracle.build_adjacency(n, ptr, np.concatenate(nets).astype(np.int32))
+    x = rng.uniform(0, 30, n).astype(np.float32)
+    y = rng.uniform(0, 30, n).astype(np.float32)
+    k = 0.75
+    fx, fy = oracle.attraction_f32(ap, ai, x, y, k)
+    for g in range(n):
+        ax = ay = f(0)
+        for q in range(ap[g], ap[g + 1]):
+            ax = ax + f(k) * (x[ai[q]] - x[g])
+            ay = ay + f(k) * (y[ai[q]] - y[g])
+        assert fx[g] == ax and fy[g] == ay, g
+    vx = rng.normal(0, 3, n).astype(np.float32)
+    vy = rng.normal(0, 3, n).astype(np.float32)
+    forces_x = (fx * f(40)).astype(np.float32)  # large enough to push some gates off the die
+    forces_y = (fy * f(40)).astype(np.float32)
+    ox, oy, ovx, ovy = x.copy(), y.copy(), vx.copy(), vy.copy()
+    oracle.integrate(ox, oy, ovx, ovy, forces_x, forces_y, 0.1, 0.9, (0.0, 0.0, 30.0, 30.0))
+    clamped = 0
+    for g in range(n):
+        wvx = (vx[g] + forces_x[g] * f(0.1)) * f(0.9)
+        wvy = (vy[g] + forces_y[g] * f(0.1)) * f(0.9)
+        px, py = x[g] + wvx * f(0.1), y[g] + wvy * f(0.1)
+        wx = min(max(px, f(0.0)), f(30.0))
+        wy = min(max(py, f(0.0)), f(30.0))
+        clamped += (wx != px) + (wy != py)
+        assert (ovx[g], ovy[g], ox[g], oy[g]) == (wvx, wvy, wx, wy), g
+    assert clamped > 0
