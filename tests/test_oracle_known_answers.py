@@ -413,3 +413,49 @@ def test_attraction_and_damped_step_match_the_literal_loops(oracle):
         clamped += (wx != px) + (wy != py)
         assert (ovx[g], ovy[g], ox[g], oy[g]) == (wvx, wvy, wx, wy), g
     assert clamped > 0
+
+
+def _bisect_literal(gates, adjacency, depth, leaves, counter, max_leaf=64, min_cluster=8,
+                    balance=0.4, iters=30):
+    """partitioner.rs:63-104 recursive_bisect and :186-212 split_by_fiedler
+    line by line (Rust's sort_by is stable, as is Python's sort)."""
+    counter[0] += 1
+    n = len(gates)
+    if n <= max_leaf or n <= min_cluster:
+        leaves.append((list(gates), depth))
+        return
+    fiedler = _fiedler_literal(gates, adjacency, iters)
+    order = sorted(range(n), key=lambda i: fiedler[i])
+    min_size = int(np.ceil(np.float32(n) * np.float32(balance)))
+    split = min(max(n // 2, min_size), n - min_size)
+    left = [gates[i] for i in order[:split]]
+    right = [gates[i] for i in order[split:]]
+    if not left or not right:
+        leaves.append((list(gates), depth))
+        return
+    _bisect_literal(left, adjacency, depth + 1, leaves, counter, max_leaf, min_cluster, balance,
+                    iters)
+    _bisect_literal(right, adjacency, depth + 1, leaves, counter, max_leaf, min_cluster, balance,
+                    iters)
+
+
+def test_hierarchy_matches_the_literal_bisection(oracle):
+    """The oracle's build_hierarchy against a literal recursive_bisect over the
+    literal Fiedler vector: 400 gates of a random netlist, default partition
+    settings; the same leaves (gates in order), depths and node count."""
+    rng = np.random.default_rng(10)
+    n = 400
+    nets = [list(rng.choice(n, size=rng.integers(2, 5), replace=False)) for _ in range(520)]
+    ptr = np.zeros(len(nets) + 1, np.int32)
+    for e, net in enumerate(nets):
+        ptr[e + 1] = ptr[e] + len(net)
+    ap, ai = oracle.build_adjacency(n, ptr, np.concatenate(nets).astype(np.int32))
+    adjacency = {g: list(ai[ap[g]:ap[g + 1]]) for g in range(n)}
+    leaves, counter = [], [0]
+    _bisect_literal(list(range(n)), adjacency, 0, leaves, counter)
+    h = oracle.build_hierarchy(n, ap, ai, 100.0, 100.0)
+    lp, lg = h["leaf_ptr"], h["leaf_gate"]
+    assert len(leaves) > 4 and len(lp) - 1 == len(leaves)
+    for l, (gs, depth) in enumerate(leaves):
+        assert list(lg[lp[l]:lp[l + 1]]) == gs and h["leaf_depth"][l] == depth, l
+    assert h["num_nodes"] == counter[0]
