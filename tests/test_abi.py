@@ -116,3 +116,25 @@ def test_adjacency_rejects_bad_csr(fx):
     c = fx.Circuit.from_nets([[0, 7]], 3)
     with pytest.raises(fx.FluxionError):
         fx.build_adjacency(c)
+
+
+def test_python_constants_match_the_header():
+    """Every FX_* integer constant of the ctypes mirror equals the header's
+    #define of the same name, and the header's schedule, precision, stage,
+    status and job codes all have a Python twin."""
+    from fluxion_b200 import _lib
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    defines = {k: int(v) for k, v in re.findall(r"#define\s+(FX_[A-Z0-9_]+)\s+(-?\d+)\b", text)}
+    mirrored = {k: v for k, v in vars(_lib).items() if k.startswith("FX_") and isinstance(v, int)}
+    assert mirrored
+    for k, v in mirrored.items():
+        assert k in defines and defines[k] == v, k
+    for k in defines:
+        if k.startswith(("FX_LEAF_", "FX_DCT_", "FX_PART_", "FX_JOB_", "FX_E")):
+            assert k in mirrored, k
+    # stage codes index the STAGES name list
+    stages = {k[len("FX_STAGE_"):].lower(): v for k, v in defines.items()
+              if k.startswith("FX_STAGE_") and k != "FX_STAGE_COUNT"}
+    assert len(_lib.STAGES) == defines["FX_STAGE_COUNT"] == len(stages)
+    for name, code in stages.items():
+        assert _lib.STAGES[code] == name, name
