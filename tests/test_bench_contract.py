@@ -1,0 +1,39 @@
+"""bench.py's JSON line, the form the round's driver reads: the reference arm
+(host cores only, so it runs here) prints one line with every required key."""
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _line(*args):
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), *args], capture_output=True,
+                       text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    return json.loads(lines[0])
+
+
+def test_reference_arm_line_has_the_required_keys():
+    d = _line("--impl", "reference", "--workload", "leaves", "--steps", "1", "--warmup", "0")
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+              "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["n_gpus"] == 1 and d["value"] > 0
+    assert d["scaling"] in ("weak", "strong") and isinstance(d["higher_is_better"], bool)
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
+    assert cb["value"] == d["value"] and cb["unit"] == d["unit"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    assert "workload" in d["config"]
+
+
+def test_unavailable_arms_say_why():
+    d = _line("--impl", "reference", "--workload", "precision", "--steps", "1", "--warmup", "0")
+    assert d["impl"] == "reference" and d["unavailable"]
