@@ -37,3 +37,22 @@ def test_reference_arm_line_has_the_required_keys():
 def test_unavailable_arms_say_why():
     d = _line("--impl", "reference", "--workload", "precision", "--steps", "1", "--warmup", "0")
     assert d["impl"] == "reference" and d["unavailable"]
+
+
+def test_reference_arm_under_torchrun_prints_one_line():
+    """Launched as the driver launches N > 1 (torchrun, one process per rank):
+    rank 0 alone prints the line, and every rank exits 0."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                        "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+                        "--master-port", str(port), str(ROOT / "bench.py"), "--impl", "reference",
+                        "--workload", "leaves", "--gpus", "2", "--steps", "1", "--warmup", "0"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
