@@ -459,3 +459,14 @@ def test_hierarchy_matches_the_literal_bisection(oracle):
     for l, (gs, depth) in enumerate(leaves):
         assert list(lg[lp[l]:lp[l + 1]]) == gs and h["leaf_depth"][l] == depth, l
     assert h["num_nodes"] == counter[0]
+
+
+def test_circuit_basic_shared_and_touching_counts(oracle):
+    # circuit.rs:196-217 test_circuit_basic: nets {0,1}, {1,2};
+    # count_shared_nets([0], [1]) = 1 and count_nets_touching([1]) = 2. In the
+    # attention score shared / touching(i) (attention.rs:64-72) that is
+    # scores[1][0] = 1 / 2 and scores[0][1] = 1 / 1; gates 0 and 2 share none.
+    scores, tops = oracle.attention_level([0, 2, 4], [0, 1, 1, 2], [[0], [1], [2]], top_k=10)
+    want = np.array([[0, 1, 0], [0.5, 0, 0.5], [0, 1, 0]], np.float32)
+    assert np.array_equal(scores, want)
+    assert tops == [[1], [0, 2], [1]]
