@@ -213,7 +213,7 @@ def algorithmic(n, m, p, a, G, gc):
         # net_ptr, pins, positions, difference array RMW, counts
         "congestion": 4 * (m + 1) + 4 * p + 8 * n + 2 * 4 * (gc + 1) ** 2 + 4 * gc * gc,
     }
-    f = {"density": 4 * 2 * G ** 3}  # 8 G^3: the four DCT GEMMs of the survey
+    f = {"density": 4 * 2 * G ** 3}  # 8 G^3: the four dense G x G DCT GEMMs of one solve
     return b, f
 
 

@@ -376,7 +376,7 @@ int fx_refine(fx_ctx *ctx, fx_design *design, const fx_refine_cfg *cfg,
               float *x, float *y, fx_refine_stats *stats, uint32_t *out_counts);
 
 /* ---- serving: continuous batching of placement and ECO jobs ------------- */
-/* A request server on one GPU (the survey's serving pattern; the reference
+/* A request server on one GPU (continuous batching; the reference
  * has no server: FluxionEngine.place runs one placement per process,
  * H/python/fluxion/engine.py:25-50). Jobs:
  *   FX_JOB_PLACE  the reference's main.rs flow (H/src/main.rs:74-111) on a
