@@ -154,8 +154,9 @@ int fx_congestion(fx_ctx *ctx, fx_design *design, const float *x,
  * The work is enqueued on the context's stream and the call returns without
  * waiting; results are ready after fx_ctx_synchronize (or anything ordered
  * after that stream). The first call on a device sets the scratch up
- * (cudaGetSymbolAddress, then a synchronous zeroing), so make that first
- * call before any stream capture begins. Calls share the scratch: two calls
+ * (cudaGetSymbolAddress, then a zeroing on the context's stream that the
+ * call waits for before it launches anything), so make that first call
+ * before any stream capture begins. Calls share the scratch: two calls
  * that overlap on one device (different contexts, streams or host threads)
  * race and corrupt each other's counts; order them. */
 int fx_congestion_noalloc(fx_ctx *ctx, const fx_design *design, const float *d_x,
@@ -268,6 +269,17 @@ int fx_iter_cfg_default(fx_iter_cfg *cfg);
  * leave them on the device). stats may be NULL. */
 int fx_force_iterate(fx_ctx *ctx, fx_design *design, const fx_iter_cfg *cfg,
                      int32_t iters, float *x, float *y, fx_iter_stats *stats);
+
+/* Force trace (no reference counterpart; a parity and diagnosis aid for
+ * fx_force_iterate). While enabled, every plain iteration also stores, per
+ * gate, the total f32 force its damped step integrated (attraction +
+ * Barnes-Hut + density, exactly the value placer.rs:276-277 multiplies by
+ * dt) and the positions and velocities it started from;
+ * fx_design_trace_get returns those of the last iteration run (host
+ * arrays of n_gates floats, each may be NULL). */
+int fx_design_trace(fx_design *design, int enable);
+int fx_design_trace_get(fx_design *design, float *out_fx, float *out_fy, float *out_x0,
+                        float *out_y0, float *out_vx0, float *out_vy0);
 
 /* Single-stage entry points on the resident positions (used by the parity
  * tests; each writes float32 forces to host arrays). */

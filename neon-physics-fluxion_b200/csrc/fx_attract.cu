@@ -91,6 +91,7 @@ struct StepArgs {
   double *e_part;
   unsigned int *done;
   double *energy;
+  float *trace;  // or null: {F_x, F_y, x, y, v_x, v_y} of every gate (6 x n)
 };
 
 __device__ __forceinline__ int bin_of(float v, float bin, int G) {
@@ -134,8 +135,18 @@ fused_step_kernel(StepArgs a) {
       fy = __fadd_rn(fy, __fmul_rn(__fmul_rn(q, a.ey[bi]), a.dweight));
       if (a.phi) e_acc = 0.5 * (double)q * (double)a.phi[bi] * (double)a.dweight;
     }
-    const float vx = __fmul_rn(__fadd_rn(a.vx[g], __fmul_rn(fx, a.dt)), a.damp);
-    const float vy = __fmul_rn(__fadd_rn(a.vy[g], __fmul_rn(fy, a.dt)), a.damp);
+    const float vx0 = a.vx[g], vy0 = a.vy[g];
+    if (a.trace) {
+      const size_t n = (size_t)a.n;
+      a.trace[g] = fx;
+      a.trace[n + g] = fy;
+      a.trace[2 * n + g] = px;
+      a.trace[3 * n + g] = py;
+      a.trace[4 * n + g] = vx0;
+      a.trace[5 * n + g] = vy0;
+    }
+    const float vx = __fmul_rn(__fadd_rn(vx0, __fmul_rn(fx, a.dt)), a.damp);
+    const float vy = __fmul_rn(__fadd_rn(vy0, __fmul_rn(fy, a.dt)), a.damp);
     nx = clampf_ref(__fadd_rn(px, __fmul_rn(vx, a.dt)), a.xlo, a.xhi);
     ny = clampf_ref(__fadd_rn(py, __fmul_rn(vy, a.dt)), a.ylo, a.yhi);
     a.vx[g] = vx;
@@ -292,7 +303,7 @@ extern "C" int fx_stage_attraction(fx_ctx *ctx, fx_design *d, float k,
 namespace fx {
 int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
                 int precision, bool need_phi, cudaStream_t s);
-int gemm_tc_error(unsigned int *out, cudaStream_t s);
+int gemm_tc_error(fx_ctx *ctx, unsigned int *out, cudaStream_t s);
 }
 
 extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
@@ -309,6 +320,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   cudaStream_t s = ctx->stream, s2 = ctx->stream2;
   if (x) FX_TRY(fx_design_set_positions(d, x, y));
   FX_TRY(step_alloc(d, s));
+  if (d->trace_on) FX_TRY(d->trace.alloc((size_t)d->n * 6));
   const bool use_bh = c.repel_weight != 0.f;
   const bool use_dens = c.density_bins > 0 && c.density_weight != 0.f;
   const bool use_cong = c.cong_cols > 0;
@@ -368,6 +380,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     a.e_part = d->step.e_part.p;
     a.done = d->step.done.p;
     a.energy = d->step.energy.p;
+    a.trace = d->trace_on ? d->trace.p : nullptr;
     cudaEvent_t ev;
     timer_begin(ctx, FX_STAGE_ATTRACT_INTEGRATE, s, &ev);
     fused_step_kernel<<<nb, kGates, 0, s>>>(a);
@@ -455,7 +468,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   }
   if (use_dens && c.dct_precision != FX_DCT_SIMT) {
     unsigned int tc_err = 0;
-    FX_TRY(gemm_tc_error(&tc_err, s));
+    FX_TRY(gemm_tc_error(ctx, &tc_err, s));
     if (tc_err) {
       set_error("tensor-core GEMM: a bounded wait expired (error word %u)", tc_err);
       return FX_ETIMEOUT;
@@ -466,5 +479,31 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   st.bh_nodes = use_bh ? d->n - 1 : 0;
   if (x && !copied_out) FX_TRY(fx_design_get_positions(d, x, y));
   if (stats) *stats = st;
+  return FX_OK;
+}
+
+extern "C" int fx_design_trace(fx_design *d, int enable) {
+  if (!d) return FX_EINVAL;
+  d->trace_on = enable != 0;
+  return FX_OK;
+}
+
+extern "C" int fx_design_trace_get(fx_design *d, float *out_fx, float *out_fy, float *out_x,
+                                   float *out_y, float *out_vx, float *out_vy) {
+  if (!d || !d->ctx) return FX_EINVAL;
+  if (!d->trace.p || d->trace.n < (size_t)d->n * 6) {
+    set_error("fx_design_trace_get: no traced iteration (enable fx_design_trace, then "
+              "run fx_force_iterate)");
+    return FX_EINVAL;
+  }
+  fx_ctx *ctx = d->ctx;
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  float *outs[6] = {out_fx, out_fy, out_x, out_y, out_vx, out_vy};
+  const size_t n = (size_t)d->n;
+  for (int i = 0; i < 6; ++i)
+    if (outs[i])
+      FX_CHECK_CUDA(cudaMemcpyAsync(outs[i], d->trace.p + i * n, n * 4,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+  FX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
   return FX_OK;
 }

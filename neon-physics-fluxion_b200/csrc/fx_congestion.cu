@@ -316,8 +316,11 @@ std::mutex g_na_mu;
 unsigned char *g_na_ptr[kNaMaxDevices] = {};
 bool g_na_dirty[kNaMaxDevices] = {};
 
-// Once per device: the device address of the scratch array, zeroed.
-int noalloc_scratch(int device, unsigned char **out) {
+// Once per device: the device address of the scratch array, zeroed. The
+// zeroing runs on the calling context's stream (non-blocking, so it would
+// not wait for a legacy-stream memset) and set-up waits for it, so this
+// call's kernels and every later call see a zero array.
+int noalloc_scratch(int device, cudaStream_t s, unsigned char **out) {
   if (device < 0 || device >= kNaMaxDevices) {
     set_error("fx_congestion_noalloc: device %d out of range", device);
     return FX_EINVAL;
@@ -330,7 +333,8 @@ int noalloc_scratch(int device, unsigned char **out) {
                 cudaGetErrorString(e));
       return FX_ECUDA;
     }
-    FX_CHECK_CUDA(cudaMemset(p, 0, kNoAllocScratchBytes));
+    FX_CHECK_CUDA(cudaMemsetAsync(p, 0, kNoAllocScratchBytes, s));
+    FX_CHECK_CUDA(cudaStreamSynchronize(s));
     g_na_ptr[device] = static_cast<unsigned char *>(p);
     g_na_dirty[device] = false;
   }
@@ -360,8 +364,8 @@ extern "C" int fx_congestion_noalloc(fx_ctx *ctx, const fx_design *d, const floa
   FX_CHECK_CUDA(cudaSetDevice(ctx->device));
   std::lock_guard<std::mutex> lock(g_na_mu);
   unsigned char *sc = nullptr;
-  FX_TRY(noalloc_scratch(ctx->device, &sc));
   cudaStream_t s = ctx->stream;
+  FX_TRY(noalloc_scratch(ctx->device, s, &sc));
   if (g_na_dirty[ctx->device]) {
     FX_CHECK_CUDA(cudaMemsetAsync(sc, 0, kNoAllocScratchBytes, s));
     g_na_dirty[ctx->device] = false;

@@ -222,6 +222,20 @@ extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
     delete c;
     return FX_ECUDA;
   }
+  // The word is zeroed on the primary stream and the creation waits for it,
+  // so no GEMM of this context (on either stream) can see a stale value.
+  if (cudaMalloc((void **)&c->tc_err, sizeof(unsigned int)) != cudaSuccess ||
+      cudaMemsetAsync(c->tc_err, 0, sizeof(unsigned int), c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error("error word allocation failed");
+    if (c->tc_err) cudaFree(c->tc_err);
+    cudaEventDestroy(c->fork);
+    cudaEventDestroy(c->join);
+    cudaStreamDestroy(c->stream);
+    cudaStreamDestroy(c->stream2);
+    delete c;
+    return FX_ECUDA;
+  }
   // Freed stream-ordered allocations stay in the device's pool for reuse,
   // so a call's temporaries cost no driver allocation after the first.
   cudaMemPool_t pool;
@@ -244,6 +258,7 @@ extern "C" int fx_ctx_destroy(fx_ctx *ctx) {
     if (e) cudaEventDestroy(e);
   cudaEventDestroy(ctx->fork);
   cudaEventDestroy(ctx->join);
+  if (ctx->tc_err) cudaFree(ctx->tc_err);
   cudaStreamDestroy(ctx->stream);
   cudaStreamDestroy(ctx->stream2);
   delete ctx;

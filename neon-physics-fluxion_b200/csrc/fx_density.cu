@@ -26,7 +26,7 @@
 
 namespace fx {
 
-int gemm_tc_error(unsigned int *out, cudaStream_t s);
+int gemm_tc_error(fx_ctx *ctx, unsigned int *out, cudaStream_t s);
 
 constexpr double kAreaScale = 4294967296.0;  // 2^32
 
@@ -467,7 +467,7 @@ extern "C" int fx_stage_density(fx_ctx *ctx, fx_design *d, int32_t bins,
   FX_CHECK_CUDA(cudaMemcpyAsync(&e, w.energy.p + 4097, 8, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
   unsigned int tc_err = 0;
-  FX_TRY(gemm_tc_error(&tc_err, s));
+  FX_TRY(gemm_tc_error(ctx, &tc_err, s));
   if (tc_err) {
     set_error("tensor-core GEMM: a bounded wait expired (error word %u)", tc_err);
     return FX_ETIMEOUT;

@@ -372,28 +372,6 @@ static int get_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap *
   return FX_OK;
 }
 
-// Error word of the tensor-core GEMMs, one per device (a library global).
-constexpr int kMaxDevices = 64;
-static DevBuf<unsigned int> g_tc_err[kMaxDevices];
-static std::mutex g_tc_mu;
-
-static int tc_err_word(unsigned int **out) {
-  int dev = 0;
-  FX_CHECK_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) {
-    set_error("tensor-core GEMM: device %d beyond the supported %d", dev, kMaxDevices);
-    return FX_EINVAL;
-  }
-  std::lock_guard<std::mutex> lock(g_tc_mu);
-  if (!g_tc_err[dev].p) {
-    AllocScope global_alloc(nullptr);  // a library global: plain cudaMalloc
-    FX_TRY(g_tc_err[dev].alloc(1));
-    FX_CHECK_CUDA(cudaMemset(g_tc_err[dev].p, 0, 4));
-  }
-  *out = g_tc_err[dev].p;
-  return FX_OK;
-}
-
 // half == false: D = A B^T on G x G operands (epilogue: S, formats).
 // half == true: the two (G/2) x G x (G/2) products of the even/odd halves
 // (A: 2 x (G/2) x (G/2), B: 2 x G x (G/2)) as raw partials in `part`.
@@ -422,8 +400,7 @@ static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands 
     tblo = tb;
   }
   FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(tc_gemm_kernel<PREC>), Cfg::kSmem));
-  unsigned int *err = nullptr;
-  FX_TRY(tc_err_word(&err));
+  unsigned int *err = ctx->tc_err;
   if (half) {
     dim3 grid(G / kTcBN, h / kTcBM, 2);
     tc_gemm_kernel<PREC><<<grid, kTcThreads, Cfg::kSmem, s>>>(
@@ -462,19 +439,17 @@ int gemm_half_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
   return FX_EINVAL;
 }
 
-// Error word of the tensor-core GEMMs (bit 1: a bounded wait expired).
-int gemm_tc_error(unsigned int *out, cudaStream_t s) {
+// Error word of the context's tensor-core GEMMs (bit 1: a bounded wait
+// expired). A set word is reported once and cleared, so one expired wait
+// does not fail every later call of the context.
+int gemm_tc_error(fx_ctx *ctx, unsigned int *out, cudaStream_t s) {
   *out = 0;
-  int dev = 0;
-  FX_CHECK_CUDA(cudaGetDevice(&dev));
-  const unsigned int *word = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_tc_mu);
-    if (dev >= 0 && dev < kMaxDevices) word = g_tc_err[dev].p;
-  }
-  if (!word) return FX_OK;
-  FX_CHECK_CUDA(cudaMemcpyAsync(out, word, 4, cudaMemcpyDeviceToHost, s));
+  FX_CHECK_CUDA(cudaMemcpyAsync(out, ctx->tc_err, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (*out) {
+    FX_CHECK_CUDA(cudaMemsetAsync(ctx->tc_err, 0, 4, s));
+    FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  }
   return FX_OK;
 }
 

@@ -242,6 +242,9 @@ struct fx_ctx {
   cudaStream_t stream2 = nullptr;  // side stream (density || Barnes-Hut)
   cudaEvent_t fork = nullptr, join = nullptr;
   int num_sms = 0;
+  // Error word of this context's tensor-core GEMMs (bit 1: a bounded wait
+  // expired); zeroed at creation, cleared again after it is reported.
+  unsigned int *tc_err = nullptr;
   fx::StageTimer timer;
   int64_t launches = 0;
   cudaEvent_t marks[16] = {};
@@ -273,6 +276,10 @@ struct fx_design {
   bool pos_in_box = false, saved_in_box = false;
   fx::DevBuf<unsigned int> box_flag;
   fx::DevBuf<float2> fattr;      // attraction-only force output (stage API)
+  // force trace (fx_design_trace): each plain iteration stores its total
+  // force, start positions and start velocities (6 x n floats)
+  bool trace_on = false;
+  fx::DevBuf<float> trace;
   // workspaces
   fx::BHWork bh;
   fx::DensityWork dens;

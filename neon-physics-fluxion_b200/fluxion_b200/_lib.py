@@ -160,6 +160,8 @@ SIGNATURES = {
     "fx_design_set_positions": (C.c_int, [P, PF32, PF32]),
     "fx_design_get_positions": (C.c_int, [P, PF32, PF32]),
     "fx_design_save_state": (C.c_int, [P]),
+    "fx_design_trace": (C.c_int, [P, C.c_int]),
+    "fx_design_trace_get": (C.c_int, [P, PF32, PF32, PF32, PF32, PF32, PF32]),
     "fx_design_restore_state": (C.c_int, [P]),
     "fx_design_device_bytes": (C.c_int64, [P]),
     "fx_congestion": (C.c_int, [P, P, PF32, PF32, I32, I32, PU32, PF64, PF64, PF32]),

@@ -253,6 +253,19 @@ class Design:
         """Restores the last save_state (stream-ordered, no host sync)."""
         check(self.lib.fx_design_restore_state(self.handle), "restore_state")
 
+    def trace(self, enable: bool = True) -> None:
+        """fx_design_trace: record each plain iteration's total force and start state."""
+        check(self.lib.fx_design_trace(self.handle, 1 if enable else 0), "fx_design_trace")
+
+    def trace_get(self) -> dict:
+        """The last traced iteration: total force fx, fy and the positions x0, y0 and
+        velocities vx0, vy0 it started from (float32 arrays of n)."""
+        out = {k: np.empty(self.n, np.float32) for k in ("fx", "fy", "x0", "y0", "vx0", "vy0")}
+        check(self.lib.fx_design_trace_get(self.handle, *[ptr(out[k], C.c_float) for k in
+                                                          ("fx", "fy", "x0", "y0", "vx0", "vy0")]),
+              "fx_design_trace_get")
+        return out
+
     def device_bytes(self) -> int:
         return int(self.lib.fx_design_device_bytes(self.handle))
 

@@ -14,36 +14,42 @@ BINARY = PKG / "fluxion"
 DEFAULT_CONFIG = PKG.parent / "config" / "default.yaml"
 
 
+def _require(path: Path, what: str) -> Path:
+    if not path.exists():
+        raise FileNotFoundError(f"{what}: {path}")
+    return path
+
+
 class FluxionEngine:
-    """
-    Usage:
-        engine = FluxionEngine("config/default.yaml")
-        engine.place("circuit.blif")
+    """Places a BLIF netlist with the HAPR flow on the GPU.
+
+    The YAML configuration is parsed once when the engine is made (a missing
+    file raises FileNotFoundError) and kept in `config`. Each `place` call
+    hands the configuration file, the netlist and the output path to the
+    `fluxion` command built next to this module, which writes a DEF file.
     """
 
     def __init__(self, config_path="default.yaml"):
-        self.config_path = Path(config_path)
-        if not self.config_path.exists():
-            raise FileNotFoundError(f"Config not found: {self.config_path}")
-        with open(self.config_path, "r") as f:
-            self.config = yaml.safe_load(f)
+        self.config_path = _require(Path(config_path), "Config not found")
+        self.config = yaml.safe_load(self.config_path.read_text())
 
-    def place(self, input_file: str, output_file: str = "placed.def"):
-        """Runs the full HAPR flow on the GPU through the `fluxion` command."""
-        input_path = Path(input_file)
-        if not input_path.exists():
-            raise FileNotFoundError(f"Input file not found: {input_path}")
+    def _command(self, netlist: Path, output_file) -> list[str]:
         if not BINARY.exists():
             raise FileNotFoundError(f"{BINARY} is missing; build it with "
                                     "`python -c 'import __graft_entry__ as g; g.build()'`")
-        cmd = [str(BINARY), "--config", str(self.config_path), "--input", str(input_path),
-               "--output", str(output_file)]
+        return [str(BINARY), "--config", str(self.config_path), "--input", str(netlist),
+                "--output", str(output_file)]
+
+    def place(self, input_file: str, output_file: str = "placed.def"):
+        """Returns `output_file` once the command has written it; a non-zero
+        exit of the command prints its stderr and raises RuntimeError."""
+        cmd = self._command(_require(Path(input_file), "Input file not found"), output_file)
         print(f"Running FLUXION core: {' '.join(cmd)}")
-        result = subprocess.run(cmd, capture_output=True, text=True)
-        if result.returncode != 0:
-            print("FLUXION Core Error:")
-            print(result.stderr)
-            raise RuntimeError("Placement failed")
-        print(result.stdout)
-        print(f"Placement saved to {output_file}")
-        return output_file
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode == 0:
+            print(proc.stdout)
+            print(f"Placement saved to {output_file}")
+            return output_file
+        print("FLUXION Core Error:")
+        print(proc.stderr)
+        raise RuntimeError("Placement failed")

@@ -431,6 +431,56 @@ def density_forces(x, y, area, die_w, die_h, G, target=0.7, weight=1.0):
     return dict(fx=fx, fy=fy, rho=charge, phi=phi, ex=ex, ey=ey, energy=energy)
 
 
+# ---- the composite plain iteration ------------------------------------------
+def plain_forces(adj_ptr, adj_idx, x, y, area, die_w, die_h, k=1.0, repel=0.5, theta=0.5,
+                 min_dist=0.1, bins=0, target=0.7, weight=0.0, threads=1):
+    """Total force of one plain iteration at positions (x, y): attraction
+    (placer.rs:243-255 over the full adjacency) + Barnes-Hut repulsion (law of
+    placer.rs:258-272, tree rules of BarnesHutTree.cpp) + the DCT Poisson
+    density force (force_electrostatic.py:107-157) when bins > 0.
+
+    Returns f64 = (fx, fy), the FP64 recomputation (Barnes-Hut over each
+    point's interaction list), and f32 = (fx, fy), the same sum in f32 in
+    the device's order ((attraction + Barnes-Hut) + (area * E) * weight) with
+    the field taken from the FP64 solve and rounded once to f32."""
+    x, y = _f32(x), _f32(y)
+    a64 = attraction_f64(adj_ptr, adj_idx, x, y, k)
+    a32 = attraction_f32(adj_ptr, adj_idx, x, y, k)
+    fx64, fy64 = np.array(a64[0], np.float64), np.array(a64[1], np.float64)
+    fx32, fy32 = a32[0].astype(np.float32), a32[1].astype(np.float32)
+    if repel != 0.0:
+        b = bh_forces(x, y, repel, theta, min_dist, threads=threads)
+        fx64 += b["fx"]
+        fy64 += b["fy"]
+        fx32 = (fx32 + b["fx32"]).astype(np.float32)
+        fy32 = (fy32 + b["fy32"]).astype(np.float32)
+    if bins > 0 and weight != 0.0:
+        d = density_forces(x, y, area, die_w, die_h, bins, target, weight)
+        fx64 += d["fx"]
+        fy64 += d["fy"]
+        col, row, _, _ = density_bins(x, y, die_w, die_h, bins)
+        q = np.asarray(area, np.float32)
+        w = np.float32(weight)
+        ex = d["ex"][row, col].astype(np.float32)
+        ey = d["ey"][row, col].astype(np.float32)
+        fx32 = (fx32 + (q * ex).astype(np.float32) * w).astype(np.float32)
+        fy32 = (fy32 + (q * ey).astype(np.float32) * w).astype(np.float32)
+    return dict(f64=(fx64, fy64), f32=(fx32, fy32))
+
+
+def plain_run(adj_ptr, adj_idx, x0, y0, area, die_w, die_h, iters, dt=0.1, damping=0.9,
+              **force_kw):
+    """`iters` plain iterations from (x0, y0) at rest: the f32 forces of
+    plain_forces, then the damped step clamped to the die (placer.rs:275-280).
+    Returns the final positions."""
+    x, y = _f32(x0).copy(), _f32(y0).copy()
+    vx, vy = np.zeros_like(x), np.zeros_like(y)
+    for _ in range(iters):
+        fx, fy = plain_forces(adj_ptr, adj_idx, x, y, area, die_w, die_h, **force_kw)["f32"]
+        integrate(x, y, vx, vy, fx, fy, dt, damping, (0.0, 0.0, die_w, die_h))
+    return x, y
+
+
 # ---- attention scores (attention.rs, hierarchy.rs) -------------------------
 def hierarchy_nodes(leaf_ptr, leaf_gate, leaf_depth):
     """The explicit binary tree of a hierarchy from its leaves in DFS order and

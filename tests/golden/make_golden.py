@@ -1,9 +1,10 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container where the reference is mounted (it reads the reference
-sources; nothing at test time does):
+Run where a checkout of the reference project is at hand, named by the
+FLUXION_REFERENCE environment variable (it reads the reference sources;
+nothing at test time does):
 
-    python tests/golden/make_golden.py
+    FLUXION_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 * golden_dct.npz -- the reference's own ElectrostaticSmoothingForce
   (neon_old_codebase/src/python/fluxion/force_electrostatic.py) on seeded
@@ -15,6 +16,7 @@ sources; nothing at test time does):
 """
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
@@ -22,7 +24,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF_PY = Path("/root/reference/neon_old_codebase/src/python")
+REF_ROOT = Path(os.environ.get("FLUXION_REFERENCE", ""))
+REF_PY = REF_ROOT / "neon_old_codebase" / "src" / "python"
 
 
 def dct_fixtures(out: dict) -> None:
@@ -87,6 +90,8 @@ def bh_fixtures(out: dict) -> None:
 
 
 def main() -> None:
+    if not (REF_PY / "fluxion").is_dir():
+        sys.exit("set FLUXION_REFERENCE to a checkout of the reference project")
     dct: dict = {}
     dct_fixtures(dct)
     np.savez_compressed(HERE / "golden_dct.npz", **dct)

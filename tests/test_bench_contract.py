@@ -1,5 +1,5 @@
-"""bench.py's JSON line, the form the round's driver reads: the reference arm
-(host cores only, so it runs here) prints one line with every required key."""
+"""bench.py's JSON line contract: the reference arm (host cores only, so it
+runs without a GPU) prints one JSON line with every required key."""
 import json
 import subprocess
 import sys

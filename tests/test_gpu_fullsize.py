@@ -96,8 +96,21 @@ def test_density_field_and_forces(fx, full_design, full, oracle):
     area = (c.gate_widths * c.gate_heights).astype(np.float64)
     ref = oracle.density_forces(p.gate_x, p.gate_y, area, c.chip_width, c.chip_height, 1024,
                                 0.7, 1.0)
-    assert _rel(out["ex"], out["ey"], ref["ex"], ref["ey"]) < 1e-4
-    assert _rel(out["fx"], out["fy"], ref["fx"], ref["fy"]) < 1e-4
+    assert _rel(out["ex"], out["ey"], ref["ex"], ref["ey"]) < 1e-5
+    assert _rel(out["fx"], out["fy"], ref["fx"], ref["fy"]) < 1e-5
+
+
+@pytest.mark.parametrize("weight,iters", [(1e-4, 3), (1.0, 1)])
+def test_benchmarked_step_with_density(fx, ctx, full, oracle, weight, iters):
+    """The bench's step at full size: attraction + Barnes-Hut + DCT density
+    (1024 x 1024, FP32) + damped step + 512 x 512 congestion, checked by the
+    same rules as the 20k-gate case (test_gpu_parity._step_parity): the last
+    iteration's total force within 1e-5 of FP64, its step bit for bit, the
+    final congestion counts bit-exact, HPWL and overflow of the run within
+    0.5 % of the oracle's run."""
+    from test_gpu_parity import _step_parity
+    _step_parity(fx, ctx, oracle, full, 1024, weight, iters, (512, 512),
+                 threads=os.cpu_count() or 1)
 
 
 def test_hierarchy(fx, full_design, full, oracle):

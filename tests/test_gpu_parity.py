@@ -309,3 +309,75 @@ def test_graph_replay_matches_eager_iterations(fx, ctx):
         d.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert out[0][2:] == out[1][2:]
+
+
+# ---- the benchmarked step: A + B + C (DCT density) + E, then D + F -----------------
+def _step_parity(fx, ctx, oracle, s, G, weight, iters, cong, threads=1, tol=1e-5):
+    """Runs `iters` plain iterations with the density term on (the composite
+    iteration the bench times; from the second iteration on, the density
+    comes from the step kernel's own scatter of the positions it wrote) and
+    checks the last one against the oracle:
+    * its total per-gate force against the FP64 recomputation at the
+      positions it started from (relative L2 <= tol), and against the
+      oracle's f32 sum (field rounded once to f32);
+    * its damped step, bit for bit, from the traced start state and force;
+    * the congestion counts of the final positions, bit for bit;
+    then the run's HPWL and overflow against the oracle's own run of the
+    same iterations (within 0.5 %)."""
+    c, p = s.circuit, s.placement
+    cols, rows = cong
+    cfg = fx.iter_cfg(density_bins=G, density_weight=weight, cong_cols=cols, cong_rows=rows)
+    area = (c.gate_widths * c.gate_heights).astype(np.float32)
+    d = fx.Design(ctx, c)
+    try:
+        d.trace(True)
+        x, y = p.gate_x.copy(), p.gate_y.copy()
+        st = d.force_iterate(cfg, iters, x, y)
+        t = d.trace_get()
+        counts, hpwl, tot, mx = d.congestion(cols, rows, x, y)
+        ap, ai = d.adjacency()
+    finally:
+        d.close()
+    f = oracle.plain_forces(ap, ai, t["x0"], t["y0"], area, c.chip_width, c.chip_height,
+                            k=1.0, repel=0.5, theta=0.5, min_dist=F32_01, bins=G,
+                            target=0.7, weight=weight, threads=threads)
+    err64 = rel_l2(t["fx"].astype(np.float64), t["fy"].astype(np.float64), *f["f64"])
+    err32 = rel_l2(t["fx"].astype(np.float64), t["fy"].astype(np.float64),
+                   *(v.astype(np.float64) for v in f["f32"]))
+    print(f"step G={G} w={weight} it={iters}: force vs FP64 {err64:.3e}, vs f32 oracle "
+          f"{err32:.3e}")
+    assert err64 <= tol, err64
+    assert err32 <= tol, err32
+    # the damped step of the traced iteration, bit for bit
+    ox, oy = t["x0"].copy(), t["y0"].copy()
+    ovx, ovy = t["vx0"].copy(), t["vy0"].copy()
+    oracle.integrate(ox, oy, ovx, ovy, t["fx"], t["fy"], 0.1, 0.9,
+                     (0.0, 0.0, c.chip_width, c.chip_height))
+    assert np.array_equal(ox, x) and np.array_equal(oy, y)
+    # congestion of the device's final positions: bit-exact counts
+    want = oracle.congestion_counts(c.net_ptr, c.net_gate, x, y, c.chip_width, c.chip_height,
+                                    cols, rows)
+    assert np.array_equal(counts, want)
+    assert hpwl == st.hpwl and tot == st.total_overflow
+    # the oracle's own run: HPWL and overflow within 0.5 %
+    rx, ry = oracle.plain_run(ap, ai, p.gate_x, p.gate_y, area, c.chip_width, c.chip_height,
+                              iters, k=1.0, repel=0.5, theta=0.5, min_dist=F32_01, bins=G,
+                              target=0.7, weight=weight, threads=threads)
+    ref_hpwl = oracle.hpwl_f64(c.net_ptr, c.net_gate, rx, ry)
+    rc = oracle.congestion_counts(c.net_ptr, c.net_gate, rx, ry, c.chip_width, c.chip_height,
+                                  cols, rows).astype(np.float32)
+    _, _, cap = oracle.grid_geometry(c.chip_width, c.chip_height, cols, rows)
+    rt, _ = oracle.overflow(rc, rc, cols, rows, cap)
+    print(f"  hpwl {st.hpwl:.6e} vs oracle {ref_hpwl:.6e}; overflow {st.total_overflow:.6e} "
+          f"vs {rt:.6e}")
+    assert abs(st.hpwl - ref_hpwl) <= 5e-3 * ref_hpwl
+    assert abs(st.total_overflow - rt) <= 5e-3 * max(rt, 1.0)
+    return err64
+
+
+@pytest.mark.parametrize("G", [128, 256])
+@pytest.mark.parametrize("weight", [1e-4, 1.0])
+@pytest.mark.parametrize("iters", [1, 3])
+def test_step_with_density_vs_oracle(fx, ctx, oracle, G, weight, iters):
+    s = fx.synth_plain(9, 20_000, 24_000, 170.0)
+    _step_parity(fx, ctx, oracle, s, G, weight, iters, (128, 128))

@@ -3,6 +3,8 @@ argument, config and input checks (exit codes of H/src/main.rs, before any GPU
 work); FluxionEngine's errors."""
 from __future__ import annotations
 
+import os
+
 import math
 import subprocess
 from pathlib import Path
@@ -31,10 +33,13 @@ def test_blif_reader_follows_the_reference_rules(fx):
     assert _nets(c) == [[0, 1, 4], [1, 2], [2, 3, 4], [0, 5], [1, 5]]
 
 
-REF_SMALL_BLIF = Path("/root/reference/HAPR_fluxion_v4/tests/fixtures/small.blif")
+# the reference project's root, when a checkout is at hand (FLUXION_REFERENCE)
+_REF = os.environ.get("FLUXION_REFERENCE", "")
+REF_SMALL_BLIF = Path(_REF, "HAPR_fluxion_v4", "tests", "fixtures", "small.blif") if _REF else None
 
 
-@pytest.mark.skipif(not REF_SMALL_BLIF.exists(), reason="the reference's fixture is not here")
+@pytest.mark.skipif(REF_SMALL_BLIF is None or not REF_SMALL_BLIF.exists(),
+                    reason="FLUXION_REFERENCE does not name a reference checkout")
 def test_blif_reader_on_the_reference_fixture(fx):
     """The reference's end-to-end fixture (tests/test_integration.py:10-38
     places it), read where it lies: four .gate lines (AND2 a b -> n1, OR2 c d

@@ -470,3 +470,34 @@ def test_circuit_basic_shared_and_touching_counts(oracle):
     want = np.array([[0, 1, 0], [0.5, 0, 0.5], [0, 1, 0]], np.float32)
     assert np.array_equal(scores, want)
     assert tops == [[1], [0, 2], [1]]
+
+
+def test_composite_iteration_oracle_is_consistent(oracle):
+    """plain_forces (the checker of the benchmarked step): its f32 sum agrees
+    with its FP64 recomputation to f32 rounding, the density term is the
+    FP64 density_forces of the same positions, and plain_run's first step is
+    the damped step of those f32 forces."""
+    rng = np.random.default_rng(3)
+    n, die = 3000, 60.0
+    nets = [rng.choice(n, size=rng.integers(2, 6), replace=False) for _ in range(3600)]
+    net_ptr = np.concatenate([[0], np.cumsum([len(e) for e in nets])]).astype(np.int32)
+    net_gate = np.concatenate(nets).astype(np.int32)
+    ap, ai = oracle.build_adjacency(n, net_ptr, net_gate)
+    x = rng.uniform(0, die, n).astype(np.float32)
+    y = rng.uniform(0, die, n).astype(np.float32)
+    area = rng.integers(1, 5, n).astype(np.float32)
+    md = float(np.float32(0.1))
+    base = oracle.plain_forces(ap, ai, x, y, area, die, die, min_dist=md)
+    full = oracle.plain_forces(ap, ai, x, y, area, die, die, min_dist=md, bins=64, weight=1.0)
+    d = oracle.density_forces(x, y, area.astype(np.float64), die, die, 64, 0.7, 1.0)
+    assert np.allclose(full["f64"][0] - base["f64"][0], d["fx"], rtol=1e-12, atol=1e-9)
+    assert np.allclose(full["f64"][1] - base["f64"][1], d["fy"], rtol=1e-12, atol=1e-9)
+    for r in (base, full):
+        num = np.sqrt(sum(((a.astype(np.float64) - b) ** 2).sum() for a, b in zip(r["f32"], r["f64"])))
+        den = np.sqrt(sum((b ** 2).sum() for b in r["f64"]))
+        assert num <= 1e-6 * den
+    rx, ry = oracle.plain_run(ap, ai, x, y, area, die, die, 1, min_dist=md, bins=64, weight=1.0)
+    ox, oy = x.copy(), y.copy()
+    vx, vy = np.zeros_like(ox), np.zeros_like(oy)
+    oracle.integrate(ox, oy, vx, vy, *full["f32"], 0.1, 0.9, (0.0, 0.0, die, die))
+    assert np.array_equal(rx, ox) and np.array_equal(ry, oy)

@@ -73,3 +73,50 @@ def test_noalloc_rejects_grids_beyond_its_scratch(fx, ctx, plain_small):
             d.congestion_noalloc(64, 64, 0)  # no count buffer
     finally:
         d.close()
+
+
+_FRESH = r"""
+import sys
+import numpy as np
+import torch
+sys.path[:0] = [sys.argv[1], sys.argv[2]]
+import fluxion_b200 as fx
+fx.load()
+s = fx.synth_plain(7, 4000, 4800, 76.0)
+c = s.circuit
+dev = torch.device("cuda", 0)
+# torch.empty and host-to-device copies launch no kernel: the no-alloc call
+# below is the first kernel work of this process on the device
+counts = torch.empty(64 * 64, dtype=torch.int32, device=dev)
+res = torch.empty(2, dtype=torch.float64, device=dev)
+mx = torch.empty(1, dtype=torch.float32, device=dev)
+dx = torch.from_numpy(s.placement.gate_x).to(dev)
+dy = torch.from_numpy(s.placement.gate_y).to(dev)
+torch.cuda.synchronize()
+ctx = fx.Context(0)
+d = fx.Design(ctx, c)
+d.congestion_noalloc(64, 64, counts.data_ptr(), dx.data_ptr(), dy.data_ptr(),
+                     res.data_ptr(), mx.data_ptr())
+ctx.synchronize()
+got = counts.cpu().numpy().view(np.uint32)
+want, hp, tot, m = d.congestion(64, 64, s.placement.gate_x, s.placement.gate_y)
+assert want.sum() > 0
+assert np.array_equal(got, want), "first no-alloc call differs"
+assert (float(res[0]), float(res[1]), float(mx[0])) == (hp, tot, m)
+d.close()
+ctx.close()
+print("fresh ok")
+"""
+
+
+def test_noalloc_first_call_in_a_fresh_process(fx):
+    """The scratch set-up and the first call's kernels in a process whose
+    device has run nothing else: the zeroing must be ordered before them."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    r = subprocess.run([sys.executable, "-c", _FRESH, str(root / "neon-physics-fluxion_b200"),
+                        str(root)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "fresh ok" in r.stdout
