@@ -19,9 +19,9 @@ path does not shard), timing is the max over ranks and `value` is the sum of
 iterations over all ranks divided by that time.
 
 --impl reference times the reference's CPU implementation of the same
-iteration on this host's cores (the oracle port of the Rust path plus the
-reference's own BarnesHutTree.cpp and its scipy DCT) on a bounded sample of
-each stage; only rank 0 runs it.
+iteration on all of this host's cores (the oracle port of the Rust path, the
+reference's own BarnesHutTree.cpp and its scipy DCT): every timed step is one
+full iteration; only rank 0 runs it, and it never loads the CUDA library.
 """
 from __future__ import annotations
 
@@ -47,7 +47,7 @@ UNIT = "iterations/s"
 ITER_STATS_D2H = 32
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
@@ -81,7 +81,7 @@ def parse():
     ap.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent jobs")
     ap.add_argument("--pool", type=int, default=16, help="serve: distinct netlists")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 PREC = {"fp32": 3, "simt": 3, "3xtf32": 0, "tf32": 1, "bf16": 2}
@@ -270,42 +270,105 @@ class SynthCache:
         self.adj = None
 
 
+def plain_config(args, pins, adj_entries, world):
+    """The `config` of the plain-1M line; both arms print it."""
+    b_alg, _ = algorithmic(args.gates, args.nets, pins, adj_entries, args.bins, args.cong)
+    B_iter = sum(b_alg.values())
+    return {"workload": f"plain-1M: {args.gates} gates, {args.nets} nets "
+                        f"({pins} pins, {adj_entries} adjacency entries), die {args.die:g}, "
+                        f"BH theta 0.5, DCT {args.bins}^2 ({args.precision}), congestion "
+                        f"{args.cong}^2",
+            "seed": args.seed, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "working set per iteration ~%d MB > 126 MB L2" % (B_iter // 2**20)}
+
+
+def cpu_iteration_full(orc, s, adj, x, y, bins, cong, threads, sample=1):
+    """One plain iteration of the CPU path from (x, y) at rest; returns the
+    seconds of each stage. Every stage runs in full when sample == 1:
+    attraction (restatement of placer.rs:243-255 over the adjacency, 1
+    thread), Barnes-Hut (the reference's BarnesHutTree.cpp: sequential build,
+    walk of every point on `threads` threads), the DCT density force (the
+    reference's scipy dctn/idctn solve, FP64), the damped step, congestion
+    (the literal loops of congestion.rs:11-62 over every net on `threads`
+    threads) and the f32 HPWL. sample > 1 (warm-up only) walks every
+    sample-th point and counts every sample-th net."""
+    ap, ai = adj
+    area = (s.gate_widths * s.gate_heights).astype(np.float64)
+    t = {}
+    t0 = time.perf_counter()
+    fa = orc.attraction_f32(ap, ai, x, y, 1.0)
+    t["attraction"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bh = orc.bh_reference(x, y, 0.5, 0.5, 0.1, threads, stride=sample)
+    t["barnes_hut"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    dens = orc.density_forces(x, y, area, s.chip_width, s.chip_height, bins, 0.7, 1e-4)
+    t["density"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fx = (fa[0] + bh[0].astype(np.float32)) + dens["fx"].astype(np.float32)
+    fy = (fa[1] + bh[1].astype(np.float32)) + dens["fy"].astype(np.float32)
+    xx, yy = x.copy(), y.copy()
+    vx, vy = np.zeros_like(xx), np.zeros_like(yy)
+    orc.integrate(xx, yy, vx, vy, fx, fy, 0.1, 0.9, (0.0, 0.0, s.chip_width, s.chip_height))
+    t["integrate"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    if sample == 1:
+        orc.congestion_parallel(s.net_ptr, s.net_gate, xx, yy, s.chip_width, s.chip_height,
+                                cong, cong, threads)
+    else:
+        orc.congestion_sample(s.net_ptr, s.net_gate, xx, yy, s.chip_width, s.chip_height,
+                              cong, cong, sample)
+    t["congestion"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.hpwl_f32(s.net_ptr, s.net_gate, xx, yy)
+    t["hpwl"] = time.perf_counter() - t0
+    return t
+
+
 def run_reference(args, rank, world):
-    """CPU implementation of the same iteration (the reference arm)."""
+    """The reference arm: the CPU implementation of the same iteration on all
+    host threads. The netlist comes from the generator built into the
+    oracle's own library (the same seeded bytes as the GPU arm); the CUDA
+    library is never loaded. Every timed step is one full, unsampled
+    iteration from the seeded start positions; the warm-up steps run the
+    same stages on a 1/16 sample (every 16th walked point and counted net),
+    which warms the code, pools and caches without the full cost."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    sc = SynthCache(args)
     from oracle import oracle as orc
     orc.build()
-    c = sc.circuit
-    sc.adj = orc.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
-    x, y = sc.placement.gate_x.copy(), sc.placement.gate_y.copy()
-    bh_stride, cong_stride = 16, 256
-    per = []
-    for i in range(args.warmup + args.steps):
-        s, parts = cpu_iteration_sample(sc, x, y, args.bins, args.cong, threads,
-                                        bh_stride, cong_stride)
-        if i >= args.warmup:
-            per.append(s)
-    sec = float(np.mean(per))
+    s = orc.synth_plain(args.seed, args.gates, args.nets, args.die)
+    adj = orc.build_adjacency(s.num_gates, s.net_ptr, s.net_gate)
+    x, y = s.gate_x.copy(), s.gate_y.copy()
+    for _ in range(args.warmup):
+        cpu_iteration_full(orc, s, adj, x, y, args.bins, args.cong, threads, sample=16)
+    per, parts = [], {}
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        t = cpu_iteration_full(orc, s, adj, x, y, args.bins, args.cong, threads)
+        per.append(sum(t.values()))
+        for k, v in t.items():
+            parts[k] = parts.get(k, 0.0) + v / args.steps
+    wall = time.perf_counter() - t_all
+    sec = wall / args.steps
     value = 1.0 / sec
-    sample = (f"one plain iteration per step on {args.gates} gates: attraction, integrate, "
-              f"HPWL and the scipy DCT density in full; Barnes-Hut with the reference "
-              f"BarnesHutTree.cpp (full build, walk of every {bh_stride}th point, scaled); "
-              f"congestion on every {cong_stride}th net (scaled); initial positions")
+    sample = (f"{args.steps} full plain iterations on {args.gates} gates from the seeded start "
+              f"positions, every stage unsampled: attraction (1 thread), the reference "
+              f"BarnesHutTree.cpp (sequential build, walk on {threads} threads), the scipy DCT "
+              f"solve, the damped step, the literal congestion loops over all nets on "
+              f"{threads} threads, HPWL")
     out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": f"plain-1M: {args.gates} gates, {args.nets} nets, die "
-                      f"{args.die:g}, BH theta 0.5, DCT {args.bins}^2, congestion "
-                      f"{args.cong}^2", "seed": args.seed},
+           "vs_baseline": None, "dtype": "f32 (density solve FP64, scipy)", "data": "synthetic",
+           "config": plain_config(args, s.num_pins, len(adj[1]), world),
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
                             "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0},
-           "stage_seconds": {k: round(v, 4) for k, v in parts.items()}}
+           "stage_seconds": {k: round(v, 4) for k, v in parts.items()},
+           "step_seconds_min_max": [round(min(per), 3), round(max(per), 3)]}
     print(json.dumps(out), flush=True)
 
 
@@ -490,11 +553,7 @@ def run_fluxion(args, rank, world, local_rank):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": it_ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": PREC_DTYPE[args.precision], "data": "synthetic",
-           "config": {"workload": f"plain-1M: {args.gates} gates, {args.nets} nets "
-                      f"({pn} pins, {a} adjacency entries), die {args.die:g}, BH theta 0.5, "
-                      f"DCT {G}^2 ({args.precision}), congestion {gc}^2",
-                      "seed": args.seed, "parallelism": "replicas" if world > 1 else "single",
-                      "l2": "working set per iteration ~%d MB > 126 MB L2" % (B_iter // 2**20)},
+           "config": plain_config(args, pn, a, world),
            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
            "clocks": clk,
            "iteration_roofline": {"bytes": B_iter, "achieved_gbs": B_iter / (it_ms * 1e-3) / 1e9,

@@ -58,6 +58,9 @@ def lib() -> C.CDLL:
                                        F32P, F32P, F32P]
         L.or_congestion.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
                                     C.c_float, C.c_int64, C.c_int64, F32P, F32P]
+        L.or_congestion_parallel.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
+                                             C.c_float, C.c_int64, C.c_int64, C.c_int32,
+                                             F32P, F32P]
         L.or_congestion_sample.argtypes = [C.c_int32, I32P, I32P, F32P, F32P, C.c_float,
                                            C.c_float, C.c_int64, C.c_int64, C.c_int32,
                                            F32P, F32P]
@@ -119,6 +122,53 @@ def ref_lib():
     return _ref
 
 
+_synth = None
+
+
+def synth_lib() -> C.CDLL:
+    """oracle/_build/libsynth.so: the seeded workload generator without the
+    CUDA library (for the CPU reference arm)."""
+    global _synth
+    if _synth is None:
+        L = C.CDLL(str(HERE / "_build" / "libsynth.so"))
+        L.fx_synth_plain.argtypes = [C.c_uint64, C.c_int32, C.c_int32, C.c_float, C.c_float,
+                                     C.c_int32, C.POINTER(C.c_void_p)]
+        L.fx_netlist_sizes.argtypes = [C.c_void_p] + [C.POINTER(C.c_int64)] * 4
+        L.fx_netlist_copy.argtypes = [C.c_void_p] + [C.c_void_p] * 9
+        L.fx_netlist_free.argtypes = [C.c_void_p]
+        L.or_synth_last_error.restype = C.c_char_p
+        _synth = L
+    return _synth
+
+
+def synth_plain(seed, n_gates, n_nets, die, leaf_size=64):
+    """The plain workload generator (fx_synth_plain) through libsynth.so:
+    a namespace with the netlist CSR (net_ptr, net_gate), gate_widths,
+    gate_heights, chip_width, chip_height, num_gates and the seeded start
+    positions gate_x, gate_y -- the same bytes the GPU arm generates."""
+    from types import SimpleNamespace
+    L = synth_lib()
+    h = C.c_void_p()
+    if L.fx_synth_plain(seed, n_gates, n_nets, die, die, leaf_size, C.byref(h)) != 0:
+        raise RuntimeError(L.or_synth_last_error().decode())
+    n, m, p, nl = (C.c_int64() for _ in range(4))
+    L.fx_netlist_sizes(h, C.byref(n), C.byref(m), C.byref(p), C.byref(nl))
+    N, M, P = n.value, m.value, p.value
+    a = dict(net_ptr=np.empty(M + 1, np.int32), net_gate=np.empty(max(P, 1), np.int32),
+             gate_widths=np.empty(N, np.float32), gate_heights=np.empty(N, np.float32),
+             gate_x=np.empty(N, np.float32), gate_y=np.empty(N, np.float32))
+    dd = np.empty(2, np.float32)
+    lp = np.empty(nl.value + 1, np.int32)
+    rg = np.empty(4 * max(nl.value, 1), np.float32)
+    L.fx_netlist_copy(h, *(a[k].ctypes.data for k in ("net_ptr", "net_gate", "gate_widths",
+                                                      "gate_heights", "gate_x", "gate_y")),
+                      dd.ctypes.data, lp.ctypes.data, rg.ctypes.data)
+    L.fx_netlist_free(h)
+    a["net_gate"] = a["net_gate"][:P]
+    return SimpleNamespace(num_gates=N, num_nets=M, num_pins=P, chip_width=float(dd[0]),
+                           chip_height=float(dd[1]), **a)
+
+
 def _p(a, t):
     return None if a is None else a.ctypes.data_as(C.POINTER(t))
 
@@ -150,6 +200,19 @@ def congestion(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows):
     lib().or_congestion(len(net_ptr) - 1, _p(net_ptr, C.c_int32), _p(net_gate, C.c_int32),
                         _p(x, C.c_float), _p(y, C.c_float), chip_w, chip_h, cols, rows,
                         _p(h, C.c_float), _p(v, C.c_float))
+    return h, v
+
+
+def congestion_parallel(net_ptr, net_gate, x, y, chip_w, chip_h, cols, rows, threads):
+    """compute_congestion_cpu's literal loops (congestion.rs:11-62) over all
+    nets on `threads` host threads (per-thread grids summed in order; the
+    counts are exact integers, so h and v equal the single-threaded loop's)."""
+    h = np.empty(rows * cols, np.float32)
+    v = np.empty(rows * cols, np.float32)
+    lib().or_congestion_parallel(len(net_ptr) - 1, _p(_i32(net_ptr), C.c_int32),
+                                 _p(_i32(net_gate), C.c_int32), _p(_f32(x), C.c_float),
+                                 _p(_f32(y), C.c_float), chip_w, chip_h, cols, rows, threads,
+                                 _p(h, C.c_float), _p(v, C.c_float))
     return h, v
 
 

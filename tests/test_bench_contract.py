@@ -56,3 +56,32 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_plain_reference_arm_runs_full_steps_without_the_cuda_library():
+    """The plain workload's reference arm at a reduced size: full iterations
+    on the host cores, the same config dict as the GPU arm's, and
+    libfluxion_b200.so never mapped into the process."""
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--gates', '20000', "
+            "'--nets', '24000', '--die', '170', '--bins', '128', '--cong', '64', '--steps', '2', "
+            "'--warmup', '1']; sys.path.insert(0, '.'); import bench; bench.main(); "
+            "print('MAPPED', open('/proc/self/maps').read().count('libfluxion_b200'))")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert "MAPPED 0" in r.stdout
+    assert d["impl"] == "reference" and d["steps"] == 2 and d["warmup"] == 1
+    # every timed step is a whole iteration: steps x ms_per_step is the timed region
+    lo, hi = d["step_seconds_min_max"]
+    assert lo > 0 and d["ms_per_step"] / 1e3 >= lo * 0.99
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from oracle import oracle as orc
+    s = orc.synth_plain(42, 20000, 24000, 170.0)
+    adj = orc.build_adjacency(s.num_gates, s.net_ptr, s.net_gate)
+    args = bench.parse(["--gates", "20000", "--nets", "24000", "--die", "170",
+                                 "--bins", "128", "--cong", "64"])
+    assert d["config"] == bench.plain_config(args, s.num_pins, len(adj[1]), 1)
