@@ -1033,7 +1033,7 @@ def run_small(args, rank, world, local_rank):
     sy = fx.synth_plain(args.seed, 10_000, 12_000, 120.0)
     c, p = sy.circuit, sy.placement
     iters = 200
-    cfg = fx.iter_cfg(density_bins=0, cong_cols=64, cong_rows=64)
+    cfg = fx.iter_cfg(density_bins=0, cong_cols=64, cong_rows=64, bh_walk=fx.FX_BH_EXACT)
     ctx = fx.Context(local_rank)
     d = fx.Design(ctx, c)
     x, y = p.gate_x.copy(), p.gate_y.copy()

@@ -235,7 +235,17 @@ typedef struct fx_iter_cfg {
   int32_t cong_rows;
   float damping;         /* placer.rs:276 (0.9)                              */
   float dt;              /* placer.rs:276-279 (0.1)                          */
+  int32_t bh_walk;       /* FX_BH_* (default FX_BH_FAST)                     */
 } fx_iter_cfg;
+
+/* Barnes-Hut walk. Both give every point the interaction list of the
+ * reference's per-point opening rule (BarnesHutTree.cpp:145-167) on the
+ * same tree; they differ in how the terms are found and summed. */
+#define FX_BH_FAST  0 /* cells decided for a whole warp of points at once are */
+                      /* summed densely from shared memory; hardware rsqrt;   */
+                      /* forces within f32 rounding of the exact walk         */
+#define FX_BH_EXACT 1 /* per-point masked walk, fixed term order, reproducible */
+                      /* rsqrt: forces bit-identical to the oracle's f32 walk */
 
 #define FX_DCT_FP32  0 /* 3xTF32 split on the tensor cores; its error grows   */
                        /* with G (6.6e-4 at 256, 4.4e-3 at 2048 measured):  */
@@ -294,6 +304,13 @@ int fx_stage_barnes_hut(fx_ctx *ctx, fx_design *design, float k, float theta,
                         float min_dist, float *out_fx, float *out_fy,
                         uint32_t *out_keys, int32_t *out_perm,
                         float *out_root);
+/* The same with the walk chosen (FX_BH_*; fx_stage_barnes_hut is
+ * FX_BH_EXACT). FX_BH_FAST can also return each gate's interaction count
+ * (out_terms[N], NULL to skip): single points plus accepted cells. */
+int fx_stage_barnes_hut_walk(fx_ctx *ctx, fx_design *design, float k, float theta,
+                             float min_dist, int32_t walk, float *out_fx, float *out_fy,
+                             uint32_t *out_keys, int32_t *out_perm, float *out_root,
+                             int32_t *out_terms);
 /* Row C: DCT Poisson density force. Optional grids (G*G, row-major, may be
  * NULL): out_rho (charge density rho - rho_target), out_phi, out_ex,
  * out_ey. */

@@ -254,6 +254,10 @@ static int validate_cfg(const fx_iter_cfg &c) {
     set_error("fx_iter_cfg: density_bins must be a multiple of 128 (<= 8192)");
     return FX_EINVAL;
   }
+  if (c.bh_walk != FX_BH_FAST && c.bh_walk != FX_BH_EXACT) {
+    set_error("fx_iter_cfg: unknown bh_walk %d", c.bh_walk);
+    return FX_EINVAL;
+  }
   if (c.dct_precision < FX_DCT_FP32 || c.dct_precision > FX_DCT_SIMT) {
     set_error("fx_iter_cfg: unknown dct_precision %d", c.dct_precision);
     return FX_EINVAL;
@@ -279,6 +283,7 @@ extern "C" int fx_iter_cfg_default(fx_iter_cfg *c) {
   c->cong_rows = 512;
   c->damping = 0.9f;
   c->dt = 0.1f;
+  c->bh_walk = FX_BH_FAST;
   return FX_OK;
 }
 
@@ -343,7 +348,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
                          c.dct_precision, last, s2));
       FX_CHECK_CUDA(cudaEventRecord(ctx->join, s2));
     }
-    if (use_bh) FX_TRY(bh_run(ctx, d, c.repel_weight, c.theta, c.min_dist, s));
+    if (use_bh) FX_TRY(bh_run(ctx, d, c.repel_weight, c.theta, c.min_dist, c.bh_walk, s));
     if (use_dens) FX_CHECK_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
     const int nxt = d->cur ^ 1;
     StepArgs a{};

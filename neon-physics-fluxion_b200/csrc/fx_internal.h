@@ -292,8 +292,8 @@ namespace fx {
 int congestion_run(fx_ctx *ctx, fx_design *d, const float *dx, const float *dy,
                    int cols, int rows, cudaStream_t s);
 int attraction_run(fx_ctx *ctx, fx_design *d, float k, float2 *out, cudaStream_t s);
-int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist,
-           cudaStream_t s);
+int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist, int walk,
+           cudaStream_t s, int32_t *term_count = nullptr);
 int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
                 int precision, bool need_phi, cudaStream_t s);
 int fused_step(fx_ctx *ctx, fx_design *d, const fx_iter_cfg &cfg,

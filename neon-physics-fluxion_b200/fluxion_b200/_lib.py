@@ -24,6 +24,9 @@ FX_DCT_TF32 = 1
 FX_DCT_BF16 = 2
 FX_DCT_SIMT = 3
 
+FX_BH_FAST = 0
+FX_BH_EXACT = 1
+
 STAGES = ["attract_integrate", "bh_keys", "bh_sort", "bh_tree", "bh_walk",
           "density", "congestion", "leaf", "fiedler", "attention"]
 
@@ -46,7 +49,7 @@ class IterCfg(C.Structure):
                 ("density_weight", C.c_float), ("target_density", C.c_float),
                 ("density_bins", C.c_int32), ("dct_precision", C.c_int32),
                 ("cong_cols", C.c_int32), ("cong_rows", C.c_int32),
-                ("damping", C.c_float), ("dt", C.c_float)]
+                ("damping", C.c_float), ("dt", C.c_float), ("bh_walk", C.c_int32)]
 
 
 class IterStats(C.Structure):
@@ -161,6 +164,9 @@ SIGNATURES = {
     "fx_design_get_positions": (C.c_int, [P, PF32, PF32]),
     "fx_design_save_state": (C.c_int, [P]),
     "fx_design_trace": (C.c_int, [P, C.c_int]),
+    "fx_stage_barnes_hut_walk": (C.c_int, [P, P, C.c_float, C.c_float, C.c_float, I32, PF32,
+                                           PF32, C.POINTER(C.c_uint32), C.POINTER(C.c_int32),
+                                           PF32, C.POINTER(C.c_int32)]),
     "fx_design_trace_get": (C.c_int, [P, PF32, PF32, PF32, PF32, PF32, PF32]),
     "fx_design_restore_state": (C.c_int, [P]),
     "fx_design_device_bytes": (C.c_int64, [P]),

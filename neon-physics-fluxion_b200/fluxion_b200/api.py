@@ -291,17 +291,24 @@ class Design:
               "fx_stage_attraction")
         return fx, fy
 
-    def barnes_hut(self, k: float = 0.5, theta: float = 0.5, min_dist: float = 0.1):
+    def barnes_hut(self, k: float = 0.5, theta: float = 0.5, min_dist: float = 0.1,
+                   walk: int = _lib.FX_BH_EXACT, terms: bool = False):
+        """fx_stage_barnes_hut_walk: forces, keys (gate order), sorted order and root
+        square; with terms=True (FX_BH_FAST only) also each gate's interaction count."""
         fx = np.empty(self.n, np.float32)
         fy = np.empty(self.n, np.float32)
         keys = np.empty(self.n, np.uint32)
         perm = np.empty(self.n, np.int32)
         root = np.empty(3, np.float32)
-        check(self.lib.fx_stage_barnes_hut(self.ctx.handle, self.handle, k, theta,
-                                           min_dist, ptr(fx, C.c_float),
-                                           ptr(fy, C.c_float), ptr(keys, C.c_uint32),
-                                           ptr(perm, C.c_int32), ptr(root, C.c_float)),
-              "fx_stage_barnes_hut")
+        cnt = np.empty(self.n, np.int32) if terms else None
+        check(self.lib.fx_stage_barnes_hut_walk(self.ctx.handle, self.handle, k, theta,
+                                                min_dist, walk, ptr(fx, C.c_float),
+                                                ptr(fy, C.c_float), ptr(keys, C.c_uint32),
+                                                ptr(perm, C.c_int32), ptr(root, C.c_float),
+                                                ptr(cnt, C.c_int32)),
+              "fx_stage_barnes_hut_walk")
+        if terms:
+            return fx, fy, keys, perm, root, cnt
         return fx, fy, keys, perm, root
 
     def density(self, bins: int, target: float = 0.7, weight: float = 1.0,

@@ -20,6 +20,8 @@ def _check(fx, ctx, oracle, x, y, chip):
         d.set_positions(x, y)
         bx, by, keys, perm, root = d.barnes_hut(0.5, 0.5, 0.1)
         bx2, by2, _, _, _ = d.barnes_hut(0.5, 0.5, 0.1)
+        qx, qy, qkeys, _, _, terms = d.barnes_hut(0.5, 0.5, 0.1, walk=fx.FX_BH_FAST,
+                                                  terms=True)
     finally:
         d.close()
     o = oracle.bh_forces(x, y, 0.5, 0.5, F32_01)
@@ -29,6 +31,10 @@ def _check(fx, ctx, oracle, x, y, chip):
     assert np.array_equal(bx, o["fx32"]) and np.array_equal(by, o["fy32"])
     assert np.array_equal(bx, bx2) and np.array_equal(by, by2)
     num = np.sqrt(((bx - o["fx"]) ** 2 + (by - o["fy"]) ** 2).sum())
+    assert num / np.sqrt((o["fx"] ** 2 + o["fy"] ** 2).sum()) < 1e-5
+    # the group-decided walk on the same (deep or shallow) tree
+    assert np.array_equal(qkeys, keys) and np.array_equal(terms, o["interactions"])
+    num = np.sqrt(((qx - o["fx"]) ** 2 + (qy - o["fy"]) ** 2).sum())
     assert num / np.sqrt((o["fx"] ** 2 + o["fy"] ** 2).sum()) < 1e-5
     return o
 
@@ -71,7 +77,7 @@ def test_fused_iterations_on_a_large_die(fx, ctx, oracle):
     centers = rng.uniform(100, 2900, (40, 2))
     p = (centers[rng.integers(0, 40, n)] + rng.uniform(0, 0.05, (n, 2))).astype(np.float32)
     x0, y0 = p[:, 0].copy(), p[:, 1].copy()
-    cfg = fx.iter_cfg(density_bins=0, cong_cols=0, cong_rows=0)
+    cfg = fx.iter_cfg(density_bins=0, cong_cols=0, cong_rows=0, bh_walk=fx.FX_BH_EXACT)
     d = fx.Design(ctx, circ)
     try:
         x, y = x0.copy(), y0.copy()

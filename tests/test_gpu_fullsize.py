@@ -71,7 +71,7 @@ def test_barnes_hut_and_one_plain_iteration(fx, full_design, full, oracle):
     assert np.array_equal(keys, o["keys"]) and np.array_equal(perm, o["perm"])
     assert np.array_equal(bx, o["fx32"]) and np.array_equal(by, o["fy32"])
     assert _rel(bx, by, o["fx"], o["fy"]) < 1e-5
-    cfg = fx.iter_cfg(density_bins=0, cong_cols=512, cong_rows=512)
+    cfg = fx.iter_cfg(density_bins=0, cong_cols=512, cong_rows=512, bh_walk=fx.FX_BH_EXACT)
     x, y = p.gate_x.copy(), p.gate_y.copy()
     st = d.force_iterate(cfg, 1, x, y)
     rp, ri = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)

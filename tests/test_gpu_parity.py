@@ -10,6 +10,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 F32_01 = float(np.float32(0.1))  # the device's f32 min_dist, exactly
+FX_BH_FAST = 0  # fx_iter_cfg.bh_walk / fx_stage_barnes_hut_walk: group-decided walk
+FX_BH_EXACT = 1  # per-point walk, bit-identical to the oracle's f32 order
 
 
 def rel_l2(ax, ay, bx, by):
@@ -117,6 +119,14 @@ def _bh_check(d, x, y, oracle, k=0.5, theta=0.5):
     assert np.array_equal(perm, o["perm"])  # stable sort order exact
     assert np.array_equal(bx, o["fx32"]) and np.array_equal(by, o["fy32"])  # bit-exact
     assert rel_l2(bx, by, o["fx"], o["fy"]) < 1e-5  # FP64, same interaction list
+    # the group-decided walk: the same tree, the same interaction count per
+    # point, forces within f32 rounding (hardware rsqrt, any term order)
+    qx, qy, qkeys, qperm, qroot, terms = d.barnes_hut(k, theta, 0.1, walk=FX_BH_FAST,
+                                                      terms=True)
+    assert np.array_equal(qkeys, keys) and np.array_equal(qperm, perm)
+    assert np.array_equal(terms, o["interactions"])
+    assert rel_l2(qx, qy, o["fx"], o["fy"]) < 1e-5
+    assert rel_l2(qx, qy, o["fx32"].astype(np.float64), o["fy32"].astype(np.float64)) < 1e-5
     return bx, by
 
 
@@ -225,7 +235,7 @@ def test_plain_small_run_matches_oracle(fx, ctx, plain_small, oracle):
     agree exactly (the 0.5 % bar is met with zero error)."""
     c, p = plain_small.circuit, plain_small.placement
     iters = 200
-    cfg = fx.iter_cfg(density_bins=0, cong_cols=64, cong_rows=64)
+    cfg = fx.iter_cfg(density_bins=0, cong_cols=64, cong_rows=64, bh_walk=FX_BH_EXACT)
     d = fx.Design(ctx, c)
     try:
         x = p.gate_x.copy(); y = p.gate_y.copy()
