@@ -62,6 +62,8 @@ def parse(argv=None):
                     choices=["fp32", "3xtf32", "tf32", "bf16", "simt"],
                     help="DCT GEMMs: fp32 (= simt, CUDA cores), 3xtf32, tf32, bf16 (tensor cores)")
     ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--bh-walk", default="fast", choices=["fast", "exact"],
+                    help="Barnes-Hut walk: group-decided (default) or the exact per-point one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--trajectory", type=int, default=500,
@@ -151,21 +153,20 @@ def peaks():
 # (`--set full -s 1 -c 1` of the bench command with --steps 2 --warmup 3;
 # summaries under profiles/). A stage missing here reports traffic null.
 NCU_DRAM_BYTES = {
-    # bh_walk_kernel: 59.513 MB read + 2.212 MB written
-    "bh_walk": 61_725_696,
     # with --precision 3xtf32: 6 x tc_gemm_kernel<0> (21.000 MB + 0.011 MB
     # each) + dens_charge_kernel (8.393 MB); dens_scatter runs in the
     # previous step's fused kernel
     "density": 6 * 21_010_944 + 8_393_472,
 }
-# Warp instructions per launch (smsp__inst_executed.sum) and threads per warp
-# instruction (smsp__thread_inst_executed_per_inst_executed.ratio) of the
-# issue-bound walk, from the same kind of capture: its roofline is the issue
-# rate, 4 warp instructions per SM per cycle.
-NCU_WALK_INST = (1_390_529_927, 20.07)
-# What bounds each stage when it is not HBM or the tensor pipe (ncu).
-NCU_LIMITER = {
-    "bh_walk": "instruction issue: 87% issue-active, 0.5% of DRAM peak, 82% warps active",
+# The same per walk kernel (the --bh-walk choice), with its warp
+# instructions per launch (smsp__inst_executed.sum), threads per warp
+# instruction (smsp__thread_inst_executed_per_inst_executed.ratio) and what
+# bounds it; the walk's roofline is the issue rate, 4 warp instructions per
+# SM per cycle.
+NCU_WALK = {
+    "exact": {"dram": 61_725_696, "inst": 1_390_529_927, "tpi": 20.07,
+              "limiter": "instruction issue: 87% issue-active, 0.5% of DRAM peak, "
+                         "82% warps active"},
 }
 
 
@@ -395,7 +396,8 @@ def run_fluxion(args, rank, world, local_rank):
     ctx = fx.Context(local_rank)
     d = fx.Design(ctx, c)
     cfg = fx.iter_cfg(density_bins=args.bins, dct_precision=PREC[args.precision],
-                      cong_cols=args.cong, cong_rows=args.cong)
+                      cong_cols=args.cong, cong_rows=args.cong,
+                      bh_walk=fx.FX_BH_EXACT if args.bh_walk == "exact" else fx.FX_BH_FAST)
     # The start state of every step: the seeded uniform placement (the state
     # the reference arm and the CPU baseline time too), velocities zero,
     # checkpointed on the device.
@@ -499,10 +501,12 @@ def run_fluxion(args, rank, world, local_rank):
         roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "traffic": NCU_DRAM_BYTES.get(dom), "kernel": dom,
                 "algorithmic_bytes": b_alg[dom], "peak_source": f"{src} HBM copy"}
-    if dom in NCU_LIMITER:
-        roof["limiter"] = NCU_LIMITER[dom]
-    if dom == "bh_walk" and args.gates == 1_000_000:
-        inst, tpi = NCU_WALK_INST
+    walk_ncu = NCU_WALK.get(args.bh_walk) if dom == "bh_walk" else None
+    if walk_ncu:
+        roof["traffic"] = walk_ncu["dram"]
+        roof["limiter"] = walk_ncu["limiter"]
+    if walk_ncu and args.gates == 1_000_000:
+        inst, tpi = walk_ncu["inst"], walk_ncu["tpi"]
         mhz = (clk.get("sm_mhz") or 1965.0) if isinstance(clk, dict) else 1965.0
         peak_i = 4 * 148 * mhz * 1e6
         ach_i = inst / (per_iter[dom] * 1e-3)
@@ -560,7 +564,9 @@ def run_fluxion(args, rank, world, local_rank):
                                   "frac_of_hbm": B_iter / (it_ms * 1e-3) / 1e9 / hbm},
            "stage_ms_per_iter": {k: round(v, 4) for k, v in per_iter.items()},
            "density_roofline": dens_roof,
-           "step_hpwl": st.hpwl, "trajectory": traj}
+           "step_hpwl": st.hpwl, "trajectory": traj,
+           "bh_walk": ("group-decided (FX_BH_FAST)" if args.bh_walk == "fast"
+                       else "exact per-point order (FX_BH_EXACT)")}
     if rank == 0:
         print(json.dumps(out), flush=True)
     d.close()

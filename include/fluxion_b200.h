@@ -362,12 +362,15 @@ int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *design, int32_t n_leaves,
  * cluster_ptr[c] .. cluster_ptr[c+1]-1] (clusters must not share gates);
  * its induced Laplacian uses the design's adjacency. The start vector is the
  * reference's sin(i * 2.71828), normalised; each iteration applies L, removes
- * the mean (deflation against the constant vector) and normalises, with FP64
- * reductions. tol = 0 runs exactly max_iters iterations (the reference uses
- * 30, H/src/main.rs:80); tol > 0 stops a cluster once its Rayleigh quotient
- * changes by at most tol relative. out_v[G] receives each cluster's vector
- * (same order as cluster_gate); out_iters[C] and out_lambda[C] (may be NULL)
- * the iterations run and the final Rayleigh quotient v^T L v. */
+ * the mean (deflation against the constant vector) and normalises.
+ * tol = 0 runs exactly max_iters iterations (the reference uses 30,
+ * H/src/main.rs:80) with the reference's f32 mean and norm (sequential
+ * folds), so the vectors are bit-identical to compute_fiedler_vector's;
+ * tol > 0 takes the mean and norm in FP64 and stops a cluster once its
+ * Rayleigh quotient changes by at most tol relative. out_v[G] receives each
+ * cluster's vector (same order as cluster_gate); out_iters[C] and
+ * out_lambda[C] (may be NULL) the iterations run and the Rayleigh quotient
+ * v^T L v / v^T v of the returned vector, in FP64. */
 int fx_fiedler(fx_ctx *ctx, fx_design *design, int32_t n_clusters,
                const int32_t *cluster_ptr, const int32_t *cluster_gate,
                int32_t max_iters, double tol, float *out_v,

@@ -110,6 +110,30 @@ __global__ void fiedler_update_kernel(FiedlerArgs a, int n) {
   a.v[p] = x;
 }
 
+// Exact mode (tol == 0): v = lv / norm, lv already deflated in place by
+// part_seq_kernel (the reference's f32 folds), or lv when norm <= 1e-10.
+__global__ void fiedler_div_kernel(FiedlerArgs a, const float *__restrict__ nrm, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  int lo = 0, hi = a.n_clusters - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.cl_ptr[mid] <= p) lo = mid; else hi = mid - 1;
+  }
+  const float r = nrm[lo];
+  a.v[p] = r > 0.0f ? __fdiv_rn(a.lv[p], r) : a.lv[p];
+}
+
+// v . L v (FP64, chunk partials of the last SpMV added in order) of the
+// returned vectors; the host divides by v . v.
+__global__ void fiedler_lambda_kernel(FiedlerArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n_clusters) return;
+  double s3 = 0.0;
+  for (int k = a.cl_chunk[c]; k < a.cl_chunk[c + 1]; ++k) s3 += a.part[3 * k + 2];
+  a.lambda[c] = s3;
+}
+
 __global__ void fiedler_retire_kernel(int32_t *active, int n_clusters, int last) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_clusters) return;
@@ -233,11 +257,22 @@ extern "C" int fx_fiedler(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
   timer_begin(ctx, FX_STAGE_FIEDLER, s, &ev);
   const int kb = (K * 32 + 255) / 256, cb = (n_clusters + 255) / 256, gb = (G + 255) / 256;
   int ran = 0;
+  // tol == 0: the reference's own f32 mean and norm (sequential folds), so
+  // the vectors are bit-identical to compute_fiedler_vector's
+  const bool exact = tol == 0.0;
+  DevBuf<float> d_nrm;
+  if (exact) FX_TRY(d_nrm.alloc((size_t)n_clusters));
   for (int it = 0; it < max_iters; ++it) {
     ++ran;
     fiedler_spmv_kernel<<<kb, 256, 0, s>>>(a);
     fiedler_stats_kernel<<<cb, 256, 0, s>>>(a);
-    fiedler_update_kernel<<<gb, 256, 0, s>>>(a, G);
+    if (exact) {
+      part_seq_kernel<<<n_clusters, 32, 0, s>>>(n_clusters, d_clp.p, d_clp.p + 1, d_lv.p, 1,
+                                                d_nrm.p);
+      fiedler_div_kernel<<<gb, 256, 0, s>>>(a, d_nrm.p, G);
+    } else {
+      fiedler_update_kernel<<<gb, 256, 0, s>>>(a, G);
+    }
     fiedler_retire_kernel<<<cb, 256, 0, s>>>(d_act.p, n_clusters, it == max_iters - 1);
     // With a tolerance, stop as soon as every cluster has converged.
     if (tol > 0.0 && (it % 16) == 15) {
@@ -250,8 +285,12 @@ extern "C" int fx_fiedler(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
       if (!any) break;
     }
   }
+  // the Rayleigh quotient of the vectors returned: one more SpMV on them
+  FX_CHECK_CUDA(up(d_act.p, ones.data(), ones.size() * 4));
+  fiedler_spmv_kernel<<<kb, 256, 0, s>>>(a);
+  fiedler_lambda_kernel<<<cb, 256, 0, s>>>(a);
   FX_CHECK_LAUNCH();
-  ctx->launches += 4 * (int64_t)ran;
+  ctx->launches += (exact ? 5 : 4) * (int64_t)ran + 2;
   timer_end(ctx, FX_STAGE_FIEDLER, s, ev);
   FX_CHECK_CUDA(cudaMemcpyAsync(out_v, d_v.p, (size_t)G * 4, cudaMemcpyDeviceToHost, s));
   if (out_iters)
@@ -261,5 +300,12 @@ extern "C" int fx_fiedler(fx_ctx *ctx, fx_design *d, int32_t n_clusters,
     FX_CHECK_CUDA(cudaMemcpyAsync(out_lambda, d_lam.p, (size_t)n_clusters * 8,
                                   cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (out_lambda)
+    for (int c = 0; c < n_clusters; ++c) {
+      double vv = 0.0;
+      for (int32_t p = cluster_ptr[c]; p < cluster_ptr[c + 1]; ++p)
+        vv += (double)out_v[p] * (double)out_v[p];
+      out_lambda[c] = vv > 0.0 ? out_lambda[c] / vv : 0.0;
+    }
   return FX_OK;
 }

@@ -303,6 +303,12 @@ int radix_sort_pairs(uint32_t *k[2], int32_t *v[2], int n, int passes,
                      uint32_t *tile_hist, uint32_t *tile_scan, uint32_t *digit_total,
                      cudaStream_t s);
 int radix_sort_tiles(int n);
+// The reference's f32 Iterator::sum folds of the power iteration, one warp
+// per cluster [beg[c], end[c]) (fx_partition.cu): with `deflate`, the mean
+// of x is subtracted in place; nrm[c] = |x| when > 1e-10, else 0.
+__global__ void part_seq_kernel(int C, const int32_t *__restrict__ beg,
+                                const int32_t *__restrict__ end, float *__restrict__ x,
+                                int deflate, float *__restrict__ nrm);
 void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a);
 void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a);
 // Raises kernel `func`'s dynamic shared-memory limit on the current device to

@@ -105,6 +105,8 @@ __global__ void part_spmv_kernel(int n, const int32_t *__restrict__ perm,
   lv[p] = l;
 }
 
+}  // namespace
+
 // FX_PART_EXACT reductions: sequential f32 folds in position order
 // (Iterator::sum), one warp per cluster. The warp stages tiles of x in
 // shared memory with coalesced loads and lane 0 folds each tile in order, so
@@ -164,6 +166,8 @@ part_seq_kernel(int C, const int32_t *__restrict__ beg, const int32_t *__restric
     nrm[c] = norm > 1e-10f ? norm : 0.f;
   }
 }
+
+namespace {
 
 // v = (x - mean) / norm, or without the division when the norm was too
 // small, for the active clusters. x may be v.

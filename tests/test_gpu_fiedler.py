@@ -7,6 +7,22 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+def _laplacian(ap, ai, g, x):
+    """L x of the cluster's induced Laplacian (partitioner.rs:124-137), FP64."""
+    pos = {int(q): i for i, q in enumerate(g)}
+    x = np.asarray(x, np.float64)
+    lx = np.zeros_like(x)
+    for i, q in enumerate(g):
+        nb = [pos[int(j)] for j in ai[ap[q]:ap[q + 1]] if int(j) in pos]
+        lx[i] = len(nb) * x[i] - x[nb].sum()
+    return lx
+
+
+def _rayleigh(ap, ai, g, v):
+    x = np.asarray(v, np.float64)
+    return float(x @ _laplacian(ap, ai, g, x)) / float(x @ x)
+
+
 def test_power_iteration_matches_reference(fx, ctx, oracle):
     s = fx.synth_plain(21, 6000, 7200, 85.0)
     c = s.circuit
@@ -24,9 +40,9 @@ def test_power_iteration_matches_reference(fx, ctx, oracle):
     for k in range(len(cp) - 1):
         ref = oracle.fiedler_vector(ap, ai, perm[cp[k]:cp[k + 1]], iters=30)
         got = v[cp[k]:cp[k + 1]]
-        assert np.max(np.abs(got - ref)) < 2e-4, k
+        assert np.array_equal(got, ref), k  # the reference's f32 folds: bit-identical
         assert abs(np.linalg.norm(got.astype(np.float64)) - 1.0) < 1e-5
-        assert lam[k] > 0
+        assert abs(_rayleigh(ap, ai, perm[cp[k]:cp[k + 1]], got) - lam[k]) <= 1e-6 * lam[k]
 
 
 def test_power_iteration_tolerance_mode(fx, ctx, oracle):
@@ -44,15 +60,14 @@ def test_power_iteration_tolerance_mode(fx, ctx, oracle):
         d.close()
     assert np.all(its <= 500) and np.all(its > 1)
     for k in range(2):
-        g = gates[cp[k]:cp[k + 1]]
+        rq = _rayleigh(ap, ai, gates[cp[k]:cp[k + 1]], v[cp[k]:cp[k + 1]])
+        assert abs(rq - lam[k]) <= 1e-6 * abs(rq)
+        # converged: one more iteration (FP64) moves the quotient by ~tol at most
         x = v[cp[k]:cp[k + 1]].astype(np.float64)
-        pos = {int(q): i for i, q in enumerate(g)}
-        lx = np.zeros_like(x)
-        for i, q in enumerate(g):
-            nb = [pos[int(j)] for j in ai[ap[q]:ap[q + 1]] if int(j) in pos]
-            lx[i] = len(nb) * x[i] - x[nb].sum()
-        rq = float(x @ lx) / float(x @ x)
-        assert abs(rq - lam[k]) <= 1e-3 * abs(rq)
+        y = _laplacian(ap, ai, gates[cp[k]:cp[k + 1]], x)
+        y -= y.mean()
+        y /= np.linalg.norm(y)
+        assert abs(_rayleigh(ap, ai, gates[cp[k]:cp[k + 1]], y) - rq) <= 1e-5 * abs(rq)
 
 
 def test_singletons_and_empty_clusters(fx, ctx):
