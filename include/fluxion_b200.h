@@ -288,6 +288,12 @@ int fx_force_iterate(fx_ctx *ctx, fx_design *design, const fx_iter_cfg *cfg,
  * fx_design_trace_get returns those of the last iteration run (host
  * arrays of n_gates floats, each may be NULL). */
 int fx_design_trace(fx_design *design, int enable);
+/* With the trace enabled, fx_hapr_place_leaves also records each slot's
+ * total force (springs + repulsion) of the first iteration, at the leaf's
+ * deterministic start positions (placer.rs:226-227); this returns those of
+ * the last batch, in leaf_gate order (out arrays of the batch's slot count,
+ * each may be NULL). */
+int fx_design_leaf_trace_get(fx_design *design, float *out_fx, float *out_fy);
 int fx_design_trace_get(fx_design *design, float *out_fx, float *out_fy, float *out_x0,
                         float *out_y0, float *out_vx0, float *out_vy0);
 
@@ -328,8 +334,15 @@ typedef struct fx_leaf_cfg {
   float damping;            /* placer.rs:276 (0.9)                            */
   float dt;                 /* placer.rs:276-279 (0.1)                        */
   int32_t schedule;         /* FX_LEAF_*                                      */
-  int32_t reserved0, reserved1;
+  int32_t precision;        /* FX_LEAF_IEEE (default) or FX_LEAF_FAST         */
+  int32_t reserved1;
 } fx_leaf_cfg;
+
+/* Arithmetic of the pair repulsion term (placer.rs:258-272). */
+#define FX_LEAF_IEEE 0 /* the reference's sqrt and three divisions: positions  */
+                       /* bit-identical to place_gates_in_leaf                 */
+#define FX_LEAF_FAST 1 /* repel * d * rsqrt(max(|d|^2, 0.01))^3, hardware      */
+                       /* rsqrt: forces within f32 rounding of the IEEE form   */
 
 #define FX_LEAF_AUTO        0 /* time the schedules once, keep the fastest   */
 #define FX_LEAF_WARP        1 /* one warp per leaf, 8 leaves per block        */

@@ -280,6 +280,9 @@ struct fx_design {
   // force, start positions and start velocities (6 x n floats)
   bool trace_on = false;
   fx::DevBuf<float> trace;
+  // and of fx_hapr_place_leaves: each slot's force in the first iteration
+  fx::DevBuf<float2> leaf_trace;
+  int32_t leaf_trace_n = 0;
   // workspaces
   fx::BHWork bh;
   fx::DensityWork dens;

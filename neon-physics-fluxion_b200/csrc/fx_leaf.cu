@@ -52,7 +52,29 @@ struct LeafBatch {
   float k, repel, damping, dt;
   float *out_x, *out_y;    // global positions (written for leaf gates)
   unsigned int *counter;   // work counter
+  float2 *trace;           // or null: each slot's total force of the first iteration
 };
+
+// The repulsion term of a pair from positions a and b (placer.rs:258-272):
+// force * (a - b) / dist with dist = max(|a - b|, 0.1), force = repel / dist^2.
+// IEEE: the reference's rounding steps (sqrt, three divisions), bit for bit.
+// Fast (FX_LEAF_FAST): repel * (a - b) * rsqrt(max(d^2, 0.1^2))^3 with the
+// hardware rsqrt, equal to f32 rounding.
+template <bool Fast>
+__device__ __forceinline__ float2 leaf_pair_force(float ax, float ay, float bx, float by,
+                                                  float repel) {
+  const float dx = __fsub_rn(ax, bx), dy = __fsub_rn(ay, by);
+  if (Fast) {
+    const float inv = rsqrtf(fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), 0.1f * 0.1f));
+    const float f = __fmul_rn(__fmul_rn(__fmul_rn(repel, inv), inv), inv);
+    return make_float2(__fmul_rn(f, dx), __fmul_rn(f, dy));
+  }
+  const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
+  const float force = __fdiv_rn(repel, __fmul_rn(dist, dist));
+  return make_float2(__fdiv_rn(__fmul_rn(force, dx), dist),
+                     __fdiv_rn(__fmul_rn(force, dy), dist));
+}
 
 __device__ __forceinline__ float rclamp(float v, float lo, float hi) {
   if (v < lo) v = lo;
@@ -74,7 +96,7 @@ __device__ __forceinline__ void group_sync(int id) {
 
 // One leaf on a group of T threads (tid in [0, T)); sm: the group's shared
 // arrays x, y, vx, vy, fx, fy (kLeafMax each).
-template <int T>
+template <int T, bool Fast>
 __device__ void place_leaf(const LeafBatch &b, int leaf, int tid, float *sm, int sid) {
   float *sx = sm, *sy = sm + kLeafMax, *svx = sm + 2 * kLeafMax;
   float *svy = sm + 3 * kLeafMax, *sfx = sm + 4 * kLeafMax, *sfy = sm + 5 * kLeafMax;
@@ -110,12 +132,9 @@ __device__ void place_leaf(const LeafBatch &b, int leaf, int tid, float *sm, int
         float tx[kPairUnroll], ty[kPairUnroll];
 #pragma unroll
         for (int u = 0; u < kPairUnroll; ++u) {
-          const float dx = __fsub_rn(xi, sx[m + u]), dy = __fsub_rn(yi, sy[m + u]);
-          const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-          const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
-          const float force = __fdiv_rn(b.repel, __fmul_rn(dist, dist));
-          tx[u] = __fdiv_rn(__fmul_rn(force, dx), dist);
-          ty[u] = __fdiv_rn(__fmul_rn(force, dy), dist);
+          const float2 t = leaf_pair_force<Fast>(xi, yi, sx[m + u], sy[m + u], b.repel);
+          tx[u] = t.x;
+          ty[u] = t.y;
         }
 #pragma unroll
         for (int u = 0; u < kPairUnroll; ++u)
@@ -126,15 +145,13 @@ __device__ void place_leaf(const LeafBatch &b, int leaf, int tid, float *sm, int
       }
       for (; m < n; ++m) {
         if (m == i) continue;
-        const float dx = __fsub_rn(xi, sx[m]), dy = __fsub_rn(yi, sy[m]);
-        const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-        const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
-        const float force = __fdiv_rn(b.repel, __fmul_rn(dist, dist));
-        ax = __fadd_rn(ax, __fdiv_rn(__fmul_rn(force, dx), dist));
-        ay = __fadd_rn(ay, __fdiv_rn(__fmul_rn(force, dy), dist));
+        const float2 t = leaf_pair_force<Fast>(xi, yi, sx[m], sy[m], b.repel);
+        ax = __fadd_rn(ax, t.x);
+        ay = __fadd_rn(ay, t.y);
       }
       sfx[i] = ax;
       sfy[i] = ay;
+      if (b.trace && it == 0) b.trace[g0 + i] = make_float2(ax, ay);
     }
     group_sync<T>(sid);
     for (int i = tid; i < n; i += T) {
@@ -158,7 +175,7 @@ __device__ void place_leaf(const LeafBatch &b, int leaf, int tid, float *sm, int
 }
 
 // T threads per leaf; the 256-thread block holds 256 / T groups.
-template <int T>
+template <int T, bool Fast>
 __global__ void __launch_bounds__(256)
 leaf_batch_kernel(LeafBatch b, int per_cluster_leaf) {
   extern __shared__ float lsm[];
@@ -167,7 +184,7 @@ leaf_batch_kernel(LeafBatch b, int per_cluster_leaf) {
   float *sm = lsm + grp * kLeafArrays * kLeafMax;
   const int sid = 1 + grp;
   if (per_cluster_leaf >= 0) {  // the one-launch-per-leaf baseline
-    if (grp == 0) place_leaf<T>(b, per_cluster_leaf, tid, sm, sid);
+    if (grp == 0) place_leaf<T, Fast>(b, per_cluster_leaf, tid, sm, sid);
     return;
   }
   __shared__ int next[kGroups];
@@ -180,7 +197,7 @@ leaf_batch_kernel(LeafBatch b, int per_cluster_leaf) {
     const int leaf = next[grp];
     group_sync<T>(sid);
     if (leaf < 0) break;
-    place_leaf<T>(b, leaf, tid, sm, sid);
+    place_leaf<T, Fast>(b, leaf, tid, sm, sid);
   }
 }
 
@@ -222,21 +239,17 @@ __device__ __forceinline__ void pair_sync() {
     asm volatile("bar.sync %0, %1;" ::"n"(kBar), "n"(G) : "memory");
 }
 
-// Repulsion term of the pair (r, c), r < c, from their positions:
-// force * (p_r - p_c) / dist with the reference's rounding steps.
+// Repulsion term of the pair (r, c), r < c, from their positions.
+template <bool Fast>
 __device__ __forceinline__ float2 pair_term(float2 pr, float2 pc, float repel) {
-  const float dx = __fsub_rn(pr.x, pc.x), dy = __fsub_rn(pr.y, pc.y);
-  const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-  const float dist = fmaxf(__fsqrt_rn(d2), 0.1f);
-  const float force = __fdiv_rn(repel, __fmul_rn(dist, dist));
-  return make_float2(__fdiv_rn(__fmul_rn(force, dx), dist), __fdiv_rn(__fmul_rn(force, dy), dist));
+  return leaf_pair_force<Fast>(pr.x, pr.y, pc.x, pc.y, repel);
 }
 
 // One leaf on a group of T threads (tid in [0, T); the block with kBar = 0,
 // or one half of it with named barrier kBar). tri: the folded triangle; pos:
 // positions (x, y) in two buffers of nmax float2 (double-buffered across
 // iterations), then velocities (nmax float2).
-template <int T, int kBar>
+template <int T, int kBar, bool Fast>
 __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 *tri,
                                  float *pos, int tid) {
   const int g0 = b.gptr[leaf];
@@ -310,7 +323,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
         const int c1 = u + 1 + col;
         const bool first = c1 < n;
         at_k[k] = at;
-        t[k] = pair_term(sxy[first ? u : n - 2 - u], sxy[first ? c1 : col], b.repel);
+        t[k] = pair_term<Fast>(sxy[first ? u : n - 2 - u], sxy[first ? c1 : col], b.repel);
         advance();
       }
 #pragma unroll
@@ -319,7 +332,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
     for (; q < npairs; q += T) {
       const int c1 = u + 1 + col;
       const bool first = c1 < n;
-      tri[at] = pair_term(sxy[first ? u : n - 2 - u], sxy[first ? c1 : col], b.repel);
+      tri[at] = pair_term<Fast>(sxy[first ? u : n - 2 - u], sxy[first ? c1 : col], b.repel);
       advance();
     }
     pair_sync<T, kBar>();
@@ -387,6 +400,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
           ay = __fadd_rn(ay, v.y);
         }
       }
+      if (b.trace && it == 0) b.trace[g0 + j] = make_float2(ax, ay);
       const float2 v0 = sv[j];
       const float vx = __fmul_rn(__fadd_rn(v0.x, __fmul_rn(ax, b.dt)), b.damping);
       const float vy = __fmul_rn(__fadd_rn(v0.y, __fmul_rn(ay, b.dt)), b.damping);
@@ -408,7 +422,7 @@ __device__ void place_leaf_pairs(const LeafBatch &b, int leaf, int nmax, float2 
 }
 
 // One half of a block: leaves order[split..) from counter[1], named barrier kBar.
-template <int H, int kBar>
+template <int H, int kBar, bool Fast>
 __device__ __forceinline__ void half_loop(const LeafBatch &b, int split, int nhalf, float2 *tri,
                                           float *pos, int ht, int *next) {
   while (true) {
@@ -420,7 +434,7 @@ __device__ __forceinline__ void half_loop(const LeafBatch &b, int split, int nha
     const int leaf = *next;
     pair_sync<H, kBar>();
     if (leaf < 0) break;
-    place_leaf_pairs<H, kBar>(b, leaf, nhalf, tri, pos, ht);
+    place_leaf_pairs<H, kBar, Fast>(b, leaf, nhalf, tri, pos, ht);
   }
 }
 
@@ -429,7 +443,7 @@ __device__ __forceinline__ void half_loop(const LeafBatch &b, int split, int nha
 // barrier and half of the shared memory) pulls the remaining leaves from
 // counter[1]. Two leaves of at most nhalf gates fit where one of nmax does,
 // so the smaller leaves run twice as many to an SM.
-template <int T>
+template <int T, bool Fast>
 __global__ void __launch_bounds__(T, 3)
 leaf_pairs_kernel(LeafBatch b, int nmax, int split, int nhalf) {
   extern __shared__ float4 lpair[];
@@ -446,7 +460,7 @@ leaf_pairs_kernel(LeafBatch b, int nmax, int split, int nhalf) {
       const int leaf = next[0];
       __syncthreads();
       if (leaf < 0) break;
-      place_leaf_pairs<T, 0>(b, leaf, nmax, tri, pos, threadIdx.x);
+      place_leaf_pairs<T, 0, Fast>(b, leaf, nmax, tri, pos, threadIdx.x);
     }
   }
   if (split >= b.n_leaves) return;
@@ -456,9 +470,9 @@ leaf_pairs_kernel(LeafBatch b, int nmax, int split, int nhalf) {
                                            h * pair_smem_bytes(nhalf));
   float *pos = reinterpret_cast<float *>(tri + (size_t)pair_rows(nhalf) * pair_stride(nhalf));
   if (h == 0)
-    half_loop<H, 1>(b, split, nhalf, tri, pos, ht, next);
+    half_loop<H, 1, Fast>(b, split, nhalf, tri, pos, ht, next);
   else
-    half_loop<H, 2>(b, split, nhalf, tri, pos, ht, next + 1);
+    half_loop<H, 2, Fast>(b, split, nhalf, tri, pos, ht, next + 1);
 }
 
 // The batch's split for leaf_pairs_kernel: the largest nhalf whose two slots
@@ -482,7 +496,7 @@ static PairPlan pair_plan(int n_leaves, const int32_t *leaf_ptr, const std::vect
   return p;
 }
 
-template <int T>
+template <int T, bool Fast>
 static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, const PairPlan &plan, cudaStream_t s) {
   if (plan.nmax > kPairMax) {
     set_error("pair schedules take leaves of at most %d gates (largest: %d)", kPairMax,
@@ -490,16 +504,17 @@ static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, const PairPlan &plan, c
     return FX_EINVAL;
   }
   const size_t smem = pair_smem_bytes(plan.nmax);
-  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(leaf_pairs_kernel<T>), (int)smem));
+  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(leaf_pairs_kernel<T, Fast>),
+                          (int)smem));
   int per_sm = 0;
-  FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_pairs_kernel<T>,
-                                                               T, smem));
+  FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, leaf_pairs_kernel<T, Fast>, T, smem));
   if (per_sm < 1) per_sm = 1;
   int grid = ctx->num_sms * per_sm;
   if (grid > b.n_leaves) grid = b.n_leaves;
   if (grid < 1) grid = 1;
   FX_CHECK_CUDA(cudaMemsetAsync(b.counter, 0, 8, s));
-  leaf_pairs_kernel<T><<<grid, T, smem, s>>>(b, plan.nmax, plan.split, plan.nhalf);
+  leaf_pairs_kernel<T, Fast><<<grid, T, smem, s>>>(b, plan.nmax, plan.split, plan.nhalf);
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   return FX_OK;
@@ -611,48 +626,56 @@ static int build_leaf_host(const fx_design *d, int L, const int32_t *leaf_ptr,
   return FX_OK;
 }
 
-template <int T>
+template <int T, bool Fast>
 static int launch_leaf(fx_ctx *ctx, const LeafBatch &b, bool per_cluster,
                        cudaStream_t s) {
   constexpr int kGroups = 256 / T;
   const size_t smem = (size_t)kGroups * kLeafArrays * kLeafMax * sizeof(float);
-  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(leaf_batch_kernel<T>), (int)smem));
+  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(leaf_batch_kernel<T, Fast>),
+                          (int)smem));
   if (per_cluster) {
     for (int l = 0; l < b.n_leaves; ++l)
-      leaf_batch_kernel<T><<<1, 256, smem, s>>>(b, l);
+      leaf_batch_kernel<T, Fast><<<1, 256, smem, s>>>(b, l);
     FX_CHECK_LAUNCH();
     ctx->launches += b.n_leaves;
     return FX_OK;
   }
   int per_sm = 0;
-  FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_batch_kernel<T>,
-                                                               256, smem));
+  FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, leaf_batch_kernel<T, Fast>, 256, smem));
   if (per_sm < 1) per_sm = 1;
   int grid = ctx->num_sms * per_sm;
   const int need = (b.n_leaves + kGroups - 1) / kGroups;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   FX_CHECK_CUDA(cudaMemsetAsync(b.counter, 0, 4, s));
-  leaf_batch_kernel<T><<<grid, 256, smem, s>>>(b, -1);
+  leaf_batch_kernel<T, Fast><<<grid, 256, smem, s>>>(b, -1);
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   return FX_OK;
 }
 
-static int run_schedule(fx_ctx *ctx, const LeafBatch &b, int schedule, const PairPlan &plan,
-                        cudaStream_t s) {
+template <bool Fast>
+static int run_schedule_p(fx_ctx *ctx, const LeafBatch &b, int schedule, const PairPlan &plan,
+                          cudaStream_t s) {
   switch (schedule) {
-    case FX_LEAF_PAIR64: return launch_pairs<64>(ctx, b, plan, s);
-    case FX_LEAF_PAIR128: return launch_pairs<128>(ctx, b, plan, s);
-    case FX_LEAF_PAIR256: return launch_pairs<256>(ctx, b, plan, s);
-    case FX_LEAF_WARP: return launch_leaf<32>(ctx, b, false, s);
-    case FX_LEAF_CTA64: return launch_leaf<64>(ctx, b, false, s);
-    case FX_LEAF_CTA128: return launch_leaf<128>(ctx, b, false, s);
-    case FX_LEAF_CTA256: return launch_leaf<256>(ctx, b, false, s);
-    case FX_LEAF_PER_CLUSTER: return launch_leaf<128>(ctx, b, true, s);
+    case FX_LEAF_PAIR64: return launch_pairs<64, Fast>(ctx, b, plan, s);
+    case FX_LEAF_PAIR128: return launch_pairs<128, Fast>(ctx, b, plan, s);
+    case FX_LEAF_PAIR256: return launch_pairs<256, Fast>(ctx, b, plan, s);
+    case FX_LEAF_WARP: return launch_leaf<32, Fast>(ctx, b, false, s);
+    case FX_LEAF_CTA64: return launch_leaf<64, Fast>(ctx, b, false, s);
+    case FX_LEAF_CTA128: return launch_leaf<128, Fast>(ctx, b, false, s);
+    case FX_LEAF_CTA256: return launch_leaf<256, Fast>(ctx, b, false, s);
+    case FX_LEAF_PER_CLUSTER: return launch_leaf<128, Fast>(ctx, b, true, s);
   }
   set_error("unknown leaf schedule %d", schedule);
   return FX_EINVAL;
+}
+
+static int run_schedule(fx_ctx *ctx, const LeafBatch &b, int schedule, const PairPlan &plan,
+                        bool fast, cudaStream_t s) {
+  return fast ? run_schedule_p<true>(ctx, b, schedule, plan, s)
+              : run_schedule_p<false>(ctx, b, schedule, plan, s);
 }
 
 }  // namespace fx
@@ -667,7 +690,7 @@ extern "C" int fx_leaf_cfg_default(fx_leaf_cfg *c) {
   c->damping = 0.9f;
   c->dt = 0.1f;
   c->schedule = FX_LEAF_AUTO;
-  c->reserved0 = 0;
+  c->precision = FX_LEAF_IEEE;
   c->reserved1 = 0;
   return FX_OK;
 }
@@ -677,10 +700,12 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
                                     const float *region, const fx_leaf_cfg *cfg,
                                     float *out_x, float *out_y, int32_t *out_schedule) {
   if (!ctx || !d || n_leaves < 0 || (n_leaves > 0 && (!leaf_ptr || !leaf_gate || !region)) ||
-      !cfg || !out_x || !out_y || cfg->force_iterations < 0) {
+      !cfg || !out_x || !out_y || cfg->force_iterations < 0 ||
+      (cfg->precision != FX_LEAF_IEEE && cfg->precision != FX_LEAF_FAST)) {
     set_error("fx_hapr_place_leaves: invalid arguments");
     return FX_EINVAL;
   }
+  const bool fast = cfg->precision == FX_LEAF_FAST;
   if (n_leaves == 0) return FX_OK;
   if (leaf_ptr[0] != 0) {
     set_error("fx_hapr_place_leaves: leaf_ptr[0] must be 0");
@@ -739,9 +764,15 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
   FX_CHECK_CUDA(up(reg.p, region, (size_t)n_leaves * 16));
   FX_CHECK_CUDA(up(ox.p, out_x, (size_t)d->n * 4));
   FX_CHECK_CUDA(up(oy.p, out_y, (size_t)d->n * 4));
+  if (d->trace_on) {
+    FX_TRY(d->leaf_trace.alloc(G > 0 ? (size_t)G : 1));
+    FX_CHECK_CUDA(cudaMemsetAsync(d->leaf_trace.p, 0, (size_t)std::max(G, 1) * 8, s));
+    d->leaf_trace_n = G;
+  }
   LeafBatch b{gptr.p, gate.p, aptr.p, aidx.p, reg.p, order.p, n_leaves,
               cfg->force_iterations, cfg->attract_weight, cfg->repel_weight,
-              cfg->damping, cfg->dt, ox.p, oy.p, counter.p};
+              cfg->damping, cfg->dt, ox.p, oy.p, counter.p,
+              d->trace_on ? d->leaf_trace.p : nullptr};
   int schedule = cfg->schedule;
   bool done = false;
   auto lg2 = [](int64_t v) {
@@ -753,7 +784,8 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
     return b;
   };
   const uint32_t shape = (uint32_t)lg2(n_leaves) | ((uint32_t)lg2(G / std::max(1, n_leaves)) << 8) |
-                         ((uint32_t)lg2(cfg->force_iterations) << 16);
+                         ((uint32_t)lg2(cfg->force_iterations) << 16) |
+                         ((uint32_t)fast << 24);
   if (schedule == FX_LEAF_AUTO) {
     auto it = ctx->leaf_tuned.find(shape);
     if (it != ctx->leaf_tuned.end()) schedule = it->second;
@@ -771,7 +803,7 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
                    FX_LEAF_PAIR64, FX_LEAF_PAIR128, FX_LEAF_PAIR256}) {
       if (sc >= FX_LEAF_PAIR64 && plan.nmax > kPairMax) continue;
       FX_CHECK_CUDA(cudaEventRecord(e0, s));
-      int rc = run_schedule(ctx, b, sc, plan, s);
+      int rc = run_schedule(ctx, b, sc, plan, fast, s);
       if (rc != FX_OK) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -796,7 +828,7 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
   if (!done) {
     cudaEvent_t ev;
     timer_begin(ctx, FX_STAGE_LEAF, s, &ev);
-    FX_TRY(run_schedule(ctx, b, schedule, plan, s));
+    FX_TRY(run_schedule(ctx, b, schedule, plan, fast, s));
     timer_end(ctx, FX_STAGE_LEAF, s, ev);
   }
   FX_CHECK_CUDA(cudaMemcpyAsync(out_x, ox.p, (size_t)d->n * 4, cudaMemcpyDeviceToHost, s));
@@ -809,5 +841,25 @@ extern "C" int fx_hapr_place_leaves(fx_ctx *ctx, fx_design *d, int32_t n_leaves,
   ox.release();
   oy.release();
   counter.release();
+  return FX_OK;
+}
+
+extern "C" int fx_design_leaf_trace_get(fx_design *d, float *out_fx, float *out_fy) {
+  if (!d || !d->ctx) return FX_EINVAL;
+  if (!d->leaf_trace.p || d->leaf_trace_n <= 0) {
+    set_error("fx_design_leaf_trace_get: no traced leaf batch (enable fx_design_trace, "
+              "then run fx_hapr_place_leaves)");
+    return FX_EINVAL;
+  }
+  fx_ctx *ctx = d->ctx;
+  FX_CHECK_CUDA(cudaSetDevice(ctx->device));
+  std::vector<float2> t((size_t)d->leaf_trace_n);
+  FX_CHECK_CUDA(cudaMemcpyAsync(t.data(), d->leaf_trace.p, t.size() * 8,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  FX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (size_t i = 0; i < t.size(); ++i) {
+    if (out_fx) out_fx[i] = t[i].x;
+    if (out_fy) out_fy[i] = t[i].y;
+  }
   return FX_OK;
 }

@@ -27,6 +27,9 @@ FX_DCT_SIMT = 3
 FX_BH_FAST = 0
 FX_BH_EXACT = 1
 
+FX_LEAF_IEEE = 0
+FX_LEAF_FAST = 1
+
 STAGES = ["attract_integrate", "bh_keys", "bh_sort", "bh_tree", "bh_walk",
           "density", "congestion", "leaf", "fiedler", "attention"]
 
@@ -63,7 +66,7 @@ class LeafCfg(C.Structure):
     _fields_ = [("force_iterations", C.c_int32), ("attract_weight", C.c_float),
                 ("repel_weight", C.c_float), ("damping", C.c_float),
                 ("dt", C.c_float), ("schedule", C.c_int32),
-                ("reserved0", C.c_int32), ("reserved1", C.c_int32)]
+                ("precision", C.c_int32), ("reserved1", C.c_int32)]
 
 
 FX_LEAF_AUTO = 0
@@ -164,6 +167,7 @@ SIGNATURES = {
     "fx_design_get_positions": (C.c_int, [P, PF32, PF32]),
     "fx_design_save_state": (C.c_int, [P]),
     "fx_design_trace": (C.c_int, [P, C.c_int]),
+    "fx_design_leaf_trace_get": (C.c_int, [P, PF32, PF32]),
     "fx_stage_barnes_hut_walk": (C.c_int, [P, P, C.c_float, C.c_float, C.c_float, I32, PF32,
                                            PF32, C.POINTER(C.c_uint32), C.POINTER(C.c_int32),
                                            PF32, C.POINTER(C.c_int32)]),

@@ -266,6 +266,15 @@ class Design:
               "fx_design_trace_get")
         return out
 
+    def leaf_trace_get(self, slots: int):
+        """fx_design_leaf_trace_get: each slot's first-iteration force (fx, fy) of the
+        last traced leaf batch, in leaf_gate order."""
+        fx = np.empty(slots, np.float32)
+        fy = np.empty(slots, np.float32)
+        check(self.lib.fx_design_leaf_trace_get(self.handle, ptr(fx, C.c_float),
+                                                ptr(fy, C.c_float)), "fx_design_leaf_trace_get")
+        return fx, fy
+
     def device_bytes(self) -> int:
         return int(self.lib.fx_design_device_bytes(self.handle))
 

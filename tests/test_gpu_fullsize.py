@@ -149,3 +149,51 @@ def test_leaf_batch_full_size(fx, ctx, oracle):
     with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
         list(ex.map(one, range(len(lp) - 1)))
     assert np.array_equal(x, ox) and np.array_equal(y, oy)
+
+
+def test_leaf_batch_fast_precision_full_size(fx, ctx, oracle):
+    """FX_LEAF_FAST on the whole batched-leaf workload (16,384 clusters,
+    300 iterations): the first iteration's total force of every gate within
+    1e-5 (relative L2) of the FP64 recomputation at the leaves' start
+    positions, and the final HPWL within 0.5 % of place_gates_in_leaf's."""
+    from concurrent.futures import ThreadPoolExecutor
+    s = fx.synth_leaves(42, 16_384, 16, 128, 1.5)
+    c = s.circuit
+    gates = np.arange(c.num_gates, dtype=np.int32)
+    d = fx.Design(ctx, c)
+    try:
+        d.trace(True)
+        x, y, _ = d.place_leaves(s.leaf_ptr, gates, s.region,
+                                 fx.leaf_cfg(force_iterations=300, precision=fx.FX_LEAF_FAST))
+        tfx, tfy = d.leaf_trace_get(c.num_gates)
+        ix, iy, _ = d.place_leaves(s.leaf_ptr, gates, s.region,
+                                   fx.leaf_cfg(force_iterations=300))
+        efx, efy = d.leaf_trace_get(c.num_gates)
+    finally:
+        d.close()
+    ap, ai = oracle.build_adjacency(c.num_gates, c.net_ptr, c.net_gate)
+    lp, reg = s.leaf_ptr, s.region.reshape(-1, 4)
+    x0 = np.zeros(c.num_gates, np.float32)
+    y0 = np.zeros(c.num_gates, np.float32)
+    rfx = np.zeros(c.num_gates)
+    rfy = np.zeros(c.num_gates)
+    ox = np.zeros(c.num_gates, np.float32)
+    oy = np.zeros(c.num_gates, np.float32)
+
+    def one(l):
+        g = gates[lp[l]:lp[l + 1]]
+        oracle.place_leaf(g, ap, ai, reg[l], 0, 1.0, 0.5, 0.9, 0.1, x0, y0)  # start positions
+        rfx[g], rfy[g] = oracle.leaf_forces_f64(g, ap, ai, x0[g], y0[g])
+        oracle.place_leaf(g, ap, ai, reg[l], 300, 1.0, 0.5, 0.9, 0.1, ox, oy)
+
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        list(ex.map(one, range(len(lp) - 1)))
+    err_fast = _rel(tfx, tfy, rfx, rfy)
+    err_ieee = _rel(efx, efy, rfx, rfy)
+    print(f"leaf forces vs FP64: fast {err_fast:.3e}, IEEE {err_ieee:.3e}")
+    assert err_fast <= 1e-5 and err_ieee <= 1e-5
+    assert np.array_equal(ix, ox) and np.array_equal(iy, oy)  # IEEE: bit-exact
+    h_fast = oracle.hpwl_f64(c.net_ptr, c.net_gate, x, y)
+    h_ref = oracle.hpwl_f64(c.net_ptr, c.net_gate, ox, oy)
+    print(f"leaf HPWL: fast {h_fast:.6e} vs reference {h_ref:.6e}")
+    assert abs(h_fast - h_ref) <= 5e-3 * h_ref
