@@ -240,12 +240,12 @@ typedef struct fx_iter_cfg {
 
 /* Barnes-Hut walk. Both give every point the interaction list of the
  * reference's per-point opening rule (BarnesHutTree.cpp:145-167) on the
- * same tree; they differ in how the terms are found and summed. */
-#define FX_BH_FAST  0 /* cells decided for a whole warp of points at once are */
-                      /* summed densely from shared memory; hardware rsqrt;   */
+ * same tree and add its terms in the same order; they differ in the
+ * inverse square root. */
+#define FX_BH_FAST  0 /* hardware rsqrt; single points share the cell code:   */
                       /* forces within f32 rounding of the exact walk         */
-#define FX_BH_EXACT 1 /* per-point masked walk, fixed term order, reproducible */
-                      /* rsqrt: forces bit-identical to the oracle's f32 walk */
+#define FX_BH_EXACT 1 /* reproducible rsqrt (bit-level estimate + 3 Newton    */
+                      /* steps): forces bit-identical to the oracle's f32 walk */
 
 #define FX_DCT_FP32  0 /* 3xTF32 split on the tensor cores; its error grows   */
                        /* with G (6.6e-4 at 256, 4.4e-3 at 2048 measured):  */

@@ -770,13 +770,69 @@ __device__ __forceinline__ unsigned bh_eval(int c, bool in, bool cell, int s,
 constexpr int kWalkGroup = 8;                    // lanes per group
 constexpr int kWalkGroups = 32 / kWalkGroup;     // groups per warp
 
-template <int Stack>
+// ---- FX_BH_FAST: the same walk with the hardware rsqrt -----------------------------
+// bh_walk_kernel<Stack, true> visits the same cells in the same order as the
+// exact walk, so every point keeps the reference rule's interaction list and
+// the terms are added in the same order; only the inverse square root is the
+// hardware rsqrt (a few ulp), and a single-point child is evaluated by the
+// cell code as a record of count 1 that every other point accepts (its own
+// lane's term is f * 0 = 0), so point and cell children share one
+// instruction stream. Forces agree with the exact walk to f32 rounding.
+template <bool Count>
+__device__ __forceinline__ unsigned fast_eval(int c, bool in, bool cell, int s, float2 p,
+                                              float k, float th2, float md2,
+                                              const float4 *__restrict__ node,
+                                              const float2 *__restrict__ spos, float &fx,
+                                              float &fy, int &terms) {
+  bool op = false;
+  if (in) {
+    float4 r0, r1;
+    if (cell) {
+      r0 = node[2 * c];
+      r1 = node[2 * c + 1];
+    } else {
+      const float2 q = spos[~c];
+      r0 = make_float4(q.x, q.y, 0.f, 0.f);
+      r1 = make_float4(1.f, 0.f, 0.f, 0.f);
+    }
+    const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
+    const float dy = __fsub_rn(__fsub_rn(p.y, r0.y), r0.w);
+    const float r2c = fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), md2);
+    if (!cell || (r1.y >= 0.f && r1.y < __fmul_rn(th2, r2c))) {
+      const float inv = rsqrtf(r2c);
+      const float f = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(k, fabsf(r1.x)), inv), inv),
+                                inv);
+      fx = __fmaf_rn(f, dx, fx);
+      fy = __fmaf_rn(f, dy, fy);
+      if (Count) terms += (cell || ~c != s) ? 1 : 0;
+    } else if (r1.x > 0.f) {
+      op = true;
+    } else {  // bucket: point by point
+      const int b = __float_as_int(r1.z), e = __float_as_int(r1.w);
+      for (int t = b; t <= e; ++t) {
+        const float2 q = spos[t];
+        const float ex = __fsub_rn(p.x, q.x), ey = __fsub_rn(p.y, q.y);
+        const float iv = rsqrtf(fmaxf(__fmaf_rn(ex, ex, __fmul_rn(ey, ey)), md2));
+        const float g = t == s ? 0.f : __fmul_rn(__fmul_rn(__fmul_rn(k, iv), iv), iv);
+        fx = __fmaf_rn(g, ex, fx);
+        fy = __fmaf_rn(g, ey, fy);
+        if (Count) terms += t == s ? 0 : 1;
+      }
+    }
+  }
+  return __ballot_sync(0xffffffffu, op);
+}
+
+// Fast: FX_BH_FAST (fast_eval instead of bh_eval); Count: also each point's
+// number of terms.
+template <int Stack, bool Fast = false, bool Count = false>
 __global__ void __launch_bounds__(kWalkWarps * 32)
 bh_walk_kernel(int n, const float2 *__restrict__ spos,
                const int32_t *__restrict__ perm,
                const int4 *__restrict__ qchild,
                const float4 *__restrict__ node, float k, float th2, float md2,
-               float2 *__restrict__ force, unsigned int *__restrict__ err) {
+               float2 *__restrict__ force, unsigned int *__restrict__ err,
+               int32_t *__restrict__ term_count = nullptr) {
   // one stack per group; the odd stride puts the groups' tops (often at the
   // same depth) in different banks
   __shared__ int32_t st_node[kWalkWarps][kWalkGroups][Stack + 1];
@@ -792,8 +848,13 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
   const float2 p = valid ? spos[s] : make_float2(0.f, 0.f);
   float fx = 0.f, fy = 0.f;
   int sp = 0;  // this group's stack depth (uniform in the group)
+  int terms = 0;
+  auto eval = [&](int c, bool in, bool cell) -> unsigned {
+    if (Fast) return fast_eval<Count>(c, in, cell, s, p, k, th2, md2, node, spos, fx, fy, terms);
+    return bh_eval(c, in, cell, s, p, k, th2, md2, node, spos, fx, fy);
+  };
   if (n >= 2) {
-    const unsigned open = bh_eval(0, valid, true, s, p, k, th2, md2, node, spos, fx, fy) & gmask;
+    const unsigned open = eval(0, valid, true) & gmask;
     if (open) {
       if (leader) {
         st_node[w][g][0] = 0;
@@ -821,8 +882,7 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
       const int c = qc[h];
-      om[h] = bh_eval(c, in && c != kNone, c >= 0, s, p, k, th2, md2, node, spos, fx, fy) &
-              gmask;
+      om[h] = eval(c, in && c != kNone, c >= 0) & gmask;
     }
     const int np = (om[0] != 0u) + (om[1] != 0u) + (om[2] != 0u) + (om[3] != 0u);
     if (sp + np > Stack) {
@@ -841,339 +901,6 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
       }
     }
     __syncwarp();
-  }
-  if (valid) force[perm[s]] = make_float2(fx, fy);
-}
-
-// ---- group-decided walk (FX_BH_FAST) ---------------------------------------------
-// The same interaction lists as bh_walk_kernel (the reference opening rule,
-// per point), found and summed with far fewer instructions. A warp's 32
-// consecutive sorted points lie in a small box B. For a cell with centre of
-// mass C and squared size s2, every point p of B has
-//   d2min(C, B) <= |p - C|^2 <= d2max(C, B),
-// and its f32 test `s2 < th2 * max(r2(p), md2)` (r2(p) the f32 rounding of
-// |p - C|^2, relative error below 1e-6) is therefore decided for the whole
-// warp at once when
-//   s2 <  th2 * max(d2min, md2) * (1 - eps)   -> every point accepts the cell,
-//   s2 >= th2 * max(d2max, md2) * (1 + eps)   -> every point opens it,
-// (FP64, eps = 4e-5, far above the f32 error). Cells accepted by all go to
-// an interaction list in shared memory that all 32 lanes evaluate densely
-// (broadcast reads, no divergence); cells opened by all are descended by the
-// warp together; single points and fully opened buckets join the list (a
-// point skips itself). Only "mixed" cells, where the points may decide
-// differently, fall back to the per-lane masked walk of bh_walk_kernel
-// (evaluated with each point's own f32 test), so every point interacts with
-// exactly the cells and points the per-point rule gives it. The terms are
-// added in a different order and the inverse square root is the hardware
-// rsqrt, so forces agree with the exact walk to f32 rounding (checked
-// against the FP64 sum over the same interaction list).
-constexpr int kFastWarps = 4;    // warps per block
-constexpr int kFastGS = 192;     // group stack (cells opened by the whole warp)
-constexpr int kFastLC = 64;      // dense interaction list entries (>= 32)
-constexpr int kFastRC = 32;      // fully opened buckets, as point ranges (>= 32)
-constexpr int kFastMC = 48;      // mixed cells awaiting the per-lane walk (>= 32)
-constexpr double kFastEps = 4e-5;
-static_assert(kFastLC >= 32 && kFastRC >= 32 && kFastMC >= 32,
-              "one classification round files up to 32 entries of a kind");
-
-// bh_eval with the hardware rsqrt: the per-lane test of child c (a cell when
-// `cell`) for the lane's point; returns the lanes that open c as a cell.
-template <bool Count>
-__device__ __forceinline__ unsigned fast_eval(int c, bool in, bool cell, int s, float2 p,
-                                              float k, float th2, float md2,
-                                              const float4 *__restrict__ node,
-                                              const float2 *__restrict__ spos, float &fx,
-                                              float &fy, int &terms) {
-  bool op = false;
-  if (in) {
-    if (!cell) {
-      if (~c != s) {
-        const float2 q = spos[~c];
-        const float dx = __fsub_rn(p.x, q.x), dy = __fsub_rn(p.y, q.y);
-        const float inv = rsqrtf(fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), md2));
-        const float f = __fmul_rn(__fmul_rn(__fmul_rn(k, inv), inv), inv);
-        fx = __fmaf_rn(f, dx, fx);
-        fy = __fmaf_rn(f, dy, fy);
-        if (Count) ++terms;
-      }
-    } else {
-      const float4 r0 = node[2 * c], r1 = node[2 * c + 1];
-      const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
-      const float dy = __fsub_rn(__fsub_rn(p.y, r0.y), r0.w);
-      const float r2c = fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), md2);
-      if (r1.y >= 0.f && r1.y < __fmul_rn(th2, r2c)) {
-        const float inv = rsqrtf(r2c);
-        const float f = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(k, fabsf(r1.x)), inv), inv),
-                                  inv);
-        fx = __fmaf_rn(f, dx, fx);
-        fy = __fmaf_rn(f, dy, fy);
-        if (Count) ++terms;
-      } else if (r1.x > 0.f) {
-        op = true;
-      } else {  // bucket: point by point
-        const int b = __float_as_int(r1.z), e = __float_as_int(r1.w);
-        for (int t = b; t <= e; ++t) {
-          const float2 q = spos[t];
-          const float ex = __fsub_rn(p.x, q.x), ey = __fsub_rn(p.y, q.y);
-          const float inv = rsqrtf(fmaxf(__fmaf_rn(ex, ex, __fmul_rn(ey, ey)), md2));
-          const float f = t == s ? 0.f : __fmul_rn(__fmul_rn(__fmul_rn(k, inv), inv), inv);
-          fx = __fmaf_rn(f, ex, fx);
-          fy = __fmaf_rn(f, ey, fy);
-          if (Count) terms += t == s ? 0 : 1;
-        }
-      }
-    }
-  }
-  return __ballot_sync(0xffffffffu, op);
-}
-
-template <int Stack>
-struct FastWarpSmem {
-  int32_t gst[kFastGS];
-  float4 lpos[kFastLC];  // {x_hi, y_hi, x_lo, y_lo}
-  float2 lkq[kFastLC];   // {k * count, point index (int bits) or -1}
-  int2 rng[kFastRC];
-  int32_t mix[kFastMC];
-  int32_t st_node[kWalkGroups][Stack + 1];
-  unsigned st_mask[kWalkGroups][Stack + 1];
-};
-
-template <int Stack, bool Count>
-__global__ void __launch_bounds__(kFastWarps * 32)
-bh_walk_fast_kernel(int n, const float2 *__restrict__ spos, const int32_t *__restrict__ perm,
-                    const int4 *__restrict__ qchild, const float4 *__restrict__ node, float k,
-                    float th2, float md2, float2 *__restrict__ force,
-                    unsigned int *__restrict__ err, int32_t *__restrict__ term_count) {
-  __shared__ FastWarpSmem<Stack> sm_all[kFastWarps];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  FastWarpSmem<Stack> &sm = sm_all[w];
-  const unsigned kAll = 0xffffffffu, lt = (1u << lane) - 1u;
-  const int s = (blockIdx.x * kFastWarps + w) * 32 + lane;
-  const bool valid = s < n;
-  if (__ballot_sync(kAll, valid) == 0u) return;
-  const float2 p = valid ? spos[s] : make_float2(0.f, 0.f);
-  float fx = 0.f, fy = 0.f;
-  int terms = 0;
-  // the box of the warp's (valid) points
-  float bx0 = valid ? p.x : FLT_MAX, by0 = valid ? p.y : FLT_MAX;
-  float bx1 = valid ? p.x : -FLT_MAX, by1 = valid ? p.y : -FLT_MAX;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    bx0 = fminf(bx0, __shfl_xor_sync(kAll, bx0, o));
-    by0 = fminf(by0, __shfl_xor_sync(kAll, by0, o));
-    bx1 = fmaxf(bx1, __shfl_xor_sync(kAll, bx1, o));
-    by1 = fmaxf(by1, __shfl_xor_sync(kAll, by1, o));
-  }
-  const double th2d = (double)th2, md2d = (double)md2;
-  const int g = lane / kWalkGroup;
-  const bool leader = (lane % kWalkGroup) == 0;
-  const unsigned gmask = ((1u << kWalkGroup) - 1u) << (g * kWalkGroup);
-  int nl = 0, nr = 0, nm = 0, gsp = 0;  // warp-uniform fill levels
-
-  // Dense evaluation of the list by all lanes (a lane's own point gets a
-  // zero scale; r2c >= md2 > 0 keeps it finite).
-  auto flush_list = [&]() {
-    __syncwarp();
-#pragma unroll 2
-    for (int e = 0; e < nl; ++e) {
-      const float4 q = sm.lpos[e];
-      const float2 kk = sm.lkq[e];
-      const float dx = __fsub_rn(__fsub_rn(p.x, q.x), q.z);
-      const float dy = __fsub_rn(__fsub_rn(p.y, q.y), q.w);
-      const float inv = rsqrtf(fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), md2));
-      const bool self = __float_as_int(kk.y) == s;
-      const float f = self ? 0.f : __fmul_rn(__fmul_rn(__fmul_rn(kk.x, inv), inv), inv);
-      fx = __fmaf_rn(f, dx, fx);
-      fy = __fmaf_rn(f, dy, fy);
-      if (Count) terms += self ? 0 : 1;
-    }
-    __syncwarp();
-    nl = 0;
-  };
-  auto flush_ranges = [&]() {
-    __syncwarp();
-    for (int r = 0; r < nr; ++r) {
-      const int2 b = sm.rng[r];
-      for (int t = b.x; t <= b.y; ++t) {
-        const float2 q = spos[t];
-        const float dx = __fsub_rn(p.x, q.x), dy = __fsub_rn(p.y, q.y);
-        const float inv = rsqrtf(fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), md2));
-        const float f = t == s ? 0.f : __fmul_rn(__fmul_rn(__fmul_rn(k, inv), inv), inv);
-        fx = __fmaf_rn(f, dx, fx);
-        fy = __fmaf_rn(f, dy, fy);
-        if (Count) terms += t == s ? 0 : 1;
-      }
-    }
-    __syncwarp();
-    nr = 0;
-  };
-  // The per-lane walk below the mixed cells: bh_walk_kernel's loop, four
-  // mixed cells at a time (as the children of one popped cell), so its
-  // stacks stay within the same bound.
-  auto flush_mixed = [&]() {
-    __syncwarp();
-    for (int i0 = 0; i0 < nm; i0 += 4) {
-      int qc[4];
-#pragma unroll
-      for (int h = 0; h < 4; ++h) qc[h] = i0 + h < nm ? sm.mix[i0 + h] : kNone;
-      unsigned om[4];
-#pragma unroll
-      for (int h = 0; h < 4; ++h)
-        om[h] = fast_eval<Count>(qc[h], valid && qc[h] != kNone, qc[h] >= 0, s, p, k, th2,
-                                 md2, node, spos, fx, fy, terms) & gmask;
-      int sp = 0;
-#pragma unroll
-      for (int h = 3; h >= 0; --h)
-        if (om[h] != 0u) {
-          if (leader) {
-            sm.st_node[g][sp] = qc[h];
-            sm.st_mask[g][sp] = om[h];
-          }
-          ++sp;
-        }
-      __syncwarp();
-      while (__any_sync(kAll, sp > 0)) {
-        const bool has = sp > 0;
-        int nd = 0;
-        unsigned mask = 0u;
-        if (has) {
-          --sp;
-          nd = sm.st_node[g][sp];
-          mask = sm.st_mask[g][sp];
-        }
-        __syncwarp();
-        int4 q = make_int4(kNone, kNone, kNone, kNone);
-        if (has) q = qchild[nd];
-        const int cc[4] = {q.x, q.y, q.z, q.w};
-        const bool in = (mask >> lane) & 1u;
-        unsigned o2[4];
-#pragma unroll
-        for (int h = 0; h < 4; ++h)
-          o2[h] = fast_eval<Count>(cc[h], in && cc[h] != kNone, cc[h] >= 0, s, p, k, th2,
-                                   md2, node, spos, fx, fy, terms) & gmask;
-        const int np = (o2[0] != 0u) + (o2[1] != 0u) + (o2[2] != 0u) + (o2[3] != 0u);
-        if (sp + np > Stack) {
-          if (leader) atomicOr(err, 1u);
-        } else {
-#pragma unroll
-          for (int h = 3; h >= 0; --h)
-            if (o2[h] != 0u) {
-              if (leader) {
-                sm.st_node[g][sp] = cc[h];
-                sm.st_mask[g][sp] = o2[h];
-              }
-              ++sp;
-            }
-        }
-        __syncwarp();
-      }
-    }
-    nm = 0;
-  };
-
-  // Decides child c (one per lane, kNone for none) for the whole warp and
-  // files it: list entry, point range, warp descent, or mixed.
-  auto classify = [&](int c) {
-    int cat = 0;  // 0 none, 1 list entry, 2 range, 3 descend together, 4 mixed
-    float4 le = make_float4(0.f, 0.f, 0.f, 0.f);
-    float2 lk = make_float2(0.f, 0.f);
-    int2 rg = make_int2(0, -1);
-    if (c != kNone) {
-      if (c < 0) {  // a single point
-        const float2 q = spos[~c];
-        le = make_float4(q.x, q.y, 0.f, 0.f);
-        lk = make_float2(k, __int_as_float(~c));
-        cat = 1;
-      } else {
-        const float4 r0 = node[2 * c], r1 = node[2 * c + 1];
-        if (r1.y < 0.f) {  // no quad level: opened by every point
-          if (r1.x > 0.f) {
-            cat = 3;
-          } else {
-            rg = make_int2(__float_as_int(r1.z), __float_as_int(r1.w));
-            cat = 2;
-          }
-        } else {
-          const double cx = (double)r0.x + (double)r0.z, cy = (double)r0.y + (double)r0.w;
-          const double ex0 = (double)bx0 - cx, ex1 = cx - (double)bx1;
-          const double ey0 = (double)by0 - cy, ey1 = cy - (double)by1;
-          const double ax = fmax(fmax(ex0, ex1), 0.0), ay = fmax(fmax(ey0, ey1), 0.0);
-          const double mx = fmax(fabs(ex0), fabs(ex1)), my = fmax(fabs(ey0), fabs(ey1));
-          const double d2min = ax * ax + ay * ay, d2max = mx * mx + my * my;
-          const double s2 = (double)r1.y;
-          if (s2 < th2d * fmax(d2min, md2d) * (1.0 - kFastEps)) {
-            le = r0;
-            lk = make_float2(__fmul_rn(k, fabsf(r1.x)), __int_as_float(-1));
-            cat = 1;
-          } else if (s2 >= th2d * fmax(d2max, md2d) * (1.0 + kFastEps)) {
-            if (r1.x > 0.f) {
-              cat = 3;
-            } else {
-              rg = make_int2(__float_as_int(r1.z), __float_as_int(r1.w));
-              cat = 2;
-            }
-          } else {
-            cat = 4;
-          }
-        }
-      }
-    }
-    unsigned m = __ballot_sync(kAll, cat == 1);
-    if (m) {
-      if (nl + __popc(m) > kFastLC) flush_list();
-      if (cat == 1) {
-        const int pos = nl + __popc(m & lt);
-        sm.lpos[pos] = le;
-        sm.lkq[pos] = lk;
-      }
-      nl += __popc(m);
-    }
-    m = __ballot_sync(kAll, cat == 2);
-    if (m) {
-      if (nr + __popc(m) > kFastRC) flush_ranges();
-      if (cat == 2) sm.rng[nr + __popc(m & lt)] = rg;
-      nr += __popc(m);
-    }
-    // cells opened by all go on the warp's stack; when it is full they take
-    // the per-lane path instead (every lane then opens them itself)
-    m = __ballot_sync(kAll, cat == 3);
-    if (m) {
-      const int room = kFastGS - gsp;
-      const int rank = __popc(m & lt);
-      if (cat == 3) {
-        if (rank < room) sm.gst[gsp + rank] = c;
-        else cat = 4;
-      }
-      gsp += min(__popc(m), room);
-    }
-    m = __ballot_sync(kAll, cat == 4);
-    if (m) {
-      if (nm + __popc(m) > kFastMC) flush_mixed();
-      if (cat == 4) sm.mix[nm + __popc(m & lt)] = c;
-      nm += __popc(m);
-    }
-    __syncwarp();
-  };
-
-  if (n >= 2) {
-    classify(lane == 0 ? 0 : kNone);  // the root
-    while (gsp > 0) {
-      // up to 8 cells at a time, one child slot per lane
-      const int take = min(gsp, 8);
-      const int slot = lane >> 2;
-      int c = kNone;
-      if (slot < take) {
-        const int4 q = qchild[sm.gst[gsp - take + slot]];
-        const int h = lane & 3;
-        c = h == 0 ? q.x : h == 1 ? q.y : h == 2 ? q.z : q.w;
-      }
-      __syncwarp();
-      gsp -= take;
-      classify(c);
-    }
-    flush_list();
-    flush_ranges();
-    flush_mixed();
   }
   if (valid) {
     force[perm[s]] = make_float2(fx, fy);
@@ -1341,9 +1068,9 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist, int 
       bh_walk_kernel<kStack><<<wb, kWalkWarps * 32, 0, s>>>(
           n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err);
   } else {
-    const int wb = (n + kFastWarps * 32 - 1) / (kFastWarps * 32);
-#define FX_FAST_WALK(ST, CNT)                                                              \
-  bh_walk_fast_kernel<ST, CNT><<<wb, kFastWarps * 32, 0, s>>>(                             \
+    const int wb = (n + kWalkWarps * 32 - 1) / (kWalkWarps * 32);
+#define FX_FAST_WALK(ST, CNT)                                                             \
+  bh_walk_kernel<ST, true, CNT><<<wb, kWalkWarps * 32, 0, s>>>(                           \
       n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err, term_count)
     if (deep) {
       if (term_count) FX_FAST_WALK(kStackDeep, true);

@@ -248,6 +248,29 @@ extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
   return FX_OK;
 }
 
+namespace fx {
+// Re-creates a fresh context's two streams at the given priorities (lower
+// numbers run first; cudaDeviceGetStreamPriorityRange gives the range). The
+// context must have no work in flight.
+int ctx_set_priorities(fx_ctx *c, int primary, int side) {
+  FX_CHECK_CUDA(cudaSetDevice(c->device));
+  FX_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+  FX_CHECK_CUDA(cudaStreamSynchronize(c->stream2));
+  cudaStream_t a = nullptr, b = nullptr;
+  FX_CHECK_CUDA(cudaStreamCreateWithPriority(&a, cudaStreamNonBlocking, primary));
+  if (cudaStreamCreateWithPriority(&b, cudaStreamNonBlocking, side) != cudaSuccess) {
+    cudaStreamDestroy(a);
+    set_error("stream creation failed");
+    return FX_ECUDA;
+  }
+  cudaStreamDestroy(c->stream);
+  cudaStreamDestroy(c->stream2);
+  c->stream = a;
+  c->stream2 = b;
+  return FX_OK;
+}
+}  // namespace fx
+
 extern "C" int fx_ctx_destroy(fx_ctx *ctx) {
   if (!ctx) return FX_OK;
   cudaSetDevice(ctx->device);

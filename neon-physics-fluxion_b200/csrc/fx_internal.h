@@ -318,4 +318,6 @@ void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a);
 // at least `bytes`. Under a lock and never downwards, so host threads that
 // launch the kernel with different sizes cannot undo each other's setting.
 int raise_smem_limit(const void *func, int bytes);
+// Re-creates an idle context's streams at the given priorities (fx_core.cu).
+int ctx_set_priorities(fx_ctx *c, int primary, int side);
 }  // namespace fx

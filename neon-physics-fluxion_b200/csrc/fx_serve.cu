@@ -2,7 +2,10 @@
 // continuous batching of placement and ECO jobs over worker slots, resident
 // designs.
 //
-// Each slot is a host thread with its own fx_ctx (two non-blocking streams).
+// Each slot is a host thread with two fx_ctx (two non-blocking streams
+// each): ECO jobs run on the slot's foreground context, PLACE jobs on its
+// background one, whose streams have the lowest priority, so an ECO job's
+// short kernels pass the queued kernels of running placements.
 // A worker takes the first queued job that (a) fits in what the HBM budget
 // has left and (b) does not wait on a design that is busy or not yet placed,
 // runs it to completion on its context, and posts the result. Jobs therefore
@@ -271,8 +274,8 @@ Job *pick(fx_server *sv) {
 }
 
 void worker(fx_server *sv, int slot) {
-  fx_ctx *ctx = sv->ctxs[slot];
-  cudaSetDevice(ctx->device);
+  fx_ctx *fg = sv->ctxs[2 * slot], *bg = sv->ctxs[2 * slot + 1];
+  cudaSetDevice(fg->device);
   for (;;) {
     Job *j = nullptr;
     fx_design *eco_d = nullptr;
@@ -287,6 +290,7 @@ void worker(fx_server *sv, int slot) {
       }
     }
     j->res.start_s = sv->now();
+    fx_ctx *ctx = j->desc.kind == FX_JOB_PLACE ? bg : fg;
     int rc = FX_OK;
     fx_design *placed = nullptr;
     if (j->desc.kind == FX_JOB_PLACE) {
@@ -373,10 +377,21 @@ extern "C" int fx_serve_create(const fx_serve_cfg *cfg, fx_server **out) {
   if (!sv) return FX_ENOMEM;
   sv->cfg = *cfg;
   sv->t0 = std::chrono::steady_clock::now();
-  for (int i = 0; i < cfg->slots; ++i) {
+  int prio_low = 0, prio_high = 0;
+  cudaSetDevice(cfg->device);
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  for (int i = 0; i < 2 * cfg->slots; ++i) {
     fx_ctx *c = nullptr;
-    const int rc = fx_ctx_create(&c, cfg->device);
+    int rc = fx_ctx_create(&c, cfg->device);
+    // odd contexts serve PLACE jobs: both streams at the lowest priority; the
+    // foreground ones keep the highest for the Barnes-Hut chain and one step
+    // above the lowest for the density stream
+    if (rc == FX_OK)
+      rc = (i & 1) ? ctx_set_priorities(c, prio_low, prio_low)
+                   : ctx_set_priorities(c, prio_high, prio_low > prio_high ? prio_low - 1
+                                                                           : prio_low);
     if (rc != FX_OK) {
+      if (c) fx_ctx_destroy(c);
       for (fx_ctx *x : sv->ctxs) fx_ctx_destroy(x);
       delete sv;
       return rc;

@@ -32,7 +32,7 @@ def _check(fx, ctx, oracle, x, y, chip):
     assert np.array_equal(bx, bx2) and np.array_equal(by, by2)
     num = np.sqrt(((bx - o["fx"]) ** 2 + (by - o["fy"]) ** 2).sum())
     assert num / np.sqrt((o["fx"] ** 2 + o["fy"] ** 2).sum()) < 1e-5
-    # the group-decided walk on the same (deep or shallow) tree
+    # the hardware-rsqrt walk on the same (deep or shallow) tree
     assert np.array_equal(qkeys, keys) and np.array_equal(terms, o["interactions"])
     num = np.sqrt(((qx - o["fx"]) ** 2 + (qy - o["fy"]) ** 2).sum())
     assert num / np.sqrt((o["fx"] ** 2 + o["fy"] ** 2).sum()) < 1e-5

@@ -10,7 +10,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 F32_01 = float(np.float32(0.1))  # the device's f32 min_dist, exactly
-FX_BH_FAST = 0  # fx_iter_cfg.bh_walk / fx_stage_barnes_hut_walk: group-decided walk
+FX_BH_FAST = 0  # fx_iter_cfg.bh_walk / fx_stage_barnes_hut_walk: hardware rsqrt
 FX_BH_EXACT = 1  # per-point walk, bit-identical to the oracle's f32 order
 
 
@@ -119,8 +119,8 @@ def _bh_check(d, x, y, oracle, k=0.5, theta=0.5):
     assert np.array_equal(perm, o["perm"])  # stable sort order exact
     assert np.array_equal(bx, o["fx32"]) and np.array_equal(by, o["fy32"])  # bit-exact
     assert rel_l2(bx, by, o["fx"], o["fy"]) < 1e-5  # FP64, same interaction list
-    # the group-decided walk: the same tree, the same interaction count per
-    # point, forces within f32 rounding (hardware rsqrt, any term order)
+    # the hardware-rsqrt walk: the same tree, the same interaction count per
+    # point, forces within f32 rounding
     qx, qy, qkeys, qperm, qroot, terms = d.barnes_hut(k, theta, 0.1, walk=FX_BH_FAST,
                                                       terms=True)
     assert np.array_equal(qkeys, keys) and np.array_equal(qperm, perm)
