@@ -467,10 +467,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     FX_CHECK_CUDA(cudaMemcpyAsync(&err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
   if (copied_out) FX_CHECK_CUDA(cudaStreamSynchronize(s2));
-  if (err) {
-    set_error("Barnes-Hut walk stack overflow");
-    return FX_EINVAL;
-  }
+  FX_TRY(bh_error(err));
   if (use_dens && c.dct_precision != FX_DCT_SIMT) {
     unsigned int tc_err = 0;
     FX_TRY(gemm_tc_error(ctx, &tc_err, s));

@@ -394,16 +394,204 @@ int radix_sort_pairs(uint32_t *k[2], int32_t *v[2], int n, int passes,
 
 int radix_sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
 
-// ---- sorted positions --------------------------------------------------------------
-__global__ void bh_gather_kernel(const float *__restrict__ x,
-                                 const float *__restrict__ y,
-                                 const int32_t *__restrict__ perm, int n,
-                                 float2 *__restrict__ spos) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += gridDim.x * blockDim.x) {
-    const int g = perm[i];
-    spos[i] = make_float2(x[g], y[g]);
+// ---- one-sweep LSD radix sort (the Barnes-Hut keys) ----------------------------
+// The same stable sort in 1 + passes launches instead of 3 per pass: one
+// kernel counts every pass's digits at once; then each pass is one kernel in
+// which a block takes the next tile (an atomic ticket, so tiles start in
+// order), ranks its keys stably as radix_scatter_kernel does, publishes its
+// per-digit counts and finds the counts of all earlier tiles by a look-back
+// over their published words (decoupled look-back). A block waits only on
+// tiles whose blocks have started and publish their own counts before they
+// wait, so every wait ends; each is still bounded, and an expired wait sets
+// bit 4 of the error word (the host turns it into FX_ETIMEOUT).
+constexpr uint32_t kOsAgg = 1u << 30, kOsInc = 2u << 30, kOsVal = (1u << 30) - 1u;
+constexpr uint32_t kOsSpin = 1u << 22;
+
+__global__ void __launch_bounds__(kSortThreads)
+os_hist_kernel(const uint32_t *__restrict__ keys, int n, int passes,
+               uint32_t *__restrict__ hist) {
+  __shared__ uint32_t h[4][256];
+  for (int i = threadIdx.x; i < 4 * 256; i += kSortThreads) (&h[0][0])[i] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * kSortThreads + threadIdx.x; i < n; i += gridDim.x * kSortThreads) {
+    const uint32_t k = keys[i];
+    for (int q = 0; q < passes; ++q) atomicAdd(&h[q][(k >> (8 * q)) & 255u], 1u);
   }
+  __syncthreads();
+  for (int q = 0; q < passes; ++q) {
+    const uint32_t c = h[q][threadIdx.x];
+    if (c) atomicAdd(hist + q * 256 + threadIdx.x, c);
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin,
+               uint32_t *__restrict__ kout, int32_t *__restrict__ iout, int n, int shift,
+               const uint32_t *__restrict__ hist, uint32_t *__restrict__ status,
+               unsigned int *__restrict__ ticket, unsigned int *__restrict__ err,
+               const float *__restrict__ px, const float *__restrict__ py,
+               float2 *__restrict__ spos) {
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ uint32_t cnt[kWarps][256];
+  __shared__ uint32_t tstart[256], gbase[256], ws[kWarps];
+  __shared__ int tile_s;
+  __shared__ uint32_t sk[kSortTile];
+  __shared__ int32_t sv[kSortTile];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  if (t == 0) tile_s = (int)atomicAdd(ticket, 1u);
+  for (int i = t; i < kWarps * 256; i += kSortThreads) (&cnt[0][0])[i] = 0;
+  __syncthreads();
+  const int tile = tile_s;
+  // base of every digit: exclusive scan of this pass's digit counts
+  uint32_t dbase;
+  {
+    const uint32_t c = hist[t];
+    uint32_t v = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
+    }
+    if (lane == 31) ws[w] = v;
+    __syncthreads();
+    dbase = v - c;
+    for (int q = 0; q < w; ++q) dbase += ws[q];
+    __syncthreads();
+  }
+  // stable ranks within the tile: per warp by __match_any_sync, then warps
+  // in order (as radix_scatter_kernel)
+  const int base = tile * kSortTile + w * (32 * kSortItems);
+  const unsigned lt_mask = (1u << lane) - 1u;
+  uint32_t k[kSortItems];
+  int32_t v[kSortItems];
+  uint32_t rank[kSortItems];
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int i = base + r * 32 + lane;
+    const bool valid = i < n;
+    k[r] = valid ? kin[i] : 0u;
+    v[r] = valid ? iin[i] : 0;
+    const uint32_t dg = valid ? ((k[r] >> shift) & 255u) : 256u;
+    const unsigned peers = __match_any_sync(0xffffffffu, dg);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t old = valid ? cnt[w][dg] : 0u;
+    __syncwarp();
+    if (valid && lane == leader) cnt[w][dg] = old + __popc(peers);
+    __syncwarp();
+    rank[r] = old + __popc(peers & lt_mask);
+  }
+  __syncthreads();
+  // thread t = digit t: warp offsets within the digit, the digit's count in
+  // this tile, and its start within the tile
+  uint32_t local;
+  {
+    uint32_t run = 0;
+#pragma unroll
+    for (int ww = 0; ww < kWarps; ++ww) {
+      const uint32_t c = cnt[ww][t];
+      cnt[ww][t] = run;
+      run += c;
+    }
+    local = run;
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    uint32_t st = x - run;
+    for (int q = 0; q < w; ++q) st += ws[q];
+    tstart[t] = st;
+  }
+  // decoupled look-back for digit t
+  {
+    volatile uint32_t *stv = status;
+    uint32_t *my = status + (size_t)tile * 256 + t;
+    if (tile == 0) {
+      atomicExch(my, kOsInc | local);
+      gbase[t] = dbase - tstart[t];
+    } else {
+      atomicExch(my, kOsAgg | local);
+      uint32_t prefix = 0;
+      for (int p = tile - 1; p >= 0;) {
+        uint32_t word = stv[(size_t)p * 256 + t];
+        uint32_t spin = 0;
+        while ((word & ~kOsVal) == 0u && spin < kOsSpin) {
+          ++spin;
+          word = stv[(size_t)p * 256 + t];
+        }
+        if ((word & ~kOsVal) == 0u) {  // expired: record it and stop
+          atomicOr(err, 4u);
+          break;
+        }
+        prefix += word & kOsVal;
+        if ((word & ~kOsVal) == kOsInc) break;
+        --p;
+      }
+      __threadfence();
+      atomicExch(my, kOsInc | (prefix + local));
+      gbase[t] = dbase + prefix - tstart[t];
+    }
+  }
+  __syncthreads();
+  // stage the tile in sorted order, then write it out coalesced
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int i = base + r * 32 + lane;
+    if (i < n) {
+      const uint32_t dg = (k[r] >> shift) & 255u;
+      const uint32_t j = tstart[dg] + cnt[w][dg] + rank[r];
+      sk[j] = k[r];
+      sv[j] = v[r];
+    }
+  }
+  __syncthreads();
+  const int m = min(kSortTile, n - tile * kSortTile);
+  for (int j = t; j < m; j += kSortThreads) {
+    const uint32_t key = sk[j];
+    const uint32_t pos = gbase[(key >> shift) & 255u] + (uint32_t)j;
+    const int32_t g = sv[j];
+    kout[pos] = key;
+    iout[pos] = g;
+    if (spos) spos[pos] = make_float2(px[g], py[g]);
+  }
+}
+
+// Stable LSD sort of (key, value) pairs on the low 8*passes (<= 4) key bits,
+// in 1 + passes launches. With spos, the last pass also writes
+// spos[i] = (px[v], py[v]) for the sorted values v. Pairs start in (k[0], v[0]); the result is in
+// (k[passes & 1], v[passes & 1]). Workspace `ws`: os_sort_words(n, passes)
+// words, cleared here.
+size_t os_sort_words(int n, int passes) {
+  return (size_t)passes * 256 + (size_t)passes * radix_sort_tiles(n) * 256 + 4;
+}
+
+int radix_sort_onesweep(uint32_t *k[2], int32_t *v[2], int n, int passes, uint32_t *ws,
+                        unsigned int *err, cudaStream_t s, const float *px,
+                        const float *py, float2 *spos) {
+  if (n <= 0) return FX_OK;
+  if (passes > 4 || n >= (int)kOsVal) {
+    set_error("radix_sort_onesweep: %d keys / %d passes out of range", n, passes);
+    return FX_EINVAL;
+  }
+  const int T = radix_sort_tiles(n);
+  uint32_t *hist = ws, *status = ws + passes * 256,
+           *ticket = status + (size_t)passes * T * 256;
+  FX_CHECK_CUDA(cudaMemsetAsync(ws, 0, os_sort_words(n, passes) * 4, s));
+  const int hb = std::min(T, 2 * 148);
+  os_hist_kernel<<<hb, kSortThreads, 0, s>>>(k[0], n, passes, hist);
+  for (int pass = 0; pass < passes; ++pass) {
+    const int src = pass & 1, dst = src ^ 1;
+    const bool last = pass == passes - 1;
+    os_pass_kernel<<<T, kSortThreads, 0, s>>>(k[src], v[src], k[dst], v[dst], n, 8 * pass,
+                                              hist + 256 * pass,
+                                              status + (size_t)pass * T * 256, ticket + pass,
+                                              err, px, py, last ? spos : nullptr);
+  }
+  FX_CHECK_LAUNCH();
+  return FX_OK;
 }
 
 // ---- radix tree (Karras 2012) -----------------------------------------------
@@ -612,14 +800,22 @@ __device__ __forceinline__ double fixed_to_double(__int128 v) {
 //   r0 = {cx_hi, cy_hi, cx_lo, cy_lo}  centre of mass as an f32 hi/lo pair
 //   r1 = {count (negative: bucket), size^2 (negative: no quad level),
 //         first, last (as int bits)}
+__device__ __forceinline__ void bh_qchild(int i, const int32_t *__restrict__ child,
+                                          const int32_t *__restrict__ dnode, int kb,
+                                          int4 *__restrict__ qchild);
+
+// Also writes the node's quad children (bh_qchild below).
 __global__ void bh_node_kernel(int n, const int32_t *__restrict__ range,
                                const int32_t *__restrict__ dnode,
                                const int32_t *__restrict__ dparent,
                                const ulonglong4 *__restrict__ prefix,
                                const float *__restrict__ root, int deep_ok,
-                               float4 *__restrict__ node) {
+                               float4 *__restrict__ node,
+                               const int32_t *__restrict__ child,
+                               int4 *__restrict__ qchild) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
+  bh_qchild(i, child, dnode, (deep_ok && root[3] > 0.f) ? kDeepBits : kKeyBits, qchild);
   const bool deep = deep_ok && root[3] > 0.f;
   const int kb = deep ? kDeepBits : kKeyBits;  // prefix length of a bucket
   const int f = range[2 * i], l = range[2 * i + 1];
@@ -661,13 +857,9 @@ __global__ void bh_node_kernel(int n, const int32_t *__restrict__ range,
 // node lists up to four children, in key order. kNone marks empty slots.
 constexpr int kNone = INT_MIN;
 
-__global__ void bh_qchild_kernel(int n, const int32_t *__restrict__ child,
-                                 const int32_t *__restrict__ dnode,
-                                 const float *__restrict__ root, int deep_ok,
-                                 int4 *__restrict__ qchild) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n - 1) return;
-  const int kb = (deep_ok && root[3] > 0.f) ? kDeepBits : kKeyBits;
+__device__ __forceinline__ void bh_qchild(int i, const int32_t *__restrict__ child,
+                                          const int32_t *__restrict__ dnode, int kb,
+                                          int4 *__restrict__ qchild) {
   int out[4] = {kNone, kNone, kNone, kNone};
   int k = 0;
   const int lv = dnode[i] >> 1;
@@ -716,36 +908,43 @@ __device__ __forceinline__ float bh_rsqrt(float x) {
 // The law k*Q/d^2 along (dx, dy)/d with d = max(|r|, min_dist), in f32:
 // inv = rsqrt(max(r2, md^2)), f = ((kQ * inv) * inv) * inv,
 // F = fma(f, r, F); r2 = fma(dx, dx, dy * dy).
+template <bool Fast>
 __device__ __forceinline__ void bh_term(float dx, float dy, float r2c, float kq,
                                         float &fx, float &fy) {
-  const float inv = bh_rsqrt(r2c);
+  const float inv = Fast ? rsqrtf(r2c) : bh_rsqrt(r2c);
   const float f = __fmul_rn(__fmul_rn(__fmul_rn(kq, inv), inv), inv);
   fx = __fmaf_rn(f, dx, fx);
   fy = __fmaf_rn(f, dy, fy);
 }
 
+template <bool Fast>
 __device__ __forceinline__ void bh_direct(float px, float py, float2 q,
                                           float kq, float md2, float &fx,
                                           float &fy) {
   const float dx = __fsub_rn(px, q.x), dy = __fsub_rn(py, q.y);
   const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-  bh_term(dx, dy, fmaxf(r2, md2), kq, fx, fy);
+  bh_term<Fast>(dx, dy, fmaxf(r2, md2), kq, fx, fy);
 }
 
 // Applies the opening rule of child c (an internal node when `cell`) to the
-// lane's point when `in`; adds accepted-cell, single-point and bucket terms.
+// lane's point when `in`; adds accepted-cell, single-point and bucket terms
+// (Fast: with the hardware rsqrt; Count: counting them in `terms`).
 // Called by all 32 lanes together (the ballot); returns the lanes that open
 // c as a cell to descend into.
+template <bool Fast, bool Count>
 __device__ __forceinline__ unsigned bh_eval(int c, bool in, bool cell, int s,
                                             float2 p, float k, float th2,
                                             float md2,
                                             const float4 *__restrict__ node,
                                             const float2 *__restrict__ spos,
-                                            float &fx, float &fy) {
+                                            float &fx, float &fy, int &terms) {
   bool op = false;
   if (in) {
     if (!cell) {  // single point ~c
-      if (~c != s) bh_direct(p.x, p.y, spos[~c], k, md2, fx, fy);
+      if (~c != s) {
+        bh_direct<Fast>(p.x, p.y, spos[~c], k, md2, fx, fy);
+        if (Count) ++terms;
+      }
     } else {
       const float4 r0 = node[2 * c], r1 = node[2 * c + 1];
       const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
@@ -754,13 +953,17 @@ __device__ __forceinline__ unsigned bh_eval(int c, bool in, bool cell, int s,
       const float r2c = fmaxf(r2, md2);
       // size^2 < 0 (a node standing for no quad level) is always opened
       if (r1.y >= 0.f && r1.y < __fmul_rn(th2, r2c)) {
-        bh_term(dx, dy, r2c, __fmul_rn(k, fabsf(r1.x)), fx, fy);
+        bh_term<Fast>(dx, dy, r2c, __fmul_rn(k, fabsf(r1.x)), fx, fy);
+        if (Count) ++terms;
       } else if (r1.x > 0.f) {
         op = true;
       } else {  // bucket: point by point
         const int b = __float_as_int(r1.z), e = __float_as_int(r1.w);
         for (int t = b; t <= e; ++t)
-          if (t != s) bh_direct(p.x, p.y, spos[t], k, md2, fx, fy);
+          if (t != s) {
+            bh_direct<Fast>(p.x, p.y, spos[t], k, md2, fx, fy);
+            if (Count) ++terms;
+          }
       }
     }
   }
@@ -770,63 +973,11 @@ __device__ __forceinline__ unsigned bh_eval(int c, bool in, bool cell, int s,
 constexpr int kWalkGroup = 8;                    // lanes per group
 constexpr int kWalkGroups = 32 / kWalkGroup;     // groups per warp
 
-// ---- FX_BH_FAST: the same walk with the hardware rsqrt -----------------------------
-// bh_walk_kernel<Stack, true> visits the same cells in the same order as the
-// exact walk, so every point keeps the reference rule's interaction list and
-// the terms are added in the same order; only the inverse square root is the
-// hardware rsqrt (a few ulp), and a single-point child is evaluated by the
-// cell code as a record of count 1 that every other point accepts (its own
-// lane's term is f * 0 = 0), so point and cell children share one
-// instruction stream. Forces agree with the exact walk to f32 rounding.
-template <bool Count>
-__device__ __forceinline__ unsigned fast_eval(int c, bool in, bool cell, int s, float2 p,
-                                              float k, float th2, float md2,
-                                              const float4 *__restrict__ node,
-                                              const float2 *__restrict__ spos, float &fx,
-                                              float &fy, int &terms) {
-  bool op = false;
-  if (in) {
-    float4 r0, r1;
-    if (cell) {
-      r0 = node[2 * c];
-      r1 = node[2 * c + 1];
-    } else {
-      const float2 q = spos[~c];
-      r0 = make_float4(q.x, q.y, 0.f, 0.f);
-      r1 = make_float4(1.f, 0.f, 0.f, 0.f);
-    }
-    const float dx = __fsub_rn(__fsub_rn(p.x, r0.x), r0.z);
-    const float dy = __fsub_rn(__fsub_rn(p.y, r0.y), r0.w);
-    const float r2c = fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), md2);
-    if (!cell || (r1.y >= 0.f && r1.y < __fmul_rn(th2, r2c))) {
-      const float inv = rsqrtf(r2c);
-      const float f = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(k, fabsf(r1.x)), inv), inv),
-                                inv);
-      fx = __fmaf_rn(f, dx, fx);
-      fy = __fmaf_rn(f, dy, fy);
-      if (Count) terms += (cell || ~c != s) ? 1 : 0;
-    } else if (r1.x > 0.f) {
-      op = true;
-    } else {  // bucket: point by point
-      const int b = __float_as_int(r1.z), e = __float_as_int(r1.w);
-      for (int t = b; t <= e; ++t) {
-        const float2 q = spos[t];
-        const float ex = __fsub_rn(p.x, q.x), ey = __fsub_rn(p.y, q.y);
-        const float iv = rsqrtf(fmaxf(__fmaf_rn(ex, ex, __fmul_rn(ey, ey)), md2));
-        const float g = t == s ? 0.f : __fmul_rn(__fmul_rn(__fmul_rn(k, iv), iv), iv);
-        fx = __fmaf_rn(g, ex, fx);
-        fy = __fmaf_rn(g, ey, fy);
-        if (Count) terms += t == s ? 0 : 1;
-      }
-    }
-  }
-  return __ballot_sync(0xffffffffu, op);
-}
-
-// Fast: FX_BH_FAST (fast_eval instead of bh_eval); Count: also each point's
+// Fast: FX_BH_FAST, the same cells and term order with the hardware rsqrt
+// (a few ulp) instead of the reproducible one; Count: also each point's
 // number of terms.
 template <int Stack, bool Fast = false, bool Count = false>
-__global__ void __launch_bounds__(kWalkWarps * 32)
+__global__ void __launch_bounds__(kWalkWarps * 32, 8)
 bh_walk_kernel(int n, const float2 *__restrict__ spos,
                const int32_t *__restrict__ perm,
                const int4 *__restrict__ qchild,
@@ -850,8 +1001,7 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
   int sp = 0;  // this group's stack depth (uniform in the group)
   int terms = 0;
   auto eval = [&](int c, bool in, bool cell) -> unsigned {
-    if (Fast) return fast_eval<Count>(c, in, cell, s, p, k, th2, md2, node, spos, fx, fy, terms);
-    return bh_eval(c, in, cell, s, p, k, th2, md2, node, spos, fx, fy);
+    return bh_eval<Fast, Count>(c, in, cell, s, p, k, th2, md2, node, spos, fx, fy, terms);
   };
   if (n >= 2) {
     const unsigned open = eval(0, valid, true) & gmask;
@@ -933,6 +1083,7 @@ static int bh_alloc(fx_design *d) {
   FX_TRY(b.root.alloc(4));
   FX_TRY(b.bbox.alloc(8));
   FX_TRY(b.force.alloc(n));
+  FX_TRY(b.os_ws.alloc(os_sort_words(n, 4)));
   b.n = n;
   return FX_OK;
 }
@@ -958,6 +1109,19 @@ static bool bh_maybe_deep(const fx_design *d, float th2, float md2) {
   const double rb = ((double)std::max(d->chip_w, d->chip_h) + 2.0) * (1.0 + 1e-6);
   const double s15 = rb / 32768.0;
   return s15 * s15 >= (double)th2 * (double)md2 * (1.0 - 1e-6);
+}
+
+// The walk's and the sort's error word (bh.bbox[4]) as a status.
+int bh_error(unsigned int err) {
+  if (err & 4u) {
+    set_error("Barnes-Hut key sort: a bounded look-back wait expired");
+    return FX_ETIMEOUT;
+  }
+  if (err) {
+    set_error("Barnes-Hut walk stack overflow");
+    return FX_EINVAL;
+  }
+  return FX_OK;
 }
 
 // Bounding box of the given positions into bh.bbox (re-armed first).
@@ -1021,17 +1185,13 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist, int 
     FX_CHECK_LAUNCH();
     launches += 9 + 2;
   }
-  for (int pass = 0; pass < 4; ++pass) {
-    const int src = pass & 1, dst = src ^ 1;
-    radix_hist_kernel<<<T, kSortThreads, 0, s>>>(b.keys[src].p, n, 8 * pass,
-                                                 b.tile_hist.p, T);
-    radix_scan_kernel<<<256, 256, 0, s>>>(b.tile_hist.p, b.tile_scan.p,
-                                          b.digit_total.p, T);
-    radix_scatter_kernel<<<T, kSortThreads, 0, s>>>(
-        b.keys[src].p, b.idx[src].p, b.keys[dst].p, b.idx[dst].p, n, 8 * pass,
-        b.tile_scan.p, b.digit_total.p, T);
+  {
+    uint32_t *kk[2] = {b.keys[0].p, b.keys[1].p};
+    int32_t *vv[2] = {b.idx[0].p, b.idx[1].p};
+    // result in buffer 0; the last pass also gathers the sorted positions
+    FX_TRY(radix_sort_onesweep(kk, vv, n, 4, b.os_ws.p, err, s, x, y, b.spos.p));
   }
-  launches += 12;
+  launches += 5;
   if (deep) {
     bh_deep_slo_kernel<<<gb, 256, 0, s>>>(gate, n, b.klo.p, b.idx[0].p, b.slo.p);
     ++launches;
@@ -1039,8 +1199,6 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist, int 
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_SORT, s, ev);
   timer_begin(ctx, FX_STAGE_BH_TREE, s, &ev);
-  bh_gather_kernel<<<gb, 256, 0, s>>>(x, y, b.idx[0].p, n, b.spos.p);
-  ++launches;
   if (n >= 2) {
     const int tb = (n - 1 + 255) / 256;
     bh_tree_kernel<<<tb, 256, 0, s>>>(b.keys[0].p, deep ? b.slo.p : nullptr, b.root.p, n,
@@ -1051,10 +1209,9 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist, int 
     fix_top_kernel<<<1, kFixThreads, 0, s>>>(b.tile_fix.p, tiles);
     fix_prefix_kernel<<<tiles, kFixThreads, 0, s>>>(b.spos.p, n, b.tile_fix.p, b.prefix.p);
     bh_node_kernel<<<tb, 256, 0, s>>>(n, b.range.p, b.dnode.p, b.dparent.p,
-                                      b.prefix.p, b.root.p, deep ? 1 : 0, b.node.p);
-    bh_qchild_kernel<<<tb, 256, 0, s>>>(n, b.child.p, b.dnode.p, b.root.p, deep ? 1 : 0,
-                                        b.qchild.p);
-    launches += 6;
+                                      b.prefix.p, b.root.p, deep ? 1 : 0, b.node.p, b.child.p,
+                                      b.qchild.p);
+    launches += 5;
   }
   FX_CHECK_LAUNCH();
   timer_end(ctx, FX_STAGE_BH_TREE, s, ev);
@@ -1122,10 +1279,7 @@ extern "C" int fx_stage_barnes_hut_walk(fx_ctx *ctx, fx_design *d, float k, floa
     FX_CHECK_CUDA(cudaMemcpyAsync(out_root, d->bh.root.p, 12, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaMemcpyAsync(&err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
-  if (err) {
-    set_error("Barnes-Hut walk stack overflow");
-    return FX_EINVAL;
-  }
+  FX_TRY(bh_error(err));
   for (size_t i = 0; i < n; ++i) {
     if (out_fx) out_fx[i] = f[i].x;
     if (out_fy) out_fy[i] = f[i].y;

@@ -146,8 +146,10 @@ struct BHWork {
   DevBuf<uint32_t> slo;         // sub-cell key in sorted order
   DevBuf<unsigned int> bbox;    // [0..3] ordered-int box, [4] error flag
   DevBuf<float2> force;         // per gate (original order)
+  DevBuf<uint32_t> os_ws;       // one-sweep key sort: digit counts, look-back words
   template <class F>
   void for_each(F &&f) {
+    f(os_ws);
     for (auto &b : keys) f(b);
     for (auto &b : idx) f(b);
     f(tile_hist); f(tile_scan); f(digit_total); f(spos); f(child); f(range);
@@ -242,6 +244,10 @@ struct fx_ctx {
   cudaStream_t stream2 = nullptr;  // side stream (density || Barnes-Hut)
   cudaEvent_t fork = nullptr, join = nullptr;
   int num_sms = 0;
+  // SMs the persistent leaf kernels spread over (0: all); a server's
+  // placement contexts leave the rest to other jobs' kernels, whose blocks
+  // could not start while a persistent grid holds every SM
+  int persistent_sms = 0;
   // Error word of this context's tensor-core GEMMs (bit 1: a bounded wait
   // expired); zeroed at creation, cleared again after it is reported.
   unsigned int *tc_err = nullptr;
@@ -306,6 +312,15 @@ int radix_sort_pairs(uint32_t *k[2], int32_t *v[2], int n, int passes,
                      uint32_t *tile_hist, uint32_t *tile_scan, uint32_t *digit_total,
                      cudaStream_t s);
 int radix_sort_tiles(int n);
+// The same sort in 1 + passes launches (decoupled look-back; fx_bh.cu): ws
+// holds os_sort_words(n, passes) words; an expired look-back sets bit 4 of
+// *err.
+size_t os_sort_words(int n, int passes);
+int radix_sort_onesweep(uint32_t *k[2], int32_t *v[2], int n, int passes, uint32_t *ws,
+                        unsigned int *err, cudaStream_t s, const float *px = nullptr,
+                        const float *py = nullptr, float2 *spos = nullptr);
+// The Barnes-Hut error word (walk stack overflow, sort look-back) as a status.
+int bh_error(unsigned int err);
 // The reference's f32 Iterator::sum folds of the power iteration, one warp
 // per cluster [beg[c], end[c]) (fx_partition.cu): with `deflate`, the mean
 // of x is subtracted in place; nrm[c] = |x| when > 1e-10, else 0.

@@ -510,7 +510,7 @@ static int launch_pairs(fx_ctx *ctx, const LeafBatch &b, const PairPlan &plan, c
   FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, leaf_pairs_kernel<T, Fast>, T, smem));
   if (per_sm < 1) per_sm = 1;
-  int grid = ctx->num_sms * per_sm;
+  int grid = (ctx->persistent_sms > 0 ? ctx->persistent_sms : ctx->num_sms) * per_sm;
   if (grid > b.n_leaves) grid = b.n_leaves;
   if (grid < 1) grid = 1;
   FX_CHECK_CUDA(cudaMemsetAsync(b.counter, 0, 8, s));
@@ -644,7 +644,7 @@ static int launch_leaf(fx_ctx *ctx, const LeafBatch &b, bool per_cluster,
   FX_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, leaf_batch_kernel<T, Fast>, 256, smem));
   if (per_sm < 1) per_sm = 1;
-  int grid = ctx->num_sms * per_sm;
+  int grid = (ctx->persistent_sms > 0 ? ctx->persistent_sms : ctx->num_sms) * per_sm;
   const int need = (b.n_leaves + kGroups - 1) / kGroups;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;

@@ -4,8 +4,9 @@
 //
 // Each slot is a host thread with two fx_ctx (two non-blocking streams
 // each): ECO jobs run on the slot's foreground context, PLACE jobs on its
-// background one, whose streams have the lowest priority, so an ECO job's
-// short kernels pass the queued kernels of running placements.
+// background one, whose streams have the lowest priority and whose
+// persistent leaf kernels spread over half the SMs, so an ECO job's short
+// kernels pass the queued kernels of running placements.
 // A worker takes the first queued job that (a) fits in what the HBM budget
 // has left and (b) does not wait on a design that is busy or not yet placed,
 // runs it to completion on its context, and posts the result. Jobs therefore
@@ -390,6 +391,8 @@ extern "C" int fx_serve_create(const fx_serve_cfg *cfg, fx_server **out) {
       rc = (i & 1) ? ctx_set_priorities(c, prio_low, prio_low)
                    : ctx_set_priorities(c, prio_high, prio_low > prio_high ? prio_low - 1
                                                                            : prio_low);
+    // and their persistent leaf kernels take half the SMs
+    if (rc == FX_OK && (i & 1)) c->persistent_sms = std::max(1, c->num_sms / 2);
     if (rc != FX_OK) {
       if (c) fx_ctx_destroy(c);
       for (fx_ctx *x : sv->ctxs) fx_ctx_destroy(x);
