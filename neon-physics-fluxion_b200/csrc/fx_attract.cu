@@ -340,16 +340,19 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   bool copied_out = false;  // positions already on their way to x, y
   // One iteration; `last` adds the potential (energy statistic).
   auto step = [&](bool last) -> int {
+    // The Barnes-Hut chain (the critical path) is issued first, so the GPU
+    // starts it while the host still issues the density solve; the density
+    // forks from the same point of the primary stream and runs beside it.
+    if (use_dens) FX_CHECK_CUDA(cudaEventRecord(ctx->fork, s));
+    if (use_bh) FX_TRY(bh_run(ctx, d, c.repel_weight, c.theta, c.min_dist, c.bh_walk, s));
     if (use_dens) {
-      FX_CHECK_CUDA(cudaEventRecord(ctx->fork, s));
       FX_CHECK_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
       // the potential only feeds the energy statistic of the last step
       FX_TRY(density_run(ctx, d, G, c.target_density, c.density_weight,
                          c.dct_precision, last, s2));
       FX_CHECK_CUDA(cudaEventRecord(ctx->join, s2));
+      FX_CHECK_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
     }
-    if (use_bh) FX_TRY(bh_run(ctx, d, c.repel_weight, c.theta, c.min_dist, c.bh_walk, s));
-    if (use_dens) FX_CHECK_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
     const int nxt = d->cur ^ 1;
     StepArgs a{};
     a.adj_ptr = d->adj_ptr.p;
@@ -453,19 +456,24 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   }
   fx_iter_stats st{};
   st.iterations = iters;
-  double res[2] = {0, 0};
-  unsigned int err = 0;
+  // the statistics come back through the context's pinned buffer (truly
+  // asynchronous copies; pageable ones would stage through the driver)
+  IterReadback &rb = *ctx->readback;
+  rb = IterReadback{};
   if (use_cong && iters > 0) {
-    FX_CHECK_CUDA(cudaMemcpyAsync(res, d->cong.result.p, 16, cudaMemcpyDeviceToHost, s));
-    FX_CHECK_CUDA(cudaMemcpyAsync(&st.max_overflow, d->cong.result_max.p, 4,
+    FX_CHECK_CUDA(cudaMemcpyAsync(rb.res, d->cong.result.p, 16, cudaMemcpyDeviceToHost, s));
+    FX_CHECK_CUDA(cudaMemcpyAsync(&rb.max_overflow, d->cong.result_max.p, 4,
                                   cudaMemcpyDeviceToHost, s));
   }
   if (use_dens && iters > 0)
-    FX_CHECK_CUDA(cudaMemcpyAsync(&st.density_energy, d->step.energy.p, 8,
-                                  cudaMemcpyDeviceToHost, s));
+    FX_CHECK_CUDA(cudaMemcpyAsync(&rb.energy, d->step.energy.p, 8, cudaMemcpyDeviceToHost, s));
   if (use_bh && iters > 0)
-    FX_CHECK_CUDA(cudaMemcpyAsync(&err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
+    FX_CHECK_CUDA(cudaMemcpyAsync(&rb.err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  const double res[2] = {rb.res[0], rb.res[1]};
+  const unsigned int err = rb.err;
+  st.max_overflow = rb.max_overflow;
+  st.density_energy = rb.energy;
   if (copied_out) FX_CHECK_CUDA(cudaStreamSynchronize(s2));
   FX_TRY(bh_error(err));
   if (use_dens && c.dct_precision != FX_DCT_SIMT) {

@@ -406,6 +406,7 @@ int radix_sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
 // bit 4 of the error word (the host turns it into FX_ETIMEOUT).
 constexpr uint32_t kOsAgg = 1u << 30, kOsInc = 2u << 30, kOsVal = (1u << 30) - 1u;
 constexpr uint32_t kOsSpin = 1u << 22;
+constexpr int kOsWin = 16;  // earlier tiles read per look-back step
 
 __global__ void __launch_bounds__(kSortThreads)
 os_hist_kernel(const uint32_t *__restrict__ keys, int n, int passes,
@@ -514,21 +515,37 @@ os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin
       gbase[t] = dbase - tstart[t];
     } else {
       atomicExch(my, kOsAgg | local);
+      // The words of the kOsWin nearest earlier tiles are loaded together
+      // (independent loads, one round trip) and added from the nearest on,
+      // up to the first inclusive one; a tile that has not published yet is
+      // waited for (bounded), then the window restarts from it.
       uint32_t prefix = 0;
+      uint32_t spin = 0;
       for (int p = tile - 1; p >= 0;) {
-        uint32_t word = stv[(size_t)p * 256 + t];
-        uint32_t spin = 0;
-        while ((word & ~kOsVal) == 0u && spin < kOsSpin) {
-          ++spin;
-          word = stv[(size_t)p * 256 + t];
+        uint32_t wv[kOsWin];
+#pragma unroll
+        for (int q = 0; q < kOsWin; ++q)
+          wv[q] = p - q >= 0 ? (uint32_t)stv[(size_t)(p - q) * 256 + t] : (uint32_t)(2u << 30);  // before tile 0: inclusive 0
+        int q = 0;
+        bool done = false;
+#pragma unroll
+        for (int r = 0; r < kOsWin; ++r) {
+          if (done || q < r) continue;  // stopped at an earlier entry
+          const uint32_t flag = wv[r] & ~kOsVal;
+          if (flag == 0u) break;         // not published yet: q == r
+          prefix += wv[r] & kOsVal;
+          q = r + 1;
+          if (flag == kOsInc) done = true;
         }
-        if ((word & ~kOsVal) == 0u) {  // expired: record it and stop
-          atomicOr(err, 4u);
-          break;
+        if (done) break;
+        p -= q;
+        if (q < kOsWin && p >= 0) {  // wait for tile p to publish
+          while ((stv[(size_t)p * 256 + t] & ~kOsVal) == 0u && spin < kOsSpin) ++spin;
+          if (spin >= kOsSpin) {  // expired: record it and stop
+            atomicOr(err, 4u);
+            break;
+          }
         }
-        prefix += word & kOsVal;
-        if ((word & ~kOsVal) == kOsInc) break;
-        --p;
       }
       __threadfence();
       atomicExch(my, kOsInc | (prefix + local));
@@ -1128,8 +1145,10 @@ int bh_error(unsigned int err) {
 int bh_bbox(fx_ctx *ctx, fx_design *d, const float *x, const float *y,
             cudaStream_t s) {
   FX_TRY(bh_alloc(d));
-  const unsigned int init[5] = {0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-  FX_CHECK_CUDA(cudaMemcpyAsync(d->bh.bbox.p, init, 20, cudaMemcpyHostToDevice, s));
+  // {0xffffffff, 0xffffffff, 0, 0, 0}: min/max seeds of the ordered box and
+  // a clear error word (memsets: no host buffer to stage)
+  FX_CHECK_CUDA(cudaMemsetAsync(d->bh.bbox.p, 0xff, 8, s));
+  FX_CHECK_CUDA(cudaMemsetAsync(d->bh.bbox.p + 2, 0, 12, s));
   int nb = (d->n + 255) / 256;
   if (nb > ctx->num_sms * 8) nb = ctx->num_sms * 8;
   bh_bbox_kernel<<<nb, 256, 0, s>>>(x, y, d->n, d->bh.bbox.p);

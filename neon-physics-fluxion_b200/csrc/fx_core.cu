@@ -224,11 +224,13 @@ extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
   }
   // The word is zeroed on the primary stream and the creation waits for it,
   // so no GEMM of this context (on either stream) can see a stale value.
-  if (cudaMalloc((void **)&c->tc_err, sizeof(unsigned int)) != cudaSuccess ||
+  if (cudaMallocHost((void **)&c->readback, sizeof(fx::IterReadback)) != cudaSuccess ||
+      cudaMalloc((void **)&c->tc_err, sizeof(unsigned int)) != cudaSuccess ||
       cudaMemsetAsync(c->tc_err, 0, sizeof(unsigned int), c->stream) != cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess) {
     set_error("error word allocation failed");
     if (c->tc_err) cudaFree(c->tc_err);
+    if (c->readback) cudaFreeHost(c->readback);
     cudaEventDestroy(c->fork);
     cudaEventDestroy(c->join);
     cudaStreamDestroy(c->stream);
@@ -282,6 +284,7 @@ extern "C" int fx_ctx_destroy(fx_ctx *ctx) {
   cudaEventDestroy(ctx->fork);
   cudaEventDestroy(ctx->join);
   if (ctx->tc_err) cudaFree(ctx->tc_err);
+  if (ctx->readback) cudaFreeHost(ctx->readback);
   cudaStreamDestroy(ctx->stream);
   cudaStreamDestroy(ctx->stream2);
   delete ctx;

@@ -236,6 +236,14 @@ struct StepWork {
   }
 };
 
+// Statistics of fx_force_iterate, read back into pinned host memory.
+struct IterReadback {
+  double res[2];        // HPWL, total overflow
+  double energy;        // density energy
+  float max_overflow;
+  unsigned int err;     // Barnes-Hut error word
+};
+
 }  // namespace fx
 
 struct fx_ctx {
@@ -251,6 +259,7 @@ struct fx_ctx {
   // Error word of this context's tensor-core GEMMs (bit 1: a bounded wait
   // expired); zeroed at creation, cleared again after it is reported.
   unsigned int *tc_err = nullptr;
+  fx::IterReadback *readback = nullptr;  // pinned host memory
   fx::StageTimer timer;
   int64_t launches = 0;
   cudaEvent_t marks[16] = {};
