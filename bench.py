@@ -59,7 +59,7 @@ def parse(argv=None):
     ap.add_argument("--bins", type=int, default=1024)
     ap.add_argument("--cong", type=int, default=512)
     ap.add_argument("--precision", default="fp32",
-                    choices=["fp32", "3xtf32", "tf32", "bf16", "simt"],
+                    choices=["fp32", "3xtf32", "tf32", "bf16", "simt", "i8"],
                     help="DCT GEMMs: fp32 (= simt, CUDA cores), 3xtf32, tf32, bf16 (tensor cores)")
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--bh-walk", default="fast", choices=["fast", "exact"],
@@ -88,11 +88,13 @@ def parse(argv=None):
     return ap.parse_args(argv)
 
 
-PREC = {"fp32": 3, "simt": 3, "3xtf32": 0, "tf32": 1, "bf16": 2}
+PREC = {"fp32": 3, "simt": 3, "3xtf32": 0, "tf32": 1, "bf16": 2, "i8": 4}
 PREC_DTYPE = {"fp32": "f32 (DCT GEMMs FP32 on CUDA cores)",
               "3xtf32": "f32 (DCT GEMMs 3xTF32, FP32 accumulate)",
               "tf32": "f32 (DCT GEMMs TF32, FP32 accumulate)",
-              "bf16": "f32 (DCT GEMMs BF16, FP32 accumulate)", "simt": "f32"}
+              "bf16": "f32 (DCT GEMMs BF16, FP32 accumulate)", "simt": "f32",
+              "i8": "f32 (DCT GEMMs on the tensor cores from exact 8-bit slices, int32 "
+                    "accumulate)"}
 
 
 # ---------------------------------------------------------------------------
@@ -973,7 +975,7 @@ def run_precision(args, rank, world, local_rank):
     d.set_positions(p.gate_x, p.gate_y)
     area = (c.gate_widths * c.gate_heights).astype(np.float64)
     codes = {"bf16": fx.FX_DCT_BF16, "tf32": fx.FX_DCT_TF32, "3xtf32": fx.FX_DCT_FP32,
-             "fp32_simt": fx.FX_DCT_SIMT}
+             "i8_slices": fx.FX_DCT_I8, "fp32_simt": fx.FX_DCT_SIMT}
     _, bf16_peak, src = peaks()
 
     def rel(a, b):
@@ -999,8 +1001,10 @@ def run_precision(args, rank, world, local_rank):
             ms = ctx.stage_times()["density"][0] / reps
             # executed: the even/odd half GEMMs (G a multiple of 256, not
             # 3xTF32) do G^3 each instead of 2 G^3; 3xTF32 runs three MMAs
-            halves = G % 256 == 0 and code != fx.FX_DCT_FP32
-            flops = 6 * (1.0 if halves else 2.0) * G ** 3 * (3 if code == fx.FX_DCT_FP32 else 1)
+            # (FX_DCT_I8: full GEMMs, ten 8-bit slice products each, int8 ops)
+            halves = G % 256 == 0 and code not in (fx.FX_DCT_FP32, fx.FX_DCT_I8)
+            flops = 6 * (1.0 if halves else 2.0) * G ** 3 * (
+                3 if code == fx.FX_DCT_FP32 else 10 if code == fx.FX_DCT_I8 else 1)
             fld = float(np.sqrt((np.linalg.norm(out["ex"] - ref["ex"]) ** 2 +
                                  np.linalg.norm(out["ey"] - ref["ey"]) ** 2) /
                                 (np.linalg.norm(ref["ex"]) ** 2 + np.linalg.norm(ref["ey"]) ** 2)))
@@ -1019,7 +1023,9 @@ def run_precision(args, rank, world, local_rank):
             hp[name] = hpwl_at
             print(f"precision sweep: G={G} {name}: {time.perf_counter() - t_phase:.1f} s",
                   file=sys.stderr, flush=True)
-            peak = bf16_peak if code == fx.FX_DCT_BF16 else bf16_peak / 2
+            # int8 dense: twice the bf16 rate (nominal ratio); tf32: half
+            peak = (bf16_peak if code == fx.FX_DCT_BF16 else
+                    2 * bf16_peak if code == fx.FX_DCT_I8 else bf16_peak / 2)
             rows.append({"G": G, "precision": name, "field_rel_l2": fld, "force_rel_l2": frc,
                          "phi_rel_l2": rel(out["phi"], ref["phi"]),
                          "energy_rel": abs(out["energy"] - ref["energy"]) / abs(ref["energy"]),
@@ -1041,10 +1047,11 @@ def run_precision(args, rank, world, local_rank):
     out = {"metric": PREC_METRIC, "value": best["tensor_tflops_executed"], "unit": "TFLOP/s",
            "n_gpus": 1, "steps": 3, "warmup": 1, "ms_per_step": best["density_ms"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "bf16/tf32/3xtf32/fp32, FP32 accumulate", "data": "synthetic",
+           "dtype": "bf16/tf32/3xtf32/fp32 (FP32 accumulate), int8 slices (int32 accumulate)",
+           "data": "synthetic",
            "config": {"workload": f"precision: {n} gates, die 2400, G in (2048, 4096), "
                                   "target density 0.7, weight 1", "seed": args.seed,
-                      "peak_source": f"{src} bf16 dense (tf32: half)"},
+                      "peak_source": f"{src} bf16 dense (tf32: half, int8: twice)"},
            "value_is": f"{best['precision']} at G=4096, executed tensor FLOP/s of the 6 GEMMs",
            "sweep": rows}
     print(json.dumps(out), flush=True)

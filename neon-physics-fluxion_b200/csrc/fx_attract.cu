@@ -258,7 +258,7 @@ static int validate_cfg(const fx_iter_cfg &c) {
     set_error("fx_iter_cfg: unknown bh_walk %d", c.bh_walk);
     return FX_EINVAL;
   }
-  if (c.dct_precision < FX_DCT_FP32 || c.dct_precision > FX_DCT_SIMT) {
+  if (c.dct_precision < FX_DCT_FP32 || c.dct_precision > FX_DCT_I8) {
     set_error("fx_iter_cfg: unknown dct_precision %d", c.dct_precision);
     return FX_EINVAL;
   }

@@ -179,7 +179,7 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   // of 256 (tiles of 128 on each half). Not for 3xTF32: rows G-1-i come out
   // as E - O, and that difference magnifies the tensor cores' accumulation
   // error (2.1e-4 instead of 5e-5 at G = 256).
-  w.halves = G % 256 == 0 && precision != FX_DCT_FP32;
+  w.halves = G % 256 == 0 && precision != FX_DCT_FP32 && precision != FX_DCT_I8;
   {
     int sp = precision == FX_DCT_SIMT ? sgemm_splits(G, d->ctx->num_sms) : 1;
     if (w.halves && precision == FX_DCT_SIMT) sp = std::max(sp, half_splits(G, d->ctx->num_sms));
@@ -262,6 +262,42 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
       ie[(size_t)ky * G + kx] = (kx == 0 && ky == 0) ? 0.0f : (float)(-1.0 / lam);
     }
   FX_CHECK_CUDA(cudaMemcpyAsync(w.inv_eig.p, ie.data(), cells * 4, cudaMemcpyHostToDevice, s));
+  if (precision == FX_DCT_I8) {
+    // the operators' 8-bit slices, cut from their FP64 values (28 bits of
+    // each row's scale), in the order [s1 s2 s3 s4] along 4G columns
+    const std::vector<double> *ops[4] = {&c, &ct, &dx, &dy};
+    std::vector<int8_t> sl((size_t)4 * cells);
+    std::vector<float> sc(G);
+    for (int o = 0; o < 4; ++o) {
+      const std::vector<double> &m = *ops[o];
+      for (int i = 0; i < G; ++i) {
+        double mx = 0.0;
+        for (int k = 0; k < G; ++k) mx = std::max(mx, std::fabs(m[(size_t)i * G + k]));
+        int e = 0;
+        if (mx > 0.0) std::frexp(mx, &e);
+        sc[i] = std::ldexp(1.0f, e);
+        for (int k = 0; k < G; ++k) {
+          double a = std::ldexp(m[(size_t)i * G + k], -e);
+          for (int t = 0; t < 4; ++t) {
+            const double q = a * 128.0;
+            const double tr = std::trunc(q);
+            sl[(size_t)i * 4 * G + (size_t)t * G + k] = (int8_t)tr;
+            a = q - tr;
+          }
+        }
+      }
+      FX_TRY(w.op8[o].alloc((size_t)4 * cells));
+      FX_TRY(w.op_sc[o].alloc(G));
+      FX_CHECK_CUDA(cudaMemcpyAsync(w.op8[o].p, sl.data(), sl.size(), cudaMemcpyHostToDevice, s));
+      FX_CHECK_CUDA(cudaMemcpyAsync(w.op_sc[o].p, sc.data(), (size_t)G * 4,
+                                    cudaMemcpyHostToDevice, s));
+      FX_CHECK_CUDA(cudaStreamSynchronize(s));  // sl and sc are reused
+    }
+    for (int i = 0; i < 2; ++i) {
+      FX_TRY(w.d8[i].alloc((size_t)4 * cells));
+      FX_TRY(w.d_sc[i].alloc(G));
+    }
+  }
   FX_TRY(upload_operand(c, precision, w.cmat.p, split ? w.cmat_lo.p : nullptr,
                         half ? w.cmat_bf.p : nullptr, s));
   FX_TRY(upload_operand(ct, precision, w.cmat_t.p, split ? w.cmat_t_lo.p : nullptr,
@@ -351,6 +387,32 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   float *WS = precision == FX_DCT_SIMT ? w.split_ws.p : nullptr;
+  if (precision == FX_DCT_I8) {
+    // the same seven products; each data operand is sliced once and kept
+    // while later products read it (phat and T3 twice)
+    float *rho = w.buf[0].p, *t1 = w.buf[1].p, *phat = w.buf[2].p, *t3 = w.buf[1].p;
+    float *t4 = w.buf[4].p;
+    auto slice = [&](const float *X, int i) {
+      return i8_slice(ctx, X, G, G, w.d8[i].p, w.d_sc[i].p, s);
+    };
+    auto mm = [&](int op, int i, const float *S, float *D) {
+      return gemm_nt_i8(ctx, G, w.op8[op].p, w.op_sc[op].p, w.d8[i].p, w.d_sc[i].p, S, D, s);
+    };
+    FX_TRY(slice(rho, 0));
+    FX_TRY(mm(0, 0, nullptr, t1));              // T1^T = C rho^T
+    FX_TRY(slice(t1, 0));
+    FX_TRY(mm(0, 0, w.inv_eig.p, phat));        // phi_hat = (C T1) * (-1/lambda)
+    FX_TRY(slice(phat, 1));
+    FX_TRY(mm(1, 1, nullptr, t3));              // T3^T = C^T phi_hat^T
+    FX_TRY(slice(t3, 0));
+    FX_TRY(mm(3, 0, nullptr, w.ey.p));          // E_y = (Dy C^T) T3
+    if (need_phi) FX_TRY(mm(1, 0, nullptr, w.buf[3].p));  // phi = C^T T3
+    FX_TRY(mm(2, 1, nullptr, t4));              // T4^T = (Dx C^T) phi_hat^T
+    FX_TRY(slice(t4, 0));
+    FX_TRY(mm(1, 0, nullptr, w.ex.p));          // E_x = C^T T4
+    timer_end(ctx, FX_STAGE_DENSITY, s, ev);
+    return FX_OK;
+  }
   if (w.halves) {
     // each product as two half-size GEMMs on the folded or split operand;
     // products come back as f32 and the folds write the GEMM formats
@@ -439,7 +501,7 @@ extern "C" int fx_stage_density(fx_ctx *ctx, fx_design *d, int32_t bins,
                                 float *out_ex, float *out_ey,
                                 double *out_energy) {
   if (!ctx || !d || bins < 128 || bins % 128 != 0 || bins > 8192 ||
-      precision < FX_DCT_FP32 || precision > FX_DCT_SIMT) {
+      precision < FX_DCT_FP32 || precision > FX_DCT_I8) {
     set_error("fx_stage_density: invalid arguments (bins must be a multiple of 128)");
     return FX_EINVAL;
   }

@@ -19,6 +19,7 @@
 // (bounded) for its own TMA copies, frees TMEM and returns.
 #include <cuda.h>
 
+#include <algorithm>
 #include <mutex>
 #include <unordered_map>
 
@@ -290,6 +291,215 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
   }
 }
 
+// ---- FX_DCT_I8: FP32-accurate products from exact 8-bit slices ---------------------
+// An operand row r is split under a power-of-two scale 2^e (the smallest with
+// every |x| < 2^e) into four signed 8-bit slices: x = 2^e sum_t s_t 2^(-7t),
+// t = 1..4, exact for every x >= 2^(e-4) (28 bits cover the 24-bit
+// significand) and within 2^(e-28) for the rest. A product of two rows is
+// then sum_w 2^(-7w) sum_{t+u=w} s_t . s'_u; the weight classes w = 2..5 keep
+// every pair above 2^-35 of the row scales. The operator A is stored with its
+// slices in order [s1 s2 s3 s4] along K, the data operand B reversed
+// [s4 s3 s2 s1], so class c = w - 2 is one GEMM over A columns [0, (c+1)K)
+// and B columns [(3-c)K, 4K). tcgen05 kind::i8 accumulates the classes
+// exactly in four 128-column int32 TMEM accumulators (|partial| <= 4K 127^2
+// < 2^31 for K <= 8192); the epilogue adds them in FP64, applies the row and
+// column scales and rounds once to f32. The tensor cores' own accumulation
+// rounding, which makes 3xTF32 lose accuracy with K, does not arise.
+constexpr int kI8Stages = 6;
+constexpr int kI8StageBytes = 2 * kTileBytes;  // one A and one B tile
+constexpr int kI8Smem = 1024 + kI8Stages * kI8StageBytes + 256;
+constexpr int kI8Cols = 512;                   // four 128-column accumulators
+// kind::i8 instruction descriptor: D s32 (2), A and B s8 (1), N / 8, M / 16
+constexpr uint32_t kI8Idesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                              ((uint32_t)(kTcBN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                        uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accum));
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+             int G, int K, const float *__restrict__ sa, const float *__restrict__ sb,
+             const float *__restrict__ S, float *__restrict__ D, unsigned int *__restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-aligned stages
+  const uint32_t bar0 = base + kI8Stages * kI8StageBytes;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 64u + 8u * s; };
+  const uint32_t done_bar = bar0 + 128u;
+  const uint32_t tmem_slot = bar0 + 136u;
+  const uint32_t abort_slot = bar0 + 140u;
+  uint8_t *gen_base = smem_raw + (base - raw);
+  volatile uint32_t *tmem_ptr = (volatile uint32_t *)(gen_base + (tmem_slot - base));
+  volatile uint32_t *abort_flag = (volatile uint32_t *)(gen_base + (abort_slot - base));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bm = blockIdx.y * kTcBM, bn = blockIdx.x * kTcBN;
+  const int KB = K / 128;  // 128-byte blocks of one slice
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kI8Stages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0u;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tmem_slot),
+                 "r"(kI8Cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_ptr;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer: class by class, the A and B K-blocks of each ----------
+    int t = 0, issued = 0;
+    bool stop = false;
+    for (int c = 0; c < 4 && !stop; ++c) {
+      for (int kb = 0; kb < (c + 1) * KB; ++kb, ++t) {
+        const int s = t % kI8Stages;
+        const uint32_t ph = (uint32_t)(t / kI8Stages) & 1u;
+        if (t >= kI8Stages && !mbar_wait(empty_bar(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(err, 2u);
+          stop = true;
+          break;
+        }
+        if (*abort_flag) {
+          stop = true;
+          break;
+        }
+        const uint32_t st = base + s * kI8StageBytes;
+        mbar_expect_tx(full_bar(s), kI8StageBytes);
+        tma_load_2d(st, &tA, full_bar(s), kb * 128, bm);
+        tma_load_2d(st + kTileBytes, &tB, full_bar(s), (3 - c) * K + kb * 128, bn);
+        issued = t + 1;
+      }
+    }
+    // Before leaving, make sure none of this CTA's copies is still in flight.
+    const int first = issued > kI8Stages ? issued - kI8Stages : 0;
+    for (int q = first; q < issued; ++q)
+      mbar_wait(full_bar(q % kI8Stages), (uint32_t)(q / kI8Stages) & 1u);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer: class c into the accumulator at column 128 c ------------
+    int t = 0;
+    bool ok = true;
+    for (int c = 0; c < 4 && ok; ++c) {
+      for (int kb = 0; kb < (c + 1) * KB; ++kb, ++t) {
+        const int s = t % kI8Stages;
+        const uint32_t ph = (uint32_t)(t / kI8Stages) & 1u;
+        if (!mbar_wait(full_bar(s), ph) || *abort_flag) {
+          *abort_flag = 1u;
+          atomicOr(err, 2u);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t st = base + s * kI8StageBytes;
+        const uint64_t a = umma_desc(st), b = umma_desc(st + kTileBytes);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)  // 32 bytes of K per instruction
+          umma_i8(tmem + 128u * c, a + 2u * k, b + 2u * k, kI8Idesc,
+                  (kb > 0 || k > 0) ? 1u : 0u);
+        umma_commit(empty_bar(s));
+      }
+    }
+    umma_commit(done_bar);
+  }
+  // ---- epilogue: all warps --------------------------------------------------------
+  __syncwarp();
+  uint32_t go = 0u;
+  if (lane == 0) {
+    const bool done_ok = mbar_wait(done_bar, 0u);
+    if (!done_ok) {
+      *abort_flag = 1u;
+      atomicOr(err, 2u);
+    }
+    go = (done_ok && !*abort_flag) ? 1u : 0u;
+  }
+  go = __shfl_sync(0xffffffffu, go, 0);
+  tc_fence_after();
+  if (go) {
+    const int r = bm + warp * 32 + lane;
+    const double sr = (double)sa[r];
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+      double acc[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+#pragma unroll 1
+      for (int c = 0; c < 4; ++c) {
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + 128u * c + (uint32_t)c0, v);
+        const double wgt = ldexp(1.0, -7 * (c + 2));
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] += (double)(int32_t)v[j] * wgt;
+      }
+      const size_t o = (size_t)r * G + bn + c0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        float x = (float)(acc[j] * sr * (double)sb[bn + c0 + j]);
+        if (S) x *= S[o + j];
+        D[o + j] = x;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kI8Cols));
+  }
+}
+
+// Slices of a data operand (rows x K f32, row-major) in the reversed order
+// [s4 s3 s2 s1] along 4K columns, and each row's scale 2^e. One warp per row.
+// Every step is exact in f32: scaling by powers of two, truncation, and the
+// remainder of a truncation.
+__global__ void i8_slice_kernel(const float *__restrict__ X, int rows, int K,
+                                int8_t *__restrict__ out, float *__restrict__ scale) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += (gridDim.x * blockDim.x) >> 5) {
+    const float *x = X + (size_t)r * K;
+    float m = 0.f;
+    for (int k = lane; k < K; k += 32) m = fmaxf(m, fabsf(x[k]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    int e = 0;
+    if (m > 0.f) frexpf(m, &e);  // m = f 2^e, f in [0.5, 1): every |x| < 2^e
+    if (lane == 0) scale[r] = ldexpf(1.f, e);
+    int8_t *o8 = out + (size_t)r * 4 * K;
+    for (int k = lane; k < K; k += 32) {
+      float a = ldexpf(x[k], -e);
+      int8_t sl[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const float q = a * 128.f;
+        const float w = truncf(q);
+        sl[t] = (int8_t)(int)w;
+        a = q - w;
+      }
+      o8[3 * K + k] = sl[0];
+      o8[2 * K + k] = sl[1];
+      o8[K + k] = sl[2];
+      o8[k] = sl[3];
+    }
+  }
+}
+
 // ---- host: tensor maps -------------------------------------------------------------
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
                                   void *, const cuuint64_t *, const cuuint64_t *,
@@ -312,9 +522,9 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// A rows x cols row-major operand as a 2-D tensor map with 128 x 128-byte
-// boxes.
-static int make_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap *out) {
+// A rows x cols row-major operand of esz-byte elements (4: f32, 2: bf16,
+// 1: int8 slices) as a 2-D tensor map with 128 x 128-byte boxes.
+static int make_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *out) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled is unavailable");
@@ -324,13 +534,16 @@ static int make_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap 
     set_error("tensor map base not 16-byte aligned");
     return FX_EINVAL;
   }
-  const int esz = bf16 ? 2 : 4;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * esz};
   const cuuint32_t box[2] = {(cuuint32_t)(128 / esz), 128u};
   const cuuint32_t estr[2] = {1u, 1u};
   const CUresult r =
-      fn(out, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+      fn(out,
+         esz == 1   ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+         : esz == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+         2,
          const_cast<void *>(ptr), dims, strides, box, estr,
          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -344,29 +557,29 @@ static int make_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap 
 struct MapKey {
   const void *p;
   int cols, rows;
-  bool bf;
+  int esz;
   bool operator==(const MapKey &o) const {
-    return p == o.p && cols == o.cols && rows == o.rows && bf == o.bf;
+    return p == o.p && cols == o.cols && rows == o.rows && esz == o.esz;
   }
 };
 struct MapKeyHash {
   size_t operator()(const MapKey &k) const {
     return std::hash<const void *>()(k.p) ^ ((size_t)k.cols << 1) ^ ((size_t)k.rows << 21) ^
-           (size_t)k.bf;
+           (size_t)k.esz;
   }
 };
 
-static int get_map(const void *ptr, int cols, int rows, bool bf16, CUtensorMap *out) {
+static int get_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *out) {
   static std::mutex mu;
   static std::unordered_map<MapKey, CUtensorMap, MapKeyHash> cache;
   std::lock_guard<std::mutex> g(mu);
-  const MapKey k{ptr, cols, rows, bf16};
+  const MapKey k{ptr, cols, rows, esz};
   auto it = cache.find(k);
   if (it != cache.end()) {
     *out = it->second;
     return FX_OK;
   }
-  FX_TRY(make_map(ptr, cols, rows, bf16, out));
+  FX_TRY(make_map(ptr, cols, rows, esz, out));
   if (cache.size() >= 4096) cache.clear();  // bounded: designs come and go
   cache.emplace(k, *out);
   return FX_OK;
@@ -390,11 +603,11 @@ static int launch(fx_ctx *ctx, int G, const GemmOperands &A, const GemmOperands 
   }
   const int h = G / 2;
   const int kc = half ? h : G, ar = half ? 2 * h : G, br = half ? 2 * G : G;
-  FX_TRY(get_map(pa, kc, ar, bf, &ta));
-  FX_TRY(get_map(pb, kc, br, bf, &tb));
+  FX_TRY(get_map(pa, kc, ar, bf ? 2 : 4, &ta));
+  FX_TRY(get_map(pb, kc, br, bf ? 2 : 4, &tb));
   if (PREC == 0) {
-    FX_TRY(get_map(A.lo, kc, ar, false, &talo));
-    FX_TRY(get_map(B.lo, kc, br, false, &tblo));
+    FX_TRY(get_map(A.lo, kc, ar, 4, &talo));
+    FX_TRY(get_map(B.lo, kc, br, 4, &tblo));
   } else {
     talo = ta;
     tblo = tb;
@@ -437,6 +650,34 @@ int gemm_half_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
   }
   set_error("gemm_half: unknown precision %d", precision);
   return FX_EINVAL;
+}
+
+// D = A B^T (times S) from the slices of A (operator, [s1..s4]) and of B
+// (data, [s4..s1]), each G x 4G int8 with a scale per row; D in f32.
+int gemm_nt_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8_t *B8,
+               const float *sb, const float *S, float *D, cudaStream_t s) {
+  if (G % 128 != 0 || G > 8192) {
+    set_error("gemm_nt_i8: G = %d must be a multiple of 128 up to 8192", G);
+    return FX_EINVAL;
+  }
+  CUtensorMap ta, tb;
+  FX_TRY(get_map(A8, 4 * G, G, 1, &ta));
+  FX_TRY(get_map(B8, 4 * G, G, 1, &tb));
+  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(tc_i8_kernel), kI8Smem));
+  dim3 grid(G / kTcBN, G / kTcBM);
+  tc_i8_kernel<<<grid, kTcThreads, kI8Smem, s>>>(ta, tb, G, G, sa, sb, S, D, ctx->tc_err);
+  FX_CHECK_LAUNCH();
+  ctx->launches += 1;
+  return FX_OK;
+}
+
+int i8_slice(fx_ctx *ctx, const float *X, int rows, int K, int8_t *out, float *scale,
+             cudaStream_t s) {
+  const int blocks = std::min((rows + 7) / 8, ctx->num_sms * 8);
+  i8_slice_kernel<<<blocks, 256, 0, s>>>(X, rows, K, out, scale);
+  FX_CHECK_LAUNCH();
+  ctx->launches += 1;
+  return FX_OK;
 }
 
 // Error word of the context's tensor-core GEMMs (bit 1: a bounded wait

@@ -189,6 +189,10 @@ struct DensityWork {
   DevBuf<uint16_t> c_h_bf, ct_h_bf, dx_h_bf, dy_h_bf;   // bf16 copies
   DevBuf<float> hw[3], hw_lo[3];
   DevBuf<uint16_t> hw_bf[3];
+  // FX_DCT_I8: 8-bit slices (G x 4G) and row scales of the operators C, C^T,
+  // Dx C^T, Dy C^T, and of two data operands at a time
+  DevBuf<int8_t> op8[4], d8[2];
+  DevBuf<float> op_sc[4], d_sc[2];
   template <class F>
   void for_each(F &&f) {
     f(area_fx); f(cmat); f(cmat_t); f(cmat_lo); f(cmat_t_lo); f(cmat_bf);
@@ -204,6 +208,10 @@ struct DensityWork {
     for (auto &b : hw) f(b);
     for (auto &b : hw_lo) f(b);
     for (auto &b : hw_bf) f(b);
+    for (auto &b : op8) f(b);
+    for (auto &b : d8) f(b);
+    for (auto &b : op_sc) f(b);
+    for (auto &b : d_sc) f(b);
   }
 };
 

@@ -23,6 +23,7 @@ FX_DCT_FP32 = 0
 FX_DCT_TF32 = 1
 FX_DCT_BF16 = 2
 FX_DCT_SIMT = 3
+FX_DCT_I8 = 4
 
 FX_BH_FAST = 0
 FX_BH_EXACT = 1

@@ -89,15 +89,22 @@ def test_barnes_hut_and_one_plain_iteration(fx, full_design, full, oracle):
     assert abs(hpwl - oracle.hpwl_f64(c.net_ptr, c.net_gate, ox, oy)) <= 1e-12 * hpwl
 
 
-def test_density_field_and_forces(fx, full_design, full, oracle):
+@pytest.mark.parametrize("prec", ["simt", "i8"])
+def test_density_field_and_forces(fx, full_design, full, oracle, prec):
+    """The 1024 x 1024 solve of the 1M-gate workload within 1e-5 of the FP64
+    FFT oracle: FP32 GEMMs on the CUDA cores, and on the tensor cores from
+    exact 8-bit slices."""
     c, p = full.circuit, full.placement
     full_design.set_positions(p.gate_x, p.gate_y)
-    out = full_design.density(1024, 0.7, 1.0, fx.FX_DCT_SIMT, grids=True)
+    code = {"simt": fx.FX_DCT_SIMT, "i8": fx.FX_DCT_I8}[prec]
+    out = full_design.density(1024, 0.7, 1.0, code, grids=True)
     area = (c.gate_widths * c.gate_heights).astype(np.float64)
     ref = oracle.density_forces(p.gate_x, p.gate_y, area, c.chip_width, c.chip_height, 1024,
                                 0.7, 1.0)
-    assert _rel(out["ex"], out["ey"], ref["ex"], ref["ey"]) < 1e-5
-    assert _rel(out["fx"], out["fy"], ref["fx"], ref["fy"]) < 1e-5
+    fe = _rel(out["ex"], out["ey"], ref["ex"], ref["ey"])
+    ff = _rel(out["fx"], out["fy"], ref["fx"], ref["fy"])
+    print(f"density 1M G=1024 {prec}: field {fe:.3e} force {ff:.3e}")
+    assert fe < 1e-5 and ff < 1e-5
 
 
 @pytest.mark.parametrize("weight,iters", [(1e-4, 3), (1.0, 1)])

@@ -184,17 +184,19 @@ def test_barnes_hut_clustered_large(fx, ctx, oracle):
 # "3xtf32" (FX_DCT_FP32) is the tensor-core split: FP32 inputs, but its error
 # grows with G (the accumulation on the tensor cores); "simt" is FP32 on the
 # CUDA cores, the iteration's default.
+# "i8" (FX_DCT_I8) is the tensor-core path from exact 8-bit slices with
+# integer accumulation: FP32-accurate at every G.
 PREC_TOL = {"simt": (1e-5, 2e-5), "3xtf32": (2e-4, 2e-4), "tf32": (1e-2, 1e-2),
-            "bf16": (5e-2, 5e-2)}
+            "bf16": (5e-2, 5e-2), "i8": (1e-5, 1e-5)}
 
 
 @pytest.mark.parametrize("G", [128, 256])
-@pytest.mark.parametrize("prec", ["simt", "3xtf32", "tf32", "bf16"])
+@pytest.mark.parametrize("prec", ["simt", "i8", "3xtf32", "tf32", "bf16"])
 def test_density_vs_fp64(fx, ctx, oracle, G, prec):
     s = fx.synth_plain(9, 20_000, 24_000, 170.0)
     c, p = s.circuit, s.placement
     code = {"simt": fx.FX_DCT_SIMT, "3xtf32": fx.FX_DCT_FP32, "tf32": fx.FX_DCT_TF32,
-            "bf16": fx.FX_DCT_BF16}[prec]
+            "bf16": fx.FX_DCT_BF16, "i8": fx.FX_DCT_I8}[prec]
     tol_phi, tol_e = PREC_TOL[prec]
     d = fx.Design(ctx, c)
     try:
