@@ -255,7 +255,7 @@ typedef struct fx_iter_cfg {
 #define FX_DCT_SIMT  3 /* FP32 CUDA-core GEMM (no tensor cores): the FP32-    */
                        /* accurate solve, the iteration's default            */
 #define FX_DCT_I8    4 /* tensor cores, FP32-accurate: each operand row split */
-                       /* into four exact 8-bit slices under a power-of-two   */
+                       /* into six exact 8-bit slices under a power-of-two    */
                        /* scale, slice products accumulated exactly in int32  */
                        /* (tcgen05 kind::i8), classes combined in FP64        */
 

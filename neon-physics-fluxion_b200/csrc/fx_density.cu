@@ -263,10 +263,11 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
     }
   FX_CHECK_CUDA(cudaMemcpyAsync(w.inv_eig.p, ie.data(), cells * 4, cudaMemcpyHostToDevice, s));
   if (precision == FX_DCT_I8) {
-    // the operators' 8-bit slices, cut from their FP64 values (28 bits of
-    // each row's scale), in the order [s1 s2 s3 s4] along 4G columns
+    // the operators' 8-bit slices, cut from their FP64 values (7 bits of
+    // each row's scale per slice), in the order [s1 ..] along NS G columns
+    const int NS = i8_slices();
     const std::vector<double> *ops[4] = {&c, &ct, &dx, &dy};
-    std::vector<int8_t> sl((size_t)4 * cells);
+    std::vector<int8_t> sl((size_t)NS * cells);
     std::vector<float> sc(G);
     for (int o = 0; o < 4; ++o) {
       const std::vector<double> &m = *ops[o];
@@ -278,15 +279,15 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
         sc[i] = std::ldexp(1.0f, e);
         for (int k = 0; k < G; ++k) {
           double a = std::ldexp(m[(size_t)i * G + k], -e);
-          for (int t = 0; t < 4; ++t) {
+          for (int t = 0; t < NS; ++t) {
             const double q = a * 128.0;
             const double tr = std::trunc(q);
-            sl[(size_t)i * 4 * G + (size_t)t * G + k] = (int8_t)tr;
+            sl[(size_t)i * NS * G + (size_t)t * G + k] = (int8_t)tr;
             a = q - tr;
           }
         }
       }
-      FX_TRY(w.op8[o].alloc((size_t)4 * cells));
+      FX_TRY(w.op8[o].alloc((size_t)NS * cells));
       FX_TRY(w.op_sc[o].alloc(G));
       FX_CHECK_CUDA(cudaMemcpyAsync(w.op8[o].p, sl.data(), sl.size(), cudaMemcpyHostToDevice, s));
       FX_CHECK_CUDA(cudaMemcpyAsync(w.op_sc[o].p, sc.data(), (size_t)G * 4,
@@ -294,7 +295,7 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
       FX_CHECK_CUDA(cudaStreamSynchronize(s));  // sl and sc are reused
     }
     for (int i = 0; i < 2; ++i) {
-      FX_TRY(w.d8[i].alloc((size_t)4 * cells));
+      FX_TRY(w.d8[i].alloc((size_t)NS * cells));
       FX_TRY(w.d_sc[i].alloc(G));
     }
   }

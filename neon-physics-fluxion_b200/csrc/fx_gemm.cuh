@@ -82,8 +82,9 @@ int gemm_half(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
               float *part, cudaStream_t s);
 
 // FX_DCT_I8 (fx_gemm_tc.cu): D = A B^T (times S) from 8-bit slices: A8 the
-// operator's G x 4G slices [s1 s2 s3 s4] with row scales sa, B8 the data
-// operand's [s4 s3 s2 s1] with row scales sb (i8_slice writes those).
+// operator's G x (i8_slices() G) slices [s1 ..] with row scales sa, B8 the
+// data operand's [.. s1] with row scales sb (i8_slice writes those).
+int i8_slices();
 int gemm_nt_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8_t *B8,
                const float *sb, const float *S, float *D, cudaStream_t s);
 int i8_slice(fx_ctx *ctx, const float *X, int rows, int K, int8_t *out, float *scale,

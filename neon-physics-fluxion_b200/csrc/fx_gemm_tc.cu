@@ -293,25 +293,32 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
 
 // ---- FX_DCT_I8: FP32-accurate products from exact 8-bit slices ---------------------
 // An operand row r is split under a power-of-two scale 2^e (the smallest with
-// every |x| < 2^e) into four signed 8-bit slices: x = 2^e sum_t s_t 2^(-7t),
-// t = 1..4, exact for every x >= 2^(e-4) (28 bits cover the 24-bit
-// significand) and within 2^(e-28) for the rest. A product of two rows is
-// then sum_w 2^(-7w) sum_{t+u=w} s_t . s'_u; the weight classes w = 2..5 keep
-// every pair above 2^-35 of the row scales. The operator A is stored with its
-// slices in order [s1 s2 s3 s4] along K, the data operand B reversed
-// [s4 s3 s2 s1], so class c = w - 2 is one GEMM over A columns [0, (c+1)K)
-// and B columns [(3-c)K, 4K). tcgen05 kind::i8 accumulates the classes
-// exactly in four 128-column int32 TMEM accumulators (|partial| <= 4K 127^2
-// < 2^31 for K <= 8192); the epilogue adds them in FP64, applies the row and
-// column scales and rounds once to f32. The tensor cores' own accumulation
+// every |x| < 2^e) into kI8Slices = 6 signed 8-bit slices:
+// x = 2^e sum_t s_t 2^(-7t), t = 1..6, exact for every x >= 2^(e-18) (42 bits
+// cover the 24-bit significand of entries down to 2^-18 of the row's
+// largest; the DCT spectra span about that within a row) and within
+// 2^(e-42) below. A product of two rows is sum_w 2^(-7w) sum_{t+u=w}
+// s_t . s'_u; the weight classes w = 2..7 (21 slice pairs) keep every pair
+// above 2^-49 of the row scales. The operator A is stored with its slices in
+// order [s1 .. s6] along K, the data operand B reversed [s6 .. s1], so class
+// c = w - 2 is one GEMM over A columns [0, (c+1)K) and B columns
+// [(5-c)K, 6K). tcgen05 kind::i8 accumulates the classes exactly in six
+// 64-column int32 TMEM accumulators (|partial| <= 6K 127^2 < 2^31 for
+// K <= 8192); the epilogue adds them in FP64, applies the row and column
+// scales and rounds once to f32. The tensor cores' own accumulation
 // rounding, which makes 3xTF32 lose accuracy with K, does not arise.
-constexpr int kI8Stages = 6;
-constexpr int kI8StageBytes = 2 * kTileBytes;  // one A and one B tile
+// Tiles are 128 x 64 (M x N), so a 1024-wide grid gives 128 CTAs.
+constexpr int kI8Slices = 6;
+constexpr int kI8BN = 64;
+constexpr int kI8Stages = 8;
+constexpr int kI8BTile = kI8BN * 128;            // B tile bytes (64 rows x 128 B)
+constexpr int kI8StageBytes = kTileBytes + kI8BTile;
 constexpr int kI8Smem = 1024 + kI8Stages * kI8StageBytes + 256;
-constexpr int kI8Cols = 512;                   // four 128-column accumulators
+constexpr int kI8Cols = 512;                     // six 64-column accumulators (384 used)
 // kind::i8 instruction descriptor: D s32 (2), A and B s8 (1), N / 8, M / 16
 constexpr uint32_t kI8Idesc = (2u << 4) | (1u << 7) | (1u << 10) |
-                              ((uint32_t)(kTcBN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
+                              ((uint32_t)(kI8BN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
+static_assert(kI8Slices * kI8BN <= kI8Cols, "accumulators exceed the TMEM allocation");
 
 __device__ __forceinline__ void umma_i8(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
                                         uint32_t accum) {
@@ -338,7 +345,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
   volatile uint32_t *tmem_ptr = (volatile uint32_t *)(gen_base + (tmem_slot - base));
   volatile uint32_t *abort_flag = (volatile uint32_t *)(gen_base + (abort_slot - base));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int bm = blockIdx.y * kTcBM, bn = blockIdx.x * kTcBN;
+  const int bm = blockIdx.y * kTcBM, bn = blockIdx.x * kI8BN;
   const int KB = K / 128;  // 128-byte blocks of one slice
 
   if (threadIdx.x == 0) {
@@ -366,7 +373,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
     // ---- TMA producer: class by class, the A and B K-blocks of each ----------
     int t = 0, issued = 0;
     bool stop = false;
-    for (int c = 0; c < 4 && !stop; ++c) {
+    for (int c = 0; c < kI8Slices && !stop; ++c) {
       for (int kb = 0; kb < (c + 1) * KB; ++kb, ++t) {
         const int s = t % kI8Stages;
         const uint32_t ph = (uint32_t)(t / kI8Stages) & 1u;
@@ -383,7 +390,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
         const uint32_t st = base + s * kI8StageBytes;
         mbar_expect_tx(full_bar(s), kI8StageBytes);
         tma_load_2d(st, &tA, full_bar(s), kb * 128, bm);
-        tma_load_2d(st + kTileBytes, &tB, full_bar(s), (3 - c) * K + kb * 128, bn);
+        tma_load_2d(st + kTileBytes, &tB, full_bar(s), (kI8Slices - 1 - c) * K + kb * 128, bn);
         issued = t + 1;
       }
     }
@@ -392,10 +399,10 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
     for (int q = first; q < issued; ++q)
       mbar_wait(full_bar(q % kI8Stages), (uint32_t)(q / kI8Stages) & 1u);
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer: class c into the accumulator at column 128 c ------------
+    // ---- MMA issuer: class c into the accumulator at column 64 c -------------
     int t = 0;
     bool ok = true;
-    for (int c = 0; c < 4 && ok; ++c) {
+    for (int c = 0; c < kI8Slices && ok; ++c) {
       for (int kb = 0; kb < (c + 1) * KB; ++kb, ++t) {
         const int s = t % kI8Stages;
         const uint32_t ph = (uint32_t)(t / kI8Stages) & 1u;
@@ -410,7 +417,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
         const uint64_t a = umma_desc(st), b = umma_desc(st + kTileBytes);
 #pragma unroll
         for (int k = 0; k < 4; ++k)  // 32 bytes of K per instruction
-          umma_i8(tmem + 128u * c, a + 2u * k, b + 2u * k, kI8Idesc,
+          umma_i8(tmem + (uint32_t)(kI8BN * c), a + 2u * k, b + 2u * k, kI8Idesc,
                   (kb > 0 || k > 0) ? 1u : 0u);
         umma_commit(empty_bar(s));
       }
@@ -434,14 +441,14 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
     const int r = bm + warp * 32 + lane;
     const double sr = (double)sa[r];
 #pragma unroll 1
-    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
+    for (int c0 = 0; c0 < kI8BN; c0 += 32) {
       double acc[32];
 #pragma unroll
       for (int j = 0; j < 32; ++j) acc[j] = 0.0;
 #pragma unroll 1
-      for (int c = 0; c < 4; ++c) {
+      for (int c = 0; c < kI8Slices; ++c) {
         uint32_t v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + 128u * c + (uint32_t)c0, v);
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kI8BN * c + c0), v);
         const double wgt = ldexp(1.0, -7 * (c + 2));
 #pragma unroll
         for (int j = 0; j < 32; ++j) acc[j] += (double)(int32_t)v[j] * wgt;
@@ -465,7 +472,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
 }
 
 // Slices of a data operand (rows x K f32, row-major) in the reversed order
-// [s4 s3 s2 s1] along 4K columns, and each row's scale 2^e. One warp per row.
+// [s6 .. s1] along 6K columns, and each row's scale 2^e. One warp per row.
 // Every step is exact in f32: scaling by powers of two, truncation, and the
 // remainder of a truncation.
 __global__ void i8_slice_kernel(const float *__restrict__ X, int rows, int K,
@@ -481,21 +488,16 @@ __global__ void i8_slice_kernel(const float *__restrict__ X, int rows, int K,
     int e = 0;
     if (m > 0.f) frexpf(m, &e);  // m = f 2^e, f in [0.5, 1): every |x| < 2^e
     if (lane == 0) scale[r] = ldexpf(1.f, e);
-    int8_t *o8 = out + (size_t)r * 4 * K;
+    int8_t *o8 = out + (size_t)r * kI8Slices * K;
     for (int k = lane; k < K; k += 32) {
       float a = ldexpf(x[k], -e);
-      int8_t sl[4];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < kI8Slices; ++t) {
         const float q = a * 128.f;
         const float w = truncf(q);
-        sl[t] = (int8_t)(int)w;
+        o8[(size_t)(kI8Slices - 1 - t) * K + k] = (int8_t)(int)w;
         a = q - w;
       }
-      o8[3 * K + k] = sl[0];
-      o8[2 * K + k] = sl[1];
-      o8[K + k] = sl[2];
-      o8[k] = sl[3];
     }
   }
 }
@@ -524,7 +526,8 @@ static EncodeTiledFn encode_fn() {
 
 // A rows x cols row-major operand of esz-byte elements (4: f32, 2: bf16,
 // 1: int8 slices) as a 2-D tensor map with 128 x 128-byte boxes.
-static int make_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *out) {
+static int make_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *out,
+                    int box_rows = 128) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled is unavailable");
@@ -536,7 +539,7 @@ static int make_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *o
   }
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * esz};
-  const cuuint32_t box[2] = {(cuuint32_t)(128 / esz), 128u};
+  const cuuint32_t box[2] = {(cuuint32_t)(128 / esz), (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1u, 1u};
   const CUresult r =
       fn(out,
@@ -557,29 +560,31 @@ static int make_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *o
 struct MapKey {
   const void *p;
   int cols, rows;
-  int esz;
+  int esz, box_rows;
   bool operator==(const MapKey &o) const {
-    return p == o.p && cols == o.cols && rows == o.rows && esz == o.esz;
+    return p == o.p && cols == o.cols && rows == o.rows && esz == o.esz &&
+           box_rows == o.box_rows;
   }
 };
 struct MapKeyHash {
   size_t operator()(const MapKey &k) const {
     return std::hash<const void *>()(k.p) ^ ((size_t)k.cols << 1) ^ ((size_t)k.rows << 21) ^
-           (size_t)k.esz;
+           (size_t)k.esz ^ ((size_t)k.box_rows << 8);
   }
 };
 
-static int get_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *out) {
+static int get_map(const void *ptr, int cols, int rows, int esz, CUtensorMap *out,
+                   int box_rows = 128) {
   static std::mutex mu;
   static std::unordered_map<MapKey, CUtensorMap, MapKeyHash> cache;
   std::lock_guard<std::mutex> g(mu);
-  const MapKey k{ptr, cols, rows, esz};
+  const MapKey k{ptr, cols, rows, esz, box_rows};
   auto it = cache.find(k);
   if (it != cache.end()) {
     *out = it->second;
     return FX_OK;
   }
-  FX_TRY(make_map(ptr, cols, rows, esz, out));
+  FX_TRY(make_map(ptr, cols, rows, esz, out, box_rows));
   if (cache.size() >= 4096) cache.clear();  // bounded: designs come and go
   cache.emplace(k, *out);
   return FX_OK;
@@ -652,8 +657,8 @@ int gemm_half_tc(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
   return FX_EINVAL;
 }
 
-// D = A B^T (times S) from the slices of A (operator, [s1..s4]) and of B
-// (data, [s4..s1]), each G x 4G int8 with a scale per row; D in f32.
+// D = A B^T (times S) from the slices of A (operator, [s1..s6]) and of B
+// (data, [s6..s1]), each G x 6G int8 with a scale per row; D in f32.
 int gemm_nt_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8_t *B8,
                const float *sb, const float *S, float *D, cudaStream_t s) {
   if (G % 128 != 0 || G > 8192) {
@@ -661,15 +666,17 @@ int gemm_nt_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8
     return FX_EINVAL;
   }
   CUtensorMap ta, tb;
-  FX_TRY(get_map(A8, 4 * G, G, 1, &ta));
-  FX_TRY(get_map(B8, 4 * G, G, 1, &tb));
+  FX_TRY(get_map(A8, kI8Slices * G, G, 1, &ta));
+  FX_TRY(get_map(B8, kI8Slices * G, G, 1, &tb, kI8BN));
   FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(tc_i8_kernel), kI8Smem));
-  dim3 grid(G / kTcBN, G / kTcBM);
+  dim3 grid(G / kI8BN, G / kTcBM);
   tc_i8_kernel<<<grid, kTcThreads, kI8Smem, s>>>(ta, tb, G, G, sa, sb, S, D, ctx->tc_err);
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   return FX_OK;
 }
+
+int i8_slices() { return kI8Slices; }
 
 int i8_slice(fx_ctx *ctx, const float *X, int rows, int K, int8_t *out, float *scale,
              cudaStream_t s) {
