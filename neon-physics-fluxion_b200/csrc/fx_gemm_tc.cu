@@ -307,18 +307,23 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA,
 // K <= 8192); the epilogue adds them in FP64, applies the row and column
 // scales and rounds once to f32. The tensor cores' own accumulation
 // rounding, which makes 3xTF32 lose accuracy with K, does not arise.
-// Tiles are 128 x 64 (M x N), so a 1024-wide grid gives 128 CTAs.
+// Tiles are 128 x 64 (M x N), so a 1024-wide grid gives 128 CTAs. Each slice
+// block crosses L2 once: per 128-byte K block, the six B slices stay in
+// shared memory (double-buffered) while the six A slices stream through a
+// ring, and A slice t meets every B slice u with t + u <= 7 (classes
+// c = t + u - 2), 84 MMAs per K block.
 constexpr int kI8Slices = 6;
 constexpr int kI8BN = 64;
-constexpr int kI8Stages = 8;
-constexpr int kI8BTile = kI8BN * 128;            // B tile bytes (64 rows x 128 B)
-constexpr int kI8StageBytes = kTileBytes + kI8BTile;
-constexpr int kI8Smem = 1024 + kI8Stages * kI8StageBytes + 256;
-constexpr int kI8Cols = 512;                     // six 64-column accumulators (384 used)
+constexpr int kI8AStages = 6;                      // A slice ring
+constexpr int kI8BTile = kI8BN * 128;              // one B slice block (64 rows x 128 B)
+constexpr int kI8BBuf = kI8Slices * kI8BTile;      // the six B slices of one K block
+constexpr int kI8Smem = 1024 + kI8AStages * kTileBytes + 2 * kI8BBuf + 256;
+constexpr int kI8Cols = 512;                       // six 64-column accumulators (384 used)
 // kind::i8 instruction descriptor: D s32 (2), A and B s8 (1), N / 8, M / 16
 constexpr uint32_t kI8Idesc = (2u << 4) | (1u << 7) | (1u << 10) |
                               ((uint32_t)(kI8BN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
 static_assert(kI8Slices * kI8BN <= kI8Cols, "accumulators exceed the TMEM allocation");
+static_assert(kI8Smem <= 227 * 1024, "shared memory");
 
 __device__ __forceinline__ void umma_i8(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
                                         uint32_t accum) {
@@ -334,13 +339,19 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
              const float *__restrict__ S, float *__restrict__ D, unsigned int *__restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-aligned stages
-  const uint32_t bar0 = base + kI8Stages * kI8StageBytes;
-  auto full_bar = [&](int s) { return bar0 + 8u * s; };
-  auto empty_bar = [&](int s) { return bar0 + 64u + 8u * s; };
-  const uint32_t done_bar = bar0 + 128u;
-  const uint32_t tmem_slot = bar0 + 136u;
-  const uint32_t abort_slot = bar0 + 140u;
+  const uint32_t base = (raw + 1023u) & ~1023u;    // 1024-aligned tiles
+  const uint32_t bbuf0 = base + kI8AStages * kTileBytes;
+  const uint32_t bar0 = bbuf0 + 2 * kI8BBuf;
+  // barriers: afull[s] at bar0 + 8s, aempty[s] at +64 + 8s, bfull[j] at
+  // +112 + 8j, bempty[j] at +128 + 8j, done at +144; then the TMEM address
+  // and the abort flag
+  auto afull = [&](int s) { return bar0 + 8u * s; };
+  auto aempty = [&](int s) { return bar0 + 64u + 8u * s; };
+  auto bfull = [&](int j) { return bar0 + 112u + 8u * j; };
+  auto bempty = [&](int j) { return bar0 + 128u + 8u * j; };
+  const uint32_t done_bar = bar0 + 144u;
+  const uint32_t tmem_slot = bar0 + 152u;
+  const uint32_t abort_slot = bar0 + 156u;
   uint8_t *gen_base = smem_raw + (base - raw);
   volatile uint32_t *tmem_ptr = (volatile uint32_t *)(gen_base + (tmem_slot - base));
   volatile uint32_t *abort_flag = (volatile uint32_t *)(gen_base + (abort_slot - base));
@@ -349,9 +360,13 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
   const int KB = K / 128;  // 128-byte blocks of one slice
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kI8Stages; ++s) {
-      mbar_init(full_bar(s), 1);
-      mbar_init(empty_bar(s), 1);
+    for (int s = 0; s < kI8AStages; ++s) {
+      mbar_init(afull(s), 1);
+      mbar_init(aempty(s), 1);
+    }
+    for (int j = 0; j < 2; ++j) {
+      mbar_init(bfull(j), 1);
+      mbar_init(bempty(j), 1);
     }
     mbar_init(done_bar, 1);
     *abort_flag = 0u;
@@ -370,14 +385,27 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
   const uint32_t tmem = *tmem_ptr;
 
   if (warp == 0 && lane == 0) {
-    // ---- TMA producer: class by class, the A and B K-blocks of each ----------
-    int t = 0, issued = 0;
+    // ---- TMA producer ------------------------------------------------------------
+    int a_issued = 0, b_issued = 0;
     bool stop = false;
-    for (int c = 0; c < kI8Slices && !stop; ++c) {
-      for (int kb = 0; kb < (c + 1) * KB; ++kb, ++t) {
-        const int s = t % kI8Stages;
-        const uint32_t ph = (uint32_t)(t / kI8Stages) & 1u;
-        if (t >= kI8Stages && !mbar_wait(empty_bar(s), ph ^ 1u)) {
+    for (int kb = 0; kb < KB && !stop; ++kb) {
+      const int j = kb & 1;
+      if (kb >= 2 && !mbar_wait(bempty(j), ((uint32_t)(kb >> 1) & 1u) ^ 1u)) {
+        *abort_flag = 1u;
+        atomicOr(err, 2u);
+        break;
+      }
+      if (*abort_flag) break;
+      const uint32_t bb = bbuf0 + j * kI8BBuf;
+      mbar_expect_tx(bfull(j), kI8BBuf);
+      for (int v = 0; v < kI8Slices; ++v)  // B layout position v holds slice 6 - v
+        tma_load_2d(bb + v * kI8BTile, &tB, bfull(j), v * K + kb * 128, bn);
+      b_issued = kb + 1;
+      for (int t = 0; t < kI8Slices; ++t) {
+        const int i = kb * kI8Slices + t;
+        const int s = i % kI8AStages;
+        const uint32_t ph = (uint32_t)(i / kI8AStages) & 1u;
+        if (i >= kI8AStages && !mbar_wait(aempty(s), ph ^ 1u)) {
           *abort_flag = 1u;
           atomicOr(err, 2u);
           stop = true;
@@ -387,40 +415,49 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
           stop = true;
           break;
         }
-        const uint32_t st = base + s * kI8StageBytes;
-        mbar_expect_tx(full_bar(s), kI8StageBytes);
-        tma_load_2d(st, &tA, full_bar(s), kb * 128, bm);
-        tma_load_2d(st + kTileBytes, &tB, full_bar(s), (kI8Slices - 1 - c) * K + kb * 128, bn);
-        issued = t + 1;
+        mbar_expect_tx(afull(s), kTileBytes);
+        tma_load_2d(base + s * kTileBytes, &tA, afull(s), t * K + kb * 128, bm);
+        a_issued = i + 1;
       }
     }
     // Before leaving, make sure none of this CTA's copies is still in flight.
-    const int first = issued > kI8Stages ? issued - kI8Stages : 0;
-    for (int q = first; q < issued; ++q)
-      mbar_wait(full_bar(q % kI8Stages), (uint32_t)(q / kI8Stages) & 1u);
+    for (int i = a_issued > kI8AStages ? a_issued - kI8AStages : 0; i < a_issued; ++i)
+      mbar_wait(afull(i % kI8AStages), (uint32_t)(i / kI8AStages) & 1u);
+    for (int q = b_issued > 2 ? b_issued - 2 : 0; q < b_issued; ++q)
+      mbar_wait(bfull(q & 1), (uint32_t)(q >> 1) & 1u);
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer: class c into the accumulator at column 64 c -------------
-    int t = 0;
+    // ---- MMA issuer: A slice t (value 2^-7(t+1)) x B slice u into class t + u --
     bool ok = true;
-    for (int c = 0; c < kI8Slices && ok; ++c) {
-      for (int kb = 0; kb < (c + 1) * KB; ++kb, ++t) {
-        const int s = t % kI8Stages;
-        const uint32_t ph = (uint32_t)(t / kI8Stages) & 1u;
-        if (!mbar_wait(full_bar(s), ph) || *abort_flag) {
+    for (int kb = 0; kb < KB && ok; ++kb) {
+      const int j = kb & 1;
+      if (!mbar_wait(bfull(j), (uint32_t)(kb >> 1) & 1u) || *abort_flag) {
+        *abort_flag = 1u;
+        atomicOr(err, 2u);
+        break;
+      }
+      const uint32_t bb = bbuf0 + j * kI8BBuf;
+      for (int t = 0; t < kI8Slices; ++t) {
+        const int i = kb * kI8Slices + t;
+        const int s = i % kI8AStages;
+        if (!mbar_wait(afull(s), (uint32_t)(i / kI8AStages) & 1u) || *abort_flag) {
           *abort_flag = 1u;
           atomicOr(err, 2u);
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t st = base + s * kI8StageBytes;
-        const uint64_t a = umma_desc(st), b = umma_desc(st + kTileBytes);
+        const uint64_t a = umma_desc(base + s * kTileBytes);
+        for (int u = 0; u < kI8Slices - t; ++u) {
+          const uint64_t b = umma_desc(bb + (kI8Slices - 1 - u) * kI8BTile);
+          const uint32_t acc_col = (uint32_t)(kI8BN * (t + u));
 #pragma unroll
-        for (int k = 0; k < 4; ++k)  // 32 bytes of K per instruction
-          umma_i8(tmem + (uint32_t)(kI8BN * c), a + 2u * k, b + 2u * k, kI8Idesc,
-                  (kb > 0 || k > 0) ? 1u : 0u);
-        umma_commit(empty_bar(s));
+          for (int k = 0; k < 4; ++k)  // 32 bytes of K per instruction
+            umma_i8(tmem + acc_col, a + 2u * k, b + 2u * k, kI8Idesc,
+                    (kb > 0 || t > 0 || k > 0) ? 1u : 0u);
+        }
+        umma_commit(aempty(s));
       }
+      if (ok) umma_commit(bempty(j));
     }
     umma_commit(done_bar);
   }
@@ -444,21 +481,21 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
     for (int c0 = 0; c0 < kI8BN; c0 += 32) {
       double acc[32];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+      for (int jj = 0; jj < 32; ++jj) acc[jj] = 0.0;
 #pragma unroll 1
       for (int c = 0; c < kI8Slices; ++c) {
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kI8BN * c + c0), v);
         const double wgt = ldexp(1.0, -7 * (c + 2));
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[j] += (double)(int32_t)v[j] * wgt;
+        for (int jj = 0; jj < 32; ++jj) acc[jj] += (double)(int32_t)v[jj] * wgt;
       }
       const size_t o = (size_t)r * G + bn + c0;
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        float x = (float)(acc[j] * sr * (double)sb[bn + c0 + j]);
-        if (S) x *= S[o + j];
-        D[o + j] = x;
+      for (int jj = 0; jj < 32; ++jj) {
+        float x = (float)(acc[jj] * sr * (double)sb[bn + c0 + jj]);
+        if (S) x *= S[o + jj];
+        D[o + jj] = x;
       }
     }
   }
