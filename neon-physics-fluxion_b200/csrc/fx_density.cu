@@ -179,7 +179,7 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
   // of 256 (tiles of 128 on each half). Not for 3xTF32: rows G-1-i come out
   // as E - O, and that difference magnifies the tensor cores' accumulation
   // error (2.1e-4 instead of 5e-5 at G = 256).
-  w.halves = G % 256 == 0 && precision != FX_DCT_FP32 && precision != FX_DCT_I8;
+  w.halves = G % 256 == 0 && precision != FX_DCT_FP32;
   {
     int sp = precision == FX_DCT_SIMT ? sgemm_splits(G, d->ctx->num_sms) : 1;
     if (w.halves && precision == FX_DCT_SIMT) sp = std::max(sp, half_splits(G, d->ctx->num_sms));
@@ -262,41 +262,48 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
       ie[(size_t)ky * G + kx] = (kx == 0 && ky == 0) ? 0.0f : (float)(-1.0 / lam);
     }
   FX_CHECK_CUDA(cudaMemcpyAsync(w.inv_eig.p, ie.data(), cells * 4, cudaMemcpyHostToDevice, s));
-  if (precision == FX_DCT_I8) {
-    // the operators' 8-bit slices, cut from their FP64 values (7 bits of
-    // each row's scale per slice), in the order [s1 ..] along NS G columns
+  // FX_DCT_I8: the operators' 8-bit slices, cut from their FP64 values (7
+  // bits of each row's scale per slice), in the order [s1 ..] along NS K
+  // columns, for rows x K operators (the full G x G ones, or the 2 x (G/2) x
+  // (G/2) half operators below)
+  auto slice_op = [&](const std::vector<double> &m, int rows, int K, int o) -> int {
     const int NS = i8_slices();
-    const std::vector<double> *ops[4] = {&c, &ct, &dx, &dy};
-    std::vector<int8_t> sl((size_t)NS * cells);
-    std::vector<float> sc(G);
-    for (int o = 0; o < 4; ++o) {
-      const std::vector<double> &m = *ops[o];
-      for (int i = 0; i < G; ++i) {
-        double mx = 0.0;
-        for (int k = 0; k < G; ++k) mx = std::max(mx, std::fabs(m[(size_t)i * G + k]));
-        int e = 0;
-        if (mx > 0.0) std::frexp(mx, &e);
-        sc[i] = std::ldexp(1.0f, e);
-        for (int k = 0; k < G; ++k) {
-          double a = std::ldexp(m[(size_t)i * G + k], -e);
-          for (int t = 0; t < NS; ++t) {
-            const double q = a * 128.0;
-            const double tr = std::trunc(q);
-            sl[(size_t)i * NS * G + (size_t)t * G + k] = (int8_t)tr;
-            a = q - tr;
-          }
+    std::vector<int8_t> sl((size_t)NS * rows * K);
+    std::vector<float> sc(rows);
+    for (int i = 0; i < rows; ++i) {
+      double mx = 0.0;
+      for (int k = 0; k < K; ++k) mx = std::max(mx, std::fabs(m[(size_t)i * K + k]));
+      int e = 0;
+      if (mx > 0.0) std::frexp(mx, &e);
+      sc[i] = std::ldexp(1.0f, e);
+      for (int k = 0; k < K; ++k) {
+        double a = std::ldexp(m[(size_t)i * K + k], -e);
+        for (int t = 0; t < NS; ++t) {
+          const double q = a * 128.0;
+          const double tr = std::trunc(q);
+          sl[(size_t)i * NS * K + (size_t)t * K + k] = (int8_t)tr;
+          a = q - tr;
         }
       }
-      FX_TRY(w.op8[o].alloc((size_t)NS * cells));
-      FX_TRY(w.op_sc[o].alloc(G));
-      FX_CHECK_CUDA(cudaMemcpyAsync(w.op8[o].p, sl.data(), sl.size(), cudaMemcpyHostToDevice, s));
-      FX_CHECK_CUDA(cudaMemcpyAsync(w.op_sc[o].p, sc.data(), (size_t)G * 4,
-                                    cudaMemcpyHostToDevice, s));
-      FX_CHECK_CUDA(cudaStreamSynchronize(s));  // sl and sc are reused
     }
-    for (int i = 0; i < 2; ++i) {
-      FX_TRY(w.d8[i].alloc((size_t)NS * cells));
-      FX_TRY(w.d_sc[i].alloc(G));
+    FX_TRY(w.op8[o].alloc(sl.size()));
+    FX_TRY(w.op_sc[o].alloc(rows));
+    FX_CHECK_CUDA(cudaMemcpyAsync(w.op8[o].p, sl.data(), sl.size(), cudaMemcpyHostToDevice, s));
+    FX_CHECK_CUDA(cudaMemcpyAsync(w.op_sc[o].p, sc.data(), (size_t)rows * 4,
+                                  cudaMemcpyHostToDevice, s));
+    FX_CHECK_CUDA(cudaStreamSynchronize(s));  // sl and sc go out of scope
+    return FX_OK;
+  };
+  if (precision == FX_DCT_I8) {
+    for (int i = 0; i < 2; ++i) {  // data slices: G x NS G (or 2G x NS G/2)
+      FX_TRY(w.d8[i].alloc((size_t)i8_slices() * cells));
+      FX_TRY(w.d_sc[i].alloc(2 * (size_t)G));
+    }
+    if (!w.halves) {
+      FX_TRY(slice_op(c, G, G, 0));
+      FX_TRY(slice_op(ct, G, G, 1));
+      FX_TRY(slice_op(dx, G, G, 2));
+      FX_TRY(slice_op(dy, G, G, 3));
     }
   }
   FX_TRY(upload_operand(c, precision, w.cmat.p, split ? w.cmat_lo.p : nullptr,
@@ -333,6 +340,12 @@ static int dens_setup(fx_design *d, int G, int precision, cudaStream_t s) {
                           bf_fmt ? w.dx_h_bf.p : nullptr, s));
     FX_TRY(upload_operand(dyh, precision, w.dy_h.p, split_fmt ? w.dy_h_lo.p : nullptr,
                           bf_fmt ? w.dy_h_bf.p : nullptr, s));
+    if (precision == FX_DCT_I8) {  // the two halves of each, as 2h rows of h
+      FX_TRY(slice_op(chh, 2 * h, h, 0));
+      FX_TRY(slice_op(cth, 2 * h, h, 1));
+      FX_TRY(slice_op(dxh, 2 * h, h, 2));
+      FX_TRY(slice_op(dyh, 2 * h, h, 3));
+    }
   }
   FX_CHECK_CUDA(cudaMemsetAsync(w.area_fx.p, 0, cells * 8, s));
   FX_CHECK_CUDA(cudaMemsetAsync(w.energy.p, 0, (4096 + 8) * 8, s));
@@ -388,7 +401,7 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   float *WS = precision == FX_DCT_SIMT ? w.split_ws.p : nullptr;
-  if (precision == FX_DCT_I8) {
+  if (precision == FX_DCT_I8 && !w.halves) {
     // the same seven products; each data operand is sliced once and kept
     // while later products read it (phat and T3 twice)
     float *rho = w.buf[0].p, *t1 = w.buf[1].p, *phat = w.buf[2].p, *t3 = w.buf[1].p;
@@ -436,6 +449,29 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
     float *rho = w.buf[0].p, *t1 = w.buf[1].p, *phat = w.buf[2].p, *t3 = w.buf[1].p;
     float *t4 = w.buf[4].p, *phi = w.buf[3].p;
     float *P = w.split_ws.p;
+    if (precision == FX_DCT_I8) {
+      // the same products from 8-bit slices; each folded or split operand
+      // is sliced by its product (into d8[0] / d_sc[0])
+      auto hm = [&](int op, int i, int mode, float sign, const float *S, float *D) {
+        return gemm_half_i8(ctx, G, w.op8[op].p, w.op_sc[op].p, w.hw[i].p, mode, sign, S, D, P,
+                            w.d8[0].p, w.d_sc[0].p, s);
+      };
+      fold(rho, H(0));
+      FX_TRY(hm(0, 0, kHalfRows, 1.f, nullptr, t1));
+      fold(t1, H(0));
+      FX_TRY(hm(0, 0, kHalfRows, 1.f, w.inv_eig.p, phat));
+      split_k(phat, H(1));
+      FX_TRY(hm(1, 1, kHalfPair, 1.f, nullptr, t3));
+      split_k(t3, H(2));
+      FX_TRY(hm(3, 2, kHalfPair, -1.f, nullptr, w.ey.p));
+      if (need_phi) FX_TRY(hm(1, 2, kHalfPair, 1.f, nullptr, phi));
+      FX_TRY(hm(2, 1, kHalfPair, -1.f, nullptr, t4));
+      split_k(t4, H(0));
+      FX_TRY(hm(1, 0, kHalfPair, 1.f, nullptr, w.ex.p));
+      FX_CHECK_LAUNCH();
+      timer_end(ctx, FX_STAGE_DENSITY, s, ev);
+      return FX_OK;
+    }
     fold(rho, H(0));
     FX_TRY(gemm_half(ctx, precision, G, Ch, H(0), kHalfRows, 1.f, nullptr, t1, P, s));
     fold(t1, H(0));

@@ -257,6 +257,18 @@ int gemm_half(fx_ctx *ctx, int precision, int G, const GemmOperands &Ah,
   return FX_OK;
 }
 
+int gemm_half_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const float *Bh,
+                 int mode, float sign, const float *S, float *D, float *part, int8_t *b8,
+                 float *bsc, cudaStream_t s) {
+  FX_TRY(i8_slice(ctx, Bh, 2 * G, G / 2, b8, bsc, s));
+  FX_TRY(gemm_half_i8_tc(ctx, G, A8, sa, b8, bsc, part, s));
+  sgemm_half_reduce_kernel<<<ctx->num_sms * 8, 256, 0, s>>>(part, 1, G, mode, sign, S, D,
+                                                            nullptr, nullptr);
+  FX_CHECK_LAUNCH();
+  ctx->launches += 1;
+  return FX_OK;
+}
+
 int gemm_nt(fx_ctx *ctx, int precision, int G, const GemmOperands &A,
             const GemmOperands &B, const float *S, const GemmOperands &D,
             cudaStream_t s, float *split_ws) {

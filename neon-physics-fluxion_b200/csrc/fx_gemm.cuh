@@ -89,5 +89,13 @@ int gemm_nt_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8
                const float *sb, const float *S, float *D, cudaStream_t s);
 int i8_slice(fx_ctx *ctx, const float *X, int rows, int K, int8_t *out, float *scale,
              cudaStream_t s);
+int gemm_half_i8_tc(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8_t *B8,
+                    const float *sb, float *part, cudaStream_t s);
+// gemm_half for FX_DCT_I8: slices Bh (2G x G/2 f32) into b8 / bsc, then the
+// two half products from the operator halves' slices (A8, sa) and the
+// placing reduce (mode, sign, S as gemm_half).
+int gemm_half_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const float *Bh,
+                 int mode, float sign, const float *S, float *D, float *part, int8_t *b8,
+                 float *bsc, cudaStream_t s);
 
 }  // namespace fx

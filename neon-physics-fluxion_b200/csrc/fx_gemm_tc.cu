@@ -333,9 +333,13 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem, uint64_t a, uint64_t b, u
       "l"(a), "l"(b), "r"(idesc), "r"(accum));
 }
 
+// Batch z (blockIdx.z; the even/odd half products) reads A rows from
+// z a_rows, B rows from z b_rows and writes D from z d_elems on; D has G
+// columns.
 __global__ void __launch_bounds__(kTcThreads, 1)
 tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
-             int G, int K, const float *__restrict__ sa, const float *__restrict__ sb,
+             int G, int K, int a_rows, int b_rows, size_t d_elems,
+             const float *__restrict__ sa, const float *__restrict__ sb,
              const float *__restrict__ S, float *__restrict__ D, unsigned int *__restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -357,6 +361,8 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
   volatile uint32_t *abort_flag = (volatile uint32_t *)(gen_base + (abort_slot - base));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int bm = blockIdx.y * kTcBM, bn = blockIdx.x * kI8BN;
+  const int am = bm + (int)blockIdx.z * a_rows, bnz = bn + (int)blockIdx.z * b_rows;
+  D += (size_t)blockIdx.z * d_elems;
   const int KB = K / 128;  // 128-byte blocks of one slice
 
   if (threadIdx.x == 0) {
@@ -399,7 +405,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
       const uint32_t bb = bbuf0 + j * kI8BBuf;
       mbar_expect_tx(bfull(j), kI8BBuf);
       for (int v = 0; v < kI8Slices; ++v)  // B layout position v holds slice 6 - v
-        tma_load_2d(bb + v * kI8BTile, &tB, bfull(j), v * K + kb * 128, bn);
+        tma_load_2d(bb + v * kI8BTile, &tB, bfull(j), v * K + kb * 128, bnz);
       b_issued = kb + 1;
       for (int t = 0; t < kI8Slices; ++t) {
         const int i = kb * kI8Slices + t;
@@ -416,7 +422,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
           break;
         }
         mbar_expect_tx(afull(s), kTileBytes);
-        tma_load_2d(base + s * kTileBytes, &tA, afull(s), t * K + kb * 128, bm);
+        tma_load_2d(base + s * kTileBytes, &tA, afull(s), t * K + kb * 128, am);
         a_issued = i + 1;
       }
     }
@@ -476,7 +482,8 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
   tc_fence_after();
   if (go) {
     const int r = bm + warp * 32 + lane;
-    const double sr = (double)sa[r];
+    const double sr = (double)sa[am + warp * 32 + lane];
+    const float *sbz = sb + (size_t)blockIdx.z * b_rows;
 #pragma unroll 1
     for (int c0 = 0; c0 < kI8BN; c0 += 32) {
       double acc[32];
@@ -493,7 +500,7 @@ tc_i8_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUt
       const size_t o = (size_t)r * G + bn + c0;
 #pragma unroll
       for (int jj = 0; jj < 32; ++jj) {
-        float x = (float)(acc[jj] * sr * (double)sb[bn + c0 + jj]);
+        float x = (float)(acc[jj] * sr * (double)sbz[bn + c0 + jj]);
         if (S) x *= S[o + jj];
         D[o + jj] = x;
       }
@@ -707,7 +714,31 @@ int gemm_nt_i8(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8
   FX_TRY(get_map(B8, kI8Slices * G, G, 1, &tb, kI8BN));
   FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(tc_i8_kernel), kI8Smem));
   dim3 grid(G / kI8BN, G / kTcBM);
-  tc_i8_kernel<<<grid, kTcThreads, kI8Smem, s>>>(ta, tb, G, G, sa, sb, S, D, ctx->tc_err);
+  tc_i8_kernel<<<grid, kTcThreads, kI8Smem, s>>>(ta, tb, G, G, 0, 0, 0, sa, sb, S, D,
+                                                 ctx->tc_err);
+  FX_CHECK_LAUNCH();
+  ctx->launches += 1;
+  return FX_OK;
+}
+
+// The even/odd halves (G a multiple of 256, h = G / 2): two products
+// part[z] (h x G) = A_z (h x h) B_z^T (G x h) in one launch, from A8
+// (2h x 6h: the two operator halves' slices) and B8 (2G x 6h: the two halves
+// of the folded or split data operand), as raw f32 partials.
+int gemm_half_i8_tc(fx_ctx *ctx, int G, const int8_t *A8, const float *sa, const int8_t *B8,
+                    const float *sb, float *part, cudaStream_t s) {
+  const int h = G / 2;
+  if (G % 256 != 0 || G > 8192) {
+    set_error("gemm_half_i8: G = %d must be a multiple of 256 up to 8192", G);
+    return FX_EINVAL;
+  }
+  CUtensorMap ta, tb;
+  FX_TRY(get_map(A8, kI8Slices * h, 2 * h, 1, &ta));
+  FX_TRY(get_map(B8, kI8Slices * h, 2 * G, 1, &tb, kI8BN));
+  FX_TRY(raise_smem_limit(reinterpret_cast<const void *>(tc_i8_kernel), kI8Smem));
+  dim3 grid(G / kI8BN, h / kTcBM, 2);
+  tc_i8_kernel<<<grid, kTcThreads, kI8Smem, s>>>(ta, tb, G, h, h, G, (size_t)h * G, sa, sb,
+                                                 nullptr, part, ctx->tc_err);
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   return FX_OK;
