@@ -58,7 +58,7 @@ def parse(argv=None):
     ap.add_argument("--die", type=float, default=1200.0)
     ap.add_argument("--bins", type=int, default=1024)
     ap.add_argument("--cong", type=int, default=512)
-    ap.add_argument("--precision", default="fp32",
+    ap.add_argument("--precision", default="i8",
                     choices=["fp32", "3xtf32", "tf32", "bf16", "simt", "i8"],
                     help="DCT GEMMs: fp32 (= simt, CUDA cores), 3xtf32, tf32, bf16 (tensor cores)")
     ap.add_argument("--seed", type=int, default=42)
@@ -526,21 +526,28 @@ def run_fluxion(args, rank, world, local_rank):
     if "density" in per_iter:
         fl = f_alg["density"] * 6 / 4  # six GEMMs per step (no potential)
         d_tf = fl / (per_iter["density"] * 1e-3) / 1e12
-        if PREC[args.precision] == 3:
+        code = PREC[args.precision]
+        halves = code != 0 and args.bins % 256 == 0  # the even/odd half products
+        executed = d_tf / 2 if halves else d_tf
+        if code == 3:
             pk, ps = 148 * 128 * 2 * 1.965e9 / 1e12, "nominal FP32 CUDA cores 148 x 128 x 2 x 1.965 GHz"
+            bound, unit = "fp32-pipe", "TFLOP/s"
+        elif code == 4:
+            # 21 slice-pair int8 products per GEMM; int8 dense = twice the bf16 rate
+            executed *= 21
+            pk, ps = 2 * bf16, f"{src} bf16 dense x 2 (int8)"
+            bound, unit = "tensor (int8)", "TOPS"
         else:
             pk = bf16 if args.precision == "bf16" else bf16 / 2
             ps = f"{src} bf16 dense" + ("" if args.precision == "bf16" else " / 2 (tf32)")
-        halves = PREC[args.precision] == 3 and args.bins % 256 == 0
-        dens_roof = {"bound": "fp32-pipe" if PREC[args.precision] == 3 else "tensor",
-                     "achieved": d_tf, "peak": pk, "unit": "TFLOP/s", "frac": d_tf / pk,
+            bound, unit = "tensor", "TFLOP/s"
+        dens_roof = {"bound": bound, "algorithmic_tflops": d_tf, "executed": executed,
+                     "unit_executed": unit, "peak": pk, "frac": executed / pk,
                      "peak_source": ps,
                      "flops": "algorithmic: the dense GEMM form, 6 x 2 G^3 per step",
-                     "executed_tflops": d_tf / 2 if halves else d_tf,
-                     "note": ("the CUDA-core path splits each GEMM in two half-size ones by the "
-                              "DCT's even/odd symmetry (half the executed flops); " if halves
-                              else "") + "side stream, overlapped with Barnes-Hut: its span "
-                                         "includes time it yields"}
+                     "note": ("split in two half-size products by the DCT's even/odd symmetry; "
+                              if halves else "") + "side stream, overlapped with Barnes-Hut: its "
+                                                   "span includes time it yields"}
     B_iter = sum(b_alg.values())
     it_ms = ms_max / args.steps
 
@@ -1001,10 +1008,10 @@ def run_precision(args, rank, world, local_rank):
             ms = ctx.stage_times()["density"][0] / reps
             # executed: the even/odd half GEMMs (G a multiple of 256, not
             # 3xTF32) do G^3 each instead of 2 G^3; 3xTF32 runs three MMAs
-            # (FX_DCT_I8: full GEMMs, ten 8-bit slice products each, int8 ops)
-            halves = G % 256 == 0 and code not in (fx.FX_DCT_FP32, fx.FX_DCT_I8)
+            # (FX_DCT_I8: 21 8-bit slice-pair products per GEMM, int8 ops)
+            halves = G % 256 == 0 and code != fx.FX_DCT_FP32
             flops = 6 * (1.0 if halves else 2.0) * G ** 3 * (
-                3 if code == fx.FX_DCT_FP32 else 10 if code == fx.FX_DCT_I8 else 1)
+                3 if code == fx.FX_DCT_FP32 else 21 if code == fx.FX_DCT_I8 else 1)
             fld = float(np.sqrt((np.linalg.norm(out["ex"] - ref["ex"]) ** 2 +
                                  np.linalg.norm(out["ey"] - ref["ey"]) ** 2) /
                                 (np.linalg.norm(ref["ex"]) ** 2 + np.linalg.norm(ref["ey"]) ** 2)))

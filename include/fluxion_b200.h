@@ -252,12 +252,12 @@ typedef struct fx_iter_cfg {
                        /* FP32 inputs, not FP32 accuracy                     */
 #define FX_DCT_TF32  1 /* single-pass TF32 inputs, FP32 accumulate           */
 #define FX_DCT_BF16  2 /* BF16 inputs, FP32 accumulate                       */
-#define FX_DCT_SIMT  3 /* FP32 CUDA-core GEMM (no tensor cores): the FP32-    */
-                       /* accurate solve, the iteration's default            */
+#define FX_DCT_SIMT  3 /* FP32 CUDA-core GEMM (no tensor cores)              */
 #define FX_DCT_I8    4 /* tensor cores, FP32-accurate: each operand row split */
                        /* into six exact 8-bit slices under a power-of-two    */
                        /* scale, slice products accumulated exactly in int32  */
-                       /* (tcgen05 kind::i8), classes combined in FP64        */
+                       /* (tcgen05 kind::i8), classes combined in FP64: the   */
+                       /* iteration's default                                  */
 
 typedef struct fx_iter_stats {
   double hpwl;            /* FP64 HPWL after the last iteration              */

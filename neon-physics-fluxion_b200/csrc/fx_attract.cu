@@ -278,7 +278,7 @@ extern "C" int fx_iter_cfg_default(fx_iter_cfg *c) {
   c->density_weight = 1.0e-4f;
   c->target_density = 0.7f;
   c->density_bins = 1024;
-  c->dct_precision = FX_DCT_SIMT;  // FP32-accurate; on the second stream
+  c->dct_precision = FX_DCT_I8;  // FP32-accurate on the tensor cores; second stream
   c->cong_cols = 512;
   c->cong_rows = 512;
   c->damping = 0.9f;
