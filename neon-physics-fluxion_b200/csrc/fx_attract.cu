@@ -336,20 +336,36 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   if (use_dens)
     FX_TRY(density_scatter(ctx, d, d->x[d->cur].p, d->y[d->cur].p, G,
                            c.dct_precision, s));
+  if (use_cong) FX_TRY(congestion_alloc(d, c.cong_cols, c.cong_rows, s));
   const int nb = (d->n + kGates - 1) / kGates;
   bool copied_out = false;  // positions already on their way to x, y
+  // The congestion of the positions a step writes only feeds the statistics
+  // (the last step's are returned), so it runs at the start of the next
+  // step on the second stream, beside that step's Barnes-Hut chain; the last
+  // step runs its own on the primary stream. Same kernels, inputs and order
+  // on the scratch as running each right after its step.
+  bool cong_pending = false;
   // One iteration; `last` adds the potential (energy statistic).
   auto step = [&](bool last) -> int {
     // The Barnes-Hut chain (the critical path) is issued first, so the GPU
-    // starts it while the host still issues the density solve; the density
-    // forks from the same point of the primary stream and runs beside it.
-    if (use_dens) FX_CHECK_CUDA(cudaEventRecord(ctx->fork, s));
+    // starts it while the host still issues the side work; the previous
+    // step's congestion and the density solve fork from the same point of
+    // the primary stream and run beside it, joined before the step kernel
+    // (which writes the other position buffer).
+    const bool side = use_dens || cong_pending;
+    if (side) FX_CHECK_CUDA(cudaEventRecord(ctx->fork, s));
     if (use_bh) FX_TRY(bh_run(ctx, d, c.repel_weight, c.theta, c.min_dist, c.bh_walk, s));
-    if (use_dens) {
+    if (side) {
       FX_CHECK_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
+      if (cong_pending) {
+        FX_TRY(congestion_run(ctx, d, d->x[d->cur].p, d->y[d->cur].p, c.cong_cols,
+                              c.cong_rows, s2));
+        cong_pending = false;
+      }
       // the potential only feeds the energy statistic of the last step
-      FX_TRY(density_run(ctx, d, G, c.target_density, c.density_weight,
-                         c.dct_precision, last, s2));
+      if (use_dens)
+        FX_TRY(density_run(ctx, d, G, c.target_density, c.density_weight,
+                           c.dct_precision, last, s2));
       FX_CHECK_CUDA(cudaEventRecord(ctx->join, s2));
       FX_CHECK_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
     }
@@ -407,10 +423,14 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
       FX_CHECK_CUDA(cudaMemcpyAsync(y, d->y[d->cur].p, bytes, cudaMemcpyDeviceToHost, s2));
       copied_out = true;
     }
-    if (use_cong)
-      FX_TRY(congestion_run(ctx, d, d->x[d->cur].p, d->y[d->cur].p, c.cong_cols,
-                            c.cong_rows, s));
-      return FX_OK;
+    if (use_cong) {
+      if (last)
+        FX_TRY(congestion_run(ctx, d, d->x[d->cur].p, d->y[d->cur].p, c.cong_cols,
+                              c.cong_rows, s));
+      else
+        cong_pending = true;
+    }
+    return FX_OK;
   };
   // Long runs replay a CUDA graph of two iterations (one per ping-pong
   // parity) after an eager first iteration has sized every buffer; the last
@@ -421,6 +441,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     FX_TRY(step(false));
     ++it;
     const int cur0 = d->cur;
+    const bool pending0 = cong_pending;
     const int64_t l0 = ctx->launches;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -435,6 +456,8 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     }
     cudaGetLastError();  // a failed capture leaves an error: fall back to eager
     d->cur = cur0;
+    // a pair of steps leaves a congestion pending exactly as it found one
+    cong_pending = pending0;
     const int64_t per_pair = ctx->launches - l0;
     ctx->launches = l0;
     if (exec) {

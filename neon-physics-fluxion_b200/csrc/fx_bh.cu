@@ -407,6 +407,11 @@ int radix_sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
 constexpr uint32_t kOsAgg = 1u << 30, kOsInc = 2u << 30, kOsVal = (1u << 30) - 1u;
 constexpr uint32_t kOsSpin = 1u << 22;
 constexpr int kOsWin = 16;  // earlier tiles read per look-back step
+// 4096-key tiles: the look-back chain (one round trip per kOsWin tiles
+// whose predecessors have not finished) is half as long as with 2048.
+constexpr int kOsItems = 16;
+constexpr int kOsTile = kSortThreads * kOsItems;
+static int os_tiles(int n) { return (n + kOsTile - 1) / kOsTile; }
 
 __global__ void __launch_bounds__(kSortThreads)
 os_hist_kernel(const uint32_t *__restrict__ keys, int n, int passes,
@@ -425,7 +430,7 @@ os_hist_kernel(const uint32_t *__restrict__ keys, int n, int passes,
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 3)
 os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin,
                uint32_t *__restrict__ kout, int32_t *__restrict__ iout, int n, int shift,
                const uint32_t *__restrict__ hist, uint32_t *__restrict__ status,
@@ -436,8 +441,8 @@ os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin
   __shared__ uint32_t cnt[kWarps][256];
   __shared__ uint32_t tstart[256], gbase[256], ws[kWarps];
   __shared__ int tile_s;
-  __shared__ uint32_t sk[kSortTile];
-  __shared__ int32_t sv[kSortTile];
+  __shared__ uint32_t sk[kOsTile];
+  __shared__ int32_t sv[kOsTile];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   if (t == 0) tile_s = (int)atomicAdd(ticket, 1u);
   for (int i = t; i < kWarps * 256; i += kSortThreads) (&cnt[0][0])[i] = 0;
@@ -461,13 +466,13 @@ os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin
   }
   // stable ranks within the tile: per warp by __match_any_sync, then warps
   // in order (as radix_scatter_kernel)
-  const int base = tile * kSortTile + w * (32 * kSortItems);
+  const int base = tile * kOsTile + w * (32 * kOsItems);
   const unsigned lt_mask = (1u << lane) - 1u;
-  uint32_t k[kSortItems];
-  int32_t v[kSortItems];
-  uint32_t rank[kSortItems];
+  uint32_t k[kOsItems];
+  int32_t v[kOsItems];
+  uint32_t rank[kOsItems];
 #pragma unroll
-  for (int r = 0; r < kSortItems; ++r) {
+  for (int r = 0; r < kOsItems; ++r) {
     const int i = base + r * 32 + lane;
     const bool valid = i < n;
     k[r] = valid ? kin[i] : 0u;
@@ -555,7 +560,7 @@ os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin
   __syncthreads();
   // stage the tile in sorted order, then write it out coalesced
 #pragma unroll
-  for (int r = 0; r < kSortItems; ++r) {
+  for (int r = 0; r < kOsItems; ++r) {
     const int i = base + r * 32 + lane;
     if (i < n) {
       const uint32_t dg = (k[r] >> shift) & 255u;
@@ -565,7 +570,7 @@ os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin
     }
   }
   __syncthreads();
-  const int m = min(kSortTile, n - tile * kSortTile);
+  const int m = min(kOsTile, n - tile * kOsTile);
   for (int j = t; j < m; j += kSortThreads) {
     const uint32_t key = sk[j];
     const uint32_t pos = gbase[(key >> shift) & 255u] + (uint32_t)j;
@@ -582,7 +587,7 @@ os_pass_kernel(const uint32_t *__restrict__ kin, const int32_t *__restrict__ iin
 // (k[passes & 1], v[passes & 1]). Workspace `ws`: os_sort_words(n, passes)
 // words, cleared here.
 size_t os_sort_words(int n, int passes) {
-  return (size_t)passes * 256 + (size_t)passes * radix_sort_tiles(n) * 256 + 4;
+  return (size_t)passes * 256 + (size_t)passes * os_tiles(n) * 256 + 4;
 }
 
 int radix_sort_onesweep(uint32_t *k[2], int32_t *v[2], int n, int passes, uint32_t *ws,
@@ -593,7 +598,7 @@ int radix_sort_onesweep(uint32_t *k[2], int32_t *v[2], int n, int passes, uint32
     set_error("radix_sort_onesweep: %d keys / %d passes out of range", n, passes);
     return FX_EINVAL;
   }
-  const int T = radix_sort_tiles(n);
+  const int T = os_tiles(n);
   uint32_t *hist = ws, *status = ws + passes * 256,
            *ticket = status + (size_t)passes * T * 256;
   FX_CHECK_CUDA(cudaMemsetAsync(ws, 0, os_sort_words(n, passes) * 4, s));

@@ -180,8 +180,7 @@ cong_scan_cols_kernel(int32_t *__restrict__ diff, uint32_t *__restrict__ counts,
   }
 }
 
-int congestion_run(fx_ctx *ctx, fx_design *d, const float *dx,
-                   const float *dy, int cols, int rows, cudaStream_t s) {
+int congestion_alloc(fx_design *d, int cols, int rows, cudaStream_t s) {
   CongWork &w = d->cong;
   if ((int64_t)(cols + 1) * (rows + 1) > (int64_t)INT32_MAX) {  // corner indexes are 31-bit
     set_error("congestion grid %d x %d too large", cols, rows);
@@ -201,6 +200,13 @@ int congestion_run(fx_ctx *ctx, fx_design *d, const float *dx,
     w.cols = cols;
     w.rows = rows;
   }
+  return FX_OK;
+}
+
+int congestion_run(fx_ctx *ctx, fx_design *d, const float *dx,
+                   const float *dy, int cols, int rows, cudaStream_t s) {
+  CongWork &w = d->cong;
+  FX_TRY(congestion_alloc(d, cols, rows, s));
   // RoutingGrid::new (grid.rs:27-31): f32 cell size and capacity.
   const float cw = d->chip_w / (float)cols;
   const float ch = d->chip_h / (float)rows;

@@ -315,6 +315,10 @@ struct fx_design {
 
 namespace fx {
 // stage launchers (return FX_* codes), all on ctx->stream unless noted.
+// Sizes the congestion scratch for a cols x rows grid (zeroed on s); a no-op
+// when it already fits. congestion_run calls it; callers that capture the
+// run into a CUDA graph call it first, outside the capture.
+int congestion_alloc(fx_design *d, int cols, int rows, cudaStream_t s);
 int congestion_run(fx_ctx *ctx, fx_design *d, const float *dx, const float *dy,
                    int cols, int rows, cudaStream_t s);
 int attraction_run(fx_ctx *ctx, fx_design *d, float k, float2 *out, cudaStream_t s);
