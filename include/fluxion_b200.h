@@ -468,7 +468,8 @@ typedef struct fx_job_desc {
   const fx_part_cfg *part;  /* stage configurations; NULL = defaults (ECO: the     */
   const fx_leaf_cfg *leaf;  /* iteration default with a G x G density grid, G the  */
   const fx_refine_cfg *refine; /* multiple of 128 nearest sqrt(n) in [128, 1024],  */
-  const fx_iter_cfg *iter;  /* and a 256 x 256 congestion grid)                    */
+  const fx_iter_cfg *iter;  /* FX_DCT_SIMT below G = 1024, and a 256 x 256        */
+                            /* congestion grid)                                    */
 } fx_job_desc;
 typedef struct fx_job_result {
   int64_t job_id, design_id;

@@ -140,6 +140,9 @@ int prepare_job(Job &j, int64_t eco_n) {
     } else {
       fx_iter_cfg_default(&j.iter);
       j.iter.density_bins = eco_bins((int32_t)eco_n);
+      // Below 1024 bins the FP32 CUDA-core products finish sooner than the
+      // int8-slice ones (short K, few tiles); both are FP32-accurate.
+      if (j.iter.density_bins < 1024) j.iter.dct_precision = FX_DCT_SIMT;
       j.iter.cong_cols = 256;
       j.iter.cong_rows = 256;
     }
