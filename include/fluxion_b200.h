@@ -465,10 +465,11 @@ typedef struct fx_job_desc {
   int32_t iterations;       /* ECO: plain iterations after the moves               */
   const int32_t *move_gate;
   const float *move_dx, *move_dy;
-  const fx_part_cfg *part;  /* stage configurations; NULL = defaults (ECO: the     */
-  const fx_leaf_cfg *leaf;  /* iteration default with a G x G density grid, G the  */
-  const fx_refine_cfg *refine; /* multiple of 128 nearest sqrt(n) in [128, 1024],  */
-  const fx_iter_cfg *iter;  /* FX_DCT_SIMT below G = 1024, and a 256 x 256        */
+  const fx_part_cfg *part;  /* stage configurations; NULL = defaults (PLACE: the   */
+  const fx_leaf_cfg *leaf;  /* leaf default with FX_LEAF_FAST; ECO: the iteration  */
+  const fx_refine_cfg *refine; /* default with a G x G density grid, G the         */
+  const fx_iter_cfg *iter;  /* multiple of 128 nearest sqrt(n) in [128, 1024],     */
+                            /* FX_DCT_SIMT below G = 1024, and a 256 x 256         */
                             /* congestion grid)                                    */
 } fx_job_desc;
 typedef struct fx_job_result {

@@ -41,12 +41,25 @@ __device__ __forceinline__ float2 spring_block(const int32_t *__restrict__ adj_p
   const int b = valid ? __ldg(adj_ptr + g) : 0;
   const int e = valid ? __ldg(adj_ptr + g + 1) : 0;
   float ax = 0.f, ay = 0.f;
+  constexpr int kPer = kChunk / kGates;  // staged entries per thread and chunk
   for (int c0 = A0; c0 < A1; c0 += kChunk) {
     const int c1 = min(c0 + kChunk, A1);
-    for (int q = c0 + t; q < c1; q += kGates) {
-      const int j = __ldg(adj_idx + q);
-      sh[q - c0] = make_float2(__ldg(x + j), __ldg(y + j));
+    // all of a thread's index loads, then all of its gathers, so that
+    // 3 x kPer independent loads are in flight instead of a chain per entry
+    int jj[kPer];
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const int q = c0 + t + r * kGates;
+      jj[r] = q < c1 ? __ldg(adj_idx + q) : -1;
     }
+    float2 pv[kPer];
+#pragma unroll
+    for (int r = 0; r < kPer; ++r)
+      pv[r] = jj[r] >= 0 ? make_float2(__ldg(x + jj[r]), __ldg(y + jj[r]))
+                         : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int r = 0; r < kPer; ++r)
+      if (jj[r] >= 0) sh[t + r * kGates] = pv[r];
     __syncthreads();
     const int lo = max(b, c0), hi = min(e, c1);
     for (int q = lo; q < hi; ++q) {

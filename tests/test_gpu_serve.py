@@ -73,7 +73,8 @@ def test_results_are_the_same_alone_and_in_the_mix(fx):
 
 
 def test_place_job_matches_the_direct_calls(fx, ctx):
-    """A PLACE job is fx_partition -> fx_hapr_place_leaves -> fx_refine."""
+    """A PLACE job is fx_partition -> fx_hapr_place_leaves (tolerance-mode
+    forces, the server's default) -> fx_refine."""
     c = _designs(fx)[0]
     sv = fx.Server(slots=2)
     try:
@@ -86,7 +87,7 @@ def test_place_job_matches_the_direct_calls(fx, ctx):
     try:
         t = d.partition()
         lx, ly, _ = d.place_leaves(t["leaf_ptr"], t["leaf_gate"], t["region"].reshape(-1),
-                                   fx.leaf_cfg())
+                                   fx.leaf_cfg(precision=fx.FX_LEAF_FAST))
         st = d.refine(fx.refine_cfg(), lx, ly)
     finally:
         d.close()
