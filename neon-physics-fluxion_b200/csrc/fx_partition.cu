@@ -81,27 +81,128 @@ __global__ void part_init_kernel(int n, const int32_t *__restrict__ perm,
   v[p] = sin_tab[p - beg[c]];
 }
 
+// The depth's induced Laplacians as one CSR in position order: row p lists
+// the positions of p's in-cluster neighbours in adjacency order, so the 30
+// products of a depth read only in-cluster entries, row after row, instead
+// of every adjacency entry through three gathers. Row lengths are the
+// degrees part_init_kernel counted (0 outside the depth's clusters); an
+// exclusive scan gives the row starts.
+constexpr int kScanItems = 8, kScanTile = 256 * kScanItems;
+
+__global__ void __launch_bounds__(256)
+part_scan_tile_kernel(int n, const int32_t *__restrict__ clp, const float *__restrict__ deg,
+                      int32_t *__restrict__ rp, int32_t *__restrict__ tsum) {
+  __shared__ int32_t wsum[8];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int base = blockIdx.x * kScanTile + t * kScanItems;
+  int c[kScanItems];
+  int run = 0;
+#pragma unroll
+  for (int r = 0; r < kScanItems; ++r) {
+    const int p = base + r;
+    c[r] = p < n && clp[p] >= 0 ? (int)deg[p] : 0;
+    run += c[r];
+  }
+  int x = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += u;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  int before = x - run;
+  for (int q = 0; q < w; ++q) before += wsum[q];
+#pragma unroll
+  for (int r = 0; r < kScanItems; ++r) {
+    const int p = base + r;
+    if (p < n) rp[p] = before;
+    before += c[r];
+  }
+  if (t == 255) tsum[blockIdx.x] = before;  // the tile's total
+}
+
+// Exclusive scan of the T tile totals in place (one block); tsum[T] = total.
+__global__ void __launch_bounds__(1024)
+part_scan_top_kernel(int T, int32_t *__restrict__ tsum) {
+  __shared__ int32_t wsum[32];
+  __shared__ int32_t carry_s;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  if (t == 0) carry_s = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < T; b0 += 1024) {
+    const int i = b0 + t;
+    const int v = i < T ? tsum[i] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int y = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) y += u;
+      }
+      wsum[lane] = y;
+    }
+    __syncthreads();
+    const int carry = carry_s;
+    const int excl = carry + (w > 0 ? wsum[w - 1] : 0) + x - v;
+    if (i < T) tsum[i] = excl;
+    __syncthreads();
+    if (t == 1023) carry_s = excl + v;
+    __syncthreads();
+  }
+  if (t == 0) tsum[T] = carry_s;
+}
+
+__global__ void part_scan_add_kernel(int n, int T, const int32_t *__restrict__ tsum,
+                                     int32_t *__restrict__ rp) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) rp[p] += tsum[p / kScanTile];
+  if (p == 0) rp[n] = tsum[T];
+}
+
+__global__ void part_csr_kernel(int n, const int32_t *__restrict__ perm,
+                                const int32_t *__restrict__ pos_of,
+                                const int32_t *__restrict__ adj_ptr,
+                                const int32_t *__restrict__ adj_idx,
+                                const int32_t *__restrict__ clp,
+                                const int32_t *__restrict__ clg,
+                                const int32_t *__restrict__ rp, int32_t *__restrict__ col) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int c = clp[p];
+  if (c < 0) return;
+  const int g = perm[p];
+  int k = rp[p];
+  for (int e = adj_ptr[g]; e < adj_ptr[g + 1]; ++e) {
+    const int j = adj_idx[e];
+    if (clg[j] == c) col[k++] = pos_of[j];
+  }
+}
+
 // lv = deg * v - A v in the reference's f32 order per row: deg*v first,
-// then minus each in-cluster neighbour in adjacency order (:158-165).
-__global__ void part_spmv_kernel(int n, const int32_t *__restrict__ perm,
-                                 const int32_t *__restrict__ pos_of,
-                                 const int32_t *__restrict__ adj_ptr,
-                                 const int32_t *__restrict__ adj_idx,
-                                 const int32_t *__restrict__ clp,
-                                 const int32_t *__restrict__ clg,
-                                 const int32_t *__restrict__ active,
-                                 const float *__restrict__ deg,
-                                 const float *__restrict__ v, float *__restrict__ lv) {
+// then minus each in-cluster neighbour in adjacency order
+// (partitioner.rs:158-165), over the depth's CSR.
+__global__ void part_spmv_csr_kernel(int n, const int32_t *__restrict__ rp,
+                                     const int32_t *__restrict__ col,
+                                     const int32_t *__restrict__ clp,
+                                     const int32_t *__restrict__ active,
+                                     const float *__restrict__ deg,
+                                     const float *__restrict__ v, float *__restrict__ lv) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const int c = clp[p];
   if (c < 0 || !active[c]) return;
-  const int g = perm[p];
   float l = __fmul_rn(deg[p], v[p]);
-  for (int e = adj_ptr[g]; e < adj_ptr[g + 1]; ++e) {
-    const int j = adj_idx[e];
-    if (clg[j] == c) l = __fsub_rn(l, v[pos_of[j]]);
-  }
+  const int e1 = rp[p + 1];
+  for (int e = rp[p]; e < e1; ++e) l = __fsub_rn(l, v[col[e]]);
   lv[p] = l;
 }
 
@@ -453,6 +554,12 @@ extern "C" int fx_partition(fx_ctx *ctx, fx_design *d, const fx_part_cfg *cfg,
     FX_TRY(dt.alloc(256));
     FX_TRY(any.alloc(1));
     const int nb = (N + 255) / 256;
+    // the depth's in-cluster CSR: row starts, tile totals, neighbour positions
+    const int st = (N + kScanTile - 1) / kScanTile;
+    DevBuf<int32_t> rp, tsum, col;
+    FX_TRY(rp.alloc((size_t)N + 1));
+    FX_TRY(tsum.alloc((size_t)st + 1));
+    FX_TRY(col.alloc(std::max<size_t>(d->adj_idx.n, 1)));
     for (int32_t depth = 0; depth < levels; ++depth) {
       // the clusters bisected at this depth, in position order (pre-order
       // lists them left to right within a depth)
@@ -499,6 +606,12 @@ extern "C" int fx_partition(fx_ctx *ctx, fx_design *d, const fx_part_cfg *cfg,
       part_fill_kernel<<<nb, 256, 0, s>>>(N, perm[cur].p, beg.p, end.p, C, clp.p, clg.p);
       part_init_kernel<<<nb, 256, 0, s>>>(N, perm[cur].p, d->adj_ptr.p, d->adj_idx.p, clp.p,
                                           clg.p, beg.p, d_sin.p, deg.p, v.p);
+      part_scan_tile_kernel<<<st, 256, 0, s>>>(N, clp.p, deg.p, rp.p, tsum.p);
+      part_scan_top_kernel<<<1, 1024, 0, s>>>(st, tsum.p);
+      part_scan_add_kernel<<<nb, 256, 0, s>>>(N, st, tsum.p, rp.p);
+      part_csr_kernel<<<nb, 256, 0, s>>>(N, perm[cur].p, pos_of.p, d->adj_ptr.p, d->adj_idx.p,
+                                         clp.p, clg.p, rp.p, col.p);
+      ctx->launches += 4;
       // normalise the start vector (:151-156)
       if (exact) {
         part_seq_kernel<<<C, 32, 0, s>>>(C, beg.p, end.p, v.p, 0, nrm.p);
@@ -513,9 +626,8 @@ extern "C" int fx_partition(fx_ctx *ctx, fx_design *d, const fx_part_cfg *cfg,
       ctx->launches += exact ? 4 : 5;
       int it = 0;
       while (it < cfg->power_iterations) {
-        part_spmv_kernel<<<nb, 256, 0, s>>>(N, perm[cur].p, pos_of.p, d->adj_ptr.p,
-                                            d->adj_idx.p, clp.p, clg.p, act.p, deg.p, v.p,
-                                            lv.p);
+        part_spmv_csr_kernel<<<nb, 256, 0, s>>>(N, rp.p, col.p, clp.p, act.p, deg.p, v.p,
+                                                lv.p);
         ++it;
         if (exact) {
           // deflate and norm in place in lv, then v = lv / norm (v = lv, :182)
