@@ -55,17 +55,34 @@ __global__ void dens_scatter_kernel(const float *__restrict__ x,
 
 // Charge grid rho - rho_target in f32 (and the operand formats the chosen
 // GEMM path reads); re-arms the accumulator.
+// Four consecutive bins per thread: two 16-byte loads in flight per thread
+// and one pass over the grid (a grid-stride loop waited out one DRAM round
+// trip per bin).
 __global__ void dens_charge_kernel(unsigned long long *__restrict__ acc,
                                    int cells, double inv_bin_area,
                                    float target, float *__restrict__ rho,
                                    float *__restrict__ rho_lo,
                                    uint16_t *__restrict__ rho_bf) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cells;
-       i += gridDim.x * blockDim.x) {
-    const double a = (double)acc[i] * (1.0 / kAreaScale) * inv_bin_area;
-    const float v = (float)(a - (double)target);
-    acc[i] = 0ull;
-    store_operand(v, i, rho, rho_lo, rho_bf);
+  const int i0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i0 >= cells) return;
+  unsigned long long q[4];
+  if (i0 + 3 < cells) {
+    const ulonglong2 a = reinterpret_cast<const ulonglong2 *>(acc)[i0 >> 1];
+    const ulonglong2 b = reinterpret_cast<const ulonglong2 *>(acc)[(i0 >> 1) + 1];
+    q[0] = a.x; q[1] = a.y; q[2] = b.x; q[3] = b.y;
+    reinterpret_cast<ulonglong2 *>(acc)[i0 >> 1] = make_ulonglong2(0ull, 0ull);
+    reinterpret_cast<ulonglong2 *>(acc)[(i0 >> 1) + 1] = make_ulonglong2(0ull, 0ull);
+  } else {
+    for (int r = 0; r < 4; ++r) {
+      q[r] = i0 + r < cells ? acc[i0 + r] : 0ull;
+      if (i0 + r < cells) acc[i0 + r] = 0ull;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    if (i0 + r >= cells) break;
+    const double a = (double)q[r] * (1.0 / kAreaScale) * inv_bin_area;
+    store_operand((float)(a - (double)target), i0 + r, rho, rho_lo, rho_bf);
   }
 }
 
@@ -396,8 +413,8 @@ int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
   auto K = [&](float *f, float *l, uint16_t *b) {
     return GemmOperands{f, split ? l : nullptr, half ? b : nullptr};
   };
-  dens_charge_kernel<<<eb, 256, 0, s>>>(w.area_fx.p, cells, inv_bin_area, target,
-                                        w.buf[0].p, LO(2), BF(0));
+  dens_charge_kernel<<<(cells + 1023) / 1024, 256, 0, s>>>(
+      w.area_fx.p, cells, inv_bin_area, target, w.buf[0].p, LO(2), BF(0));
   FX_CHECK_LAUNCH();
   ctx->launches += 1;
   float *WS = precision == FX_DCT_SIMT ? w.split_ws.p : nullptr;
