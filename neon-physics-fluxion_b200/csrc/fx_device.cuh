@@ -92,10 +92,23 @@ __device__ __forceinline__ void last_block_sum(double block_value,
   }
 }
 
+// Global adds whose old value is not needed, issued as reductions: the warp
+// does not wait for the L2 round trip of an atomic that returns a value.
+__device__ __forceinline__ void red_add_global(int *p, int v) {
+  asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)),
+               "r"(v)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_global(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)),
+               "l"(v)
+               : "memory");
+}
+
 // Warp-aggregated atomic adds: lanes naming the same element (idx >= 0) are
 // combined and one lane issues the atomic. Every lane of the warp must call
-// these (idx < 0 = nothing to add). Sums of integers are exact, so the
-// result does not depend on the grouping.
+// these (idx < 0 = nothing to add); base is global memory. Sums of integers
+// are exact, so the result does not depend on the grouping.
 __device__ __forceinline__ void agg_add_u64(unsigned long long *base, long long idx,
                                             unsigned long long v) {
   const unsigned lane = threadIdx.x & 31u;
@@ -103,7 +116,7 @@ __device__ __forceinline__ void agg_add_u64(unsigned long long *base, long long 
   const unsigned peers = __match_any_sync(0xffffffffu, (int)idx);
   const bool alone = __all_sync(0xffffffffu, peers == (1u << lane));
   if (alone) {
-    if (idx >= 0) atomicAdd(base + idx, v);
+    if (idx >= 0) red_add_global(base + idx, v);
     return;
   }
   unsigned long long sum = 0;
@@ -112,7 +125,7 @@ __device__ __forceinline__ void agg_add_u64(unsigned long long *base, long long 
     const unsigned long long w = __shfl_sync(0xffffffffu, v, src);
     if ((peers >> src) & 1u) sum += w;
   }
-  if (idx >= 0 && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(base + idx, sum);
+  if (idx >= 0 && lane == (unsigned)(__ffs(peers) - 1)) red_add_global(base + idx, sum);
 }
 
 // Adds the same constant `v` from every lane naming idx (>= 0).
@@ -121,7 +134,7 @@ __device__ __forceinline__ void agg_add_const_i32(int *base, long long idx, int 
   // indexes fit 31 bits: a 32-bit match is the cheaper instruction
   const unsigned peers = __match_any_sync(0xffffffffu, (int)idx);
   if (idx >= 0 && lane == (unsigned)(__ffs(peers) - 1))
-    atomicAdd(base + idx, v * __popc(peers));
+    red_add_global(base + idx, v * __popc(peers));
 }
 
 // Order-preserving float <-> uint mapping for atomicMin/atomicMax.
