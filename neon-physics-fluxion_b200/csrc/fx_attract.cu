@@ -321,7 +321,29 @@ extern "C" int fx_stage_attraction(fx_ctx *ctx, fx_design *d, float k,
 namespace fx {
 int density_run(fx_ctx *ctx, fx_design *d, int G, float target, float weight,
                 int precision, bool need_phi, cudaStream_t s);
-int gemm_tc_error(fx_ctx *ctx, unsigned int *out, cudaStream_t s);
+
+// A run's statistics and error words, written by one thread straight into
+// the context's pinned readback block: one launch before the final
+// synchronisation instead of a copy per value (and a second round trip for
+// the tensor-core error word).
+__global__ void iter_stats_kernel(const double *__restrict__ cong_res,
+                                  const float *__restrict__ cong_max,
+                                  const double *__restrict__ energy,
+                                  const unsigned int *__restrict__ bh_err,
+                                  const unsigned int *__restrict__ tc_err,
+                                  IterReadback *__restrict__ out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  IterReadback r{};
+  if (cong_res) {
+    r.res[0] = cong_res[0];
+    r.res[1] = cong_res[1];
+    r.max_overflow = cong_max[0];
+  }
+  if (energy) r.energy = energy[0];
+  if (bh_err) r.err = bh_err[0];
+  if (tc_err) r.tc_err = tc_err[0];
+  *out = r;
+}
 }
 
 extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
@@ -496,15 +518,16 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   // asynchronous copies; pageable ones would stage through the driver)
   IterReadback &rb = *ctx->readback;
   rb = IterReadback{};
-  if (use_cong && iters > 0) {
-    FX_CHECK_CUDA(cudaMemcpyAsync(rb.res, d->cong.result.p, 16, cudaMemcpyDeviceToHost, s));
-    FX_CHECK_CUDA(cudaMemcpyAsync(&rb.max_overflow, d->cong.result_max.p, 4,
-                                  cudaMemcpyDeviceToHost, s));
+  const bool tc = use_dens && c.dct_precision != FX_DCT_SIMT;
+  if (iters > 0) {
+    iter_stats_kernel<<<1, 32, 0, s>>>(use_cong ? d->cong.result.p : nullptr,
+                                       use_cong ? d->cong.result_max.p : nullptr,
+                                       use_dens ? d->step.energy.p : nullptr,
+                                       use_bh ? d->bh.bbox.p + 4 : nullptr,
+                                       tc ? ctx->tc_err : nullptr, ctx->readback_dev);
+    FX_CHECK_LAUNCH();
+    ctx->launches += 1;
   }
-  if (use_dens && iters > 0)
-    FX_CHECK_CUDA(cudaMemcpyAsync(&rb.energy, d->step.energy.p, 8, cudaMemcpyDeviceToHost, s));
-  if (use_bh && iters > 0)
-    FX_CHECK_CUDA(cudaMemcpyAsync(&rb.err, d->bh.bbox.p + 4, 4, cudaMemcpyDeviceToHost, s));
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
   const double res[2] = {rb.res[0], rb.res[1]};
   const unsigned int err = rb.err;
@@ -512,13 +535,13 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   st.density_energy = rb.energy;
   if (copied_out) FX_CHECK_CUDA(cudaStreamSynchronize(s2));
   FX_TRY(bh_error(err));
-  if (use_dens && c.dct_precision != FX_DCT_SIMT) {
-    unsigned int tc_err = 0;
-    FX_TRY(gemm_tc_error(ctx, &tc_err, s));
-    if (tc_err) {
-      set_error("tensor-core GEMM: a bounded wait expired (error word %u)", tc_err);
-      return FX_ETIMEOUT;
-    }
+  if (rb.tc_err) {
+    const unsigned int tc_err = rb.tc_err;
+    // cleared so that the context's next GEMMs report only their own waits
+    FX_CHECK_CUDA(cudaMemsetAsync(ctx->tc_err, 0, 4, s));
+    FX_CHECK_CUDA(cudaStreamSynchronize(s));
+    set_error("tensor-core GEMM: a bounded wait expired (error word %u)", tc_err);
+    return FX_ETIMEOUT;
   }
   st.hpwl = res[0];
   st.total_overflow = res[1];

@@ -225,6 +225,7 @@ extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
   // The word is zeroed on the primary stream and the creation waits for it,
   // so no GEMM of this context (on either stream) can see a stale value.
   if (cudaMallocHost((void **)&c->readback, sizeof(fx::IterReadback)) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&c->readback_dev, c->readback, 0) != cudaSuccess ||
       cudaMalloc((void **)&c->tc_err, sizeof(unsigned int)) != cudaSuccess ||
       cudaMemsetAsync(c->tc_err, 0, sizeof(unsigned int), c->stream) != cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess) {

@@ -250,6 +250,7 @@ struct IterReadback {
   double energy;        // density energy
   float max_overflow;
   unsigned int err;     // Barnes-Hut error word
+  unsigned int tc_err;  // tensor-core GEMM error word
 };
 
 }  // namespace fx
@@ -268,6 +269,7 @@ struct fx_ctx {
   // expired); zeroed at creation, cleared again after it is reported.
   unsigned int *tc_err = nullptr;
   fx::IterReadback *readback = nullptr;  // pinned host memory
+  fx::IterReadback *readback_dev = nullptr;  // the same block, as the device addresses it
   fx::StageTimer timer;
   int64_t launches = 0;
   cudaEvent_t marks[16] = {};
