@@ -54,6 +54,10 @@ int fx_ctx_create(fx_ctx **out_ctx, int device);
 int fx_ctx_destroy(fx_ctx *ctx);
 /* Turns per-stage CUDA-event timing on (1) or off (0). */
 int fx_ctx_set_profiling(fx_ctx *ctx, int enable);
+/* Limits the timing to the stages whose bit (1 << FX_STAGE_*) is set in
+ * stage_mask (all stages by default). Each timed stage adds two events to
+ * its stream, so a long timed run can time only the stages it reports. */
+int fx_ctx_set_profiling_stages(fx_ctx *ctx, uint32_t stage_mask);
 /* Per-stage timing accumulated since the last reset, in milliseconds:
  * out_ms[s] total device time and out_calls[s] launches of stage s
  * (FX_STAGE_*). n = capacity of both arrays. */

@@ -57,8 +57,7 @@ void StageTimer::destroy() {
 
 void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a) {
   *a = nullptr;
-  if (!ctx->timer.enabled) return;
-  (void)stage;
+  if (!ctx->timer.enabled || !((ctx->timer.mask >> stage) & 1u)) return;
   *a = ctx->timer.get_event();
   if (*a) cudaEventRecord(*a, s);
 }
@@ -295,6 +294,12 @@ extern "C" int fx_ctx_destroy(fx_ctx *ctx) {
 extern "C" int fx_ctx_set_profiling(fx_ctx *ctx, int enable) {
   if (!ctx) return FX_EINVAL;
   ctx->timer.enabled = enable != 0;
+  return FX_OK;
+}
+
+extern "C" int fx_ctx_set_profiling_stages(fx_ctx *ctx, uint32_t stage_mask) {
+  if (!ctx) return FX_EINVAL;
+  ctx->timer.mask = stage_mask;
   return FX_OK;
 }
 
@@ -570,17 +575,50 @@ extern "C" int fx_design_get_positions(fx_design *d, float *out_x,
   return FX_OK;
 }
 
+namespace fx {
+namespace {
+// The four state arrays (x, y, vx, vy) in one launch: four floats of each
+// per thread, 16-byte accesses where the array is long enough.
+struct State4 {
+  const float *src[4];
+  float *dst[4];
+};
+__global__ void state_copy_kernel(int n, State4 a) {
+  const int i = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= n) return;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (i + 3 < n) {
+      reinterpret_cast<float4 *>(a.dst[k])[i >> 2] =
+          reinterpret_cast<const float4 *>(a.src[k])[i >> 2];
+    } else {
+      for (int j = i; j < n; ++j) a.dst[k][j] = a.src[k][j];
+    }
+  }
+}
+
+int state_copy(fx_design *d, const State4 &a, cudaStream_t s) {
+  if (d->n <= 0) return FX_OK;
+  const int threads = (d->n + 3) / 4;
+  state_copy_kernel<<<(threads + 255) / 256, 256, 0, s>>>(d->n, a);
+  FX_CHECK_LAUNCH();
+  d->ctx->launches += 1;
+  return FX_OK;
+}
+}  // namespace
+}  // namespace fx
+
 extern "C" int fx_design_save_state(fx_design *d) {
   if (!d) return FX_EINVAL;
   FX_CHECK_CUDA(cudaSetDevice(d->ctx->device));
   AllocScope alloc_scope(d->ctx->stream);
   cudaStream_t s = d->ctx->stream;
-  const size_t b = (size_t)d->n * 4;
-  const float *src[4] = {d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p};
+  fx::State4 a{{d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p}, {}};
   for (int i = 0; i < 4; ++i) {
     if (!d->saved[i].p) FX_TRY(d->saved[i].alloc(d->n));
-    FX_CHECK_CUDA(cudaMemcpyAsync(d->saved[i].p, src[i], b, cudaMemcpyDeviceToDevice, s));
+    a.dst[i] = d->saved[i].p;
   }
+  FX_TRY(fx::state_copy(d, a, s));
   d->saved_in_box = d->pos_in_box;
   return FX_OK;
 }
@@ -593,10 +631,9 @@ extern "C" int fx_design_restore_state(fx_design *d) {
   }
   FX_CHECK_CUDA(cudaSetDevice(d->ctx->device));
   cudaStream_t s = d->ctx->stream;
-  const size_t b = (size_t)d->n * 4;
-  float *dst[4] = {d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p};
-  for (int i = 0; i < 4; ++i)
-    FX_CHECK_CUDA(cudaMemcpyAsync(dst[i], d->saved[i].p, b, cudaMemcpyDeviceToDevice, s));
+  fx::State4 a{{d->saved[0].p, d->saved[1].p, d->saved[2].p, d->saved[3].p},
+               {d->x[d->cur].p, d->y[d->cur].p, d->vx.p, d->vy.p}};
+  FX_TRY(fx::state_copy(d, a, s));
   d->pos_in_box = d->saved_in_box;
   return FX_OK;
 }

@@ -107,6 +107,7 @@ struct DevBuf {
 // ---- per-stage timing ------------------------------------------------------
 struct StageTimer {
   bool enabled = false;
+  uint32_t mask = ~0u;  // stages timed while enabled (bit per FX_STAGE_*)
   double ms[FX_STAGE_COUNT] = {};
   int64_t calls[FX_STAGE_COUNT] = {};
   // Pending (start, stop) pairs, resolved lazily on query.

@@ -153,6 +153,7 @@ SIGNATURES = {
     "fx_ctx_create": (C.c_int, [C.POINTER(P), C.c_int]),
     "fx_ctx_destroy": (C.c_int, [P]),
     "fx_ctx_set_profiling": (C.c_int, [P, C.c_int]),
+    "fx_ctx_set_profiling_stages": (C.c_int, [P, C.c_uint32]),
     "fx_ctx_stage_times": (C.c_int, [P, PF64, PI64, C.c_int]),
     "fx_ctx_reset_stage_times": (C.c_int, [P]),
     "fx_ctx_kernel_launches": (C.c_int64, [P]),

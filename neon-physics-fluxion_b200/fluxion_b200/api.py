@@ -163,7 +163,11 @@ class Context:
         except Exception:
             pass
 
-    def set_profiling(self, on: bool = True) -> None:
+    def set_profiling(self, on: bool = True, stages=None) -> None:
+        """Per-stage event timing on or off; `stages` (names from STAGES)
+        limits it to those stages, None times all of them."""
+        mask = 0xFFFFFFFF if stages is None else sum(1 << _lib.STAGES.index(s) for s in stages)
+        check(self.lib.fx_ctx_set_profiling_stages(self.handle, mask), "set_profiling_stages")
         check(self.lib.fx_ctx_set_profiling(self.handle, int(on)), "set_profiling")
 
     def stage_times(self) -> dict:
