@@ -482,6 +482,7 @@ extern "C" int fx_design_free(fx_design *d) {
   cudaSetDevice(d->ctx->device);
   cudaStreamSynchronize(d->ctx->stream);
   cudaStreamSynchronize(d->ctx->stream2);
+  for (auto &g : d->g1) g.reset();
   d->net_ptr.release();
   d->net_gate.release();
   d->adj_ptr.release();

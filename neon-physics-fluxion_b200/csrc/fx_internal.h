@@ -314,6 +314,21 @@ struct fx_design {
   fx::DensityWork dens;
   fx::CongWork cong;
   fx::StepWork step;
+  // Single-iteration calls of fx_force_iterate on resident positions, as a
+  // CUDA graph per ping-pong parity. `key` fingerprints what the graph was
+  // captured with (configuration, context, the state flag the tree build
+  // reads, and the address and size of every buffer it touches); `seen` is
+  // the key an eager call left behind, so a second call with the same key
+  // captures and later ones replay.
+  struct IterGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> key, seen, failed;  // failed: a key whose capture failed
+    int64_t launches = 0;
+    void reset() {
+      if (exec) cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+  } g1[2];
 };
 
 namespace fx {
