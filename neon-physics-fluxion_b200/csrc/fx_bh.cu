@@ -995,29 +995,25 @@ __device__ __forceinline__ unsigned bh_eval(int c, bool in, bool cell, int s,
 constexpr int kWalkGroup = 8;                    // lanes per group
 constexpr int kWalkGroups = 32 / kWalkGroup;     // groups per warp
 
-// Fast: FX_BH_FAST, the same cells and term order with the hardware rsqrt
-// (a few ulp) instead of the reproducible one; Count: also each point's
-// number of terms.
-template <int Stack, bool Fast = false, bool Count = false>
-__global__ void __launch_bounds__(kWalkWarps * 32, 8)
-bh_walk_kernel(int n, const float2 *__restrict__ spos,
-               const int32_t *__restrict__ perm,
-               const int4 *__restrict__ qchild,
-               const float4 *__restrict__ node, float k, float th2, float md2,
-               float2 *__restrict__ force, unsigned int *__restrict__ err,
-               int32_t *__restrict__ term_count = nullptr) {
-  // one stack per group; the odd stride puts the groups' tops (often at the
-  // same depth) in different banks
-  __shared__ int32_t st_node[kWalkWarps][kWalkGroups][Stack + 1];
-  __shared__ unsigned st_mask[kWalkWarps][kWalkGroups][Stack + 1];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+// The walk of the 32 points of one warp (sorted positions base .. base + 31),
+// groups of kWalkGroup lanes each with their own stack in st_node / st_mask
+// (this warp's [kWalkGroups][Stack + 1] arrays). Fast: FX_BH_FAST, the same
+// cells and term order with the hardware rsqrt (a few ulp) instead of the
+// reproducible one; Count: also each point's number of terms.
+template <int Stack, bool Fast, bool Count>
+__device__ __forceinline__ void bh_group_walk(
+    int base, int n, const float2 *__restrict__ spos, const int32_t *__restrict__ perm,
+    const int4 *__restrict__ qchild, const float4 *__restrict__ node, float k, float th2,
+    float md2, float2 *__restrict__ force, unsigned int *__restrict__ err,
+    int32_t *__restrict__ term_count, int32_t (*st_node)[Stack + 1],
+    unsigned (*st_mask)[Stack + 1]) {
+  const int lane = threadIdx.x & 31;
   const int g = lane / kWalkGroup;
   const bool leader = (lane % kWalkGroup) == 0;
   const unsigned gmask = (kWalkGroup == 32 ? 0xffffffffu
                                            : ((1u << kWalkGroup) - 1u) << (g * kWalkGroup));
-  const int s = (blockIdx.x * kWalkWarps + w) * 32 + lane;
+  const int s = base + lane;
   const bool valid = s < n;
-  if (__ballot_sync(0xffffffffu, valid) == 0u) return;
   const float2 p = valid ? spos[s] : make_float2(0.f, 0.f);
   float fx = 0.f, fy = 0.f;
   int sp = 0;  // this group's stack depth (uniform in the group)
@@ -1029,8 +1025,8 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
     const unsigned open = eval(0, valid, true) & gmask;
     if (open) {
       if (leader) {
-        st_node[w][g][0] = 0;
-        st_mask[w][g][0] = open;
+        st_node[g][0] = 0;
+        st_mask[g][0] = open;
       }
       sp = 1;
     }
@@ -1042,8 +1038,8 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
     unsigned mask = 0u;
     if (has) {
       --sp;
-      nd = st_node[w][g][sp];
-      mask = st_mask[w][g][sp];
+      nd = st_node[g][sp];
+      mask = st_mask[g][sp];
     }
     __syncwarp();
     int4 q = make_int4(kNone, kNone, kNone, kNone);
@@ -1065,14 +1061,183 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
       for (int h = 3; h >= 0; --h) {
         if (om[h] != 0u) {
           if (leader) {
-            st_node[w][g][sp] = qc[h];
-            st_mask[w][g][sp] = om[h];
+            st_node[g][sp] = qc[h];
+            st_mask[g][sp] = om[h];
           }
           ++sp;
         }
       }
     }
     __syncwarp();
+  }
+  if (valid) {
+    force[perm[s]] = make_float2(fx, fy);
+    if (Count) term_count[perm[s]] = terms;
+  }
+}
+
+template <int Stack, bool Fast = false, bool Count = false>
+__global__ void __launch_bounds__(kWalkWarps * 32, 8)
+bh_walk_kernel(int n, const float2 *__restrict__ spos,
+               const int32_t *__restrict__ perm,
+               const int4 *__restrict__ qchild,
+               const float4 *__restrict__ node, float k, float th2, float md2,
+               float2 *__restrict__ force, unsigned int *__restrict__ err,
+               int32_t *__restrict__ term_count = nullptr) {
+  // one stack per group; the odd stride puts the groups' tops (often at the
+  // same depth) in different banks
+  __shared__ int32_t st_node[kWalkWarps][kWalkGroups][Stack + 1];
+  __shared__ unsigned st_mask[kWalkWarps][kWalkGroups][Stack + 1];
+  const int w = threadIdx.x >> 5;
+  const int base = (blockIdx.x * kWalkWarps + w) * 32;
+  if (base >= n) return;  // warp-uniform
+  bh_group_walk<Stack, Fast, Count>(base, n, spos, perm, qchild, node, k, th2, md2, force,
+                                    err, term_count, st_node[w], st_mask[w]);
+}
+
+// ---- batched walk (FX_BH_FAST) ----------------------------------------------
+// The same cells, decisions and terms as the group walk, organised by cell
+// instead of by point. Each warp owns 32 consecutive sorted points and a
+// stack of (cell, lane mask) entries: the cells opened by at least one of
+// its points, with the lanes that must evaluate them. A pass pops up to 32
+// entries, one per lane; each lane loads its entry's walk record into shared
+// memory, then every lane evaluates all popped entries for its own point
+// (broadcast reads), adds the accepted terms and votes which lanes open each
+// entry. Opened cells push their quad children with that vote as the mask;
+// opened buckets are walked point by point. Every lane does the same work in
+// every step (no divergence between cells, points and buckets), and a cell
+// is loaded once per warp instead of once per group. Per point the
+// interaction list is exactly the group walk's (the same opening rule with
+// the same f32 operations); the terms are added in another order.
+// The stack holds kBatchStack entries: a warp whose stack would overflow
+// (possible only for strongly clustered points) starts over with the group
+// walk, whose stacks are bounded, in the same shared memory.
+constexpr int kBatchWarps = 8;
+constexpr int kBatchStack = 400;
+static_assert(kBatchStack * sizeof(int2) >= 2 * kWalkGroups * (kStackDeep + 1) * sizeof(int32_t),
+              "the group walk's stacks must fit in a warp's batch stack");
+
+template <int Stack, bool Count>
+__global__ void __launch_bounds__(kBatchWarps * 32, 6)
+bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__restrict__ perm,
+                     const int4 *__restrict__ qchild, const float4 *__restrict__ node,
+                     float k, float th2, float md2, float2 *__restrict__ force,
+                     unsigned int *__restrict__ err, int32_t *__restrict__ term_count) {
+  __shared__ int2 st[kBatchWarps][kBatchStack];
+  __shared__ float4 rec_a[kBatchWarps][32];  // cx_hi, cy_hi, cx_lo, cy_lo
+  __shared__ float4 rec_b[kBatchWarps][32];  // k*mass, size^2 rule, lane mask, self
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int base = (blockIdx.x * kBatchWarps + w) * 32;
+  if (base >= n) return;  // warp-uniform
+  const int s = base + lane;
+  const bool valid = s < n;
+  const unsigned lanebit = 1u << lane;
+  const float2 p = valid ? spos[s] : make_float2(0.f, 0.f);
+  float fx = 0.f, fy = 0.f;
+  int terms = 0;
+  int sp = 0;  // stack depth (warp-uniform)
+  if (n >= 2) {
+    const unsigned vm = __ballot_sync(full, valid);
+    if (lane == 0) st[w][0] = make_int2(0, (int)vm);
+    sp = 1;
+  }
+  __syncwarp();
+  bool overflow = false;
+  while (sp > 0) {
+    const int cnt = min(sp, 32);
+    sp -= cnt;
+    int c = kNone, bf = 0, bl = -1;
+    bool bucket = false;
+    if (lane < cnt) {
+      const int2 e = st[w][sp + lane];
+      c = e.x;
+      float4 a, b;
+      if (c >= 0) {
+        a = node[2 * c];
+        const float4 r1 = node[2 * c + 1];
+        // size^2 < 0 (a node standing for no quad level): never accepted
+        b = make_float4(__fmul_rn(k, fabsf(r1.x)), r1.y >= 0.f ? r1.y : __int_as_float(0x7f800000),
+                        __int_as_float(e.y), __int_as_float(-1));
+        bucket = !(r1.x > 0.f);
+        bf = __float_as_int(r1.z);
+        bl = __float_as_int(r1.w);
+      } else {  // single point ~c: always accepted
+        const float2 q = spos[~c];
+        a = make_float4(q.x, q.y, 0.f, 0.f);
+        b = make_float4(k, -1.f, __int_as_float(e.y), __int_as_float(~c));
+      }
+      rec_a[w][lane] = a;
+      rec_b[w][lane] = b;
+    }
+    __syncwarp();
+    unsigned myopen = 0u;
+#pragma unroll 2
+    for (int j = 0; j < cnt; ++j) {
+      const float4 a = rec_a[w][j];
+      const float4 b = rec_b[w][j];
+      const float dx = __fsub_rn(__fsub_rn(p.x, a.x), a.z);
+      const float dy = __fsub_rn(__fsub_rn(p.y, a.y), a.w);
+      const float r2c = fmaxf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), md2);
+      const bool in = (__float_as_uint(b.z) & lanebit) != 0u;
+      const bool acc = b.y < __fmul_rn(th2, r2c);
+      const unsigned om = __ballot_sync(full, in && !acc);
+      if (lane == j) myopen = om;
+      const float inv = rsqrtf(r2c);
+      const float f = __fmul_rn(__fmul_rn(__fmul_rn(b.x, inv), inv), inv);
+      const float fu = (in && acc) ? f : 0.f;
+      fx = __fmaf_rn(fu, dx, fx);
+      fy = __fmaf_rn(fu, dy, fy);
+      if (Count) terms += (in && acc && __float_as_int(b.w) != s) ? 1 : 0;
+    }
+    // opened buckets: their points one by one
+    unsigned bk = __ballot_sync(full, bucket && myopen != 0u);
+    while (bk) {
+      const int j = __ffs(bk) - 1;
+      bk &= bk - 1u;
+      const unsigned om = __shfl_sync(full, myopen, j);
+      const int f = __shfl_sync(full, bf, j), l = __shfl_sync(full, bl, j);
+      const bool in = (om & lanebit) != 0u;
+      for (int t = f; t <= l; ++t) {
+        const float2 q = spos[t];
+        if (in && t != s) {
+          bh_direct<true>(p.x, p.y, q, k, md2, fx, fy);
+          if (Count) ++terms;
+        }
+      }
+    }
+    // opened cells: push their quad children with the opening lanes as mask
+    const bool op = myopen != 0u && c >= 0 && !bucket;
+    int4 q = make_int4(kNone, kNone, kNone, kNone);
+    if (op) q = qchild[c];
+    const int nc = (q.x != kNone) + (q.y != kNone) + (q.z != kNone) + (q.w != kNone);
+    int incl = nc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    if (sp + total > kBatchStack) {
+      overflow = true;
+      break;
+    }
+    int pos = sp + incl - nc;
+    const int qc[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int h = 0; h < 4; ++h)
+      if (qc[h] != kNone) st[w][pos++] = make_int2(qc[h], (int)myopen);
+    sp += total;
+    __syncwarp();
+  }
+  if (overflow) {  // warp-uniform: start over with the bounded group walk
+    __syncwarp();
+    int32_t *mem = reinterpret_cast<int32_t *>(&st[w][0]);
+    bh_group_walk<Stack, true, Count>(
+        base, n, spos, perm, qchild, node, k, th2, md2, force, err, term_count,
+        reinterpret_cast<int32_t(*)[Stack + 1]>(mem),
+        reinterpret_cast<unsigned(*)[Stack + 1]>(mem + kWalkGroups * (Stack + 1)));
+    return;
   }
   if (valid) {
     force[perm[s]] = make_float2(fx, fy);
@@ -1249,9 +1414,9 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist, int 
       bh_walk_kernel<kStack><<<wb, kWalkWarps * 32, 0, s>>>(
           n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err);
   } else {
-    const int wb = (n + kWalkWarps * 32 - 1) / (kWalkWarps * 32);
+    const int wb = (n + kBatchWarps * 32 - 1) / (kBatchWarps * 32);
 #define FX_FAST_WALK(ST, CNT)                                                             \
-  bh_walk_kernel<ST, true, CNT><<<wb, kWalkWarps * 32, 0, s>>>(                           \
+  bh_batch_walk_kernel<ST, CNT><<<wb, kBatchWarps * 32, 0, s>>>(                          \
       n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err, term_count)
     if (deep) {
       if (term_count) FX_FAST_WALK(kStackDeep, true);
