@@ -394,6 +394,7 @@ static std::vector<uint64_t> iter_graph_key(fx_ctx *ctx, fx_design *d, const fx_
   k.push_back((uint64_t)(uint32_t)d->cong.cols);
   k.push_back((uint64_t)(uint32_t)d->cong.rows);
   k.push_back((uint64_t)(uint32_t)d->bh.n);
+  k.push_back(ctx->timer.enabled ? 1u + (uint64_t)ctx->timer.mask : 0u);
   return k;
 }
 
@@ -529,8 +530,11 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
   // the key differ and the call run eagerly.
   int it = 0;
   bool replayed = false;
-  // (Not while stage timing is on: its events are recorded per launch.)
-  if (iters == 1 && !x && !ctx->timer.enabled && !d->trace_on) {
+  const fx_design::IterGraph *timed_graph = nullptr;  // its stage events to read
+  // With stage timing on, the graph carries the timed stages' events as
+  // event record nodes, read after each replay (the key holds the timer's
+  // state, so turning timing on or off captures another graph).
+  if (iters == 1 && !x && !d->trace_on) {
     const int cur_start = d->cur;
     const bool box_start = d->pos_in_box;
     fx_design::IterGraph &g = d->g1[cur_start];
@@ -541,6 +545,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
       d->cur ^= 1;
       d->pos_in_box = true;  // the step clamps every position to the die
       replayed = true;
+      if (!g.timing.empty()) timed_graph = &g;
     } else {
       g.reset();
       if (g.seen == key && g.failed != key) {
@@ -548,6 +553,14 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         int rc = FX_OK;
+        auto drop_captured = [&]() {
+          for (auto &t : ctx->timer.captured) {
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+          }
+          ctx->timer.captured.clear();
+        };
+        drop_captured();
         if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
           rc = prologue();
           if (rc == FX_OK) rc = step(true);
@@ -566,6 +579,11 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
           g.exec = exec;
           g.key = key;
           g.launches = per_call;
+          g.timing.swap(ctx->timer.captured);
+          if (!g.timing.empty()) timed_graph = &g;
+        }
+        drop_captured();
+        if (exec) {
           FX_CHECK_CUDA(cudaGraphLaunch(g.exec, s));
           ctx->launches += per_call;
           d->cur ^= 1;
@@ -650,6 +668,7 @@ extern "C" int fx_force_iterate(fx_ctx *ctx, fx_design *d,
     ctx->launches += 1;
   }
   FX_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (timed_graph) ctx->timer.add_elapsed(timed_graph->timing);
   const double res[2] = {rb.res[0], rb.res[1]};
   const unsigned int err = rb.err;
   st.max_overflow = rb.max_overflow;

@@ -1112,6 +1112,14 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
 // The stack holds kBatchStack entries: a warp whose stack would overflow
 // (possible only for strongly clustered points) starts over with the group
 // walk, whose stacks are bounded, in the same shared memory.
+// The hardware reciprocal square root without the subnormal handling of
+// rsqrtf (the argument here is at least min_dist^2).
+__device__ __forceinline__ float rsqrt_approx_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 constexpr int kBatchWarps = 8;
 constexpr int kBatchStack = 400;
 static_assert(kBatchStack * sizeof(int2) >= 2 * kWalkGroups * (kStackDeep + 1) * sizeof(int32_t),
@@ -1126,8 +1134,10 @@ bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__re
   __shared__ int2 st[kBatchWarps][kBatchStack];
   __shared__ float4 rec_a[kBatchWarps][32];  // cx_hi, cy_hi, cx_lo, cy_lo
   __shared__ float4 rec_b[kBatchWarps][32];  // k*mass, size^2 rule, lane mask, self
+  __shared__ unsigned open_s[kBatchWarps][32];  // per popped entry: the lanes opening it
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool lane0 = lane == 0;
   const int base = (blockIdx.x * kBatchWarps + w) * 32;
   if (base >= n) return;  // warp-uniform
   const int s = base + lane;
@@ -1171,7 +1181,6 @@ bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__re
       rec_b[w][lane] = b;
     }
     __syncwarp();
-    unsigned myopen = 0u;
 #pragma unroll 2
     for (int j = 0; j < cnt; ++j) {
       const float4 a = rec_a[w][j];
@@ -1182,14 +1191,16 @@ bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__re
       const bool in = (__float_as_uint(b.z) & lanebit) != 0u;
       const bool acc = b.y < __fmul_rn(th2, r2c);
       const unsigned om = __ballot_sync(full, in && !acc);
-      if (lane == j) myopen = om;
-      const float inv = rsqrtf(r2c);
+      if (lane0) open_s[w][j] = om;
+      const float inv = rsqrt_approx_ftz(r2c);  // r2c >= md2 > 0: never subnormal
       const float f = __fmul_rn(__fmul_rn(__fmul_rn(b.x, inv), inv), inv);
       const float fu = (in && acc) ? f : 0.f;
       fx = __fmaf_rn(fu, dx, fx);
       fy = __fmaf_rn(fu, dy, fy);
       if (Count) terms += (in && acc && __float_as_int(b.w) != s) ? 1 : 0;
     }
+    __syncwarp();
+    const unsigned myopen = lane < cnt ? open_s[w][lane] : 0u;
     // opened buckets: their points one by one
     unsigned bk = __ballot_sync(full, bucket && myopen != 0u);
     while (bk) {

@@ -49,23 +49,54 @@ void StageTimer::resolve() {
   pending.clear();
 }
 
+void StageTimer::add_elapsed(const std::vector<Pending> &pairs) {
+  for (auto &p : pairs) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) {
+      ms[p.stage] += t;
+      calls[p.stage] += 1;
+    }
+  }
+}
+
 void StageTimer::destroy() {
   resolve();
+  for (auto &p : captured) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  captured.clear();
   for (auto e : pool) cudaEventDestroy(e);
   pool.clear();
+}
+
+// Under stream capture the events are recorded as event record nodes of the
+// graph (cudaEventRecordExternal) and the pair is kept in `captured`.
+static bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(s, &st) == cudaSuccess && st == cudaStreamCaptureStatusActive;
 }
 
 void timer_begin(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t *a) {
   *a = nullptr;
   if (!ctx->timer.enabled || !((ctx->timer.mask >> stage) & 1u)) return;
   *a = ctx->timer.get_event();
-  if (*a) cudaEventRecord(*a, s);
+  if (!*a) return;
+  if (capturing(s))
+    cudaEventRecordWithFlags(*a, s, cudaEventRecordExternal);
+  else
+    cudaEventRecord(*a, s);
 }
 
 void timer_end(fx_ctx *ctx, int stage, cudaStream_t s, cudaEvent_t a) {
   if (!ctx->timer.enabled || !a) return;
   cudaEvent_t b = ctx->timer.get_event();
   if (!b) return;
+  if (capturing(s)) {
+    cudaEventRecordWithFlags(b, s, cudaEventRecordExternal);
+    ctx->timer.captured.push_back({stage, a, b});
+    return;
+  }
   cudaEventRecord(b, s);
   ctx->timer.pending.push_back({stage, a, b});
   if (ctx->timer.pending.size() > 4096) ctx->timer.resolve();

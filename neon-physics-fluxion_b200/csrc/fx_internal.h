@@ -117,8 +117,13 @@ struct StageTimer {
   };
   std::vector<Pending> pending;
   std::vector<cudaEvent_t> pool;
+  // Pairs recorded while a stream was being captured into a CUDA graph (as
+  // event record nodes): they belong to that graph and are read after each
+  // of its replays (add_elapsed), not resolved here.
+  std::vector<Pending> captured;
   cudaEvent_t get_event();
   void resolve();
+  void add_elapsed(const std::vector<Pending> &pairs);
   void destroy();
 };
 
@@ -320,13 +325,21 @@ struct fx_design {
   // reads, and the address and size of every buffer it touches); `seen` is
   // the key an eager call left behind, so a second call with the same key
   // captures and later ones replay.
+  // With stage timing on, the graph records its stages' events itself
+  // (`timing`), read after every replay.
   struct IterGraph {
     cudaGraphExec_t exec = nullptr;
     std::vector<uint64_t> key, seen, failed;  // failed: a key whose capture failed
     int64_t launches = 0;
+    std::vector<fx::StageTimer::Pending> timing;
     void reset() {
       if (exec) cudaGraphExecDestroy(exec);
       exec = nullptr;
+      for (auto &t : timing) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+      }
+      timing.clear();
     }
   } g1[2];
 };

@@ -9,7 +9,9 @@ compute path in this package.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -142,6 +144,24 @@ class RoutingGrid:
 
 
 # ---------------------------------------------------------------------------
+# Handles still open when the interpreter exits are closed by an exit hook,
+# designs and servers before the contexts they run on, while every object and
+# the CUDA runtime are still alive (the teardown of module globals frees them
+# in no particular order).
+_OPEN = {"design": weakref.WeakSet(), "server": weakref.WeakSet(), "ctx": weakref.WeakSet()}
+
+
+@atexit.register
+def _close_open_handles() -> None:
+    for kind in ("design", "server", "ctx"):
+        for obj in list(_OPEN[kind]):
+            try:
+                obj.close()
+            except Exception:
+                pass
+
+
+# ---------------------------------------------------------------------------
 # device context and resident designs
 class Context:
     """A CUDA context on one B200 (fx_ctx)."""
@@ -151,6 +171,7 @@ class Context:
         h = C.c_void_p()
         check(self.lib.fx_ctx_create(C.byref(h), device), "fx_ctx_create")
         self.handle = h
+        _OPEN["ctx"].add(self)
 
     def close(self) -> None:
         if getattr(self, "handle", None):
@@ -213,6 +234,7 @@ class Design:
                                       circuit.chip_width, circuit.chip_height,
                                       C.byref(d)), "fx_design_load")
         self.handle = d
+        _OPEN["design"].add(self)
         n, m, p, a = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64())
         check(self.lib.fx_design_sizes(d, C.byref(n), C.byref(m), C.byref(p),
                                        C.byref(a)), "fx_design_sizes")
@@ -579,6 +601,7 @@ class Server:
         h = C.c_void_p()
         check(self.lib.fx_serve_create(C.byref(cfg), C.byref(h)), "fx_serve_create")
         self.handle = h
+        _OPEN["server"].add(self)
 
     def close(self) -> None:
         if getattr(self, "handle", None):

@@ -89,25 +89,38 @@ def test_replay_after_positions_change(fx, ctx):
 
 
 def test_stage_times_count_every_call(fx, ctx):
-    """With stage timing on (which runs every call eagerly, its events being
-    per launch), each call adds the walk's and the density solve's times."""
+    """With stage timing on, single-iteration calls still replay a cached
+    graph, which records the timed stages' events itself: each call adds the
+    walk's and the density solve's times once, and the results stay those of
+    eager calls."""
     s = fx.synth_plain(33, 20000, 24000, 170.0)
     d = fx.Design(ctx, s.circuit)
     try:
         cfg = fx.iter_cfg(density_bins=128, cong_cols=64, cong_rows=64)
         d.set_positions(s.placement.gate_x, s.placement.gate_y)
         d.save_state()
+        ref = _run(fx, ctx, d, cfg, 2, eager=True)
         ctx.reset_stage_times()
         ctx.set_profiling(True, stages=("bh_walk", "density"))
         try:
-            for _ in range(10):
-                d.restore_state()
-                d.force_iterate(cfg, 1)
+            got = _run(fx, ctx, d, cfg, 10, eager=False)
         finally:
             ctx.set_profiling(False)
+        for i, g in enumerate(got):
+            _same(g, ref[i % 2])
         t = ctx.stage_times()
         assert t["bh_walk"][1] == 10 and t["density"][1] == 10
         assert t["bh_walk"][0] > 0 and t["density"][0] > 0
         assert t["bh_sort"][1] == 0  # not in the mask
+        # the replays' walk times are of the same order as the eager calls'
+        ctx.reset_stage_times()
+        ctx.set_profiling(True, stages=("bh_walk",))
+        try:
+            _run(fx, ctx, d, cfg, 2, eager=True)
+        finally:
+            ctx.set_profiling(False)
+        te = ctx.stage_times()["bh_walk"]
+        assert te[1] == 2
+        assert 0.2 < (t["bh_walk"][0] / 10) / (te[0] / 2) < 5.0
     finally:
         d.close()
