@@ -39,6 +39,7 @@
 // restatement of the same rules.
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 
 #include "fx_internal.h"
 #include "fx_device.cuh"
@@ -1109,9 +1110,10 @@ bh_walk_kernel(int n, const float2 *__restrict__ spos,
 // is loaded once per warp instead of once per group. Per point the
 // interaction list is exactly the group walk's (the same opening rule with
 // the same f32 operations); the terms are added in another order.
-// The stack holds kBatchStack entries: a warp whose stack would overflow
-// (possible only for strongly clustered points) starts over with the group
-// walk, whose stacks are bounded, in the same shared memory.
+// The stack holds kBatchStack entries (the 1M-gate uniform placement peaks at
+// 219; clustered, line and radial sets of 20k-200k points at 160-224 in a CPU
+// model of this walk): a warp whose stack would overflow starts over with
+// the group walk, whose stacks are bounded, in the same shared memory.
 // The hardware reciprocal square root without the subnormal handling of
 // rsqrtf (the argument here is at least min_dist^2).
 __device__ __forceinline__ float rsqrt_approx_ftz(float x) {
@@ -1125,12 +1127,25 @@ constexpr int kBatchStack = 400;
 static_assert(kBatchStack * sizeof(int2) >= 2 * kWalkGroups * (kStackDeep + 1) * sizeof(int32_t),
               "the group walk's stacks must fit in a warp's batch stack");
 
+// The stack entries a warp may use (kBatchStack; less when the environment
+// variable FLUXION_BH_BATCH_STACK asks for it, a test setting that sends more
+// warps down the group-walk path).
+static int batch_stack_cap() {
+  static const int cap = [] {
+    const char *e = std::getenv("FLUXION_BH_BATCH_STACK");
+    const int v = e ? std::atoi(e) : kBatchStack;
+    return std::min(kBatchStack, std::max(4, v));
+  }();
+  return cap;
+}
+
 template <int Stack, bool Count>
 __global__ void __launch_bounds__(kBatchWarps * 32, 6)
 bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__restrict__ perm,
                      const int4 *__restrict__ qchild, const float4 *__restrict__ node,
                      float k, float th2, float md2, float2 *__restrict__ force,
-                     unsigned int *__restrict__ err, int32_t *__restrict__ term_count) {
+                     unsigned int *__restrict__ err, int32_t *__restrict__ term_count,
+                     int stack_cap) {
   __shared__ int2 st[kBatchWarps][kBatchStack];
   __shared__ float4 rec_a[kBatchWarps][32];  // cx_hi, cy_hi, cx_lo, cy_lo
   __shared__ float4 rec_b[kBatchWarps][32];  // k*mass, size^2 rule, lane mask, self
@@ -1229,7 +1244,7 @@ bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__re
       if (lane >= o) incl += v;
     }
     const int total = __shfl_sync(full, incl, 31);
-    if (sp + total > kBatchStack) {
+    if (sp + total > stack_cap) {  // stack_cap <= kBatchStack
       overflow = true;
       break;
     }
@@ -1428,7 +1443,8 @@ int bh_run(fx_ctx *ctx, fx_design *d, float k, float theta, float min_dist, int 
     const int wb = (n + kBatchWarps * 32 - 1) / (kBatchWarps * 32);
 #define FX_FAST_WALK(ST, CNT)                                                             \
   bh_batch_walk_kernel<ST, CNT><<<wb, kBatchWarps * 32, 0, s>>>(                          \
-      n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err, term_count)
+      n, b.spos.p, b.idx[0].p, b.qchild.p, b.node.p, k, th2, md2, b.force.p, err, term_count, \
+      batch_stack_cap())
     if (deep) {
       if (term_count) FX_FAST_WALK(kStackDeep, true);
       else FX_FAST_WALK(kStackDeep, false);
