@@ -1140,7 +1140,7 @@ static int batch_stack_cap() {
 }
 
 template <int Stack, bool Count>
-__global__ void __launch_bounds__(kBatchWarps * 32, 6)
+__global__ void __launch_bounds__(kBatchWarps * 32, 5)
 bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__restrict__ perm,
                      const int4 *__restrict__ qchild, const float4 *__restrict__ node,
                      float k, float th2, float md2, float2 *__restrict__ force,
@@ -1196,7 +1196,7 @@ bh_batch_walk_kernel(int n, const float2 *__restrict__ spos, const int32_t *__re
       rec_b[w][lane] = b;
     }
     __syncwarp();
-#pragma unroll 2
+#pragma unroll 4
     for (int j = 0; j < cnt; ++j) {
       const float4 a = rec_a[w][j];
       const float4 b = rec_b[w][j];
