@@ -171,10 +171,10 @@ NCU_WALK = {
     "exact": {"dram": 61_725_696, "inst": 1_390_529_927, "tpi": 20.07,
               "limiter": "instruction issue: 87% issue-active, 0.5% of DRAM peak, "
                          "82% warps active"},
-    # bh_batch_walk_kernel<64, false>: 59.509 MB read + 1.334 MB written
-    "fast": {"dram": 60_842_496, "inst": 614_866_079, "tpi": 31.78,
-             "limiter": "instruction issue: 79% issue-active (ALU pipe 65%, FMA 31%), "
-                        "1.0% of DRAM peak, 63% warps active"},
+    # bh_batch_walk_kernel<64, false>: 59.529 MB read + 1.481 MB written
+    "fast": {"dram": 61_009_920, "inst": 587_039_746, "tpi": 31.77,
+             "limiter": "instruction issue: 83% issue-active (ALU pipe 66%, FMA 33%), "
+                        "1.1% of DRAM peak, 52% warps active"},
 }
 
 
