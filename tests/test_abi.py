@@ -138,3 +138,32 @@ def test_python_constants_match_the_header():
     assert len(_lib.STAGES) == defines["FX_STAGE_COUNT"] == len(stages)
     for name, code in stages.items():
         assert _lib.STAGES[code] == name, name
+
+
+def test_exit_hook_closes_designs_and_servers_before_contexts(fx):
+    """The interpreter-exit hook closes every handle still open, designs and
+    servers before the contexts they run on (order recorded on stand-ins)."""
+    from fluxion_b200 import api
+    closed = []
+
+    class Stub:
+        def __init__(self, kind):
+            self.kind = kind
+
+        def close(self):
+            closed.append(self.kind)
+
+    saved = {k: list(v) for k, v in api._OPEN.items()}
+    stubs = [Stub("ctx"), Stub("design"), Stub("server"), Stub("design")]
+    try:
+        for k in api._OPEN:
+            api._OPEN[k].clear()
+        for st in stubs:
+            api._OPEN[st.kind].add(st)
+        api._close_open_handles()
+    finally:
+        for k in api._OPEN:
+            api._OPEN[k].clear()
+            for o in saved[k]:
+                api._OPEN[k].add(o)
+    assert closed == ["design", "design", "server", "ctx"]
