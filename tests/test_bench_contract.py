@@ -40,7 +40,7 @@ def test_unavailable_arms_say_why():
 
 
 def test_reference_arm_under_torchrun_prints_one_line():
-    """Launched as the driver launches N > 1 (torchrun, one process per rank):
+    """Launched as an N > 1 run is (torchrun, one process per rank):
     rank 0 alone prints the line, and every rank exits 0."""
     import socket
     with socket.socket() as s:
