@@ -229,7 +229,7 @@ extern "C" int fx_ctx_create(fx_ctx **out_ctx, int device) {
   cudaDeviceProp prop;
   FX_CHECK_CUDA(cudaGetDeviceProperties(&prop, device));
   if (prop.major != 10) {
-    set_error("device %d is sm_%d%d; this build targets sm_100a", device,
+    set_error("device %d is sm_%d%d; the library targets sm_100a", device,
               prop.major, prop.minor);
     return FX_ENODEV;
   }

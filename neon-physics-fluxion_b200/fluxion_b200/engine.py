@@ -1,5 +1,5 @@
 """FluxionEngine: the reference's Python entry point (H/python/fluxion/engine.py)
-on this build. `place` runs the `fluxion` command (the reference ran
+over this library. `place` runs the `fluxion` command (the reference ran
 `cargo run --release -- ...`; there is no cargo here), with the same
 arguments, output and errors."""
 from __future__ import annotations
